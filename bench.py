@@ -1,0 +1,335 @@
+#!/usr/bin/env python
+"""Benchmark of the sparse iterative-solve path on B200.
+
+Headline step: one Csr SpMV (FP64 values, int32 indices, 1 right-hand side)
+on the 3D 7-point Poisson matrix of a 128^3 grid (n = 2,097,152,
+nnz = 14,581,760), x ~ N(0, 1) from a seed.  value = algorithmic bytes of
+one SpMV / device time, in GB/s; the roofline fraction is against the
+measured HBM copy bandwidth.  The matrix and vectors (217 MB) exceed the
+126 MB L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+--impl reference times the CPU restatement of the reference executor's
+SpMV (oracle/, OpenMP over all host cores) on the same workload.  Under
+torchrun every rank runs its own replica (the path does not shard); rank 0
+prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("time-to-1e-10 rel. residual, mixed vs FP64 on GPU; "
+          "SpMV GB/s as % of HBM peak")
+GRID = 128
+SEED = 0
+
+
+def csr_bytes(n, nnz, k, vb, ib=4, beta=False):
+    """Compulsory bytes of one Csr SpMV: values + col_idxs + row_ptrs + x
+    read once + y written once (+ y read when beta != 0)."""
+    return nnz * (vb + ib) + (n + 1) * ib + k * n * (vb + vb) + (k * n * vb if beta else 0)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic(name):
+    """DRAM bytes per launch of the named kernel from the committed ncu
+    summary (profiles/traffic.json), or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f).get(name)
+    return None
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons in the background."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,"
+              "clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def __enter__(self):
+        def loop():
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(
+                        ["nvidia-smi", "-i", str(self.index),
+                         "--query-gpu=" + self.FIELDS,
+                         "--format=csv,noheader,nounits"],
+                        capture_output=True, text=True, timeout=5).stdout
+                    parts = [p.strip() for p in out.strip().split(",")]
+                    if len(parts) == 7:
+                        self.samples.append(parts)
+                except Exception:
+                    pass
+                self._stop.wait(0.1)
+        self._t = threading.Thread(target=loop, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4)
+                          if s[3 + i].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def build_matrix():
+    from ginkgo_b200 import stencils
+    rp, ci, v = stencils.poisson_3d_7pt(GRID)
+    return rp, ci, v
+
+
+def run_reference(args):
+    """CPU restatement of the reference's Csr SpMV (oracle, OpenMP)."""
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import oracle as orc
+    rp, ci, v = build_matrix()
+    n, nnz = len(rp) - 1, len(ci)
+    x = np.random.default_rng(SEED).standard_normal(n)
+    y = np.empty(n)
+    threads = os.cpu_count() or 1
+    for _ in range(max(args.warmup, 1)):
+        orc.csr_spmv_par(rp, ci, v, x, y, threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        orc.csr_spmv_par(rp, ci, v, x, y, threads)
+    dt = (time.perf_counter() - t0) / args.steps
+    gbs = csr_bytes(n, nnz, 1, 8) / dt / 1e9
+    out = {
+        "impl": "reference", "metric": METRIC, "value": round(gbs, 2),
+        "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "csr_spmv_poisson3d_7pt_128", "n": n,
+                   "nnz": nnz, "num_rhs": 1, "format": "csr",
+                   "value_type": "f64", "index_type": "int32"},
+        "cpu_baseline": {"value": round(gbs, 2), "unit": "GB/s",
+                         "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} full SpMVs (n={n})"},
+        "e2e": {"value": round(gbs, 2), "unit": "GB/s",
+                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def cpu_baseline(rp, ci, v, budget_s=12.0):
+    from oracle import oracle as orc
+    n, nnz = len(rp) - 1, len(ci)
+    x = np.random.default_rng(SEED).standard_normal(n)
+    y = np.empty(n)
+    threads = os.cpu_count() or 1
+    orc.csr_spmv_par(rp, ci, v, x, y, threads)
+    reps, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < budget_s and reps < 2000:
+        orc.csr_spmv_par(rp, ci, v, x, y, threads)
+        reps += 1
+    dt = (time.perf_counter() - t0) / reps
+    return {"value": round(csr_bytes(n, nnz, 1, 8) / dt / 1e9, 2),
+            "unit": "GB/s", "cores": threads, "kind": "port",
+            "sample": f"{reps} full Csr FP64 SpMVs of the same matrix "
+                      f"({dt * 1e3:.2f} ms each), oracle with OpenMP"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="b200")
+    ap.add_argument("--strategy", default="auto",
+                    choices=["auto", "classical", "load_balance"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sweep", action="store_true",
+                    help="also time every format / precision / k on matrix A")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from ginkgo_b200.matrix import Csr, CudaExecutor
+
+    exe = CudaExecutor.create(local)
+    rp, ci, v = build_matrix()
+    n, nnz = len(rp) - 1, len(ci)
+    A = Csr.read(exe, rp, ci, v)
+    x = torch.from_numpy(np.random.default_rng(SEED).standard_normal(n)).cuda()
+    y = torch.empty(n, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def time_op(op, steps, warmup):
+        for _ in range(warmup):
+            op()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            op()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / steps
+
+    # pick the faster Csr strategy for the headline (both are reported)
+    per_strategy = {}
+    for strat in ("classical", "load_balance"):
+        A.set_strategy(strat)
+        per_strategy[strat] = time_op(lambda: A.apply(x, y), 20, 3)
+    strategy = (min(per_strategy, key=per_strategy.get)
+                if args.strategy == "auto" else args.strategy)
+    A.set_strategy(strategy)
+
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t_step = time_op(lambda: A.apply(x, y), args.steps, args.warmup)
+        # end-to-end through the public API with host buffers
+        xh = torch.from_numpy(np.random.default_rng(SEED).standard_normal(n)).pin_memory()
+        yh = torch.empty(n, dtype=torch.float64).pin_memory()
+        xd = torch.empty_like(x)
+
+        def e2e_step():
+            xd.copy_(xh, non_blocking=True)
+            A.apply(xd, y)
+            yh.copy_(y, non_blocking=True)
+        t_e2e = time_op(e2e_step, max(args.steps // 4, 5), 3)
+    if world > 1:
+        t = torch.tensor([t_step, t_e2e], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        t_step, t_e2e = float(t[0]), float(t[1])
+
+    nbytes = csr_bytes(n, nnz, 1, 8)
+    gbs = nbytes / t_step / 1e9
+    peak, peak_kind = measured_peaks()
+    kernel = f"csr_{strategy}"
+    result = {
+        "metric": METRIC,
+        "value": round(gbs * world, 2),
+        "unit": "GB/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(t_step * 1e3, 5),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "csr_spmv_poisson3d_7pt_128", "n": n, "nnz": nnz,
+                   "num_rhs": 1, "format": "csr", "strategy": strategy,
+                   "value_type": "f64", "index_type": "int32",
+                   "l2": "inputs (217 MB) larger than L2 (126 MB), no flush",
+                   "parallelism": f"replicas{world}"},
+        "roofline": {"bound": "hbm", "achieved": round(gbs, 1),
+                     "peak": peak, "unit": "GB/s",
+                     "frac": round(gbs / peak, 4),
+                     "peak_kind": peak_kind,
+                     "frac_of_8tbs_spec": round(gbs / 8000.0, 4),
+                     "traffic": committed_traffic(kernel),
+                     "algorithmic_bytes": nbytes, "kernel": kernel},
+        "strategies_ms": {k: round(t * 1e3, 5) for k, t in per_strategy.items()},
+        "e2e": {"value": round(nbytes / t_e2e / 1e9 * world, 2), "unit": "GB/s",
+                "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 8,
+                "ms_per_step": round(t_e2e * 1e3, 4)},
+        "gpu_launches": args.steps + max(args.steps // 4, 5),
+        "clocks": clk.summary(),
+    }
+    if args.sweep:
+        result["sweep"] = sweep(exe, rp, ci, v, time_op)
+    if rank == 0 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(rp, ci, v)
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def sweep(exe, rp, ci, v, time_op):
+    import torch
+    from ginkgo_b200.matrix import Csr
+    n, nnz = len(rp) - 1, len(ci)
+    out = {}
+    rng = np.random.default_rng(1)
+    for dt, vb in ((torch.float64, 8), (torch.float32, 4)):
+        A = Csr.read(exe, rp, ci, v, dtype=dt)
+        E = A.convert_to_ell()
+        S = A.convert_to_sellp(32, 1)
+        for k in (1, 4, 16):
+            x = torch.from_numpy(rng.standard_normal((n, k))).to(dt).cuda()
+            y = torch.empty((n, k), dtype=dt, device="cuda")
+            for name, op, mat_bytes in (
+                    ("csr_classical", A.set_strategy("classical"), None),
+                    ("csr_load_balance", A.set_strategy("load_balance"), None),
+                    ("ell", E, E.width * E.stride * (vb + 4)),
+                    ("sellp32", S, S.num_stored_elements * (vb + 4) +
+                     (S.slice_sets.numel() + S.slice_lengths.numel()) * 8)):
+                if name.startswith("csr"):
+                    A.set_strategy(name[4:])
+                    op = A
+                    nb = csr_bytes(n, nnz, k, vb)
+                else:
+                    nb = mat_bytes + k * n * 2 * vb
+                t = time_op(lambda: op.apply(x, y), 20, 3)
+                out[f"{name}_{'f64' if vb == 8 else 'f32'}_k{k}"] = {
+                    "ms": round(t * 1e3, 5), "gbs": round(nb / t / 1e9, 1)}
+    return out
+
+
+if __name__ == "__main__":
+    main()

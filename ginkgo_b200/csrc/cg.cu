@@ -1,0 +1,370 @@
+// Fused preconditioned CG (scalar Jacobi or identity), the loop of
+// core/solver/cg.cpp:91-189 with the kernels of
+// common/unified/solver/cg_kernels.cpp:23-107 regrouped into two passes per
+// iteration and no host synchronisation inside the loop:
+//
+//   spmv pass   p' = z + (rho / prev_rho) p  with z = D^-1 r, formed on the
+//               fly for every column index the SpMV touches (p is double
+//               buffered, so every row reads the old p); q = A p';
+//               dot(p', q) reduced in-kernel; the last block sets
+//               alpha = rho / dot(p', q)  (step_1 + SpMV + dot)
+//   update pass x += alpha p', r -= alpha q; rho' = dot(r, D^-1 r) and
+//               ||r||^2 reduced in-kernel; the last block advances the
+//               iteration, swaps rho, and applies the Iteration and
+//               ResidualNorm(rhs_norm) checks  (step_2 + precond + 2 dots +
+//               residual_norm check)
+//
+// z is never stored.  Per-column stopping status uses the reference's bit
+// layout; stopped columns are frozen as in the reference.  The host replays
+// a CUDA graph of `check_every` iterations and reads the stop flag once per
+// replay.
+#include "solver_common.cuh"
+
+namespace b2s {
+namespace {
+
+template <typename T>
+struct CgScalars {
+    T rho[kMaxRhs], prev_rho[kMaxRhs], alpha[kMaxRhs], tau[kMaxRhs],
+        start[kMaxRhs];
+};
+
+template <typename T>
+__device__ __forceinline__ T cg_p(T d, T r, T beta, T p, bool from_z)
+{
+    const T z = mul_rn(d, r);
+    return from_z ? z : add_rn(z, mul_rn(beta, p));
+}
+
+template <typename T, int K>
+__global__ void __launch_bounds__(kSolverBlock)
+    cg_init_kernel(int64_t n, const T* __restrict__ dinv,
+                   const T* __restrict__ b, int64_t ldb, int k,
+                   const T* __restrict__ r, T* __restrict__ p_old,
+                   SolveCtl* ctl, CgScalars<T>* sc, T* __restrict__ partials)
+{
+    __shared__ T red[kSolverBlock / kWarp * 3 * K];
+    __shared__ T tot[3 * K];
+    __shared__ int last;
+    T acc[3 * K];
+#pragma unroll
+    for (int j = 0; j < 3 * K; ++j) acc[j] = T(0);
+    for (int64_t i = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * kSolverBlock) {
+        const T d = dinv ? dinv[i] : T(1);
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            const T rr = r[i * K + j];
+            const T bb = j < k ? b[i * ldb + j] : T(0);
+            p_old[i * K + j] = T(0);
+            acc[j] += bb * bb;
+            acc[K + j] += rr * mul_rn(d, rr);
+            acc[2 * K + j] += rr * rr;
+        }
+    }
+    block_partials<T, 3 * K>(acc, partials, red);
+    if (last_block_done(&ctl->ticket, &last)) {
+        sum_partials<T, 3 * K>(partials, gridDim.x, tot, red);
+        if (threadIdx.x == 0) {
+            ctl->ticket = 0;
+            ctl->iter = 0;
+            int all = 1;
+            for (int j = 0; j < K; ++j) {
+                uint8_t s = 0;
+                if (j >= k) {
+                    stop_status(s, kIterationId, true);  // padding column
+                }
+                sc->start[j] = sqrt(tot[j]);
+                sc->rho[j] = tot[K + j];
+                sc->prev_rho[j] = T(1);
+                sc->alpha[j] = T(0);
+                sc->tau[j] = sqrt(tot[2 * K + j]);
+                if (ctl->max_iters <= 0) stop_status(s, kIterationId, true);
+                if (double(sc->tau[j]) <= ctl->reduction * double(sc->start[j])) {
+                    converge_status(s, kResidualId, true);
+                }
+                ctl->status[j] = s;
+                all &= has_stopped(s);
+            }
+            ctl->all_stopped = all;
+        }
+    }
+}
+
+template <typename T, int SW, int K>
+__global__ void __launch_bounds__(kSolverBlock)
+    cg_spmv_kernel(int64_t n, const int32_t* __restrict__ rp,
+                   const int32_t* __restrict__ ci, const T* __restrict__ v,
+                   const T* __restrict__ dinv, const T* __restrict__ r,
+                   const T* __restrict__ p_old, T* __restrict__ p_new,
+                   T* __restrict__ q, SolveCtl* ctl, CgScalars<T>* sc,
+                   T* __restrict__ partials)
+{
+    __shared__ T red[kSolverBlock / kWarp * K];
+    __shared__ T tot[K];
+    __shared__ int last;
+    if (ctl->all_stopped) return;
+    bool active[K], from_z[K];
+    T beta[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        active[j] = !has_stopped(ctl->status[j]);
+        const T pr = sc->prev_rho[j];
+        from_z[j] = pr == T(0);
+        beta[j] = from_z[j] ? T(0) : sc->rho[j] / pr;
+    }
+    T dot[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) dot[j] = T(0);
+    const int lane = threadIdx.x % SW;
+    const int64_t nsub = int64_t(gridDim.x) * kSolverBlock / SW;
+    for (int64_t row = (blockIdx.x * int64_t(kSolverBlock) + threadIdx.x) / SW;
+         row < n; row += nsub) {
+        T acc[K];
+#pragma unroll
+        for (int j = 0; j < K; ++j) acc[j] = T(0);
+        const int end = rp[row + 1];
+        for (int e = rp[row] + lane; e < end; e += SW) {
+            const T a = v[e];
+            const int64_t c = ci[e];
+            const T d = dinv ? dinv[c] : T(1);
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                if (active[j]) {
+                    acc[j] += a * cg_p(d, r[c * K + j], beta[j], p_old[c * K + j],
+                                       from_z[j]);
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < K; ++j) acc[j] = subwarp_sum<SW>(acc[j]);
+        if (lane == 0) {
+            const T d = dinv ? dinv[row] : T(1);
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                if (active[j]) {
+                    const T pn = cg_p(d, r[row * K + j], beta[j],
+                                      p_old[row * K + j], from_z[j]);
+                    p_new[row * K + j] = pn;
+                    q[row * K + j] = acc[j];
+                    dot[j] += pn * acc[j];
+                }
+            }
+        }
+    }
+    block_partials<T, K>(dot, partials, red);
+    if (last_block_done(&ctl->ticket, &last)) {
+        sum_partials<T, K>(partials, gridDim.x, tot, red);
+        if (threadIdx.x < K) {
+            const T pq = tot[threadIdx.x];
+            // step_2 skips the update when dot(p, q) == 0
+            sc->alpha[threadIdx.x] = pq != T(0) ? sc->rho[threadIdx.x] / pq : T(0);
+        }
+        if (threadIdx.x == 0) ctl->ticket = 0;
+    }
+}
+
+template <typename T, int K>
+__global__ void __launch_bounds__(kSolverBlock)
+    cg_update_kernel(int64_t n, const T* __restrict__ dinv, T* __restrict__ x,
+                     int64_t ldx, T* __restrict__ r, const T* __restrict__ p,
+                     const T* __restrict__ q, SolveCtl* ctl, CgScalars<T>* sc,
+                     T* __restrict__ partials)
+{
+    __shared__ T red[kSolverBlock / kWarp * 2 * K];
+    __shared__ T tot[2 * K];
+    __shared__ int last;
+    if (ctl->all_stopped) return;
+    bool active[K];
+    T alpha[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        active[j] = !has_stopped(ctl->status[j]);
+        alpha[j] = sc->alpha[j];
+    }
+    T acc[2 * K];
+#pragma unroll
+    for (int j = 0; j < 2 * K; ++j) acc[j] = T(0);
+    for (int64_t i = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * kSolverBlock) {
+        const T d = dinv ? dinv[i] : T(1);
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            if (active[j]) {
+                x[i * ldx + j] += alpha[j] * p[i * K + j];
+                const T rr = r[i * K + j] - alpha[j] * q[i * K + j];
+                r[i * K + j] = rr;
+                acc[j] += rr * mul_rn(d, rr);
+                acc[K + j] += rr * rr;
+            }
+        }
+    }
+    block_partials<T, 2 * K>(acc, partials, red);
+    if (last_block_done(&ctl->ticket, &last)) {
+        sum_partials<T, 2 * K>(partials, gridDim.x, tot, red);
+        if (threadIdx.x == 0) {
+            ctl->ticket = 0;
+            const int iter = ctl->iter + 1;
+            ctl->iter = iter;
+            int all = 1;
+            for (int j = 0; j < K; ++j) {
+                uint8_t s = ctl->status[j];
+                if (!has_stopped(s)) {
+                    sc->prev_rho[j] = sc->rho[j];
+                    sc->rho[j] = tot[j];
+                    sc->tau[j] = sqrt(tot[K + j]);
+                    if (double(sc->tau[j]) <= ctl->reduction * double(sc->start[j])) {
+                        converge_status(s, kResidualId, true);
+                    }
+                    if (iter >= ctl->max_iters) stop_status(s, kIterationId, true);
+                    ctl->status[j] = s;
+                }
+                all &= has_stopped(s);
+            }
+            ctl->all_stopped = all;
+        }
+    }
+}
+
+struct CgLayout {
+    int64_t bytes;
+    int64_t off_ctl, off_sc, off_r, off_p0, off_p1, off_q, off_partials;
+};
+
+template <typename T>
+CgLayout cg_layout(int64_t n, int K)
+{
+    Carver c{nullptr};
+    CgLayout l;
+    l.off_ctl = reinterpret_cast<int64_t>(c.take<SolveCtl>(1));
+    l.off_sc = reinterpret_cast<int64_t>(c.take<CgScalars<T>>(1));
+    l.off_r = reinterpret_cast<int64_t>(c.take<T>(n * K));
+    l.off_p0 = reinterpret_cast<int64_t>(c.take<T>(n * K));
+    l.off_p1 = reinterpret_cast<int64_t>(c.take<T>(n * K));
+    l.off_q = reinterpret_cast<int64_t>(c.take<T>(n * K));
+    l.off_partials = reinterpret_cast<int64_t>(c.take<T>(int64_t(kSolverGrid) * 3 * K));
+    l.bytes = c.used;
+    return l;
+}
+
+template <typename T>
+int cg_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
+             int64_t max_row_nnz, const T* dinv, const T* b, int64_t ldb, T* x,
+             int64_t ldx, int64_t k, int64_t max_iters, double reduction,
+             int64_t check_every, void* workspace, int64_t workspace_bytes,
+             int64_t* iterations, double* residual_norms, uint8_t* status,
+             void* stream)
+{
+    B2S_CHECK_ARG(n >= 0 && k >= 1 && k <= kMaxRhs, "num_rhs must be 1..16");
+    B2S_CHECK_ARG(ldb >= k && ldx >= k, "leading dimension < num_rhs");
+    B2S_CHECK_ARG(max_iters >= 0 && max_iters < (int64_t(1) << 30),
+                  "max_iters out of range");
+    const int K = rhs_bucket(k);
+    const CgLayout lay = cg_layout<T>(n, K);
+    if (workspace_bytes < lay.bytes) {
+        set_error("workspace of %lld bytes < %lld", (long long)workspace_bytes,
+                  (long long)lay.bytes);
+        return B2S_ERR_WORKSPACE;
+    }
+    B2S_CHECK_ARG(workspace != nullptr && b && x && rp, "null pointer");
+    cudaStream_t st = as_stream(stream);
+    char* w = static_cast<char*>(workspace);
+    auto* ctl = reinterpret_cast<SolveCtl*>(w + lay.off_ctl);
+    auto* sc = reinterpret_cast<CgScalars<T>*>(w + lay.off_sc);
+    T* r = reinterpret_cast<T*>(w + lay.off_r);
+    T* p[2] = {reinterpret_cast<T*>(w + lay.off_p0),
+               reinterpret_cast<T*>(w + lay.off_p1)};
+    T* q = reinterpret_cast<T*>(w + lay.off_q);
+    T* partials = reinterpret_cast<T*>(w + lay.off_partials);
+
+    SolveCtl h{};
+    h.max_iters = int(max_iters);
+    h.reduction = reduction;
+    B2S_CUDA_TRY(cudaMemcpyAsync(ctl, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+    const int sw = solver_subwarp(max_row_nnz);
+    const int64_t row_blocks = std::max<int64_t>(1, ceildiv(n * sw, kSolverBlock));
+    const int grid_spmv = int(std::min<int64_t>(row_blocks, kSolverGrid));
+    const int grid_vec = int(std::min<int64_t>(
+        std::max<int64_t>(1, ceildiv(n, kSolverBlock)), kSolverGrid));
+    const int chunk = int(std::max<int64_t>(2, (check_every + 1) / 2 * 2));
+
+    B2S_DISPATCH_RHS(K, {
+        B2S_DISPATCH_SW(sw, {
+            residual_kernel<T, SW, K><<<grid_spmv, kSolverBlock, 0, st>>>(
+                n, rp, ci, v, x, ldx, b, ldb, int(k), r);
+        });
+        B2S_LAUNCH_CHECK();
+        cg_init_kernel<T, K><<<grid_vec, kSolverBlock, 0, st>>>(
+            n, dinv, b, ldb, int(k), r, p[0], ctl, sc, partials);
+        B2S_LAUNCH_CHECK();
+    });
+    auto capture = [&](cudaStream_t cs) -> int {
+        for (int it = 0; it < chunk; ++it) {
+            T* po = p[it % 2];
+            T* pn = p[(it + 1) % 2];
+            B2S_DISPATCH_RHS(K, {
+                B2S_DISPATCH_SW(sw, {
+                    cg_spmv_kernel<T, SW, K><<<grid_spmv, kSolverBlock, 0, cs>>>(
+                        n, rp, ci, v, dinv, r, po, pn, q, ctl, sc, partials);
+                });
+                cg_update_kernel<T, K><<<grid_vec, kSolverBlock, 0, cs>>>(
+                    n, dinv, x, ldx, r, pn, q, ctl, sc, partials);
+            });
+            B2S_LAUNCH_CHECK();
+        }
+        return B2S_OK;
+    };
+    // the graph always runs an even number of iterations, so p[0] holds the
+    // current direction at every replay boundary
+    int rc = run_graph_loop(st, ctl, int(max_iters), chunk, capture, &h);
+    if (rc != B2S_OK) return rc;
+    CgScalars<T> hs;
+    B2S_CUDA_TRY(cudaMemcpyAsync(&hs, sc, sizeof(hs), cudaMemcpyDeviceToHost, st));
+    B2S_CUDA_TRY(cudaMemcpyAsync(&h, ctl, sizeof(h), cudaMemcpyDeviceToHost, st));
+    B2S_CUDA_TRY(cudaStreamSynchronize(st));
+    if (iterations) *iterations = h.iter;
+    for (int64_t j = 0; j < k; ++j) {
+        if (residual_norms) residual_norms[j] = double(hs.tau[j]);
+        if (status) status[j] = h.status[j];
+    }
+    return B2S_OK;
+}
+
+}  // namespace
+}  // namespace b2s
+
+using namespace b2s;
+
+extern "C" {
+
+int64_t b2s_cg_workspace_bytes(int64_t num_rows, int64_t num_rhs,
+                               int value_bytes)
+{
+    const int K = rhs_bucket(num_rhs);
+    if (K < 0 || num_rows < 0) return -1;
+    return value_bytes == 8 ? cg_layout<double>(num_rows, K).bytes
+                            : cg_layout<float>(num_rows, K).bytes;
+}
+
+#define B2S_CG_ENTRY(T, S)                                                    \
+    int b2s_cg_solve_##S(int64_t num_rows, const int32_t* row_ptrs,           \
+                         const int32_t* col_idxs, const T* values,            \
+                         int64_t max_row_nnz, const T* inv_diag, const T* b,  \
+                         int64_t ldb, T* x, int64_t ldx, int64_t num_rhs,     \
+                         int64_t max_iters, double reduction_factor,          \
+                         int64_t check_every, void* workspace,                \
+                         int64_t workspace_bytes, int64_t* iterations,        \
+                         double* residual_norms, uint8_t* status,             \
+                         void* stream)                                        \
+    {                                                                         \
+        return cg_solve<T>(num_rows, row_ptrs, col_idxs, values, max_row_nnz, \
+                           inv_diag, b, ldb, x, ldx, num_rhs, max_iters,      \
+                           reduction_factor, check_every, workspace,          \
+                           workspace_bytes, iterations, residual_norms,       \
+                           status, stream);                                   \
+    }
+
+B2S_CG_ENTRY(double, f64)
+B2S_CG_ENTRY(float, f32)
+
+}  // extern "C"

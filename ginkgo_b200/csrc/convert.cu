@@ -1,0 +1,483 @@
+// Format conversions on the GPU: Csr -> Ell, Csr -> Sellp (slice sets and
+// scatter), Csr transpose, plus the scalar Jacobi generate/apply.  Every
+// output is bit-exact with the reference executor:
+//   convert_to_ell     reference/matrix/csr_kernels.cpp:576-601
+//   compute_slice_sets reference/matrix/sellp_kernels.cpp:109-131
+//   convert_to_sellp   reference/matrix/csr_kernels.cpp:529-570
+//   transpose          reference/matrix/csr_kernels.cpp:678-730
+//   jacobi             common/unified/preconditioner/jacobi_kernels.cpp:24-101
+#include "common.cuh"
+
+namespace b2s {
+namespace {
+
+constexpr int kBlock = 256;
+
+// ---- device-wide exclusive scan (3 phases, deterministic) ----------------
+constexpr int kScanItems = 8;                   // per thread
+constexpr int kScanTile = kBlock * kScanItems;  // per block
+
+template <typename I>
+__device__ I block_exclusive_scan(I v, I* sh, I* total)
+{
+    const int lane = threadIdx.x % kWarp, wid = threadIdx.x / kWarp;
+    I x = v;
+#pragma unroll
+    for (int off = 1; off < kWarp; off *= 2) {
+        I y = __shfl_up_sync(0xffffffffu, x, off);
+        if (lane >= off) x += y;
+    }
+    if (lane == kWarp - 1) sh[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        I w = lane < kBlock / kWarp ? sh[lane] : I(0);
+#pragma unroll
+        for (int off = 1; off < kWarp; off *= 2) {
+            I y = __shfl_up_sync(0xffffffffu, w, off);
+            if (lane >= off) w += y;
+        }
+        if (lane < kBlock / kWarp) sh[lane] = w;
+    }
+    __syncthreads();
+    const I warp_off = wid > 0 ? sh[wid - 1] : I(0);
+    if (total) *total = sh[kBlock / kWarp - 1];
+    __syncthreads();
+    return warp_off + x - v;
+}
+
+template <typename I>
+__global__ void __launch_bounds__(kBlock)
+    scan_tile_sums(const I* __restrict__ in, int64_t n, I* __restrict__ sums)
+{
+    __shared__ I sh[kBlock / kWarp];
+    const int64_t base = blockIdx.x * int64_t(kScanTile) + threadIdx.x * kScanItems;
+    I acc = 0;
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) {
+        if (base + q < n) acc += in[base + q];
+    }
+    I total;
+    block_exclusive_scan(acc, sh, &total);
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+template <typename I>
+__global__ void __launch_bounds__(kBlock)
+    scan_single_block(I* __restrict__ data, int64_t n)
+{
+    // in-place exclusive scan of up to any n, one block, sequential tiles
+    __shared__ I sh[kBlock / kWarp];
+    I carry = 0;
+    for (int64_t t0 = 0; t0 < n; t0 += kScanTile) {
+        const int64_t base = t0 + threadIdx.x * kScanItems;
+        I vals[kScanItems];
+        I acc = 0;
+#pragma unroll
+        for (int q = 0; q < kScanItems; ++q) {
+            vals[q] = base + q < n ? data[base + q] : I(0);
+            acc += vals[q];
+        }
+        I total;
+        I ex = block_exclusive_scan(acc, sh, &total) + carry;
+#pragma unroll
+        for (int q = 0; q < kScanItems; ++q) {
+            if (base + q < n) data[base + q] = ex;
+            ex += vals[q];
+        }
+        carry += total;
+    }
+}
+
+template <typename I>
+__global__ void __launch_bounds__(kBlock)
+    scan_apply(const I* __restrict__ in, int64_t n, const I* __restrict__ sums,
+               I* __restrict__ out)
+{
+    __shared__ I sh[kBlock / kWarp];
+    const int64_t base = blockIdx.x * int64_t(kScanTile) + threadIdx.x * kScanItems;
+    I vals[kScanItems];
+    I acc = 0;
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) {
+        vals[q] = base + q < n ? in[base + q] : I(0);
+        acc += vals[q];
+    }
+    I ex = block_exclusive_scan(acc, sh, (I*)nullptr) + sums[blockIdx.x];
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) {
+        if (base + q < n) out[base + q] = ex;
+        ex += vals[q];
+    }
+}
+
+// out[i] = sum(in[0..i)) for i in [0, n]; out may alias in only if it has
+// n + 1 entries and in[n] is ignored.  Workspace: ceil(n / kScanTile) + 1
+// entries of I.
+template <typename I>
+int exclusive_scan(const I* in, int64_t n, I* out, I* work, cudaStream_t st)
+{
+    const int64_t tiles = ceildiv(n, kScanTile);
+    if (n > 0) {
+        scan_tile_sums<I><<<tiles, kBlock, 0, st>>>(in, n, work);
+        B2S_LAUNCH_CHECK();
+    }
+    // work[tiles] collects the grand total through the one-block scan
+    B2S_CUDA_TRY(cudaMemsetAsync(work + tiles, 0, sizeof(I), st));
+    scan_single_block<I><<<1, kBlock, 0, st>>>(work, tiles + 1);
+    B2S_LAUNCH_CHECK();
+    if (n > 0) {
+        scan_apply<I><<<tiles, kBlock, 0, st>>>(in, n, work, out);
+        B2S_LAUNCH_CHECK();
+    }
+    B2S_CUDA_TRY(cudaMemcpyAsync(out + n, work + tiles, sizeof(I),
+                                 cudaMemcpyDeviceToDevice, st));
+    return B2S_OK;
+}
+
+template <typename I>
+int64_t scan_work_entries(int64_t n)
+{
+    return ceildiv(n, kScanTile) + 1;
+}
+
+// ---- max row length -------------------------------------------------------
+__global__ void __launch_bounds__(kBlock)
+    max_row_nnz_kernel(int64_t n, const int32_t* __restrict__ rp,
+                       unsigned long long* __restrict__ out)
+{
+    int64_t i = blockIdx.x * int64_t(kBlock) + threadIdx.x;
+    unsigned long long m = 0;
+    for (; i < n; i += int64_t(gridDim.x) * kBlock) {
+        m = max(m, (unsigned long long)(rp[i + 1] - rp[i]));
+    }
+    for (int off = 16; off > 0; off /= 2) {
+        m = max(m, __shfl_xor_sync(0xffffffffu, m, off));
+    }
+    if (threadIdx.x % kWarp == 0 && m > 0) atomicMax(out, m);
+}
+
+// ---- Csr -> Ell -------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(kBlock)
+    csr_to_ell_kernel(int64_t n, const int32_t* __restrict__ rp,
+                      const int32_t* __restrict__ ci, const T* __restrict__ v,
+                      int64_t width, int64_t stride, int32_t* __restrict__ eci,
+                      T* __restrict__ ev)
+{
+    const int64_t row = blockIdx.x * int64_t(kBlock) + threadIdx.x;
+    if (row >= n) return;
+    const int64_t b = rp[row], len = rp[row + 1] - b;
+    for (int64_t i = 0; i < width; ++i) {
+        const bool in = i < len;
+        eci[row + i * stride] = in ? ci[b + i] : -1;
+        ev[row + i * stride] = in ? v[b + i] : T(0);
+    }
+}
+
+// ---- Csr -> Sellp -------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock)
+    slice_lengths_kernel(int64_t n, const int32_t* __restrict__ rp,
+                         int64_t slice_size, int64_t stride_factor,
+                         int64_t num_slices, uint64_t* __restrict__ lens)
+{
+    const int64_t s = blockIdx.x * int64_t(kBlock) + threadIdx.x;
+    if (s >= num_slices) return;
+    uint64_t len = 0;
+    for (int64_t l = 0; l < slice_size; ++l) {
+        const int64_t row = s * slice_size + l;
+        const int64_t rl = row < n ? rp[row + 1] - rp[row] : 0;
+        const uint64_t padded =
+            uint64_t(ceildiv(rl, stride_factor) * stride_factor);
+        len = padded > len ? padded : len;
+    }
+    lens[s] = len;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBlock)
+    csr_to_sellp_kernel(int64_t n, const int32_t* __restrict__ rp,
+                        const int32_t* __restrict__ ci, const T* __restrict__ v,
+                        int64_t slice_size,
+                        const uint64_t* __restrict__ slice_sets,
+                        const uint64_t* __restrict__ slice_lengths,
+                        int32_t* __restrict__ sci, T* __restrict__ sv)
+{
+    const int64_t row = blockIdx.x * int64_t(kBlock) + threadIdx.x;
+    if (row >= n) return;
+    const int64_t s = row / slice_size, local = row - s * slice_size;
+    const int64_t b = rp[row], len = rp[row + 1] - b;
+    const int64_t slen = int64_t(slice_lengths[s]);
+    int64_t idx = int64_t(slice_sets[s]) * slice_size + local;
+    for (int64_t i = 0; i < slen; ++i, idx += slice_size) {
+        const bool in = i < len;
+        sci[idx] = in ? ci[b + i] : -1;
+        sv[idx] = in ? v[b + i] : T(0);
+    }
+}
+
+// ---- transpose -------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock)
+    count_cols_kernel(int64_t nnz, const int32_t* __restrict__ ci,
+                      int32_t* __restrict__ counts)
+{
+    for (int64_t e = blockIdx.x * int64_t(kBlock) + threadIdx.x; e < nnz;
+         e += int64_t(gridDim.x) * kBlock) {
+        atomicAdd(counts + ci[e], 1);
+    }
+}
+
+// Scatter (in any order) into per-column slots; one thread per source row.
+template <typename T>
+__global__ void __launch_bounds__(kBlock)
+    scatter_transpose_kernel(int64_t nrows, const int32_t* __restrict__ rp,
+                             const int32_t* __restrict__ ci,
+                             const T* __restrict__ v,
+                             int32_t* __restrict__ fill,
+                             int32_t* __restrict__ tmp_row,
+                             T* __restrict__ tmp_val)
+{
+    const int64_t row = blockIdx.x * int64_t(kBlock) + threadIdx.x;
+    if (row >= nrows) return;
+    for (int64_t e = rp[row]; e < rp[row + 1]; ++e) {
+        const int32_t dst = atomicAdd(fill + ci[e], 1);
+        tmp_row[dst] = int32_t(row);
+        tmp_val[dst] = v[e];
+    }
+}
+
+// One warp per transposed row: the source rows in one column are distinct,
+// so the rank of each entry (number of smaller row indices) is its slot.
+// This reproduces the increasing-row order of the sequential scatter.
+template <typename T>
+__global__ void __launch_bounds__(kBlock)
+    rank_transpose_kernel(int64_t ncols, const int32_t* __restrict__ trp,
+                          const int32_t* __restrict__ tmp_row,
+                          const T* __restrict__ tmp_val,
+                          int32_t* __restrict__ tci, T* __restrict__ tv)
+{
+    const int64_t col = (blockIdx.x * int64_t(kBlock) + threadIdx.x) / kWarp;
+    const int lane = threadIdx.x % kWarp;
+    if (col >= ncols) return;
+    const int32_t b = trp[col], len = trp[col + 1] - b;
+    for (int32_t i = lane; i < len; i += kWarp) {
+        const int32_t key = tmp_row[b + i];
+        int32_t rank = 0;
+        for (int32_t j = 0; j < len; ++j) rank += tmp_row[b + j] < key;
+        tci[b + rank] = key;
+        tv[b + rank] = tmp_val[b + i];
+    }
+}
+
+// ---- scalar Jacobi ----------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(kBlock)
+    invert_diagonal_kernel(int64_t n, const int32_t* __restrict__ rp,
+                           const int32_t* __restrict__ ci,
+                           const T* __restrict__ v, T* __restrict__ inv)
+{
+    const int64_t row = blockIdx.x * int64_t(kBlock) + threadIdx.x;
+    if (row >= n) return;
+    T d = T(0);
+    for (int64_t e = rp[row]; e < rp[row + 1]; ++e) {
+        if (ci[e] == row) d = v[e];
+    }
+    inv[row] = d == T(0) ? T(1) : T(1) / d;
+}
+
+// x = diag^-1 b (simple_scalar_apply) or x = alpha diag^-1 b + beta x
+// (scalar_apply); common/unified/preconditioner/jacobi_kernels.cpp:39-101.
+template <typename T>
+__global__ void __launch_bounds__(kBlock)
+    jacobi_apply_kernel(int64_t n, int64_t k, const T* __restrict__ inv,
+                        const T* __restrict__ b, int64_t ldb,
+                        T* __restrict__ x, int64_t ldx,
+                        const T* __restrict__ alpha, const T* __restrict__ beta)
+{
+    const int64_t i = blockIdx.x * int64_t(kBlock) + threadIdx.x;
+    if (i >= n * k) return;
+    const int64_t row = i / k, col = i - row * k;
+    const T val = inv[row] * b[row * ldb + col];
+    T* dst = x + row * ldx + col;
+    *dst = combine(val, alpha, beta, dst);
+}
+
+}  // namespace
+}  // namespace b2s
+
+using namespace b2s;
+
+extern "C" {
+
+int b2s_csr_max_row_nnz(int64_t num_rows, const int32_t* row_ptrs,
+                        int64_t* result, void* workspace, void* stream)
+{
+    B2S_CHECK_ARG(result != nullptr && workspace != nullptr, "null pointer");
+    cudaStream_t st = as_stream(stream);
+    auto* w = static_cast<unsigned long long*>(workspace);
+    B2S_CUDA_TRY(cudaMemsetAsync(w, 0, sizeof(*w), st));
+    if (num_rows > 0) {
+        const int64_t grid = std::min<int64_t>(ceildiv(num_rows, kBlock), 4 * kNumSMs);
+        max_row_nnz_kernel<<<grid, kBlock, 0, st>>>(num_rows, row_ptrs, w);
+        B2S_LAUNCH_CHECK();
+    }
+    unsigned long long h = 0;
+    B2S_CUDA_TRY(cudaMemcpyAsync(&h, w, sizeof(h), cudaMemcpyDeviceToHost, st));
+    B2S_CUDA_TRY(cudaStreamSynchronize(st));
+    *result = int64_t(h);
+    return B2S_OK;
+}
+
+int64_t b2s_sellp_slice_sets_workspace_bytes(int64_t num_rows, int64_t slice_size)
+{
+    if (slice_size < 1) return -1;
+    const int64_t ns = ceildiv(num_rows, slice_size);
+    return scan_work_entries<unsigned long long>(ns) * 8;
+}
+
+int b2s_sellp_compute_slice_sets(int64_t num_rows, const int32_t* row_ptrs,
+                                 int64_t slice_size, int64_t stride_factor,
+                                 uint64_t* slice_sets, uint64_t* slice_lengths,
+                                 void* workspace, int64_t workspace_bytes,
+                                 void* stream)
+{
+    B2S_CHECK_ARG(num_rows >= 0 && slice_size >= 1 && stride_factor >= 1,
+                  "bad Sellp parameters");
+    const int64_t need = b2s_sellp_slice_sets_workspace_bytes(num_rows, slice_size);
+    if (workspace_bytes < need) {
+        set_error("workspace of %lld bytes < %lld", (long long)workspace_bytes,
+                  (long long)need);
+        return B2S_ERR_WORKSPACE;
+    }
+    cudaStream_t st = as_stream(stream);
+    const int64_t ns = ceildiv(num_rows, slice_size);
+    if (ns > 0) {
+        slice_lengths_kernel<<<ceildiv(ns, kBlock), kBlock, 0, st>>>(
+            num_rows, row_ptrs, slice_size, stride_factor, ns, slice_lengths);
+        B2S_LAUNCH_CHECK();
+    }
+    using U = unsigned long long;
+    return exclusive_scan<U>(reinterpret_cast<const U*>(slice_lengths), ns,
+                             reinterpret_cast<U*>(slice_sets),
+                             static_cast<U*>(workspace), st);
+}
+
+int64_t b2s_csr_transpose_workspace_bytes(int64_t num_rows, int64_t num_cols,
+                                          int64_t nnz, int value_bytes)
+{
+    // fill counters, scan work, tmp rows, tmp values
+    return (num_cols + 1) * 4 + scan_work_entries<int32_t>(num_cols) * 4 +
+           nnz * 4 + nnz * int64_t(value_bytes) + 64;
+}
+
+#define B2S_CONVERT_ENTRIES(T, S)                                              \
+    int b2s_csr_convert_to_ell_##S(int64_t num_rows, const int32_t* row_ptrs,  \
+                                   const int32_t* col_idxs, const T* values,   \
+                                   int64_t width, int64_t stride,              \
+                                   int32_t* ell_col_idxs, T* ell_values,       \
+                                   void* stream)                               \
+    {                                                                          \
+        B2S_CHECK_ARG(stride >= num_rows && width >= 0, "bad Ell shape");      \
+        if (num_rows == 0) return B2S_OK;                                      \
+        csr_to_ell_kernel<T><<<ceildiv(num_rows, kBlock), kBlock, 0,           \
+                               as_stream(stream)>>>(                           \
+            num_rows, row_ptrs, col_idxs, values, width, stride,               \
+            ell_col_idxs, ell_values);                                         \
+        B2S_LAUNCH_CHECK();                                                    \
+        return B2S_OK;                                                         \
+    }                                                                          \
+    int b2s_csr_convert_to_sellp_##S(                                          \
+        int64_t num_rows, const int32_t* row_ptrs, const int32_t* col_idxs,    \
+        const T* values, int64_t slice_size, const uint64_t* slice_sets,       \
+        const uint64_t* slice_lengths, int32_t* sellp_col_idxs,                \
+        T* sellp_values, void* stream)                                         \
+    {                                                                          \
+        B2S_CHECK_ARG(slice_size >= 1, "slice_size must be >= 1");             \
+        if (num_rows == 0) return B2S_OK;                                      \
+        csr_to_sellp_kernel<T><<<ceildiv(num_rows, kBlock), kBlock, 0,         \
+                                 as_stream(stream)>>>(                         \
+            num_rows, row_ptrs, col_idxs, values, slice_size, slice_sets,      \
+            slice_lengths, sellp_col_idxs, sellp_values);                      \
+        B2S_LAUNCH_CHECK();                                                    \
+        return B2S_OK;                                                         \
+    }                                                                          \
+    int b2s_csr_transpose_##S(int64_t num_rows, int64_t num_cols, int64_t nnz, \
+                              const int32_t* row_ptrs,                         \
+                              const int32_t* col_idxs, const T* values,        \
+                              int32_t* t_row_ptrs, int32_t* t_col_idxs,        \
+                              T* t_values, void* workspace,                    \
+                              int64_t workspace_bytes, void* stream)           \
+    {                                                                          \
+        B2S_CHECK_ARG(num_rows >= 0 && num_cols >= 0 && nnz >= 0,              \
+                      "negative size");                                        \
+        const int64_t need = b2s_csr_transpose_workspace_bytes(                \
+            num_rows, num_cols, nnz, sizeof(T));                               \
+        if (workspace_bytes < need) {                                          \
+            set_error("workspace of %lld bytes < %lld",                        \
+                      (long long)workspace_bytes, (long long)need);            \
+            return B2S_ERR_WORKSPACE;                                          \
+        }                                                                      \
+        cudaStream_t st = as_stream(stream);                                   \
+        char* w = static_cast<char*>(workspace);                               \
+        int32_t* counts = reinterpret_cast<int32_t*>(w);                       \
+        w += (num_cols + 1) * 4;                                               \
+        int32_t* scan_work = reinterpret_cast<int32_t*>(w);                    \
+        w += scan_work_entries<int32_t>(num_cols) * 4;                         \
+        T* tmp_val = reinterpret_cast<T*>(                                     \
+            (reinterpret_cast<uintptr_t>(w) + 15) & ~uintptr_t(15));           \
+        int32_t* tmp_row = reinterpret_cast<int32_t*>(tmp_val + nnz);          \
+        B2S_CUDA_TRY(cudaMemsetAsync(counts, 0, (num_cols + 1) * 4, st));      \
+        if (nnz > 0) {                                                         \
+            const int64_t grid =                                               \
+                std::min<int64_t>(ceildiv(nnz, kBlock), 16 * kNumSMs);         \
+            count_cols_kernel<<<grid, kBlock, 0, st>>>(nnz, col_idxs, counts); \
+            B2S_LAUNCH_CHECK();                                                \
+        }                                                                      \
+        int rc = exclusive_scan<int32_t>(counts, num_cols, t_row_ptrs,         \
+                                         scan_work, st);                       \
+        if (rc != B2S_OK) return rc;                                           \
+        if (nnz == 0) return B2S_OK;                                           \
+        B2S_CUDA_TRY(cudaMemcpyAsync(counts, t_row_ptrs, num_cols * 4,         \
+                                     cudaMemcpyDeviceToDevice, st));           \
+        scatter_transpose_kernel<T><<<ceildiv(num_rows, kBlock), kBlock, 0,    \
+                                      st>>>(num_rows, row_ptrs, col_idxs,      \
+                                            values, counts, tmp_row, tmp_val); \
+        B2S_LAUNCH_CHECK();                                                    \
+        rank_transpose_kernel<T><<<ceildiv(num_cols * kWarp, kBlock), kBlock,  \
+                                   0, st>>>(num_cols, t_row_ptrs, tmp_row,     \
+                                            tmp_val, t_col_idxs, t_values);    \
+        B2S_LAUNCH_CHECK();                                                    \
+        return B2S_OK;                                                         \
+    }                                                                          \
+    int b2s_jacobi_invert_diagonal_##S(int64_t num_rows,                       \
+                                       const int32_t* row_ptrs,                \
+                                       const int32_t* col_idxs,                \
+                                       const T* values, T* inv_diag,           \
+                                       void* stream)                           \
+    {                                                                          \
+        if (num_rows == 0) return B2S_OK;                                      \
+        invert_diagonal_kernel<T><<<ceildiv(num_rows, kBlock), kBlock, 0,      \
+                                    as_stream(stream)>>>(                      \
+            num_rows, row_ptrs, col_idxs, values, inv_diag);                   \
+        B2S_LAUNCH_CHECK();                                                    \
+        return B2S_OK;                                                         \
+    }                                                                          \
+    int b2s_jacobi_apply_##S(int64_t num_rows, int64_t num_rhs,                \
+                             const T* inv_diag, const T* b, int64_t ldb, T* x, \
+                             int64_t ldx, const T* alpha, const T* beta,       \
+                             void* stream)                                     \
+    {                                                                          \
+        B2S_CHECK_ARG((alpha == nullptr) == (beta == nullptr),                 \
+                      "alpha and beta must both be given or both be null");    \
+        const int64_t total = num_rows * num_rhs;                              \
+        if (total == 0) return B2S_OK;                                         \
+        jacobi_apply_kernel<T><<<ceildiv(total, kBlock), kBlock, 0,            \
+                                 as_stream(stream)>>>(                         \
+            num_rows, num_rhs, inv_diag, b, ldb, x, ldx, alpha, beta);         \
+        B2S_LAUNCH_CHECK();                                                    \
+        return B2S_OK;                                                         \
+    }
+
+B2S_CONVERT_ENTRIES(double, f64)
+B2S_CONVERT_ENTRIES(float, f32)
+
+}  // extern "C"

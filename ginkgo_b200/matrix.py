@@ -1,0 +1,262 @@
+"""Host-side matrix formats over the C ABI, named after the reference's
+``gko::matrix`` classes (Csr, Ell, Sellp) and ``gko::CudaExecutor``.
+
+Device storage is torch tensors (torch is used for memory, streams and the
+autograd entry point only).  Dense operands are torch tensors of shape (n,)
+or (n, k), row-major; ``apply(b, x)`` computes x = A b and
+``apply(alpha, b, beta, x)`` computes x = alpha A b + beta x, as
+``gko::LinOp::apply`` does (include/ginkgo/core/base/lin_op.hpp:129-203).
+Every kernel launches on the current torch CUDA stream.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from ._lib import call, lib
+
+_SFX = {torch.float64: "f64", torch.float32: "f32"}
+
+
+class CudaExecutor:
+    """One device; kernels go to torch's current stream on that device
+    (the reference's CudaExecutor owns one stream, executor.hpp:1723)."""
+
+    def __init__(self, device_id: int = 0):
+        self.device = torch.device("cuda", device_id)
+
+    @staticmethod
+    def create(device_id: int = 0):
+        return CudaExecutor(device_id)
+
+    @property
+    def stream(self):
+        return C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def synchronize(self):
+        torch.cuda.synchronize(self.device)
+
+
+def _stream(t: torch.Tensor):
+    return C.c_void_p(torch.cuda.current_stream(t.device).cuda_stream)
+
+
+def _p(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+def _as2d(t: torch.Tensor):
+    return t.unsqueeze(1) if t.dim() == 1 else t
+
+
+def _check_dense(t: torch.Tensor, rows: int, dtype, what: str):
+    if not t.is_cuda:
+        raise ValueError(f"{what} must be a CUDA tensor")
+    if t.dtype != dtype:
+        raise TypeError(f"{what} has dtype {t.dtype}, expected {dtype}")
+    t2 = _as2d(t)
+    if t2.shape[0] != rows:
+        raise ValueError(f"{what} has {t2.shape[0]} rows, expected {rows} "
+                         "(DimensionMismatch)")
+    if t2.dim() != 2 or t2.stride(1) != 1:
+        raise ValueError(f"{what} must be row-major with unit column stride")
+    return t2
+
+
+def _scalar(v, dtype, device):
+    if v is None:
+        return None
+    if isinstance(v, torch.Tensor):
+        return v.to(device=device, dtype=dtype).reshape(1)
+    return torch.tensor([v], dtype=dtype, device=device)
+
+
+class _SparseBase:
+    dtype: torch.dtype
+    shape: tuple
+
+    def _apply_args(self, args):
+        if len(args) == 2:
+            b, x = args
+            alpha = beta = None
+        elif len(args) == 4:
+            alpha, b, beta, x = args
+        else:
+            raise TypeError("apply(b, x) or apply(alpha, b, beta, x)")
+        n, m = self.shape
+        b2 = _check_dense(b, m, self.dtype, "b")
+        x2 = _check_dense(x, n, self.dtype, "x")
+        if b2.shape[1] != x2.shape[1]:
+            raise ValueError("b and x have different numbers of columns")
+        dev = x2.device
+        return (b2, x2, _scalar(alpha, self.dtype, dev),
+                _scalar(beta, self.dtype, dev))
+
+
+class Csr(_SparseBase):
+    """Compressed sparse row matrix (int32 indices, float64/float32 values).
+
+    strategy: "classical" (subwarp per row) or "load_balance" (merge-path
+    tiles), the two strategies of include/ginkgo/core/matrix/csr.hpp:176-699.
+    """
+
+    def __init__(self, exec_, shape, row_ptrs, col_idxs, values,
+                 strategy: str = "classical"):
+        self.exec = exec_
+        dev = exec_.device
+        self.shape = (int(shape[0]), int(shape[1]))
+        self.row_ptrs = torch.as_tensor(row_ptrs, dtype=torch.int32, device=dev).contiguous()
+        self.col_idxs = torch.as_tensor(col_idxs, dtype=torch.int32, device=dev).contiguous()
+        vals = torch.as_tensor(values, device=dev)
+        if vals.dtype not in _SFX:
+            vals = vals.to(torch.float64)
+        self.values = vals.contiguous()
+        self.dtype = self.values.dtype
+        if self.row_ptrs.numel() != self.shape[0] + 1:
+            raise ValueError("row_ptrs must have num_rows + 1 entries")
+        self.nnz = int(self.col_idxs.numel())
+        self._max_row_nnz = None
+        self._tiles = None
+        self.set_strategy(strategy)
+
+    @classmethod
+    def read(cls, exec_, rp, ci, v, shape=None, strategy="classical",
+             dtype=torch.float64):
+        rp = np.asarray(rp)
+        n = len(rp) - 1
+        shape = (n, n) if shape is None else shape
+        vals = torch.as_tensor(np.asarray(v)).to(dtype)
+        return cls(exec_, shape, torch.from_numpy(np.asarray(rp, np.int32)),
+                   torch.from_numpy(np.asarray(ci, np.int32)), vals, strategy)
+
+    def set_strategy(self, strategy: str):
+        if strategy not in ("classical", "load_balance"):
+            raise ValueError(f"unknown Csr strategy {strategy!r}")
+        self.strategy = strategy
+        if strategy == "load_balance" and self._tiles is None:
+            nt = lib().b2s_csr_load_balance_num_tiles(self.shape[0], self.nnz)
+            self._tiles = torch.empty(nt + 1, dtype=torch.int32,
+                                      device=self.values.device)
+            call("b2s_csr_load_balance_setup", self.shape[0], self.nnz,
+                 _p(self.row_ptrs), nt, _p(self._tiles), _stream(self.values))
+        return self
+
+    @property
+    def max_row_nnz(self) -> int:
+        if self._max_row_nnz is None:
+            ws = torch.empty(1, dtype=torch.int64, device=self.values.device)
+            out = C.c_int64(0)
+            call("b2s_csr_max_row_nnz", self.shape[0], _p(self.row_ptrs),
+                 C.byref(out), _p(ws), _stream(self.values))
+            self._max_row_nnz = int(out.value)
+        return self._max_row_nnz
+
+    def apply(self, *args):
+        b2, x2, alpha, beta = self._apply_args(args)
+        strat = 1 if self.strategy == "load_balance" else 0
+        nt = 0 if self._tiles is None else self._tiles.numel() - 1
+        call(f"b2s_csr_spmv_{_SFX[self.dtype]}", strat, self.shape[0],
+             self.shape[1], _p(self.row_ptrs), _p(self.col_idxs),
+             _p(self.values), self.max_row_nnz if strat == 0 else 0,
+             _p(self._tiles), nt, _p(b2), b2.stride(0), _p(x2), x2.stride(0),
+             x2.shape[1], _p(alpha), _p(beta), _stream(x2))
+        return args[-1]
+
+    def convert_to_precision(self, dtype):
+        return Csr(self.exec, self.shape, self.row_ptrs, self.col_idxs,
+                   self.values.to(dtype), self.strategy)
+
+    def convert_to_ell(self, stride=None):
+        n = self.shape[0]
+        width = self.max_row_nnz
+        stride = n if stride is None else int(stride)
+        dev = self.values.device
+        ci = torch.empty(width * stride, dtype=torch.int32, device=dev)
+        v = torch.empty(width * stride, dtype=self.dtype, device=dev)
+        call(f"b2s_csr_convert_to_ell_{_SFX[self.dtype]}", n, _p(self.row_ptrs),
+             _p(self.col_idxs), _p(self.values), width, stride, _p(ci), _p(v),
+             _stream(v))
+        return Ell(self.exec, self.shape, width, stride, ci, v)
+
+    def convert_to_sellp(self, slice_size: int = 64, stride_factor: int = 1):
+        n = self.shape[0]
+        dev = self.values.device
+        ns = (n + slice_size - 1) // slice_size
+        sets = torch.empty(ns + 1, dtype=torch.int64, device=dev)
+        lens = torch.empty(max(ns, 1), dtype=torch.int64, device=dev)
+        wsb = lib().b2s_sellp_slice_sets_workspace_bytes(n, slice_size)
+        ws = torch.empty(max(wsb, 8), dtype=torch.uint8, device=dev)
+        call("b2s_sellp_compute_slice_sets", n, _p(self.row_ptrs), slice_size,
+             stride_factor, _p(sets), _p(lens), _p(ws), wsb, _stream(sets))
+        total = int(sets[-1].item()) * slice_size  # host read, as csr.cpp:473
+        # slots of the rows past num_rows in the last slice are never
+        # written by the conversion; they hold padding (-1, 0)
+        ci = torch.full((max(total, 1),), -1, dtype=torch.int32, device=dev)
+        v = torch.zeros(max(total, 1), dtype=self.dtype, device=dev)
+        call(f"b2s_csr_convert_to_sellp_{_SFX[self.dtype]}", n,
+             _p(self.row_ptrs), _p(self.col_idxs), _p(self.values), slice_size,
+             _p(sets), _p(lens), _p(ci), _p(v), _stream(v))
+        return Sellp(self.exec, self.shape, slice_size, stride_factor, sets,
+                     lens[:ns], ci[:total], v[:total])
+
+    def transpose(self):
+        n, m = self.shape
+        dev = self.values.device
+        wsb = lib().b2s_csr_transpose_workspace_bytes(
+            n, m, self.nnz, self.values.element_size())
+        ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+        trp = torch.empty(m + 1, dtype=torch.int32, device=dev)
+        tci = torch.empty(max(self.nnz, 1), dtype=torch.int32, device=dev)
+        tv = torch.empty(max(self.nnz, 1), dtype=self.dtype, device=dev)
+        call(f"b2s_csr_transpose_{_SFX[self.dtype]}", n, m, self.nnz,
+             _p(self.row_ptrs), _p(self.col_idxs), _p(self.values), _p(trp),
+             _p(tci), _p(tv), _p(ws), wsb, _stream(tv))
+        return Csr(self.exec, (m, n), trp, tci[:self.nnz], tv[:self.nnz],
+                   self.strategy)
+
+
+class Ell(_SparseBase):
+    """Column-major padded Ell (include/ginkgo/core/matrix/ell.hpp)."""
+
+    def __init__(self, exec_, shape, width, stride, col_idxs, values):
+        self.exec = exec_
+        self.shape = tuple(shape)
+        self.width, self.stride = int(width), int(stride)
+        self.col_idxs, self.values = col_idxs, values
+        self.dtype = values.dtype
+
+    def apply(self, *args):
+        b2, x2, alpha, beta = self._apply_args(args)
+        call(f"b2s_ell_spmv_{_SFX[self.dtype]}", self.shape[0], self.shape[1],
+             self.width, self.stride, _p(self.col_idxs), _p(self.values),
+             _p(b2), b2.stride(0), _p(x2), x2.stride(0), x2.shape[1],
+             _p(alpha), _p(beta), _stream(x2))
+        return args[-1]
+
+
+class Sellp(_SparseBase):
+    """Sliced Ellpack (include/ginkgo/core/matrix/sellp.hpp); slice_sets and
+    slice_lengths are uint64 on the device (held as int64 tensors)."""
+
+    def __init__(self, exec_, shape, slice_size, stride_factor, slice_sets,
+                 slice_lengths, col_idxs, values):
+        self.exec = exec_
+        self.shape = tuple(shape)
+        self.slice_size, self.stride_factor = int(slice_size), int(stride_factor)
+        self.slice_sets, self.slice_lengths = slice_sets, slice_lengths
+        self.col_idxs, self.values = col_idxs, values
+        self.dtype = values.dtype
+
+    @property
+    def num_stored_elements(self):
+        return int(self.values.numel())
+
+    def apply(self, *args):
+        b2, x2, alpha, beta = self._apply_args(args)
+        call(f"b2s_sellp_spmv_{_SFX[self.dtype]}", self.shape[0], self.shape[1],
+             self.slice_size, _p(self.slice_sets), _p(self.slice_lengths),
+             _p(self.col_idxs), _p(self.values), _p(b2), b2.stride(0), _p(x2),
+             x2.stride(0), x2.shape[1], _p(alpha), _p(beta), _stream(x2))
+        return args[-1]

@@ -1,0 +1,280 @@
+/*
+ * libginkgo_b200 — C ABI of the B200 (sm_100a) sparse iterative-solve path.
+ *
+ * Every entry point takes plain device pointers, sizes and a CUDA stream
+ * (passed as void*, the cudaStream_t value; NULL = legacy default stream),
+ * launches asynchronously on that stream unless documented otherwise, and
+ * returns B2S_OK (0) or a negative B2S_ERR_* code; b2s_last_error() then
+ * holds a message.  The library allocates no device memory: where scratch
+ * space is needed the caller passes a workspace of the size the matching
+ * *_workspace_bytes() query reports, as the reference's kernels take a
+ * gko::array<char> from the executor.
+ *
+ * Data layout (the reference's):
+ *   Csr    row_ptrs int32[n+1], col_idxs int32[nnz], values[nnz]
+ *          (include/ginkgo/core/matrix/csr.hpp)
+ *   Ell    column-major, entry i of row r at r + i*stride, padding column -1
+ *          (include/ginkgo/core/matrix/ell.hpp:31-41)
+ *   Sellp  entry i of local row l in slice s at (slice_sets[s] + i)*slice_size
+ *          + l; slice_sets/slice_lengths are uint64 (size_type)
+ *          (include/ginkgo/core/matrix/sellp.hpp:379-383)
+ *   Dense  row-major n x k with leading dimension ld (matrix::view::dense,
+ *          include/ginkgo/core/matrix/device_views.hpp:24-43)
+ * Scalars alpha/beta are device pointers to one value (a 1x1 Dense); both
+ * NULL selects the simple form c = A b.  beta == 0 ignores c (NaN included).
+ *
+ * Each declaration names the reference kernel interface it stands in for.
+ */
+#ifndef GINKGO_B200_H
+#define GINKGO_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B2S_VERSION 1
+
+#define B2S_OK 0
+#define B2S_ERR_INVALID_ARG -1
+#define B2S_ERR_CUDA -2
+#define B2S_ERR_WORKSPACE -3
+#define B2S_ERR_UNSUPPORTED -4
+
+#define B2S_CSR_CLASSICAL 0
+#define B2S_CSR_LOAD_BALANCE 1
+
+/* Message of the last failed call on this host thread. */
+const char* b2s_last_error(void);
+/* B2S_VERSION of the loaded library. */
+int b2s_version(void);
+
+/* ---------------------------------------------------------------- SpMV -- */
+
+/* Number of tiles of the load_balance partition (rows binned by their
+ * merge-path start row + row_ptrs[row] into tiles of 2048 items).  The
+ * partition array has num_tiles + 1 int32 entries.  Stands in for the host
+ * computed srow of Csr::load_balance (include/ginkgo/core/matrix/csr.hpp:
+ * 417-468, make_srow :1651-1655). */
+int64_t b2s_csr_load_balance_num_tiles(int64_t num_rows, int64_t nnz);
+/* Builds the load_balance partition on the GPU (one binary search per
+ * tile); called once per matrix like Csr::make_srow. */
+int b2s_csr_load_balance_setup(int64_t num_rows, int64_t nnz,
+                               const int32_t* row_ptrs, int64_t num_tiles,
+                               int32_t* tile_rows, void* stream);
+
+/* c = A b or c = alpha A b + beta c for Csr A.
+ * strategy B2S_CSR_CLASSICAL: subwarp per row sized from max_row_nnz;
+ * strategy B2S_CSR_LOAD_BALANCE: tile_rows/num_tiles from the setup above.
+ * Replaces csr::spmv / csr::advanced_spmv
+ * (core/matrix/csr_kernels.hpp:29-42; CUDA dispatch
+ * common/cuda_hip/matrix/csr_kernels.template.cpp:2368-2485). */
+int b2s_csr_spmv_f64(int strategy, int64_t num_rows, int64_t num_cols,
+                     const int32_t* row_ptrs, const int32_t* col_idxs,
+                     const double* values, int64_t max_row_nnz,
+                     const int32_t* tile_rows, int64_t num_tiles,
+                     const double* b, int64_t ldb, double* c, int64_t ldc,
+                     int64_t num_rhs, const double* alpha, const double* beta,
+                     void* stream);
+int b2s_csr_spmv_f32(int strategy, int64_t num_rows, int64_t num_cols,
+                     const int32_t* row_ptrs, const int32_t* col_idxs,
+                     const float* values, int64_t max_row_nnz,
+                     const int32_t* tile_rows, int64_t num_tiles,
+                     const float* b, int64_t ldb, float* c, int64_t ldc,
+                     int64_t num_rhs, const float* alpha, const float* beta,
+                     void* stream);
+
+/* Ell SpMV; replaces ell::spmv / ell::advanced_spmv
+ * (core/matrix/ell_kernels.hpp:21-35). */
+int b2s_ell_spmv_f64(int64_t num_rows, int64_t num_cols, int64_t width,
+                     int64_t stride, const int32_t* col_idxs,
+                     const double* values, const double* b, int64_t ldb,
+                     double* c, int64_t ldc, int64_t num_rhs,
+                     const double* alpha, const double* beta, void* stream);
+int b2s_ell_spmv_f32(int64_t num_rows, int64_t num_cols, int64_t width,
+                     int64_t stride, const int32_t* col_idxs,
+                     const float* values, const float* b, int64_t ldb,
+                     float* c, int64_t ldc, int64_t num_rhs,
+                     const float* alpha, const float* beta, void* stream);
+
+/* Sellp SpMV; replaces sellp::spmv / sellp::advanced_spmv
+ * (core/matrix/sellp_kernels.hpp:21-35). */
+int b2s_sellp_spmv_f64(int64_t num_rows, int64_t num_cols, int64_t slice_size,
+                       const uint64_t* slice_sets,
+                       const uint64_t* slice_lengths, const int32_t* col_idxs,
+                       const double* values, const double* b, int64_t ldb,
+                       double* c, int64_t ldc, int64_t num_rhs,
+                       const double* alpha, const double* beta, void* stream);
+int b2s_sellp_spmv_f32(int64_t num_rows, int64_t num_cols, int64_t slice_size,
+                       const uint64_t* slice_sets,
+                       const uint64_t* slice_lengths, const int32_t* col_idxs,
+                       const float* values, const float* b, int64_t ldb,
+                       float* c, int64_t ldc, int64_t num_rhs,
+                       const float* alpha, const float* beta, void* stream);
+
+/* ------------------------------------------------------- conversions -- */
+
+/* Longest row; synchronises the stream and writes *result on the host.
+ * workspace: 8 device bytes.  Replaces ell::compute_max_row_nnz
+ * (core/matrix/ell_kernels.hpp:37-40). */
+int b2s_csr_max_row_nnz(int64_t num_rows, const int32_t* row_ptrs,
+                        int64_t* result, void* workspace, void* stream);
+
+/* Csr -> Ell with the given width and stride (>= num_rows); replaces
+ * csr::convert_to_ell (core/matrix/csr_kernels.hpp:99-103). */
+int b2s_csr_convert_to_ell_f64(int64_t num_rows, const int32_t* row_ptrs,
+                               const int32_t* col_idxs, const double* values,
+                               int64_t width, int64_t stride,
+                               int32_t* ell_col_idxs, double* ell_values,
+                               void* stream);
+int b2s_csr_convert_to_ell_f32(int64_t num_rows, const int32_t* row_ptrs,
+                               const int32_t* col_idxs, const float* values,
+                               int64_t width, int64_t stride,
+                               int32_t* ell_col_idxs, float* ell_values,
+                               void* stream);
+
+/* Sellp slice lengths (max row length per slice rounded up to
+ * stride_factor) and slice_sets (num_slices + 1 entries, exclusive prefix
+ * sum); replaces sellp::compute_slice_sets
+ * (core/matrix/sellp_kernels.hpp:41-45). */
+int64_t b2s_sellp_slice_sets_workspace_bytes(int64_t num_rows,
+                                             int64_t slice_size);
+int b2s_sellp_compute_slice_sets(int64_t num_rows, const int32_t* row_ptrs,
+                                 int64_t slice_size, int64_t stride_factor,
+                                 uint64_t* slice_sets, uint64_t* slice_lengths,
+                                 void* workspace, int64_t workspace_bytes,
+                                 void* stream);
+
+/* Csr -> Sellp scatter into slice_sets[num_slices] * slice_size slots;
+ * replaces csr::convert_to_sellp (core/matrix/csr_kernels.hpp:117-120). */
+int b2s_csr_convert_to_sellp_f64(int64_t num_rows, const int32_t* row_ptrs,
+                                 const int32_t* col_idxs, const double* values,
+                                 int64_t slice_size, const uint64_t* slice_sets,
+                                 const uint64_t* slice_lengths,
+                                 int32_t* sellp_col_idxs, double* sellp_values,
+                                 void* stream);
+int b2s_csr_convert_to_sellp_f32(int64_t num_rows, const int32_t* row_ptrs,
+                                 const int32_t* col_idxs, const float* values,
+                                 int64_t slice_size, const uint64_t* slice_sets,
+                                 const uint64_t* slice_lengths,
+                                 int32_t* sellp_col_idxs, float* sellp_values,
+                                 void* stream);
+
+/* Transpose (num_cols x num_rows result, columns sorted, same order as the
+ * reference's sequential scatter); replaces csr::transpose
+ * (core/matrix/csr_kernels.hpp:122-125; cuSPARSE csr2csc in
+ * common/cuda_hip/matrix/csr_kernels.template.cpp:3010-3056). */
+int64_t b2s_csr_transpose_workspace_bytes(int64_t num_rows, int64_t num_cols,
+                                          int64_t nnz, int value_bytes);
+int b2s_csr_transpose_f64(int64_t num_rows, int64_t num_cols, int64_t nnz,
+                          const int32_t* row_ptrs, const int32_t* col_idxs,
+                          const double* values, int32_t* t_row_ptrs,
+                          int32_t* t_col_idxs, double* t_values,
+                          void* workspace, int64_t workspace_bytes,
+                          void* stream);
+int b2s_csr_transpose_f32(int64_t num_rows, int64_t num_cols, int64_t nnz,
+                          const int32_t* row_ptrs, const int32_t* col_idxs,
+                          const float* values, int32_t* t_row_ptrs,
+                          int32_t* t_col_idxs, float* t_values,
+                          void* workspace, int64_t workspace_bytes,
+                          void* stream);
+
+/* --------------------------------------------------------- Jacobi ------ */
+
+/* inv_diag = 1 / diag(A), 1 where the diagonal is zero or missing;
+ * replaces the scalar Jacobi generate (jacobi::invert_diagonal,
+ * core/preconditioner/jacobi_kernels.hpp:42-45, after extract_diagonal,
+ * core/preconditioner/jacobi.cpp:337-369). */
+int b2s_jacobi_invert_diagonal_f64(int64_t num_rows, const int32_t* row_ptrs,
+                                   const int32_t* col_idxs,
+                                   const double* values, double* inv_diag,
+                                   void* stream);
+int b2s_jacobi_invert_diagonal_f32(int64_t num_rows, const int32_t* row_ptrs,
+                                   const int32_t* col_idxs,
+                                   const float* values, float* inv_diag,
+                                   void* stream);
+/* x = inv_diag .* b, or alpha inv_diag .* b + beta x; replaces
+ * jacobi::simple_scalar_apply / scalar_apply
+ * (core/preconditioner/jacobi_kernels.hpp:61-65, 79-85). */
+int b2s_jacobi_apply_f64(int64_t num_rows, int64_t num_rhs,
+                         const double* inv_diag, const double* b, int64_t ldb,
+                         double* x, int64_t ldx, const double* alpha,
+                         const double* beta, void* stream);
+int b2s_jacobi_apply_f32(int64_t num_rows, int64_t num_rhs,
+                         const float* inv_diag, const float* b, int64_t ldb,
+                         float* x, int64_t ldx, const float* alpha,
+                         const float* beta, void* stream);
+
+/* ------------------------------------------------------ fused solvers -- */
+
+/* Whole-solve entry points.  They run the reference's solver loop on the
+ * device with fused kernels and no host synchronisation inside an
+ * iteration; the host checks the device stop flag once per replay of a
+ * captured CUDA graph.  They synchronise `stream` before returning and
+ * write the host outputs (iterations, residual norms, status).  Stopping:
+ * Iteration(max_iters) + ResidualNorm(reduction_factor, rhs_norm baseline)
+ * per right-hand-side column; status[j] uses the bit layout of
+ * gko::stopping_status (include/ginkgo/core/stop/stopping_status.hpp):
+ * bit 7 converged, bit 6 finalized, bits 0-5 criterion id (1 iteration
+ * limit, 2 residual norm).  inv_diag: scalar Jacobi (from
+ * b2s_jacobi_invert_diagonal_*) or NULL for no preconditioner. */
+
+/* Preconditioned CG, 1..16 right-hand sides (b, x row-major with leading
+ * dimensions).  Replaces Cg<V>::apply_dense_impl (core/solver/cg.cpp:91-189)
+ * with cg::initialize/step_1/step_2 (core/solver/cg_kernels.hpp:25-52), the
+ * dots, the Jacobi apply and residual_norm::residual_norm
+ * (core/stop/residual_norm_kernels.hpp:21-29). */
+int64_t b2s_cg_workspace_bytes(int64_t num_rows, int64_t num_rhs,
+                               int value_bytes);
+int b2s_cg_solve_f64(int64_t num_rows, const int32_t* row_ptrs,
+                     const int32_t* col_idxs, const double* values,
+                     int64_t max_row_nnz, const double* inv_diag,
+                     const double* b, int64_t ldb, double* x, int64_t ldx,
+                     int64_t num_rhs, int64_t max_iters,
+                     double reduction_factor, int64_t check_every,
+                     void* workspace, int64_t workspace_bytes,
+                     int64_t* iterations, double* residual_norms,
+                     uint8_t* status, void* stream);
+int b2s_cg_solve_f32(int64_t num_rows, const int32_t* row_ptrs,
+                     const int32_t* col_idxs, const float* values,
+                     int64_t max_row_nnz, const float* inv_diag,
+                     const float* b, int64_t ldb, float* x, int64_t ldx,
+                     int64_t num_rhs, int64_t max_iters,
+                     double reduction_factor, int64_t check_every,
+                     void* workspace, int64_t workspace_bytes,
+                     int64_t* iterations, double* residual_norms,
+                     uint8_t* status, void* stream);
+
+#define B2S_GMRES_F64 0
+#define B2S_GMRES_MIXED_F32 1
+#define B2S_GMRES_MIXED_BF16 2
+
+/* Restarted GMRES(krylov_dim <= 32), right scalar-Jacobi preconditioning,
+ * one right-hand side, FP64 matrix/b/x/inv_diag.  variant B2S_GMRES_F64 is
+ * plain FP64 GMRES (Gmres<double>, core/solver/gmres.cpp:325-640);
+ * B2S_GMRES_MIXED_F32 / _BF16 is iterative refinement (Ir<double>,
+ * core/solver/ir.cpp:191-257) whose every outer step computes r = b - A x
+ * and ||r|| in FP64 and runs one GMRES cycle on an FP32 copy of A with FP32
+ * vectors and an FP32 or BF16 Krylov basis.  Hessenberg, Givens and the
+ * triangular solve are FP64 in all variants.  max_iters bounds the total
+ * Arnoldi steps; reduction_factor is the goal on the explicit FP64 residual
+ * relative to ||b||; inner_reduction ends an inner cycle early once its
+ * estimate falls below inner_reduction * ||r||.  *restarts counts cycles. */
+int64_t b2s_gmres_workspace_bytes(int64_t num_rows, int64_t nnz,
+                                  int64_t krylov_dim, int variant);
+int b2s_gmres_solve(int variant, int64_t num_rows, const int32_t* row_ptrs,
+                    const int32_t* col_idxs, const double* values,
+                    int64_t max_row_nnz, const double* inv_diag,
+                    const double* b, double* x, int64_t krylov_dim,
+                    int64_t max_iters, double reduction_factor,
+                    double inner_reduction, void* workspace,
+                    int64_t workspace_bytes, int64_t* iterations,
+                    int64_t* restarts, double* residual_norm, int* converged,
+                    void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GINKGO_B200_H */

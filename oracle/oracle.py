@@ -182,8 +182,8 @@ def csr_to_sellp(rp, ci, v, slice_size=64, stride_factor=1):
     n = len(rp) - 1
     sets, lens = sellp_slice_sets(rp, slice_size, stride_factor)
     total = int(sets[-1]) * slice_size
-    sci = np.empty(total, np.int32)
-    sv = np.empty(total, v.dtype)
+    sci = np.full(total, -1, np.int32)
+    sv = np.zeros(total, v.dtype)
     getattr(lib(), f"orc_csr_to_sellp_{_sfx(v.dtype)}")(
         n, _ptr(rp), _ptr(ci), _ptr(v), slice_size, _ptr(sets), _ptr(lens),
         _ptr(sci), _ptr(sv))

@@ -1,0 +1,181 @@
+"""SpMV and format conversion on the GPU against the CPU oracle.
+
+Tolerances: FP64 results agree with the oracle to 1e-14 relative, scaled by
+the row's absolute sum |A||x| (the reduction order differs); FP32 to 1e-5 on
+the same scale.  Conversions, row pointers and patterns are bit-exact.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import dense_to_csr, to_array
+from ginkgo_b200 import stencils
+from ginkgo_b200.matrix import Csr, CudaExecutor
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+TOL = {torch.float64: 1e-14, torch.float32: 1e-5}
+NP = {torch.float64: np.float64, torch.float32: np.float32}
+
+
+@pytest.fixture(scope="module")
+def exe():
+    return CudaExecutor.create(0)
+
+
+def assert_spmv_close(rp, ci, v, x, got, ref, tol, alpha=1.0, beta_y=None):
+    """|got - ref| <= tol * (|alpha| |A| |x| + |beta y|) row by row."""
+    absA = np.abs(v).astype(np.float64)
+    scale = abs(alpha) * orc.csr_spmv(rp, ci, absA, np.abs(x).astype(np.float64))
+    if beta_y is not None:
+        scale = scale + np.abs(beta_y).reshape(scale.shape)
+    scale = np.maximum(scale, np.finfo(np.float64).tiny)
+    err = np.abs(got.astype(np.float64) - ref.astype(np.float64)) / scale
+    assert err.max() <= tol, err.max()
+
+
+def formats(A, fmt):
+    if fmt == "classical":
+        return A.set_strategy("classical")
+    if fmt == "load_balance":
+        return A.set_strategy("load_balance")
+    if fmt == "ell":
+        return A.convert_to_ell()
+    if fmt == "sellp":
+        return A.convert_to_sellp(32, 1)
+    raise ValueError(fmt)
+
+
+FORMATS = ["classical", "load_balance", "ell", "sellp"]
+
+
+@pytest.mark.parametrize("fmt", FORMATS)
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+def test_known_answers(exe, known, fmt, dt):
+    for case in known["spmv"]:
+        m = case["matrix"]
+        A = Csr(exe, (m["n_rows"], m["n_cols"]), m["row_ptrs"], m["col_idxs"],
+                torch.tensor(m["values"], dtype=dt))
+        op = formats(A, fmt)
+        x = torch.tensor(to_array(case["x"]), dtype=dt, device="cuda")
+        if "alpha" in case:
+            y = torch.tensor(to_array(case["y"]), dtype=dt, device="cuda")
+            op.apply(case["alpha"], x, case["beta"], y)
+        else:
+            y = torch.empty((2, x.shape[1]), dtype=dt, device="cuda")
+            op.apply(x, y)
+        np.testing.assert_array_equal(y.cpu().numpy(),
+                                      to_array(case["expected"], NP[dt]),
+                                      err_msg=f"{fmt} {case['name']}")
+
+
+@pytest.mark.parametrize("fmt", FORMATS)
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+@pytest.mark.parametrize("k", [1, 3, 4, 16])
+def test_random_power_law_matches_oracle(exe, fmt, dt, k):
+    # long rows (up to 3000 > the 2048-entry chunk), empty-free, unsorted
+    rng = np.random.default_rng(7 + k)
+    rp, ci, v = stencils.power_law(20000, seed=11, mu=2.0, sigma=1.2, max_len=3000)
+    v = v.astype(NP[dt])
+    x = rng.standard_normal((20000, k)).astype(NP[dt])
+    ref = orc.csr_spmv(rp, ci, v, x)
+    A = Csr.read(exe, rp, ci, v, dtype=dt)
+    op = formats(A, fmt)
+    xd = torch.from_numpy(x).cuda()
+    y = torch.full((20000, k), float("nan"), dtype=dt, device="cuda")
+    op.apply(xd, y)
+    assert_spmv_close(rp, ci, v, x, y.cpu().numpy(), ref, TOL[dt])
+    # advanced apply, beta != 0
+    y0 = rng.standard_normal((20000, k)).astype(NP[dt])
+    ref2 = orc.csr_spmv(rp, ci, v, x, y0, -0.5, 2.0)
+    y2 = torch.from_numpy(y0).cuda()
+    op.apply(-0.5, xd, 2.0, y2)
+    assert_spmv_close(rp, ci, v, x, y2.cpu().numpy(), ref2, TOL[dt] * 4,
+                      alpha=0.5, beta_y=2.0 * y0.astype(np.float64))
+
+
+@pytest.mark.parametrize("fmt", ["classical", "load_balance"])
+def test_empty_rows_and_single_long_row(exe, fmt):
+    n = 9000
+    lens = np.zeros(n, np.int64)
+    lens[::3] = 2          # every third row has two entries, the rest empty
+    lens[4500] = 7000      # one row spanning several load_balance chunks
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    rng = np.random.default_rng(5)
+    ci = np.concatenate([np.sort(rng.choice(n, l, replace=False)) for l in lens]).astype(np.int32)
+    v = rng.standard_normal(int(rp[-1]))
+    x = rng.standard_normal((n, 2))
+    ref = orc.csr_spmv(rp, ci, v, x)
+    A = formats(Csr.read(exe, rp, ci, v), fmt)
+    y = torch.full((n, 2), float("nan"), dtype=torch.float64, device="cuda")
+    A.apply(torch.from_numpy(x).cuda(), y)
+    assert_spmv_close(rp, ci, v, x, y.cpu().numpy(), ref, 1e-14)
+
+
+@pytest.mark.parametrize("fmt", FORMATS)
+def test_empty_matrix(exe, fmt):
+    A = Csr(exe, (0, 0), torch.zeros(1, dtype=torch.int32), torch.zeros(0, dtype=torch.int32),
+            torch.zeros(0, dtype=torch.float64))
+    op = formats(A, fmt)
+    x = torch.zeros((0, 1), dtype=torch.float64, device="cuda")
+    y = torch.zeros((0, 1), dtype=torch.float64, device="cuda")
+    op.apply(x, y)
+
+
+def test_conversions_bit_exact(exe, known):
+    rp, ci, v = stencils.power_law(5000, seed=2, mu=1.8, max_len=400)
+    A = Csr.read(exe, rp, ci, v)
+    w, s, eci, ev = orc.csr_to_ell(rp, ci, v)
+    E = A.convert_to_ell()
+    assert (E.width, E.stride) == (w, s)
+    np.testing.assert_array_equal(E.col_idxs.cpu().numpy(), eci)
+    np.testing.assert_array_equal(E.values.cpu().numpy(), ev)
+    for ss, sf in [(32, 1), (64, 1), (2, 2), (7, 3)]:
+        sets, lens, sci, sv = orc.csr_to_sellp(rp, ci, v, ss, sf)
+        S = A.convert_to_sellp(ss, sf)
+        np.testing.assert_array_equal(S.slice_sets.cpu().numpy(), sets.astype(np.int64))
+        np.testing.assert_array_equal(S.slice_lengths.cpu().numpy(), lens.astype(np.int64))
+        np.testing.assert_array_equal(S.col_idxs.cpu().numpy(), sci)
+        np.testing.assert_array_equal(S.values.cpu().numpy(), sv)
+    case = known["convert_to_sellp"]
+    m = case["matrix"]
+    S = Csr(exe, (2, 3), m["row_ptrs"], m["col_idxs"],
+            torch.tensor(m["values"], dtype=torch.float64)).convert_to_sellp(64, 1)
+    np.testing.assert_array_equal(S.slice_sets.cpu().numpy(), case["slice_sets"])
+    for idx, (c, val) in case["checks"].items():
+        assert S.col_idxs[int(idx)].item() == c and S.values[int(idx)].item() == val
+
+
+def test_transpose_bit_exact(exe, known):
+    for case in known["transpose"]:
+        d = np.array(case["dense"])
+        rp, ci, v = dense_to_csr(d)
+        T = Csr.read(exe, rp, ci, v, shape=d.shape).transpose()
+        erp, eci, ev = dense_to_csr(case["expected_dense"])
+        np.testing.assert_array_equal(T.row_ptrs.cpu().numpy(), erp)
+        np.testing.assert_array_equal(T.col_idxs.cpu().numpy(), eci)
+        np.testing.assert_array_equal(T.values.cpu().numpy(), ev)
+    rp, ci, v = stencils.power_law(6000, seed=4, mu=2.0, max_len=300)
+    trp, tci, tv = orc.csr_transpose(rp, ci, v, 6000)
+    T = Csr.read(exe, rp, ci, v).transpose()
+    np.testing.assert_array_equal(T.row_ptrs.cpu().numpy(), trp)
+    np.testing.assert_array_equal(T.col_idxs.cpu().numpy(), tci)
+    np.testing.assert_array_equal(T.values.cpu().numpy(), tv)
+
+
+def test_poisson_128_full_size_fp64(exe):
+    """The benchmark matrix (3D 7-point, 128^3) at full size, k = 1 and 16."""
+    rp, ci, v = stencils.poisson_3d_7pt(128)
+    n = len(rp) - 1
+    A = Csr.read(exe, rp, ci, v)
+    rng = np.random.default_rng(0)
+    for k in (1, 16):
+        x = rng.standard_normal((n, k))
+        ref = orc.csr_spmv(rp, ci, v, x)
+        xd = torch.from_numpy(x).cuda()
+        for fmt in FORMATS:
+            op = formats(A, fmt)
+            y = torch.empty((n, k), dtype=torch.float64, device="cuda")
+            op.apply(xd, y)
+            assert_spmv_close(rp, ci, v, x, y.cpu().numpy(), ref, 1e-14)
