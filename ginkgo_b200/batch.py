@@ -1,0 +1,211 @@
+"""Batched solve over many independent systems of uneven size, named after
+the reference's ``gko::batch::matrix::Ell`` and
+``gko::batch::solver::Bicgstab``:
+
+    A = BatchEll.from_csr(exec, systems)          # list of (rp, ci, v)
+    solver = (BatchBicgstab.build().with_max_iterations(500)
+              .with_tolerance(1e-8).with_tolerance_type("relative")
+              .with_preconditioner("jacobi").on(exec).generate(A))
+    solver.apply(b, x)        # b, x: concatenated per-system vectors
+    solver.logger.iterations  # per system, as batch::log::BatchConvergence
+
+The reference's batches are uniform (one size, shared column indices); this
+batch is ragged: every system has its own size and pattern.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import stencils
+from ._lib import call, lib
+from .matrix import _p, _stream
+
+_SFX = {torch.float64: "f64", torch.float32: "f32"}
+
+
+class BatchEll:
+    """Ragged batch Ell: system s owns rows [row_offsets[s], row_offsets[s+1])
+    and its entries at values[width * row_offsets[s] + j * n_s + r]."""
+
+    def __init__(self, exec_, row_offsets, width, col_idxs, values):
+        dev = exec_.device
+        self.exec = exec_
+        self.host_row_offsets = np.ascontiguousarray(row_offsets, dtype=np.int32)
+        self.row_offsets = torch.from_numpy(self.host_row_offsets).to(dev)
+        self.width = int(width)
+        self.col_idxs = torch.as_tensor(col_idxs, dtype=torch.int32).to(dev).contiguous()
+        self.values = torch.as_tensor(values).to(dev).contiguous()
+        self.dtype = self.values.dtype
+        self.num_systems = len(self.host_row_offsets) - 1
+        self.total_rows = int(self.host_row_offsets[-1])
+
+    @property
+    def sizes(self):
+        return np.diff(self.host_row_offsets)
+
+    @classmethod
+    def from_csr(cls, exec_, systems, width=None, dtype=torch.float64):
+        """systems: list of (row_ptrs, col_idxs, values), local indices."""
+        sizes = np.array([len(rp) - 1 for rp, _, _ in systems], dtype=np.int64)
+        offs = np.zeros(len(systems) + 1, dtype=np.int64)
+        np.cumsum(sizes, out=offs[1:])
+        if width is None:
+            width = max(int(np.diff(rp).max()) if len(rp) > 1 else 0
+                        for rp, _, _ in systems)
+        ci = np.full(int(offs[-1]) * width, -1, dtype=np.int32)
+        v = np.zeros(int(offs[-1]) * width, dtype=np.float64)
+        for s, (rp, c, val) in enumerate(systems):
+            n = len(rp) - 1
+            rp = np.asarray(rp)
+            lens = np.diff(rp)
+            rows = np.repeat(np.arange(n), lens)
+            slot = np.arange(len(c)) - np.repeat(rp[:-1], lens)
+            idx = width * offs[s] + slot * n + rows
+            ci[idx] = c
+            v[idx] = val
+        return cls(exec_, offs, width, torch.from_numpy(ci),
+                   torch.from_numpy(v).to(dtype))
+
+    def to_csr_list(self):
+        """Host CSR per system (for checking)."""
+        ci = self.col_idxs.cpu().numpy()
+        v = self.values.cpu().numpy()
+        out = []
+        for s in range(self.num_systems):
+            o, n = int(self.host_row_offsets[s]), int(self.sizes[s])
+            base = self.width * o
+            rows, cols, vals = [], [], []
+            for j in range(self.width):
+                c = ci[base + j * n: base + (j + 1) * n]
+                m = c >= 0
+                rows.append(np.nonzero(m)[0])
+                cols.append(c[m])
+                vals.append(v[base + j * n: base + (j + 1) * n][m])
+            rows, cols, vals = map(np.concatenate, (rows, cols, vals))
+            order = np.lexsort((cols, rows))
+            rp = np.zeros(n + 1, dtype=np.int64)
+            np.cumsum(np.bincount(rows, minlength=n), out=rp[1:])
+            out.append((rp.astype(np.int32), cols[order], vals[order]))
+        return out
+
+
+def convection_diffusion_batch(exec_, num_systems, lo=32, hi=1024, seed=0,
+                               dtype=torch.float64):
+    """The batched workload: system sizes ~ U[lo, hi]; each system a 5-point
+    convection-diffusion stencil on the most-square grid with nx * ny = n,
+    diffusion ~ U[0.5, 2], velocity components ~ U[-1, 1] (central
+    differences, unit mesh width)."""
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(lo, hi + 1, size=num_systems)
+    diff = rng.uniform(0.5, 2.0, size=num_systems)
+    vel = rng.uniform(-1.0, 1.0, size=(num_systems, 2))
+    systems = []
+    cache = {}
+    for s in range(num_systems):
+        n = int(sizes[s])
+        nx, ny = stencils.most_square_grid(n)
+        key = (nx, ny)
+        if key not in cache:
+            cache[key] = stencils.convection_diffusion_2d(nx, ny, 1.0, 0.0, 0.0)
+        rp, ci, _ = cache[key]
+        # weights of the pattern: diag, east, west, north, south
+        d = diff[s]
+        vx, vy = vel[s]
+        rows = np.repeat(np.arange(n), np.diff(rp))
+        off = ci.astype(np.int64) - rows
+        w = np.where(off == 0, 4 * d,
+            np.where(off == 1, -d + 0.5 * vx,
+            np.where(off == -1, -d - 0.5 * vx,
+            np.where(off == nx, -d + 0.5 * vy, -d - 0.5 * vy))))
+        systems.append((rp, ci, w))
+    return BatchEll.from_csr(exec_, systems, width=5, dtype=dtype), systems
+
+
+class _Builder:
+    def __init__(self):
+        self.p = {"max_iterations": 100, "tolerance": 1e-11,
+                  "tolerance_type": "absolute", "preconditioner": None}
+
+    def __getattr__(self, name):
+        if name.startswith("with_"):
+            def setter(v):
+                self.p[name[5:]] = v
+                return self
+            return setter
+        raise AttributeError(name)
+
+    def on(self, exec_):
+        return _BatchFactory(exec_, dict(self.p))
+
+
+class _BatchFactory:
+    def __init__(self, exec_, params):
+        self.exec = exec_
+        self.p = params
+
+    def generate(self, A: BatchEll):
+        return _BatchSolver(self, A)
+
+
+class BatchLog:
+    def __init__(self, iterations, residual_norms):
+        self.iterations = iterations
+        self.residual_norms = residual_norms
+
+
+class _BatchSolver:
+    def __init__(self, f, A):
+        self.f = f
+        self.A = A
+        self.tune_table = None
+        dev = A.values.device
+        self.iters = torch.zeros(A.num_systems, dtype=torch.int32, device=dev)
+        self.res = torch.zeros(A.num_systems, dtype=torch.float64, device=dev)
+        nbytes = lib().b2s_batch_bicgstab_workspace_bytes(
+            A.num_systems, A.total_rows, A.values.element_size())
+        self.ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        self.logger = None
+
+    def _args(self, b, x):
+        A, p = self.A, self.f.p
+        for t, nm in ((b, "b"), (x, "x")):
+            if t.dtype != A.dtype or t.numel() != A.total_rows or not t.is_contiguous():
+                raise ValueError(f"{nm} must be a contiguous {A.dtype} vector of "
+                                 f"{A.total_rows} entries")
+        tol_abs = 1 if p["tolerance_type"] == "absolute" else 0
+        jac = 1 if p["preconditioner"] in ("jacobi", "scalar_jacobi") else 0
+        return (A.num_systems, _p(A.row_offsets),
+                A.host_row_offsets.ctypes.data_as(C.c_void_p), A.width,
+                _p(A.col_idxs), _p(A.values), _p(b), _p(x),
+                int(p["max_iterations"]), float(p["tolerance"]), tol_abs, jac)
+
+    def apply(self, b, x):
+        tt = None if self.tune_table is None else \
+            self.tune_table.ctypes.data_as(C.c_void_p)
+        call(f"b2s_batch_ell_bicgstab_solve_{_SFX[self.A.dtype]}",
+             *self._args(b, x), tt, _p(self.ws), self.ws.numel(),
+             _p(self.iters), _p(self.res), _stream(x))
+        self.logger = BatchLog(self.iters, self.res)
+        return x
+
+    def tune(self, b, x):
+        """Autotunes threads-per-system and vector placement per size bucket
+        (and solves); later applies reuse the table."""
+        table = np.zeros(24, dtype=np.int32)
+        call(f"b2s_batch_ell_bicgstab_tune_{_SFX[self.A.dtype]}",
+             *self._args(b, x), _p(self.ws), self.ws.numel(), _p(self.iters),
+             _p(self.res), table.ctypes.data_as(C.c_void_p), _stream(x))
+        self.tune_table = table
+        self.logger = BatchLog(self.iters, self.res)
+        return table
+
+
+class BatchBicgstab:
+    """batch::solver::Bicgstab (core/solver/batch_bicgstab.cpp)."""
+
+    @staticmethod
+    def build():
+        return _Builder()

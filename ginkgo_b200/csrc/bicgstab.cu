@@ -1,0 +1,482 @@
+// Fused preconditioned BiCGStab (scalar Jacobi or identity), the loop of
+// core/solver/bicgstab.cpp:95-250 with the kernels of
+// common/unified/solver/bicgstab_kernels.cpp:23-195 regrouped into three
+// passes per iteration, no host synchronisation inside the loop:
+//
+//   spmv1   p' = r + tmp (p - omega v), tmp = rho/prev_rho * alpha/omega
+//           (p' = r when prev_rho * omega == 0) formed on the fly at every
+//           column index; v' = A D^-1 p'; dot(rr, v') in-kernel; the last
+//           block sets alpha = rho / dot(rr, v')   (step_1 + precond + SpMV
+//           + dot + the alpha of step_2)
+//   spmv2   s = r - alpha v' formed on the fly; t = A D^-1 s; dot(s, t),
+//           dot(t, t), ||s||^2; the last block checks ||s|| (a column that
+//           converges here is finalised by the next pass) and sets
+//           omega = dot(s, t) / dot(t, t)     (step_2 + check + precond +
+//           SpMV + the dots of step_3)
+//   update  x += alpha D^-1 p' + omega D^-1 s, r = s - omega t (or only
+//           x += alpha D^-1 p' for a column finalised at s); dot(rr, r),
+//           ||r||^2; the last block advances the iteration and checks
+//           (step_3 / finalize + next dot + check)
+//
+// p and v are double-buffered so every row reads the previous iterate.
+#include "solver_common.cuh"
+
+namespace b2s {
+namespace {
+
+template <typename T>
+struct BicgScalars {
+    T rho[kMaxRhs], prev_rho[kMaxRhs], alpha[kMaxRhs], omega[kMaxRhs],
+        start[kMaxRhs], tau[kMaxRhs];
+};
+
+template <typename T>
+__device__ __forceinline__ T bicg_p(T r, T p, T v, T tmp, T omega, bool from_r)
+{
+    return from_r ? r : add_rn(r, mul_rn(tmp, add_rn(p, -mul_rn(omega, v))));
+}
+
+template <typename T>
+__device__ __forceinline__ T bicg_s(T r, T v, T alpha)
+{
+    return add_rn(r, -mul_rn(alpha, v));
+}
+
+template <typename T, int K>
+__global__ void __launch_bounds__(kSolverBlock)
+    bicg_init_kernel(int64_t n, const T* __restrict__ b, int64_t ldb, int k,
+                     const T* __restrict__ r, T* __restrict__ rr,
+                     T* __restrict__ p, T* __restrict__ v, SolveCtl* ctl,
+                     BicgScalars<T>* sc, T* __restrict__ partials)
+{
+    __shared__ T red[kSolverBlock / kWarp * 3 * K];
+    __shared__ T tot[3 * K];
+    __shared__ int last;
+    T acc[3 * K];
+#pragma unroll
+    for (int j = 0; j < 3 * K; ++j) acc[j] = T(0);
+    for (int64_t i = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * kSolverBlock) {
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            const T ri = r[i * K + j];
+            const T bb = j < k ? b[i * ldb + j] : T(0);
+            rr[i * K + j] = ri;
+            p[i * K + j] = T(0);
+            v[i * K + j] = T(0);
+            acc[j] += bb * bb;
+            acc[K + j] += ri * ri;  // dot(rr, r) with rr = r
+            acc[2 * K + j] += ri * ri;
+        }
+    }
+    block_partials<T, 3 * K>(acc, partials, red);
+    if (last_block_done(&ctl->ticket, &last)) {
+        sum_partials<T, 3 * K>(partials, gridDim.x, tot, red);
+        if (threadIdx.x == 0) {
+            ctl->ticket = 0;
+            ctl->iter = 0;
+            int all = 1;
+            for (int j = 0; j < K; ++j) {
+                uint8_t s = 0;
+                if (j >= k) stop_status(s, kIterationId, true);
+                sc->start[j] = sqrt(tot[j]);
+                sc->rho[j] = tot[K + j];
+                sc->prev_rho[j] = T(1);
+                sc->alpha[j] = T(1);
+                sc->omega[j] = T(1);
+                sc->tau[j] = sqrt(tot[2 * K + j]);
+                if (ctl->max_iters <= 0) stop_status(s, kIterationId, true);
+                if (double(sc->tau[j]) <= ctl->reduction * double(sc->start[j])) {
+                    converge_status(s, kResidualId, true);
+                }
+                ctl->status[j] = s;
+                all &= has_stopped(s);
+            }
+            ctl->all_stopped = all;
+        }
+    }
+}
+
+template <typename T, int SW, int K>
+__global__ void __launch_bounds__(kSolverBlock)
+    bicg_spmv1_kernel(int64_t n, const int32_t* __restrict__ rp,
+                      const int32_t* __restrict__ ci, const T* __restrict__ a,
+                      const T* __restrict__ dinv, const T* __restrict__ r,
+                      const T* __restrict__ rr, const T* __restrict__ p_old,
+                      const T* __restrict__ v_old, T* __restrict__ p_new,
+                      T* __restrict__ v_new, SolveCtl* ctl, BicgScalars<T>* sc,
+                      T* __restrict__ partials)
+{
+    __shared__ T red[kSolverBlock / kWarp * K];
+    __shared__ T tot[K];
+    __shared__ int last;
+    if (ctl->all_stopped) return;
+    bool active[K], from_r[K];
+    T tmp[K], om[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        active[j] = !has_stopped(ctl->status[j]);
+        om[j] = sc->omega[j];
+        from_r[j] = sc->prev_rho[j] * om[j] == T(0);
+        tmp[j] = from_r[j] ? T(0) : sc->rho[j] / sc->prev_rho[j] * sc->alpha[j] / om[j];
+    }
+    T dot[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) dot[j] = T(0);
+    const int lane = threadIdx.x % SW;
+    const int64_t nsub = int64_t(gridDim.x) * kSolverBlock / SW;
+    // warp-uniform trip count: all lanes of a warp run every iteration, so
+    // the subwarp shuffles below always see the whole warp
+    for (int64_t wbase = (blockIdx.x * int64_t(kSolverBlock) + threadIdx.x) /
+                         kWarp * (kWarp / SW);
+         wbase < n; wbase += nsub) {
+        const int64_t row = wbase + (threadIdx.x % kWarp) / SW;
+        const bool valid = row < n;
+        T acc[K];
+#pragma unroll
+        for (int j = 0; j < K; ++j) acc[j] = T(0);
+        const int end = valid ? rp[row + 1] : 0;
+        for (int e = (valid ? rp[row] : end) + lane; e < end; e += SW) {
+            const T av = a[e];
+            const int64_t c = ci[e];
+            const T d = dinv ? dinv[c] : T(1);
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                if (active[j]) {
+                    const T pc = bicg_p(r[c * K + j], p_old[c * K + j],
+                                        v_old[c * K + j], tmp[j], om[j], from_r[j]);
+                    acc[j] += av * mul_rn(d, pc);
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < K; ++j) acc[j] = subwarp_sum<SW>(acc[j]);
+        if (valid && lane == 0) {
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                if (active[j]) {
+                    p_new[row * K + j] = bicg_p(r[row * K + j], p_old[row * K + j],
+                                                v_old[row * K + j], tmp[j], om[j],
+                                                from_r[j]);
+                    v_new[row * K + j] = acc[j];
+                    dot[j] += rr[row * K + j] * acc[j];
+                }
+            }
+        }
+    }
+    block_partials<T, K>(dot, partials, red);
+    if (last_block_done(&ctl->ticket, &last)) {
+        sum_partials<T, K>(partials, gridDim.x, tot, red);
+        if (threadIdx.x < K) {
+            const T bv = tot[threadIdx.x];
+            sc->alpha[threadIdx.x] = bv != T(0) ? sc->rho[threadIdx.x] / bv : T(0);
+        }
+        if (threadIdx.x == 0) ctl->ticket = 0;
+    }
+}
+
+template <typename T, int SW, int K>
+__global__ void __launch_bounds__(kSolverBlock)
+    bicg_spmv2_kernel(int64_t n, const int32_t* __restrict__ rp,
+                      const int32_t* __restrict__ ci, const T* __restrict__ a,
+                      const T* __restrict__ dinv, const T* __restrict__ r,
+                      const T* __restrict__ vv, T* __restrict__ s,
+                      T* __restrict__ t, SolveCtl* ctl, BicgScalars<T>* sc,
+                      T* __restrict__ partials)
+{
+    __shared__ T red[kSolverBlock / kWarp * 3 * K];
+    __shared__ T tot[3 * K];
+    __shared__ int last;
+    if (ctl->all_stopped) return;
+    bool active[K];
+    T alpha[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        active[j] = !has_stopped(ctl->status[j]);
+        alpha[j] = sc->alpha[j];
+    }
+    T acc3[3 * K];
+#pragma unroll
+    for (int j = 0; j < 3 * K; ++j) acc3[j] = T(0);
+    const int lane = threadIdx.x % SW;
+    const int64_t nsub = int64_t(gridDim.x) * kSolverBlock / SW;
+    // warp-uniform trip count: all lanes of a warp run every iteration, so
+    // the subwarp shuffles below always see the whole warp
+    for (int64_t wbase = (blockIdx.x * int64_t(kSolverBlock) + threadIdx.x) /
+                         kWarp * (kWarp / SW);
+         wbase < n; wbase += nsub) {
+        const int64_t row = wbase + (threadIdx.x % kWarp) / SW;
+        const bool valid = row < n;
+        T acc[K];
+#pragma unroll
+        for (int j = 0; j < K; ++j) acc[j] = T(0);
+        const int end = valid ? rp[row + 1] : 0;
+        for (int e = (valid ? rp[row] : end) + lane; e < end; e += SW) {
+            const T av = a[e];
+            const int64_t c = ci[e];
+            const T d = dinv ? dinv[c] : T(1);
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                if (active[j]) {
+                    acc[j] += av * mul_rn(d, bicg_s(r[c * K + j], vv[c * K + j], alpha[j]));
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < K; ++j) acc[j] = subwarp_sum<SW>(acc[j]);
+        if (valid && lane == 0) {
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                if (active[j]) {
+                    const T sr = bicg_s(r[row * K + j], vv[row * K + j], alpha[j]);
+                    s[row * K + j] = sr;
+                    t[row * K + j] = acc[j];
+                    acc3[j] += sr * acc[j];
+                    acc3[K + j] += acc[j] * acc[j];
+                    acc3[2 * K + j] += sr * sr;
+                }
+            }
+        }
+    }
+    block_partials<T, 3 * K>(acc3, partials, red);
+    if (last_block_done(&ctl->ticket, &last)) {
+        sum_partials<T, 3 * K>(partials, gridDim.x, tot, red);
+        if (threadIdx.x == 0) {
+            ctl->ticket = 0;
+            for (int j = 0; j < K; ++j) {
+                uint8_t st = ctl->status[j];
+                if (has_stopped(st)) continue;
+                const T tau_s = sqrt(tot[2 * K + j]);
+                // check on s without finalising (core/solver/bicgstab.cpp
+                // second check): the update pass adds alpha y and finalises
+                if (double(tau_s) <= ctl->reduction * double(sc->start[j])) {
+                    converge_status(st, kResidualId, false);
+                    sc->tau[j] = tau_s;
+                }
+                ctl->status[j] = st;
+                const T tt = tot[K + j];
+                sc->omega[j] = tt != T(0) ? tot[j] / tt : T(0);
+            }
+        }
+    }
+}
+
+template <typename T, int K>
+__global__ void __launch_bounds__(kSolverBlock)
+    bicg_update_kernel(int64_t n, const T* __restrict__ dinv,
+                       T* __restrict__ x, int64_t ldx, T* __restrict__ r,
+                       const T* __restrict__ rr, const T* __restrict__ p,
+                       const T* __restrict__ s, const T* __restrict__ t,
+                       SolveCtl* ctl, BicgScalars<T>* sc,
+                       T* __restrict__ partials)
+{
+    __shared__ T red[kSolverBlock / kWarp * 2 * K];
+    __shared__ T tot[2 * K];
+    __shared__ int last;
+    if (ctl->all_stopped) return;
+    int mode[K];  // 0 frozen, 1 finalise at s, 2 full update
+    T alpha[K], omega[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        const uint8_t st = ctl->status[j];
+        mode[j] = !has_stopped(st) ? 2 : (is_finalized(st) ? 0 : 1);
+        alpha[j] = sc->alpha[j];
+        omega[j] = sc->omega[j];
+    }
+    T acc[2 * K];
+#pragma unroll
+    for (int j = 0; j < 2 * K; ++j) acc[j] = T(0);
+    for (int64_t i = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * kSolverBlock) {
+        const T d = dinv ? dinv[i] : T(1);
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            if (mode[j] == 1) {
+                x[i * ldx + j] += alpha[j] * mul_rn(d, p[i * K + j]);
+            } else if (mode[j] == 2) {
+                const T si = s[i * K + j];
+                x[i * ldx + j] += alpha[j] * mul_rn(d, p[i * K + j]) +
+                                  omega[j] * mul_rn(d, si);
+                const T ri = si - omega[j] * t[i * K + j];
+                r[i * K + j] = ri;
+                acc[j] += rr[i * K + j] * ri;
+                acc[K + j] += ri * ri;
+            }
+        }
+    }
+    block_partials<T, 2 * K>(acc, partials, red);
+    if (last_block_done(&ctl->ticket, &last)) {
+        sum_partials<T, 2 * K>(partials, gridDim.x, tot, red);
+        if (threadIdx.x == 0) {
+            ctl->ticket = 0;
+            int all_after_s = 1;
+            for (int j = 0; j < K; ++j) all_after_s &= has_stopped(ctl->status[j]);
+            const int iter = all_after_s ? ctl->iter : ctl->iter + 1;
+            ctl->iter = iter;
+            int all = 1;
+            for (int j = 0; j < K; ++j) {
+                uint8_t st = ctl->status[j];
+                if (has_stopped(st)) {
+                    st |= kFinalizedMask;
+                } else {
+                    sc->prev_rho[j] = sc->rho[j];
+                    sc->rho[j] = tot[j];
+                    sc->tau[j] = sqrt(tot[K + j]);
+                    if (double(sc->tau[j]) <= ctl->reduction * double(sc->start[j])) {
+                        converge_status(st, kResidualId, true);
+                    }
+                    if (iter >= ctl->max_iters) stop_status(st, kIterationId, true);
+                }
+                ctl->status[j] = st;
+                all &= has_stopped(st);
+            }
+            ctl->all_stopped = all;
+        }
+    }
+}
+
+struct BicgLayout {
+    int64_t bytes, off_ctl, off_sc, off_r, off_rr, off_p0, off_p1, off_v0,
+        off_v1, off_s, off_t, off_partials;
+};
+
+template <typename T>
+BicgLayout bicg_layout(int64_t n, int K)
+{
+    Carver c{nullptr};
+    BicgLayout l;
+    l.off_ctl = c.take<SolveCtl>(1);
+    l.off_sc = c.take<BicgScalars<T>>(1);
+    l.off_r = c.take<T>(n * K);
+    l.off_rr = c.take<T>(n * K);
+    l.off_p0 = c.take<T>(n * K);
+    l.off_p1 = c.take<T>(n * K);
+    l.off_v0 = c.take<T>(n * K);
+    l.off_v1 = c.take<T>(n * K);
+    l.off_s = c.take<T>(n * K);
+    l.off_t = c.take<T>(n * K);
+    l.off_partials = c.take<T>(int64_t(kSolverGrid) * 3 * K);
+    l.bytes = c.used;
+    return l;
+}
+
+template <typename T>
+int bicgstab_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
+                   int64_t max_row_nnz, const T* dinv, const T* b, int64_t ldb,
+                   T* x, int64_t ldx, int64_t k, int64_t max_iters,
+                   double reduction, int64_t check_every, void* workspace,
+                   int64_t workspace_bytes, int64_t* iterations,
+                   double* residual_norms, uint8_t* status, void* stream)
+{
+    B2S_CHECK_ARG(n >= 0 && k >= 1 && k <= kMaxRhs, "num_rhs must be 1..16");
+    B2S_CHECK_ARG(ldb >= k && ldx >= k, "leading dimension < num_rhs");
+    B2S_CHECK_ARG(max_iters >= 0 && max_iters < (int64_t(1) << 30),
+                  "max_iters out of range");
+    const int K = rhs_bucket(k);
+    const BicgLayout lay = bicg_layout<T>(n, K);
+    if (workspace_bytes < lay.bytes) {
+        set_error("workspace of %lld bytes < %lld", (long long)workspace_bytes,
+                  (long long)lay.bytes);
+        return B2S_ERR_WORKSPACE;
+    }
+    B2S_CHECK_ARG(workspace != nullptr && b && x && rp, "null pointer");
+    cudaStream_t st = as_stream(stream);
+    char* w = static_cast<char*>(workspace);
+    auto* ctl = reinterpret_cast<SolveCtl*>(w + lay.off_ctl);
+    auto* sc = reinterpret_cast<BicgScalars<T>*>(w + lay.off_sc);
+    T* r = reinterpret_cast<T*>(w + lay.off_r);
+    T* rr = reinterpret_cast<T*>(w + lay.off_rr);
+    T* p[2] = {reinterpret_cast<T*>(w + lay.off_p0), reinterpret_cast<T*>(w + lay.off_p1)};
+    T* vv[2] = {reinterpret_cast<T*>(w + lay.off_v0), reinterpret_cast<T*>(w + lay.off_v1)};
+    T* s = reinterpret_cast<T*>(w + lay.off_s);
+    T* t = reinterpret_cast<T*>(w + lay.off_t);
+    T* partials = reinterpret_cast<T*>(w + lay.off_partials);
+
+    SolveCtl h{};
+    h.max_iters = int(max_iters);
+    h.reduction = reduction;
+    B2S_CUDA_TRY(cudaMemcpyAsync(ctl, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+    const int sw = solver_subwarp(max_row_nnz);
+    const int grid_spmv = int(std::min<int64_t>(
+        std::max<int64_t>(1, ceildiv(n * sw, kSolverBlock)), kSolverGrid));
+    const int grid_vec = int(std::min<int64_t>(
+        std::max<int64_t>(1, ceildiv(n, kSolverBlock)), kSolverGrid));
+    const int chunk = int(std::max<int64_t>(2, (check_every + 1) / 2 * 2));
+    B2S_DISPATCH_RHS(K, {
+        B2S_DISPATCH_SW(sw, {
+            residual_kernel<T, SW, K><<<grid_spmv, kSolverBlock, 0, st>>>(
+                n, rp, ci, v, x, ldx, b, ldb, int(k), r);
+        });
+        B2S_LAUNCH_CHECK();
+        bicg_init_kernel<T, K><<<grid_vec, kSolverBlock, 0, st>>>(
+            n, b, ldb, int(k), r, rr, p[0], vv[0], ctl, sc, partials);
+        B2S_LAUNCH_CHECK();
+    });
+    auto capture = [&](cudaStream_t cs) -> int {
+        for (int it = 0; it < chunk; ++it) {
+            const int o = it % 2, nw = (it + 1) % 2;
+            B2S_DISPATCH_RHS(K, {
+                B2S_DISPATCH_SW(sw, {
+                    bicg_spmv1_kernel<T, SW, K><<<grid_spmv, kSolverBlock, 0, cs>>>(
+                        n, rp, ci, v, dinv, r, rr, p[o], vv[o], p[nw], vv[nw],
+                        ctl, sc, partials);
+                    bicg_spmv2_kernel<T, SW, K><<<grid_spmv, kSolverBlock, 0, cs>>>(
+                        n, rp, ci, v, dinv, r, vv[nw], s, t, ctl, sc, partials);
+                });
+                bicg_update_kernel<T, K><<<grid_vec, kSolverBlock, 0, cs>>>(
+                    n, dinv, x, ldx, r, rr, p[nw], s, t, ctl, sc, partials);
+            });
+            B2S_LAUNCH_CHECK();
+        }
+        return B2S_OK;
+    };
+    int rc = run_graph_loop(st, ctl, int(max_iters), chunk, capture, &h);
+    if (rc != B2S_OK) return rc;
+    BicgScalars<T> hs;
+    B2S_CUDA_TRY(cudaMemcpyAsync(&hs, sc, sizeof(hs), cudaMemcpyDeviceToHost, st));
+    B2S_CUDA_TRY(cudaMemcpyAsync(&h, ctl, sizeof(h), cudaMemcpyDeviceToHost, st));
+    B2S_CUDA_TRY(cudaStreamSynchronize(st));
+    if (iterations) *iterations = h.iter;
+    for (int64_t j = 0; j < k; ++j) {
+        if (residual_norms) residual_norms[j] = double(hs.tau[j]);
+        if (status) status[j] = h.status[j];
+    }
+    return B2S_OK;
+}
+
+}  // namespace
+}  // namespace b2s
+
+using namespace b2s;
+
+extern "C" {
+
+int64_t b2s_bicgstab_workspace_bytes(int64_t num_rows, int64_t num_rhs,
+                                     int value_bytes)
+{
+    const int K = rhs_bucket(num_rhs);
+    if (K < 0 || num_rows < 0) return -1;
+    return value_bytes == 8 ? bicg_layout<double>(num_rows, K).bytes
+                            : bicg_layout<float>(num_rows, K).bytes;
+}
+
+#define B2S_BICG_ENTRY(T, S)                                                  \
+    int b2s_bicgstab_solve_##S(                                               \
+        int64_t num_rows, const int32_t* row_ptrs, const int32_t* col_idxs,   \
+        const T* values, int64_t max_row_nnz, const T* inv_diag, const T* b,  \
+        int64_t ldb, T* x, int64_t ldx, int64_t num_rhs, int64_t max_iters,   \
+        double reduction_factor, int64_t check_every, void* workspace,        \
+        int64_t workspace_bytes, int64_t* iterations, double* residual_norms, \
+        uint8_t* status, void* stream)                                        \
+    {                                                                         \
+        return bicgstab_solve<T>(num_rows, row_ptrs, col_idxs, values,        \
+                                 max_row_nnz, inv_diag, b, ldb, x, ldx,       \
+                                 num_rhs, max_iters, reduction_factor,        \
+                                 check_every, workspace, workspace_bytes,     \
+                                 iterations, residual_norms, status, stream); \
+    }
+
+B2S_BICG_ENTRY(double, f64)
+B2S_BICG_ENTRY(float, f32)
+
+}  // extern "C"

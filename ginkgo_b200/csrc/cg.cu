@@ -118,13 +118,18 @@ __global__ void __launch_bounds__(kSolverBlock)
     for (int j = 0; j < K; ++j) dot[j] = T(0);
     const int lane = threadIdx.x % SW;
     const int64_t nsub = int64_t(gridDim.x) * kSolverBlock / SW;
-    for (int64_t row = (blockIdx.x * int64_t(kSolverBlock) + threadIdx.x) / SW;
-         row < n; row += nsub) {
+    // warp-uniform trip count: all lanes of a warp run every iteration, so
+    // the subwarp shuffles below always see the whole warp
+    for (int64_t wbase = (blockIdx.x * int64_t(kSolverBlock) + threadIdx.x) /
+                         kWarp * (kWarp / SW);
+         wbase < n; wbase += nsub) {
+        const int64_t row = wbase + (threadIdx.x % kWarp) / SW;
+        const bool valid = row < n;
         T acc[K];
 #pragma unroll
         for (int j = 0; j < K; ++j) acc[j] = T(0);
-        const int end = rp[row + 1];
-        for (int e = rp[row] + lane; e < end; e += SW) {
+        const int end = valid ? rp[row + 1] : 0;
+        for (int e = (valid ? rp[row] : end) + lane; e < end; e += SW) {
             const T a = v[e];
             const int64_t c = ci[e];
             const T d = dinv ? dinv[c] : T(1);
@@ -138,7 +143,7 @@ __global__ void __launch_bounds__(kSolverBlock)
         }
 #pragma unroll
         for (int j = 0; j < K; ++j) acc[j] = subwarp_sum<SW>(acc[j]);
-        if (lane == 0) {
+        if (valid && lane == 0) {
             const T d = dinv ? dinv[row] : T(1);
 #pragma unroll
             for (int j = 0; j < K; ++j) {
@@ -236,13 +241,13 @@ CgLayout cg_layout(int64_t n, int K)
 {
     Carver c{nullptr};
     CgLayout l;
-    l.off_ctl = reinterpret_cast<int64_t>(c.take<SolveCtl>(1));
-    l.off_sc = reinterpret_cast<int64_t>(c.take<CgScalars<T>>(1));
-    l.off_r = reinterpret_cast<int64_t>(c.take<T>(n * K));
-    l.off_p0 = reinterpret_cast<int64_t>(c.take<T>(n * K));
-    l.off_p1 = reinterpret_cast<int64_t>(c.take<T>(n * K));
-    l.off_q = reinterpret_cast<int64_t>(c.take<T>(n * K));
-    l.off_partials = reinterpret_cast<int64_t>(c.take<T>(int64_t(kSolverGrid) * 3 * K));
+    l.off_ctl = c.take<SolveCtl>(1);
+    l.off_sc = c.take<CgScalars<T>>(1);
+    l.off_r = c.take<T>(n * K);
+    l.off_p0 = c.take<T>(n * K);
+    l.off_p1 = c.take<T>(n * K);
+    l.off_q = c.take<T>(n * K);
+    l.off_partials = c.take<T>(int64_t(kSolverGrid) * 3 * K);
     l.bytes = c.used;
     return l;
 }

@@ -98,17 +98,22 @@ __global__ void __launch_bounds__(kSolverBlock)
     TB* vj = V + int64_t(j) * n;
     const int lane = threadIdx.x % SW;
     const int64_t nsub = int64_t(gridDim.x) * kSolverBlock / SW;
-    for (int64_t row = (blockIdx.x * int64_t(kSolverBlock) + threadIdx.x) / SW;
-         row < n; row += nsub) {
+    // warp-uniform trip count: all lanes of a warp run every iteration, so
+    // the subwarp shuffles below always see the whole warp
+    for (int64_t wbase = (blockIdx.x * int64_t(kSolverBlock) + threadIdx.x) /
+                         kWarp * (kWarp / SW);
+         wbase < n; wbase += nsub) {
+        const int64_t row = wbase + (threadIdx.x % kWarp) / SW;
+        const bool valid = row < n;
         TA acc = TA(0);
-        const int end = rp[row + 1];
-        for (int e = rp[row] + lane; e < end; e += SW) {
+        const int end = valid ? rp[row + 1] : 0;
+        for (int e = (valid ? rp[row] : end) + lane; e < end; e += SW) {
             const int64_t c = ci[e];
             const TA d = dinv ? dinv[c] : TA(1);
             acc += v[e] * mul_rn(d, basis_value<TA, TB>(j, c, r64, w_src, scale));
         }
         acc = subwarp_sum<SW>(acc);
-        if (lane == 0) {
+        if (valid && lane == 0) {
             vj[row] = to_basis<TB>(basis_value<TA, TB>(j, row, r64, w_src, scale));
             w_dst[row] = acc;
         }
@@ -320,13 +325,18 @@ __global__ void __launch_bounds__(kSolverBlock)
     const int lane = threadIdx.x % SW;
     const int64_t nsub = int64_t(gridDim.x) * kSolverBlock / SW;
     double acc2[2] = {0.0, 0.0};
-    for (int64_t row = (blockIdx.x * int64_t(kSolverBlock) + threadIdx.x) / SW;
-         row < n; row += nsub) {
+    // warp-uniform trip count: all lanes of a warp run every iteration, so
+    // the subwarp shuffles below always see the whole warp
+    for (int64_t wbase = (blockIdx.x * int64_t(kSolverBlock) + threadIdx.x) /
+                         kWarp * (kWarp / SW);
+         wbase < n; wbase += nsub) {
+        const int64_t row = wbase + (threadIdx.x % kWarp) / SW;
+        const bool valid = row < n;
         double acc = 0.0;
-        const int end = rp[row + 1];
-        for (int e = rp[row] + lane; e < end; e += SW) acc += v[e] * x[ci[e]];
+        const int end = valid ? rp[row + 1] : 0;
+        for (int e = (valid ? rp[row] : end) + lane; e < end; e += SW) acc += v[e] * x[ci[e]];
         acc = subwarp_sum<SW>(acc);
-        if (lane == 0) {
+        if (valid && lane == 0) {
             const double bb = b[row];
             const double rr = bb - acc;
             r[row] = rr;
@@ -379,15 +389,14 @@ GmresLayout gmres_layout(int64_t n, int64_t nnz, int d, bool mixed)
 {
     Carver c{nullptr};
     GmresLayout l;
-    l.off_st = reinterpret_cast<int64_t>(c.take<GmresState>(1));
-    l.off_r = reinterpret_cast<int64_t>(c.take<double>(n));
-    l.off_w0 = reinterpret_cast<int64_t>(c.take<TA>(n));
-    l.off_w1 = reinterpret_cast<int64_t>(c.take<TA>(n));
-    l.off_v = reinterpret_cast<int64_t>(c.take<TB>((int64_t(d) + 1) * n));
-    l.off_partials = reinterpret_cast<int64_t>(
-        c.take<double>(int64_t(kSolverGrid) * (kMaxKrylov + 1)));
-    l.off_a32 = mixed ? reinterpret_cast<int64_t>(c.take<float>(nnz)) : 0;
-    l.off_d32 = mixed ? reinterpret_cast<int64_t>(c.take<float>(n)) : 0;
+    l.off_st = c.take<GmresState>(1);
+    l.off_r = c.take<double>(n);
+    l.off_w0 = c.take<TA>(n);
+    l.off_w1 = c.take<TA>(n);
+    l.off_v = c.take<TB>((int64_t(d) + 1) * n);
+    l.off_partials = c.take<double>(int64_t(kSolverGrid) * (kMaxKrylov + 1));
+    l.off_a32 = mixed ? c.take<float>(nnz) : 0;
+    l.off_d32 = mixed ? c.take<float>(n) : 0;
     l.bytes = c.used;
     return l;
 }

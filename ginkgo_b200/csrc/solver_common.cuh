@@ -154,13 +154,18 @@ __global__ void __launch_bounds__(kSolverBlock)
 {
     const int lane = threadIdx.x % SW;
     const int64_t nsub = int64_t(gridDim.x) * kSolverBlock / SW;
-    for (int64_t row = (blockIdx.x * int64_t(kSolverBlock) + threadIdx.x) / SW;
-         row < n; row += nsub) {
+    // warp-uniform trip count: all lanes of a warp run every iteration, so
+    // the subwarp shuffles below always see the whole warp
+    for (int64_t wbase = (blockIdx.x * int64_t(kSolverBlock) + threadIdx.x) /
+                         kWarp * (kWarp / SW);
+         wbase < n; wbase += nsub) {
+        const int64_t row = wbase + (threadIdx.x % kWarp) / SW;
+        const bool valid = row < n;
         T acc[K];
 #pragma unroll
         for (int j = 0; j < K; ++j) acc[j] = T(0);
-        const int end = rp[row + 1];
-        for (int e = rp[row] + lane; e < end; e += SW) {
+        const int end = valid ? rp[row + 1] : 0;
+        for (int e = (valid ? rp[row] : end) + lane; e < end; e += SW) {
             const T a = v[e];
             const int64_t c = ci[e];
 #pragma unroll
@@ -170,7 +175,7 @@ __global__ void __launch_bounds__(kSolverBlock)
         }
 #pragma unroll
         for (int j = 0; j < K; ++j) acc[j] = subwarp_sum<SW>(acc[j]);
-        if (lane == 0) {
+        if (valid && lane == 0) {
 #pragma unroll
             for (int j = 0; j < K; ++j) {
                 r[row * K + j] = j < k ? b[row * ldb + j] - acc[j] : T(0);
@@ -216,15 +221,16 @@ inline int rhs_bucket(int64_t k)
 // Workspace carving: 256-byte aligned bump allocation inside the caller's
 // buffer (the library itself never allocates device memory).
 struct Carver {
-    char* base;
+    char* base;  // unused: layouts only record byte offsets
     int64_t used = 0;
+    // byte offset of a new 256-byte aligned block of count T
     template <typename T>
-    T* take(int64_t count)
+    int64_t take(int64_t count)
     {
         used = (used + 255) / 256 * 256;
-        T* p = reinterpret_cast<T*>(base ? base + used : nullptr);
+        const int64_t off = used;
         used += count * int64_t(sizeof(T));
-        return p;
+        return off;
     }
 };
 

@@ -92,11 +92,15 @@ __global__ void csr_tile_rows_kernel(int64_t n, const int32_t* __restrict__ rp,
     tile_rows[t] = int32_t(t == num_tiles ? n : lo);
 }
 
+// One pad word per 16: thread t scans the 8-byte words [8t, 8t + 8), which
+// would otherwise fall into the same banks every other thread.
+__device__ __forceinline__ int lb_pad(int w) { return w + (w >> 4); }
+
 template <typename T, int K>
 struct LbSmem {
     static constexpr int kIpt = K >= 8 ? 1 : 8 / K;  // entries per thread
     static constexpr int kChunk = kBlock * kIpt;
-    T prod[kChunk * K];
+    T prod[kChunk * K + kChunk * K / 16 + 1];
     unsigned char head[kChunk];
     int32_t rows[kTileItems + 1];  // rp[r0 .. r1]
     T carry[K];
@@ -147,7 +151,7 @@ __global__ void __launch_bounds__(kBlock)
                 T xr[K];
                 RowLoad<T, K, VEC>::load(b + col * ldb, xr);
 #pragma unroll
-                for (int j = 0; j < K; ++j) sm.prod[i * K + j] = val * xr[j];
+                for (int j = 0; j < K; ++j) sm.prod[lb_pad(i * K + j)] = val * xr[j];
             }
         }
         __syncthreads();
@@ -175,8 +179,8 @@ __global__ void __launch_bounds__(kBlock)
                 }
 #pragma unroll
                 for (int j = 0; j < K; ++j) {
-                    run[j] += sm.prod[i * K + j];
-                    sm.prod[i * K + j] = run[j];
+                    run[j] += sm.prod[lb_pad(i * K + j)];
+                    sm.prod[lb_pad(i * K + j)] = run[j];
                 }
             }
         }
@@ -242,7 +246,7 @@ __global__ void __launch_bounds__(kBlock)
             if (i < cnt) {
                 if (sm.head[i]) break;
 #pragma unroll
-                for (int j = 0; j < K; ++j) sm.prod[i * K + j] += ex[j];
+                for (int j = 0; j < K; ++j) sm.prod[lb_pad(i * K + j)] += ex[j];
             }
         }
         __syncthreads();
@@ -254,7 +258,7 @@ __global__ void __launch_bounds__(kBlock)
                 T* dst = c + int64_t(r0 + i) * ldc;
 #pragma unroll
                 for (int j = 0; j < K; ++j) {
-                    T val = sm.prod[(e - 1 - cs) * K + j];
+                    T val = sm.prod[lb_pad((e - 1 - cs) * K + j)];
                     if (s < cs) val += sm.carry[j];
                     dst[j] = combine(val, alpha, beta, dst + j);
                 }
@@ -274,7 +278,7 @@ __global__ void __launch_bounds__(kBlock)
                     hi = mid;
                 }
             }
-            const T part = sm.prod[(cnt - 1) * K + tid];
+            const T part = sm.prod[lb_pad((cnt - 1) * K + tid)];
             sm.carry[tid] = sm.rows[lo] < cs ? sm.carry[tid] + part : part;
         }
         __syncthreads();
@@ -316,9 +320,10 @@ __global__ void __launch_bounds__(kBlock)
     for (int j = 0; j < K; ++j) dst[j] = combine(acc[j], alpha, beta, dst + j);
 }
 
+// Row count fits in int32 (the index type); slice arithmetic in 32 bits.
 template <typename T, int K, bool VEC>
 __global__ void __launch_bounds__(kBlock)
-    sellp_kernel(int64_t n, int64_t slice_size,
+    sellp_kernel(int n, int slice_size,
                  const uint64_t* __restrict__ slice_sets,
                  const uint64_t* __restrict__ slice_lengths,
                  const int32_t* __restrict__ ci, const T* __restrict__ v,
@@ -326,19 +331,38 @@ __global__ void __launch_bounds__(kBlock)
                  int64_t ldc, const T* __restrict__ alpha,
                  const T* __restrict__ beta)
 {
-    const int64_t row = blockIdx.x * int64_t(kBlock) + threadIdx.x;
+    const int row = blockIdx.x * kBlock + threadIdx.x;
     if (row >= n) return;
-    const int64_t slice = row / slice_size;
-    const int64_t local = row - slice * slice_size;
-    const int64_t len = int64_t(__ldg(slice_lengths + slice));
-    int64_t idx = int64_t(__ldg(slice_sets + slice)) * slice_size + local;
+    const unsigned slice = unsigned(row) / unsigned(slice_size);
+    const unsigned local = unsigned(row) - slice * unsigned(slice_size);
+    const int len = int(__ldg(slice_lengths + slice));
+    const T* vp = v + int64_t(__ldg(slice_sets + slice)) * slice_size + local;
+    const int32_t* cp = ci + (vp - v);
     T acc[K];
 #pragma unroll
     for (int j = 0; j < K; ++j) acc[j] = T(0);
-#pragma unroll 4
-    for (int64_t i = 0; i < len; ++i, idx += slice_size) {
-        const int32_t col = ld_stream(ci + idx);
-        const T val = ld_stream(v + idx);
+    int i = 0;
+    for (; i + 4 <= len; i += 4) {
+        int32_t col[4];
+        T val[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            col[u] = ld_stream(cp + (i + u) * slice_size);
+            val[u] = ld_stream(vp + (i + u) * slice_size);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (col[u] != -1) {
+                T xr[K];
+                RowLoad<T, K, VEC>::load(b + int64_t(col[u]) * ldb, xr);
+#pragma unroll
+                for (int j = 0; j < K; ++j) acc[j] += val[u] * xr[j];
+            }
+        }
+    }
+    for (; i < len; ++i) {
+        const int32_t col = ld_stream(cp + i * slice_size);
+        const T val = ld_stream(vp + i * slice_size);
         if (col != -1) {
             T xr[K];
             RowLoad<T, K, VEC>::load(b + int64_t(col) * ldb, xr);
@@ -346,9 +370,206 @@ __global__ void __launch_bounds__(kBlock)
             for (int j = 0; j < K; ++j) acc[j] += val * xr[j];
         }
     }
-    T* dst = c + row * ldc;
+    T* dst = c + int64_t(row) * ldc;
 #pragma unroll
     for (int j = 0; j < K; ++j) dst[j] = combine(acc[j], alpha, beta, dst + j);
+}
+
+// ---------------------------------------------------------------------------
+// Csr, one and two right-hand sides: each warp owns 32 consecutive rows and
+// streams their entries [rp[r0], rp[r0 + 32]) with fully coalesced loads into
+// shared memory as products val * b(col, :); every lane then sums its own row
+// in order, so a row is reduced exactly as the reference's sequential loop
+// does (reference/matrix/csr_kernels.cpp:65-74).  A group with more than CAP
+// entries (long rows) is reduced row by row by the whole warp.
+// ---------------------------------------------------------------------------
+template <typename T, int K, bool VEC>
+__global__ void __launch_bounds__(kBlock)
+    csr_stream_kernel(int64_t n, const int32_t* __restrict__ rp,
+                      const int32_t* __restrict__ ci, const T* __restrict__ v,
+                      const T* __restrict__ b, int64_t ldb, T* __restrict__ c,
+                      int64_t ldc, const T* __restrict__ alpha,
+                      const T* __restrict__ beta)
+{
+    constexpr int CAP = 256 / K;   // staged entries per warp
+    constexpr int PER = CAP / kWarp;
+    constexpr unsigned kFull = 0xffffffffu;
+    __shared__ T prod[kBlock / kWarp][CAP * K];
+    const int lane = threadIdx.x % kWarp, wid = threadIdx.x / kWarp;
+    const int64_t row0 = (blockIdx.x * int64_t(kBlock)) + wid * kWarp;
+    const int64_t row = row0 + lane;
+    const int rs = __ldg(rp + (row < n ? row : n));
+    int re = __shfl_down_sync(kFull, rs, 1);
+    if (lane == kWarp - 1) re = __ldg(rp + (row0 + kWarp < n ? row0 + kWarp : n));
+    const int start = __shfl_sync(kFull, rs, 0);
+    const int cnt = __shfl_sync(kFull, re, kWarp - 1) - start;
+    T acc[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) acc[j] = T(0);
+    if (cnt <= CAP) {
+        T* pw = prod[wid];
+        T vals[PER];
+        int32_t cols[PER];
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            const int i = lane + q * kWarp;
+            if (i < cnt) {
+                vals[q] = ld_stream(v + start + i);
+                cols[q] = ld_stream(ci + start + i);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            const int i = lane + q * kWarp;
+            if (i < cnt) {
+                T xr[K];
+                RowLoad<T, K, VEC>::load(b + int64_t(cols[q]) * ldb, xr);
+#pragma unroll
+                for (int j = 0; j < K; ++j) pw[i * K + j] = vals[q] * xr[j];
+            }
+        }
+        __syncwarp();
+        for (int i = rs - start; i < re - start; ++i) {
+#pragma unroll
+            for (int j = 0; j < K; ++j) acc[j] += pw[i * K + j];
+        }
+    } else {
+        for (int l = 0; l < kWarp; ++l) {
+            const int s = __shfl_sync(kFull, rs, l), e = __shfl_sync(kFull, re, l);
+            T a[K];
+#pragma unroll
+            for (int j = 0; j < K; ++j) a[j] = T(0);
+            for (int ee = s + lane; ee < e; ee += kWarp) {
+                const T val = ld_stream(v + ee);
+                T xr[K];
+                RowLoad<T, K, VEC>::load(b + int64_t(ld_stream(ci + ee)) * ldb, xr);
+#pragma unroll
+                for (int j = 0; j < K; ++j) a[j] += val * xr[j];
+            }
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                a[j] = warp_sum(a[j]);
+                if (lane == l) acc[j] = a[j];
+            }
+        }
+    }
+    if (row < n) {
+        T* dst = c + row * ldc;
+#pragma unroll
+        for (int j = 0; j < K; ++j) dst[j] = combine(acc[j], alpha, beta, dst + j);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Four or more right-hand sides: KL = K / VW lanes share one row and each
+// owns VW consecutive columns (one 16-byte vector), so the lanes of a row
+// read one contiguous stretch of b(col, :) and write one of c(row, :); the
+// row's values and column indices are broadcast loads.  Used for Csr, Ell
+// and Sellp; needs 16-byte aligned b/c rows.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<double> {
+    using type = double2;
+    static constexpr int width = 2;
+};
+template <>
+struct Vec16<float> {
+    using type = float4;
+    static constexpr int width = 4;
+};
+
+template <typename T>
+__device__ __forceinline__ void fma_vec(typename Vec16<T>::type& acc, T a,
+                                        const T* p)
+{
+    const auto x = __ldg(reinterpret_cast<const typename Vec16<T>::type*>(p));
+    if constexpr (Vec16<T>::width == 2) {
+        acc.x += a * x.x;
+        acc.y += a * x.y;
+    } else {
+        acc.x += a * x.x;
+        acc.y += a * x.y;
+        acc.z += a * x.z;
+        acc.w += a * x.w;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void store_vec(T* dst, const typename Vec16<T>::type& acc,
+                                          const T* alpha, const T* beta)
+{
+    constexpr int W = Vec16<T>::width;
+    const T* a = reinterpret_cast<const T*>(&acc);
+    T out[W];
+#pragma unroll
+    for (int u = 0; u < W; ++u) out[u] = combine(a[u], alpha, beta, dst + u);
+    *reinterpret_cast<typename Vec16<T>::type*>(dst) =
+        *reinterpret_cast<const typename Vec16<T>::type*>(out);
+}
+
+// FMT 0: Csr, 1: Ell, 2: Sellp
+template <typename T, int K, int FMT>
+__global__ void __launch_bounds__(kBlock)
+    rhs_lanes_kernel(int64_t n, const int32_t* __restrict__ rp,
+                     int64_t width_or_slice, int64_t stride,
+                     const uint64_t* __restrict__ slice_sets,
+                     const uint64_t* __restrict__ slice_lengths,
+                     const int32_t* __restrict__ ci, const T* __restrict__ v,
+                     const T* __restrict__ b, int64_t ldb, T* __restrict__ c,
+                     int64_t ldc, const T* __restrict__ alpha,
+                     const T* __restrict__ beta)
+{
+    using V = typename Vec16<T>::type;
+    constexpr int VW = Vec16<T>::width;
+    constexpr int KL = K / VW;
+    const int64_t g = blockIdx.x * int64_t(kBlock) + threadIdx.x;
+    const int64_t row = g / KL;
+    if (row >= n) return;
+    const int sub = int(g % KL);
+    const T* bc = b + sub * VW;
+    V acc;
+    {
+        T* a = reinterpret_cast<T*>(&acc);
+#pragma unroll
+        for (int u = 0; u < VW; ++u) a[u] = T(0);
+    }
+    int64_t first, step, len;
+    if constexpr (FMT == 0) {
+        first = rp[row];
+        len = rp[row + 1] - first;
+        step = 1;
+    } else if constexpr (FMT == 1) {
+        first = row;
+        len = width_or_slice;
+        step = stride;
+    } else {
+        const int64_t s = row / width_or_slice;
+        first = int64_t(slice_sets[s]) * width_or_slice + (row - s * width_or_slice);
+        len = int64_t(slice_lengths[s]);
+        step = width_or_slice;
+    }
+    int64_t i = 0;
+    for (; i + 4 <= len; i += 4) {
+        int32_t col[4];
+        T val[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            col[u] = __ldg(ci + first + (i + u) * step);
+            val[u] = __ldg(v + first + (i + u) * step);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (FMT == 0 || col[u] != -1) fma_vec<T>(acc, val[u], bc + int64_t(col[u]) * ldb);
+        }
+    }
+    for (; i < len; ++i) {
+        const int32_t col = __ldg(ci + first + i * step);
+        const T val = __ldg(v + first + i * step);
+        if (FMT == 0 || col != -1) fma_vec<T>(acc, val, bc + int64_t(col) * ldb);
+    }
+    store_vec<T>(c + row * ldc + sub * VW, acc, alpha, beta);
 }
 
 // ---------------------------------------------------------------------------
@@ -371,6 +592,29 @@ bool vec_ok(const T* b, int64_t ldb, int64_t col0, int kk)
     const size_t bytes = sizeof(T);
     return (reinterpret_cast<uintptr_t>(b + col0) % 16 == 0) &&
            ((ldb * bytes) % 16 == 0);
+}
+
+// 16-byte vector path for >= 4 right-hand sides: both b and c rows aligned
+template <typename T>
+bool lanes_ok(const T* b, int64_t ldb, const T* c, int64_t ldc, int64_t col0,
+              int kk)
+{
+    return kk >= 4 && kk % Vec16<T>::width == 0 && vec_ok(b, ldb, col0, kk) &&
+           vec_ok(static_cast<const T*>(c), ldc, col0, kk);
+}
+
+template <typename T, int K, int FMT>
+void launch_lanes(int64_t n, const int32_t* rp, int64_t w_or_s, int64_t stride,
+                  const uint64_t* sets, const uint64_t* lens, const int32_t* ci,
+                  const T* v, const T* b, int64_t ldb, T* c, int64_t ldc,
+                  const T* alpha, const T* beta, cudaStream_t st)
+{
+    if constexpr (K >= 4 && K % Vec16<T>::width == 0) {
+        constexpr int KL = K / Vec16<T>::width;
+        rhs_lanes_kernel<T, K, FMT><<<ceildiv(n * KL, kBlock), kBlock, 0, st>>>(
+            n, rp, w_or_s, stride, sets, lens, ci, v, b, ldb, c, ldc, alpha,
+            beta);
+    }
 }
 
 #define B2S_DISPATCH_K(kk, VEC, ...)                   \
@@ -448,6 +692,23 @@ int csr_spmv(int strategy, int64_t n, int64_t num_cols, const int32_t* rp,
                         tile_rows, rp, ci, v, bb, ldb, cc, ldc, alpha, beta);
                 }
             });
+        } else if (lanes_ok(b, ldb, c, ldc, col0, kk)) {
+            B2S_DISPATCH_K(kk, VEC, {
+                launch_lanes<T, K, 0>(n, rp, 0, 0, nullptr, nullptr, ci, v, bb,
+                                      ldb, cc, ldc, alpha, beta, st);
+            });
+        } else if (kk <= 2) {
+            const int64_t grid = ceildiv(n, kBlock);
+            if (kk == 2 && vec) {
+                csr_stream_kernel<T, 2, true><<<grid, kBlock, 0, st>>>(
+                    n, rp, ci, v, bb, ldb, cc, ldc, alpha, beta);
+            } else if (kk == 2) {
+                csr_stream_kernel<T, 2, false><<<grid, kBlock, 0, st>>>(
+                    n, rp, ci, v, bb, ldb, cc, ldc, alpha, beta);
+            } else {
+                csr_stream_kernel<T, 1, false><<<grid, kBlock, 0, st>>>(
+                    n, rp, ci, v, bb, ldb, cc, ldc, alpha, beta);
+            }
         } else {
             B2S_DISPATCH_K(kk, VEC, {
                 if (vec) {
@@ -483,6 +744,16 @@ int ell_spmv(int64_t n, int64_t num_cols, int64_t width, int64_t stride,
     for (int64_t col0 = 0; col0 < k;) {
         const int kk = rhs_chunk(k - col0);
         const bool vec = vec_ok(b, ldb, col0, kk);
+        if (lanes_ok(b, ldb, c, ldc, col0, kk)) {
+            B2S_DISPATCH_K(kk, VEC, {
+                launch_lanes<T, K, 1>(n, nullptr, width, stride, nullptr,
+                                      nullptr, ci, v, b + col0, ldb, c + col0,
+                                      ldc, alpha, beta, st);
+            });
+            B2S_LAUNCH_CHECK();
+            col0 += kk;
+            continue;
+        }
         B2S_DISPATCH_K(kk, VEC, {
             if (vec) {
                 ell_kernel<T, K, true><<<grid, kBlock, 0, st>>>(
@@ -508,7 +779,9 @@ int sellp_spmv(int64_t n, int64_t num_cols, int64_t slice_size,
                void* stream)
 {
     B2S_CHECK_ARG(n >= 0 && k >= 0, "negative size");
-    B2S_CHECK_ARG(slice_size >= 1, "slice_size must be >= 1");
+    B2S_CHECK_ARG(slice_size >= 1 && slice_size <= (1 << 20),
+                  "slice_size must be in 1..2^20");
+    B2S_CHECK_ARG(n < (int64_t(1) << 31), "row count exceeds int32");
     B2S_CHECK_ARG((alpha == nullptr) == (beta == nullptr),
                   "alpha and beta must both be given or both be null");
     B2S_CHECK_ARG(k == 0 || (ldb >= k && ldc >= k), "leading dimension < k");
@@ -518,14 +791,24 @@ int sellp_spmv(int64_t n, int64_t num_cols, int64_t slice_size,
     for (int64_t col0 = 0; col0 < k;) {
         const int kk = rhs_chunk(k - col0);
         const bool vec = vec_ok(b, ldb, col0, kk);
+        if (lanes_ok(b, ldb, c, ldc, col0, kk)) {
+            B2S_DISPATCH_K(kk, VEC, {
+                launch_lanes<T, K, 2>(n, nullptr, slice_size, 0, slice_sets,
+                                      slice_lengths, ci, v, b + col0, ldb,
+                                      c + col0, ldc, alpha, beta, st);
+            });
+            B2S_LAUNCH_CHECK();
+            col0 += kk;
+            continue;
+        }
         B2S_DISPATCH_K(kk, VEC, {
             if (vec) {
                 sellp_kernel<T, K, true><<<grid, kBlock, 0, st>>>(
-                    n, slice_size, slice_sets, slice_lengths, ci, v, b + col0,
+                    int(n), int(slice_size), slice_sets, slice_lengths, ci, v, b + col0,
                     ldb, c + col0, ldc, alpha, beta);
             } else {
                 sellp_kernel<T, K, false><<<grid, kBlock, 0, st>>>(
-                    n, slice_size, slice_sets, slice_lengths, ci, v, b + col0,
+                    int(n), int(slice_size), slice_sets, slice_lengths, ci, v, b + col0,
                     ldb, c + col0, ldc, alpha, beta);
             }
         });

@@ -1,0 +1,299 @@
+"""Solver factories over the fused C-ABI solvers, named after the
+reference's ``gko::solver`` / ``gko::stop`` / ``gko::preconditioner`` API:
+
+    solver = (Cg.build()
+              .with_criteria(Iteration.build().with_max_iters(1000),
+                             ResidualNorm.build().with_reduction_factor(1e-10))
+              .with_preconditioner(Jacobi.build().with_max_block_size(1))
+              .on(exec)
+              .generate(A))
+    solver.apply(b, x)                # x holds the initial guess
+    solver.logger.num_iterations      # like gko::log::Convergence
+
+Only scalar Jacobi (max_block_size 1) or no preconditioner is supported on
+this path; stopping is Iteration + ResidualNorm with the rhs_norm baseline
+(the defaults of include/ginkgo/core/stop/residual_norm.hpp).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from ._lib import GinkgoError, call, lib
+from .matrix import Csr, _check_dense, _p, _stream
+
+_SFX = {torch.float64: "f64", torch.float32: "f32"}
+
+
+# --------------------------------------------------------------- criteria --
+class _Builder:
+    """Generic ``X.build().with_a(v).with_b(w)`` parameter builder."""
+
+    def __init__(self, cls, **defaults):
+        self._cls = cls
+        self._params = dict(defaults)
+
+    def __getattr__(self, name):
+        if name.startswith("with_"):
+            key = name[5:]
+
+            def setter(*args):
+                self._params[key] = args[0] if len(args) == 1 else args
+                return self
+            return setter
+        raise AttributeError(name)
+
+    def on(self, exec_):
+        return self._cls(exec_, **self._params)
+
+    def params(self):
+        return dict(self._params)
+
+
+class Iteration:
+    """stop::Iteration (core/stop/iteration.cpp:14-24)."""
+
+    @staticmethod
+    def build():
+        return _Builder(Iteration, max_iters=0)
+
+    def __init__(self, exec_=None, max_iters=0):
+        self.max_iters = int(max_iters)
+
+
+class ResidualNorm:
+    """stop::ResidualNorm with the rhs_norm baseline
+    (core/stop/residual_norm.cpp:95-230): ||r|| <= reduction_factor ||b||."""
+
+    @staticmethod
+    def build():
+        return _Builder(ResidualNorm, reduction_factor=1e-15, baseline="rhs_norm")
+
+    def __init__(self, exec_=None, reduction_factor=1e-15, baseline="rhs_norm"):
+        if baseline != "rhs_norm":
+            raise NotImplementedError("only the rhs_norm baseline is on this path")
+        self.reduction_factor = float(reduction_factor)
+
+
+def _criteria(crits):
+    max_iters, red = None, None
+    for c in crits:
+        if isinstance(c, _Builder):
+            c = c.on(None)
+        if isinstance(c, Iteration):
+            max_iters = c.max_iters if max_iters is None else min(max_iters, c.max_iters)
+        elif isinstance(c, ResidualNorm):
+            red = c.reduction_factor
+        else:
+            raise TypeError(f"unsupported criterion {c!r}")
+    if max_iters is None:
+        raise ValueError("an Iteration criterion is required")
+    return max_iters, (0.0 if red is None else red)
+
+
+# ---------------------------------------------------------- preconditioner --
+class Jacobi:
+    """Scalar Jacobi (preconditioner::Jacobi with max_block_size 1,
+    core/preconditioner/jacobi.cpp:149-196, 337-369)."""
+
+    @staticmethod
+    def build():
+        return _Builder(JacobiFactory, max_block_size=32)
+
+    def __init__(self, A: Csr):
+        self.A = A
+        self.inv_diag = torch.empty(A.shape[0], dtype=A.dtype, device=A.values.device)
+        call(f"b2s_jacobi_invert_diagonal_{_SFX[A.dtype]}", A.shape[0],
+             _p(A.row_ptrs), _p(A.col_idxs), _p(A.values), _p(self.inv_diag),
+             _stream(self.inv_diag))
+
+    def apply(self, b, x):
+        b2 = _check_dense(b, self.A.shape[0], self.A.dtype, "b")
+        x2 = _check_dense(x, self.A.shape[0], self.A.dtype, "x")
+        call(f"b2s_jacobi_apply_{_SFX[self.A.dtype]}", b2.shape[0], b2.shape[1],
+             _p(self.inv_diag), _p(b2), b2.stride(0), _p(x2), x2.stride(0),
+             None, None, _stream(x2))
+        return x
+
+
+class JacobiFactory:
+    def __init__(self, exec_, max_block_size=32):
+        if int(max_block_size) != 1:
+            raise NotImplementedError(
+                "this path provides scalar Jacobi only: use with_max_block_size(1)")
+
+    def generate(self, A):
+        return Jacobi(A)
+
+
+# ---------------------------------------------------------------- logging --
+@dataclass
+class ConvergenceLog:
+    """What gko::log::Convergence records for one apply."""
+    num_iterations: int = 0
+    residual_norm: list = field(default_factory=list)
+    has_converged: bool = False
+    status: list = field(default_factory=list)
+    restarts: int = 0
+
+
+# ----------------------------------------------------------------- solvers --
+class _SolverFactory:
+    kind = ""
+
+    def __init__(self, exec_, criteria=(), preconditioner=None, krylov_dim=100,
+                 check_every=8, storage_precision=None, inner_reduction=1e-6):
+        self.exec = exec_
+        crit = criteria if isinstance(criteria, (list, tuple)) else (criteria,)
+        self.max_iters, self.reduction = _criteria(crit)
+        self.preconditioner = preconditioner
+        # the device Hessenberg holds at most 32 columns
+        self.krylov_dim = min(int(krylov_dim), 32)
+        self.check_every = int(check_every)
+        self.storage_precision = storage_precision
+        self.inner_reduction = float(inner_reduction)
+
+    def generate(self, A: Csr):
+        return _Solver(self, A)
+
+
+class _Solver:
+    def __init__(self, factory, A):
+        self.f = factory
+        self.A = A
+        self.logger = ConvergenceLog()
+        prec = factory.preconditioner
+        if isinstance(prec, _Builder):
+            prec = prec.on(factory.exec)
+        self.precond = prec.generate(A) if prec is not None else None
+        self._ws = None
+
+    def _workspace(self, nbytes):
+        if nbytes < 0:
+            raise GinkgoError("workspace", -1, "unsupported size")
+        if self._ws is None or self._ws.numel() < nbytes:
+            self._ws = torch.empty(max(nbytes, 256), dtype=torch.uint8,
+                                   device=self.A.values.device)
+        return self._ws
+
+    @property
+    def inv_diag(self):
+        return None if self.precond is None else self.precond.inv_diag
+
+    def apply(self, b, x):
+        kind = self.f.kind
+        if kind in ("cg", "bicgstab"):
+            return self._apply_cg(b, x)
+        if kind in ("gmres", "ir"):
+            return self._apply_gmres(b, x)
+        raise NotImplementedError(kind)
+
+    def _apply_cg(self, b, x):
+        A = self.A
+        n = A.shape[0]
+        b2 = _check_dense(b, n, A.dtype, "b")
+        x2 = _check_dense(x, n, A.dtype, "x")
+        k = b2.shape[1]
+        name = self.f.kind
+        nbytes = getattr(lib(), f"b2s_{name}_workspace_bytes")(
+            n, k, A.values.element_size())
+        ws = self._workspace(nbytes)
+        it = C.c_int64(0)
+        res = np.zeros(k, np.float64)
+        st = np.zeros(k, np.uint8)
+        call(f"b2s_{name}_solve_{_SFX[A.dtype]}", n, _p(A.row_ptrs), _p(A.col_idxs),
+             _p(A.values), A.max_row_nnz, _p(self.inv_diag), _p(b2), b2.stride(0),
+             _p(x2), x2.stride(0), k, self.f.max_iters, self.f.reduction,
+             self.f.check_every, _p(ws), ws.numel(), C.byref(it),
+             res.ctypes.data_as(C.c_void_p), st.ctypes.data_as(C.c_void_p),
+             _stream(x2))
+        self.logger = ConvergenceLog(int(it.value), res.tolist(),
+                                     bool(np.all(st & 0x80)), st.tolist())
+        return x
+
+    def _apply_gmres(self, b, x):
+        A = self.A
+        if A.dtype != torch.float64:
+            raise TypeError("GMRES on this path takes the FP64 matrix; the "
+                            "low-precision inner solve converts it itself")
+        n = A.shape[0]
+        b2 = _check_dense(b, n, A.dtype, "b")
+        x2 = _check_dense(x, n, A.dtype, "x")
+        if b2.shape[1] != 1 or not x2.is_contiguous() or not b2.is_contiguous():
+            raise NotImplementedError("GMRES here takes one contiguous right-hand side")
+        variant = {None: 0, "f64": 0, "f32": 1, "bf16": 2}[self.f.storage_precision]
+        nbytes = lib().b2s_gmres_workspace_bytes(n, A.nnz, self.f.krylov_dim, variant)
+        ws = self._workspace(nbytes)
+        it, rs = C.c_int64(0), C.c_int64(0)
+        rn, conv = C.c_double(0), C.c_int(0)
+        call("b2s_gmres_solve", variant, n, _p(A.row_ptrs), _p(A.col_idxs),
+             _p(A.values), A.max_row_nnz, _p(self.inv_diag), _p(b2), _p(x2),
+             self.f.krylov_dim, self.f.max_iters, self.f.reduction,
+             self.f.inner_reduction, _p(ws), ws.numel(), C.byref(it),
+             C.byref(rs), C.byref(rn), C.byref(conv), _stream(x2))
+        self.logger = ConvergenceLog(int(it.value), [rn.value], bool(conv.value),
+                                     [0x82 if conv.value else 0x01], int(rs.value))
+        return x
+
+
+class _CgFactory(_SolverFactory):
+    kind = "cg"
+
+
+class _BicgstabFactory(_SolverFactory):
+    kind = "bicgstab"
+
+
+class _GmresFactory(_SolverFactory):
+    kind = "gmres"
+
+
+class _IrFactory(_SolverFactory):
+    kind = "ir"
+
+    def __init__(self, exec_, criteria=(), solver=None, **kw):
+        inner = solver.params() if isinstance(solver, _Builder) else dict(solver or {})
+        sp = inner.get("storage_precision", "f32")
+        super().__init__(exec_, criteria=criteria,
+                         preconditioner=inner.get("preconditioner", kw.pop("preconditioner", None)),
+                         krylov_dim=inner.get("krylov_dim", 30),
+                         storage_precision=sp if sp != "f64" else "f32",
+                         inner_reduction=inner.get("inner_reduction", 1e-6), **kw)
+
+
+class Cg:
+    """solver::Cg (core/solver/cg.cpp)."""
+
+    @staticmethod
+    def build():
+        return _Builder(_CgFactory)
+
+
+class Bicgstab:
+    """solver::Bicgstab (core/solver/bicgstab.cpp)."""
+
+    @staticmethod
+    def build():
+        return _Builder(_BicgstabFactory)
+
+
+class Gmres:
+    """solver::Gmres (core/solver/gmres.cpp); krylov_dim <= 32 here (the
+    reference default of 100 is capped).  with_storage_precision("f32" or
+    "bf16") selects the low-precision Arnoldi used inside Ir."""
+
+    @staticmethod
+    def build():
+        return _Builder(_GmresFactory, krylov_dim=30)
+
+
+class Ir:
+    """solver::Ir (core/solver/ir.cpp) with a low-precision GMRES cycle as
+    the inner solver and the FP64 residual outside."""
+
+    @staticmethod
+    def build():
+        return _Builder(_IrFactory)

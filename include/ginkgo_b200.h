@@ -246,6 +246,31 @@ int b2s_cg_solve_f32(int64_t num_rows, const int32_t* row_ptrs,
                      int64_t* iterations, double* residual_norms,
                      uint8_t* status, void* stream);
 
+/* Preconditioned BiCGStab, 1..16 right-hand sides.  Replaces
+ * Bicgstab<V>::apply_dense_impl (core/solver/bicgstab.cpp:95-250) with
+ * bicgstab::initialize/step_1/step_2/step_3/finalize
+ * (core/solver/bicgstab_kernels.hpp:25-88). */
+int64_t b2s_bicgstab_workspace_bytes(int64_t num_rows, int64_t num_rhs,
+                                     int value_bytes);
+int b2s_bicgstab_solve_f64(int64_t num_rows, const int32_t* row_ptrs,
+                           const int32_t* col_idxs, const double* values,
+                           int64_t max_row_nnz, const double* inv_diag,
+                           const double* b, int64_t ldb, double* x,
+                           int64_t ldx, int64_t num_rhs, int64_t max_iters,
+                           double reduction_factor, int64_t check_every,
+                           void* workspace, int64_t workspace_bytes,
+                           int64_t* iterations, double* residual_norms,
+                           uint8_t* status, void* stream);
+int b2s_bicgstab_solve_f32(int64_t num_rows, const int32_t* row_ptrs,
+                           const int32_t* col_idxs, const float* values,
+                           int64_t max_row_nnz, const float* inv_diag,
+                           const float* b, int64_t ldb, float* x, int64_t ldx,
+                           int64_t num_rhs, int64_t max_iters,
+                           double reduction_factor, int64_t check_every,
+                           void* workspace, int64_t workspace_bytes,
+                           int64_t* iterations, double* residual_norms,
+                           uint8_t* status, void* stream);
+
 #define B2S_GMRES_F64 0
 #define B2S_GMRES_MIXED_F32 1
 #define B2S_GMRES_MIXED_BF16 2
@@ -272,6 +297,79 @@ int b2s_gmres_solve(int variant, int64_t num_rows, const int32_t* row_ptrs,
                     int64_t workspace_bytes, int64_t* iterations,
                     int64_t* restarts, double* residual_norm, int* converged,
                     void* stream);
+
+/* -------------------------------------------------------- gradients -- */
+
+/* out[e] = alpha * sum_k u(row_e, k) * w(col_e, k) over the stored entries
+ * of a Csr pattern (1..16 columns).  The backward of the differentiable
+ * solve: with u = lambda, w = x, alpha = -1 it is dL/dA = -lambda x^T on A's
+ * pattern.  No counterpart in the reference (it has no autograd path). */
+int b2s_csr_sddmm_f64(int64_t num_rows, const int32_t* row_ptrs,
+                      const int32_t* col_idxs, int64_t max_row_nnz,
+                      const double* u, int64_t ldu, const double* w,
+                      int64_t ldw, int64_t num_rhs, double alpha, double* out,
+                      void* stream);
+int b2s_csr_sddmm_f32(int64_t num_rows, const int32_t* row_ptrs,
+                      const int32_t* col_idxs, int64_t max_row_nnz,
+                      const float* u, int64_t ldu, const float* w,
+                      int64_t ldw, int64_t num_rhs, double alpha, float* out,
+                      void* stream);
+
+/* ---------------------------------------------------- batched solver -- */
+
+/* Batched BiCGStab over num_systems independent systems of uneven size in a
+ * ragged batch Ell: system s has row_offsets[s+1] - row_offsets[s] rows
+ * (1..2048) and its entries at values[width * row_offsets[s] + j * n_s + r]
+ * (column-major per system, local column indices, -1 padding).  For equal
+ * sizes this is the value layout of gko::batch::matrix::Ell
+ * (include/ginkgo/core/matrix/batch_ell.hpp:149-221), column indices
+ * stored per system.  b, x: concatenated per-system vectors (x = initial
+ * guess in, solution out).  Stop: ||r|| <= tolerance * ||b|| (relative) or
+ * ||r|| <= tolerance (tolerance_absolute != 0), or max_iters.  Outputs per
+ * system on the device: iteration count and final residual norm (what
+ * gko::batch::log::BatchConvergence records).  host_row_offsets: the same
+ * offsets in host memory (used to sort systems into size buckets).
+ * tune_table: NULL for the built-in choice, or 24 int32 from
+ * b2s_batch_ell_bicgstab_tune_* (per size bucket 2^k rows: threads per
+ * system, 1 = vectors in shared memory / 0 = global scratch).  Synchronises
+ * the stream.  Replaces batch_bicgstab::apply
+ * (core/solver/batch_bicgstab_kernels.hpp:177-190;
+ * cuda/solver/batch_bicgstab_kernels.cu:24-153). */
+int64_t b2s_batch_bicgstab_workspace_bytes(int64_t num_systems,
+                                           int64_t total_rows,
+                                           int value_bytes);
+int b2s_batch_ell_bicgstab_solve_f64(
+    int64_t num_systems, const int32_t* row_offsets,
+    const int32_t* host_row_offsets, int64_t width, const int32_t* col_idxs,
+    const double* values, const double* b, double* x, int64_t max_iters,
+    double tolerance, int tolerance_absolute, int use_jacobi,
+    const int32_t* tune_table, void* workspace, int64_t workspace_bytes,
+    int32_t* iterations, double* residual_norms, void* stream);
+int b2s_batch_ell_bicgstab_solve_f32(
+    int64_t num_systems, const int32_t* row_offsets,
+    const int32_t* host_row_offsets, int64_t width, const int32_t* col_idxs,
+    const float* values, const float* b, float* x, int64_t max_iters,
+    double tolerance, int tolerance_absolute, int use_jacobi,
+    const int32_t* tune_table, void* workspace, int64_t workspace_bytes,
+    int32_t* iterations, double* residual_norms, void* stream);
+/* Autotuner: for every size bucket, times each threads-per-system and
+ * vector-placement candidate on that bucket's systems (x restored between
+ * trials), writes the fastest into tune_table_out (24 int32), then solves
+ * with it. */
+int b2s_batch_ell_bicgstab_tune_f64(
+    int64_t num_systems, const int32_t* row_offsets,
+    const int32_t* host_row_offsets, int64_t width, const int32_t* col_idxs,
+    const double* values, const double* b, double* x, int64_t max_iters,
+    double tolerance, int tolerance_absolute, int use_jacobi,
+    void* workspace, int64_t workspace_bytes, int32_t* iterations,
+    double* residual_norms, int32_t* tune_table_out, void* stream);
+int b2s_batch_ell_bicgstab_tune_f32(
+    int64_t num_systems, const int32_t* row_offsets,
+    const int32_t* host_row_offsets, int64_t width, const int32_t* col_idxs,
+    const float* values, const float* b, float* x, int64_t max_iters,
+    double tolerance, int tolerance_absolute, int use_jacobi,
+    void* workspace, int64_t workspace_bytes, int32_t* iterations,
+    double* residual_norms, int32_t* tune_table_out, void* stream);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,114 @@
+"""Batched BiCGStab on a ragged batch Ell against the oracle (one system at
+a time, the reference algorithm) and the reference's known answer."""
+import numpy as np
+import pytest
+import torch
+
+from ginkgo_b200.batch import BatchBicgstab, BatchEll, convection_diffusion_batch
+from ginkgo_b200.matrix import CudaExecutor
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def exe():
+    return CudaExecutor.create(0)
+
+
+def solver(exe, A, max_it, tol, jacobi=True, tol_type="relative"):
+    return (BatchBicgstab.build().with_max_iterations(max_it).with_tolerance(tol)
+            .with_tolerance_type(tol_type)
+            .with_preconditioner("jacobi" if jacobi else None).on(exe).generate(A))
+
+
+def test_known_answer_stencil(exe, known):
+    c = known["batch_bicgstab"]
+    n = c["num_rows"]
+    lo, d, up = c["stencil"]
+    rows = np.arange(n)
+    systems = []
+    for _ in range(c["num_batch_items"]):
+        rp = [0]
+        ci, v = [], []
+        for i in rows:
+            for j, w in ((i - 1, lo), (i, d), (i + 1, up)):
+                if 0 <= j < n:
+                    ci.append(j)
+                    v.append(w)
+            rp.append(len(ci))
+        systems.append((np.array(rp), np.array(ci), np.array(v)))
+    for dt in (torch.float64, torch.float32):
+        A = BatchEll.from_csr(exe, systems, width=3, dtype=dt)
+        xs = np.full(n, c["exact_solution"])
+        b = np.concatenate([orc.csr_spmv(*s, xs) for s in systems])
+        bd = torch.from_numpy(b).to(dt).cuda()
+        x = torch.zeros_like(bd)
+        s = solver(exe, A, c["max_iters"], c["tol"], jacobi=False)
+        s.apply(bd, x)
+        it = s.logger.iterations.cpu().numpy()
+        assert np.all(it <= c["max_logged_iters"]), it
+        xr = x.cpu().numpy().reshape(-1, n)
+        for i in range(c["num_batch_items"]):
+            res = np.linalg.norm(b[i * n:(i + 1) * n] - orc.csr_spmv(*systems[i], xr[i].astype(np.float64)))
+            assert res / np.linalg.norm(b[i * n:(i + 1) * n]) <= 2 * c["tol"]
+        np.testing.assert_allclose(xr, c["exact_solution"], atol=c["tol"] * 10 * 2.5)
+
+
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+def test_ragged_batch_matches_oracle(exe, dt):
+    A, systems = convection_diffusion_batch(exe, 300, lo=2, hi=1024, seed=5, dtype=dt)
+    rng = np.random.default_rng(1)
+    b = rng.standard_normal(A.total_rows)
+    bd = torch.from_numpy(b).to(dt).cuda()
+    x = torch.zeros_like(bd)
+    tol = 1e-8 if dt == torch.float64 else 1e-4
+    s = solver(exe, A, 500, tol)
+    s.apply(bd, x)
+    it = s.logger.iterations.cpu().numpy()
+    res = s.logger.residual_norms.cpu().numpy()
+    xg = x.cpu().numpy().astype(np.float64)
+    offs = A.host_row_offsets
+    npdt = np.float64 if dt == torch.float64 else np.float32
+    for i in range(A.num_systems):
+        o, e = offs[i], offs[i + 1]
+        rp, ci, v = systems[i]
+        bi = b[o:e].astype(npdt)
+        w, st, eci, ev = orc.csr_to_ell(rp, ci, v.astype(npdt))
+        xo, it_o, res_o, conv_o = orc.batch_bicgstab_ell(e - o, w, st, eci, ev, bi,
+                                                         max_iters=500, tol=tol)
+        assert conv_o
+        assert abs(int(it[i]) - it_o) <= max(2, it_o // 10), (i, it[i], it_o)
+        rel = np.linalg.norm(bi.astype(np.float64) - orc.csr_spmv(rp, ci, v, xg[o:e])) \
+            / np.linalg.norm(bi)
+        assert rel <= tol * (1.5 if dt == torch.float64 else 10), (i, rel)
+        assert res[i] <= tol * np.linalg.norm(bi) * 1.01
+
+
+def test_autotuner_and_reuse(exe):
+    A, systems = convection_diffusion_batch(exe, 400, lo=32, hi=1024, seed=2)
+    b = torch.from_numpy(np.random.default_rng(3).standard_normal(A.total_rows)).cuda()
+    s = solver(exe, A, 500, 1e-8)
+    x1 = torch.zeros_like(b)
+    table = s.tune(b, x1)
+    buckets = {int(np.ceil(np.log2(n))) for n in A.sizes}
+    for bk in buckets:
+        assert table[2 * bk] in (32, 64, 128, 256)
+    x2 = torch.zeros_like(b)
+    s.apply(b, x2)  # tuned configuration
+    assert torch.equal(s.logger.iterations.cpu() > 0, torch.ones(A.num_systems, dtype=torch.bool))
+    # the tuned and the default configurations solve the same systems
+    s2 = solver(exe, A, 500, 1e-8)
+    x3 = torch.zeros_like(b)
+    s2.apply(b, x3)
+    assert torch.allclose(x2, x3, rtol=1e-6, atol=1e-9)
+
+
+def test_zero_rhs_and_absolute_tolerance(exe):
+    A, systems = convection_diffusion_batch(exe, 20, lo=32, hi=64, seed=9)
+    b = torch.zeros(A.total_rows, dtype=torch.float64, device="cuda")
+    x = torch.zeros_like(b)
+    s = solver(exe, A, 100, 1e-10, tol_type="absolute")
+    s.apply(b, x)
+    assert torch.count_nonzero(s.logger.iterations) == 0
+    assert torch.count_nonzero(x) == 0
