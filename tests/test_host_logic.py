@@ -1,0 +1,91 @@
+"""Host-side logic that needs no GPU: generators, batch layout, factory
+parameters, the conductivity assembly used by the differentiable solve."""
+import numpy as np
+import pytest
+import torch
+
+from ginkgo_b200 import stencils
+from oracle import oracle as orc
+
+
+def test_generator_sizes_match_the_workloads():
+    assert len(stencils.poisson_2d_5pt(256)[1]) == 326656
+    rp, ci, _ = stencils.poisson_3d_7pt(64)
+    assert (len(rp) - 1, len(ci)) == (262144, 1810432)
+    rp, ci, v = stencils.anisotropic_27pt(8)
+    n = len(rp) - 1
+    # symmetric, positive definite
+    dense = np.zeros((n, n))
+    dense[np.repeat(np.arange(n), np.diff(rp)), ci] = v
+    assert np.allclose(dense, dense.T)
+    assert np.linalg.eigvalsh(dense).min() > 0
+
+
+def test_power_law_rows_sorted_and_unique():
+    rp, ci, v = stencils.power_law(5000, seed=1, max_len=800)
+    for r in range(0, 5000, 97):
+        row = ci[rp[r]:rp[r + 1]]
+        assert np.all(np.diff(row) > 0)
+    assert rp[-1] == len(ci) == len(v)
+
+
+def test_std_uniform_reproduces_mt19937():
+    # first outputs of std::mt19937(5489) are 3499211612, 581869302
+    w = np.frombuffer(np.random.RandomState(5489).bytes(8), "<u4")
+    assert list(w) == [3499211612, 581869302]
+    u = stencils.std_uniform(5489, 1, 0.0, 1.0)[0]
+    assert u == (3499211612 + 581869302 * 2.0 ** 32) / 2.0 ** 64
+
+
+def test_batch_ell_layout_matches_per_system_ell():
+    from ginkgo_b200.batch import BatchEll
+
+    class FakeExec:
+        device = torch.device("cpu")
+
+    systems = [stencils.convection_diffusion_2d(nx, ny, 1.0, 0.3, -0.2)
+               for nx, ny in ((5, 4), (7, 3), (1, 9))]
+    A = BatchEll.from_csr(FakeExec(), systems, width=5)
+    ci = A.col_idxs.numpy()
+    v = A.values.numpy()
+    for s, (rp, c, val) in enumerate(systems):
+        w, st, eci, ev = orc.csr_to_ell(rp, c, val, width=5)
+        o = 5 * A.host_row_offsets[s]
+        assert np.array_equal(ci[o:o + len(eci)], eci)
+        assert np.array_equal(v[o:o + len(ev)], ev)
+    back = A.to_csr_list()
+    for (rp, c, val), (rp2, c2, v2) in zip(systems, back):
+        assert np.array_equal(rp, rp2) and np.array_equal(c, c2)
+        assert np.allclose(val, v2)
+
+
+def test_conductivity_assembly_matches_generator():
+    from ginkgo_b200.autograd import ConductivityOperator
+    op = ConductivityOperator(5, device="cpu")
+    th = torch.rand(op.num_edges, dtype=torch.float64) + 0.25
+    rp, ci, v = stencils.conductivity_matrix(5, th.numpy())
+    assert np.array_equal(op.row_ptrs.numpy(), rp)
+    assert np.array_equal(op.col_idxs.numpy(), ci)
+    assert np.allclose(op.values(th).numpy(), v)
+    # gradient of sum(values) w.r.t. theta: interior edges 2 - 2 = 0, boundary 1
+    th.requires_grad_(True)
+    op.values(th).sum().backward()
+    ei, ej = stencils.conductivity_edges(5)
+    assert np.allclose(th.grad.numpy(), np.where(ej >= 0, 0.0, 1.0))
+
+
+def test_solver_factory_parameters():
+    from ginkgo_b200.solver import (Cg, Gmres, Iteration, Jacobi, ResidualNorm,
+                                    _criteria)
+    m, r = _criteria((Iteration.build().with_max_iters(50),
+                      ResidualNorm.build().with_reduction_factor(1e-8)))
+    assert (m, r) == (50, 1e-8)
+    with pytest.raises(ValueError):
+        _criteria((ResidualNorm.build().with_reduction_factor(1e-8),))
+    with pytest.raises(NotImplementedError):
+        Jacobi.build().with_max_block_size(4).on(None)
+    f = (Gmres.build().with_krylov_dim(100)
+         .with_criteria(Iteration.build().with_max_iters(5)).on(None))
+    assert f.krylov_dim == 32  # capped by the device Hessenberg
+    f = Cg.build().with_criteria(Iteration.build().with_max_iters(3)).on(None)
+    assert f.kind == "cg" and f.max_iters == 3 and f.reduction == 0.0
