@@ -206,6 +206,152 @@ int b2s_jacobi_apply_f32(int64_t num_rows, int64_t num_rhs,
                          float* x, int64_t ldx, const float* alpha,
                          const float* beta, void* stream);
 
+/* ------------------------------------------------ Krylov step kernels -- */
+
+/* Kernel-level stand-ins for a caller that keeps the reference's solver
+ * loop.  Dense operands are row-major (values, stride); scalars are device
+ * arrays of k = num_rhs entries; stop_status is the reference's
+ * stopping_status array (one uint8 per column: bit 7 converged, bit 6
+ * finalized, bits 0-5 criterion id). */
+
+/* cg::initialize / step_1 / step_2 (core/solver/cg_kernels.hpp:25-52). */
+int b2s_cg_initialize_f64(int64_t n, int64_t k, const double* b, int64_t ldb,
+                          double* r, int64_t ldr, double* z, int64_t ldz,
+                          double* p, int64_t ldp, double* q, int64_t ldq,
+                          double* prev_rho, double* rho, uint8_t* stop_status,
+                          void* stream);
+int b2s_cg_initialize_f32(int64_t n, int64_t k, const float* b, int64_t ldb,
+                          float* r, int64_t ldr, float* z, int64_t ldz,
+                          float* p, int64_t ldp, float* q, int64_t ldq,
+                          float* prev_rho, float* rho, uint8_t* stop_status,
+                          void* stream);
+int b2s_cg_step_1_f64(int64_t n, int64_t k, double* p, int64_t ldp,
+                      const double* z, int64_t ldz, const double* rho,
+                      const double* prev_rho, const uint8_t* stop_status,
+                      void* stream);
+int b2s_cg_step_1_f32(int64_t n, int64_t k, float* p, int64_t ldp,
+                      const float* z, int64_t ldz, const float* rho,
+                      const float* prev_rho, const uint8_t* stop_status,
+                      void* stream);
+int b2s_cg_step_2_f64(int64_t n, int64_t k, double* x, int64_t ldx, double* r,
+                      int64_t ldr, const double* p, int64_t ldp,
+                      const double* q, int64_t ldq, const double* beta,
+                      const double* rho, const uint8_t* stop_status,
+                      void* stream);
+int b2s_cg_step_2_f32(int64_t n, int64_t k, float* x, int64_t ldx, float* r,
+                      int64_t ldr, const float* p, int64_t ldp, const float* q,
+                      int64_t ldq, const float* beta, const float* rho,
+                      const uint8_t* stop_status, void* stream);
+
+/* bicgstab::step_1 / step_2 / step_3 / finalize
+ * (core/solver/bicgstab_kernels.hpp:42-88). */
+int b2s_bicgstab_step_1_f64(int64_t n, int64_t k, const double* r,
+                            int64_t ldr, double* p, int64_t ldp,
+                            const double* v, int64_t ldv, const double* rho,
+                            const double* prev_rho, const double* alpha,
+                            const double* omega, const uint8_t* stop_status,
+                            void* stream);
+int b2s_bicgstab_step_1_f32(int64_t n, int64_t k, const float* r, int64_t ldr,
+                            float* p, int64_t ldp, const float* v, int64_t ldv,
+                            const float* rho, const float* prev_rho,
+                            const float* alpha, const float* omega,
+                            const uint8_t* stop_status, void* stream);
+int b2s_bicgstab_step_2_f64(int64_t n, int64_t k, const double* r,
+                            int64_t ldr, double* s, int64_t lds,
+                            const double* v, int64_t ldv, const double* rho,
+                            double* alpha, const double* beta,
+                            const uint8_t* stop_status, void* stream);
+int b2s_bicgstab_step_2_f32(int64_t n, int64_t k, const float* r, int64_t ldr,
+                            float* s, int64_t lds, const float* v, int64_t ldv,
+                            const float* rho, float* alpha, const float* beta,
+                            const uint8_t* stop_status, void* stream);
+int b2s_bicgstab_step_3_f64(int64_t n, int64_t k, double* x, int64_t ldx,
+                            double* r, int64_t ldr, const double* s,
+                            int64_t lds, const double* t, int64_t ldt,
+                            const double* y, int64_t ldy, const double* z,
+                            int64_t ldz, const double* alpha,
+                            const double* beta, const double* gamma,
+                            double* omega, const uint8_t* stop_status,
+                            void* stream);
+int b2s_bicgstab_step_3_f32(int64_t n, int64_t k, float* x, int64_t ldx,
+                            float* r, int64_t ldr, const float* s, int64_t lds,
+                            const float* t, int64_t ldt, const float* y,
+                            int64_t ldy, const float* z, int64_t ldz,
+                            const float* alpha, const float* beta,
+                            const float* gamma, float* omega,
+                            const uint8_t* stop_status, void* stream);
+int b2s_bicgstab_finalize_f64(int64_t n, int64_t k, double* x, int64_t ldx,
+                              const double* y, int64_t ldy,
+                              const double* alpha, uint8_t* stop_status,
+                              void* stream);
+int b2s_bicgstab_finalize_f32(int64_t n, int64_t k, float* x, int64_t ldx,
+                              const float* y, int64_t ldy, const float* alpha,
+                              uint8_t* stop_status, void* stream);
+
+/* common_gmres::hessenberg_qr and solve_krylov
+ * (core/solver/common_gmres_kernels.hpp:32-50): hessenberg_iter is
+ * (iter + 2) x k, givens_* krylov_dim x k, residual_norm_collection
+ * (krylov_dim + 1) x k; hessenberg(j, i * k + c) holds H(i, j). */
+int b2s_gmres_hessenberg_qr_f64(int64_t k, int64_t iter, double* givens_sin,
+                                int64_t ld_sin, double* givens_cos,
+                                int64_t ld_cos, double* residual_norm,
+                                double* residual_norm_collection,
+                                int64_t ld_rnc, double* hessenberg_iter,
+                                int64_t ld_h, int64_t* final_iter_nums,
+                                const uint8_t* stop_status, void* stream);
+int b2s_gmres_hessenberg_qr_f32(int64_t k, int64_t iter, float* givens_sin,
+                                int64_t ld_sin, float* givens_cos,
+                                int64_t ld_cos, float* residual_norm,
+                                float* residual_norm_collection,
+                                int64_t ld_rnc, float* hessenberg_iter,
+                                int64_t ld_h, int64_t* final_iter_nums,
+                                const uint8_t* stop_status, void* stream);
+int b2s_gmres_solve_krylov_f64(int64_t k,
+                               const double* residual_norm_collection,
+                               int64_t ld_rnc, const double* hessenberg,
+                               int64_t ld_h, double* y, int64_t ld_y,
+                               const int64_t* final_iter_nums,
+                               const uint8_t* stop_status, void* stream);
+int b2s_gmres_solve_krylov_f32(int64_t k, const float* residual_norm_collection,
+                               int64_t ld_rnc, const float* hessenberg,
+                               int64_t ld_h, float* y, int64_t ld_y,
+                               const int64_t* final_iter_nums,
+                               const uint8_t* stop_status, void* stream);
+
+/* dense::compute_conj_dot / compute_norm2 per column, result on the device
+ * (core/matrix/dense_kernels.hpp:100-118); deterministic two-level sum.
+ * workspace: b2s_dense_reduction_workspace_bytes(k, value_bytes). */
+int64_t b2s_dense_reduction_workspace_bytes(int64_t num_rhs, int value_bytes);
+int b2s_dense_compute_dot_f64(int64_t n, int64_t k, const double* a,
+                              int64_t lda, const double* b, int64_t ldb,
+                              double* result, void* workspace,
+                              int64_t workspace_bytes, void* stream);
+int b2s_dense_compute_dot_f32(int64_t n, int64_t k, const float* a,
+                              int64_t lda, const float* b, int64_t ldb,
+                              float* result, void* workspace,
+                              int64_t workspace_bytes, void* stream);
+int b2s_dense_compute_norm2_f64(int64_t n, int64_t k, const double* a,
+                                int64_t lda, double* result, void* workspace,
+                                int64_t workspace_bytes, void* stream);
+int b2s_dense_compute_norm2_f32(int64_t n, int64_t k, const float* a,
+                                int64_t lda, float* result, void* workspace,
+                                int64_t workspace_bytes, void* stream);
+
+/* residual_norm::residual_norm (core/stop/residual_norm_kernels.hpp:21-29):
+ * converges column c when tau[c] <= goal * orig_tau[c]; device_flags[0] is
+ * cleared when an unstopped column is not converged (all converged),
+ * device_flags[1] set when one changed.  The host reads the two flags. */
+int b2s_residual_norm_check_f64(int64_t k, const double* tau,
+                                const double* orig_tau, double goal,
+                                int stopping_id, int set_finalized,
+                                uint8_t* stop_status, int* device_flags,
+                                void* stream);
+int b2s_residual_norm_check_f32(int64_t k, const float* tau,
+                                const float* orig_tau, double goal,
+                                int stopping_id, int set_finalized,
+                                uint8_t* stop_status, int* device_flags,
+                                void* stream);
+
 /* ------------------------------------------------------ fused solvers -- */
 
 /* Whole-solve entry points.  They run the reference's solver loop on the

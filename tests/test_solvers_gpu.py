@@ -31,7 +31,7 @@ def crit(max_iters, red):
 
 def explicit_rel_res(rp, ci, v, x, b):
     r = b - orc.csr_spmv(rp, ci, v.astype(np.float64), x.astype(np.float64))
-    return np.linalg.norm(r, axis=0) / np.linalg.norm(b, axis=0)
+    return np.atleast_1d(np.linalg.norm(r, axis=0) / np.linalg.norm(b, axis=0))
 
 
 @pytest.mark.parametrize("dt", [torch.float64, torch.float32])
