@@ -6,6 +6,8 @@
 //   convert_to_sellp   reference/matrix/csr_kernels.cpp:529-570
 //   transpose          reference/matrix/csr_kernels.cpp:678-730
 //   jacobi             common/unified/preconditioner/jacobi_kernels.cpp:24-101
+#include <mutex>
+
 #include "common.cuh"
 
 namespace b2s {
@@ -481,3 +483,86 @@ B2S_CONVERT_ENTRIES(double, f64)
 B2S_CONVERT_ENTRIES(float, f32)
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free Sellp slice sets.
+//
+// Some callers cannot allocate device memory when they build a Sellp matrix:
+// hosts that hand the library one fixed device arena and forbid any further
+// allocation, and latency-sensitive loops that must not call cudaMalloc
+// (it can synchronise the whole device).  For them the scan scratch of the
+// slice-set computation lives in this file-scope device array instead of a
+// caller workspace.  Limit: 4096 scratch entries, i.e. at most
+// 4095 * 2048 = 8,386,560 slices per call.  Every GPU that loads the library
+// holds these 32 KiB until the process exits.  All calls share the array:
+// calls that overlap on the GPU (different streams or threads at the same
+// time) race on it and give wrong results.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int64_t kNoAllocScanEntries = 4096;
+constexpr int64_t kNoAllocMaxSlices = (kNoAllocScanEntries - 1) * b2s::kScanTile;
+constexpr int kNoAllocMaxDevices = 64;
+}  // namespace
+
+static __device__ __align__(256) unsigned long long
+    g_slice_scan_scratch[kNoAllocScanEntries];
+
+namespace {
+std::mutex g_noalloc_mutex;
+void* g_noalloc_scratch[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device, looked up once
+// per device (the name is only a host-side stand-in for the device symbol).
+int noalloc_scratch(void** out)
+{
+    int dev = -1;
+    B2S_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) {
+        b2s::set_error("device %d out of range for the static scratch", dev);
+        return B2S_ERR_UNSUPPORTED;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_scratch[dev] == nullptr) {
+        void* p = nullptr;
+        B2S_CUDA_TRY(cudaGetSymbolAddress(&p, g_slice_scan_scratch));
+        g_noalloc_scratch[dev] = p;
+    }
+    *out = g_noalloc_scratch[dev];
+    return B2S_OK;
+}
+}  // namespace
+
+extern "C" int b2s_sellp_compute_slice_sets_noalloc(
+    int64_t num_rows, const int32_t* row_ptrs, int64_t slice_size,
+    int64_t stride_factor, uint64_t* slice_sets, uint64_t* slice_lengths,
+    void* stream)
+{
+    B2S_CHECK_ARG(num_rows >= 0 && slice_size >= 1 && stride_factor >= 1,
+                  "bad Sellp parameters");
+    const int64_t ns = b2s::ceildiv(num_rows, slice_size);
+    if (ns > kNoAllocMaxSlices) {
+        b2s::set_error(
+            "%lld slices exceed the static scratch of the allocation-free "
+            "entry point (at most %lld slices); use "
+            "b2s_sellp_compute_slice_sets with a workspace",
+            (long long)ns, (long long)kNoAllocMaxSlices);
+        return B2S_ERR_INVALID_ARG;
+    }
+    B2S_CHECK_ARG(slice_sets != nullptr, "null slice_sets");
+    void* scratch = nullptr;
+    const int rc = noalloc_scratch(&scratch);
+    if (rc != B2S_OK) return rc;
+    cudaStream_t st = b2s::as_stream(stream);
+    if (ns > 0) {
+        b2s::slice_lengths_kernel<<<b2s::ceildiv(ns, b2s::kBlock), b2s::kBlock,
+                                    0, st>>>(num_rows, row_ptrs, slice_size,
+                                             stride_factor, ns, slice_lengths);
+        B2S_LAUNCH_CHECK();
+    }
+    // exclusive_scan rewrites every scratch entry it reads and clears the
+    // one it accumulates into, so no state leaks between calls
+    using U = unsigned long long;
+    return b2s::exclusive_scan<U>(reinterpret_cast<const U*>(slice_lengths), ns,
+                                  reinterpret_cast<U*>(slice_sets),
+                                  static_cast<U*>(scratch), st);
+}

@@ -146,6 +146,26 @@ int b2s_sellp_compute_slice_sets(int64_t num_rows, const int32_t* row_ptrs,
                                  void* workspace, int64_t workspace_bytes,
                                  void* stream);
 
+/* The same slice lengths and slice sets as b2s_sellp_compute_slice_sets,
+ * for callers that cannot allocate device memory: a host that gives this
+ * library one fixed device arena and forbids further allocations, or a
+ * latency-sensitive loop that must not call cudaMalloc because it can
+ * synchronise the whole device.  It takes no workspace: its scan scratch is
+ * a 32 KiB array inside the library (4096 uint64 entries), so it handles at
+ * most 8,386,560 slices per call and rejects more with B2S_ERR_INVALID_ARG.
+ * The first call on a device looks up the array's device address once (with
+ * that device current); make that first call before any stream capture.
+ * All calls share the array, so calls that overlap on the GPU race.  It
+ * allocates nothing.  No counterpart in the reference: Ginkgo always takes
+ * its scratch from the executor. */
+int b2s_sellp_compute_slice_sets_noalloc(int64_t num_rows,
+                                         const int32_t* row_ptrs,
+                                         int64_t slice_size,
+                                         int64_t stride_factor,
+                                         uint64_t* slice_sets,
+                                         uint64_t* slice_lengths,
+                                         void* stream);
+
 /* Csr -> Sellp scatter into slice_sets[num_slices] * slice_size slots;
  * replaces csr::convert_to_sellp (core/matrix/csr_kernels.hpp:117-120). */
 int b2s_csr_convert_to_sellp_f64(int64_t num_rows, const int32_t* row_ptrs,
