@@ -1,54 +1,68 @@
 // Restarted GMRES(d) with right scalar-Jacobi preconditioning and an FP64
 // restart residual, in three precisions behind one engine:
 //
-//   b2s_gmres_solve_f64            Arnoldi in FP64, FP64 basis
-//   b2s_ir_gmres_solve_f32         mixed precision: every restart (outer
-//   b2s_ir_gmres_solve_bf16basis   iteration of iterative refinement)
-//                                  computes r = b - A x and ||r|| in FP64;
-//                                  the Arnoldi cycle runs on an FP32 copy of
-//                                  A with FP32 vectors and an FP32 or BF16
-//                                  basis; x += M V y is added in FP64.
+//   B2S_GMRES_F64         Arnoldi in FP64, FP64 basis
+//   B2S_GMRES_MIXED_F32   mixed precision: every restart (an outer step of
+//   B2S_GMRES_MIXED_BF16  iterative refinement) computes r = b - A x and
+//                         ||r|| in FP64; the Arnoldi cycle runs on an FP32
+//                         copy of A with FP32 vectors and an FP32 or BF16
+//                         basis; x += M V y is accumulated in FP64.
 //
 // Reference behaviour: core/solver/gmres.cpp:325-640 (restart, Arnoldi,
 // Givens QR, solve_krylov, multi_axpy), core/solver/ir.cpp:191-257 with
 // update_residual.hpp:20-60 (outer residual and check),
 // reference/solver/common_gmres_kernels.cpp:29-180 (Givens formulas).
 // Differences, all on the device: orthogonalisation is classical
-// Gram-Schmidt with one re-orthogonalisation (CGS2, the reference's
-// ortho_method::cgs2), each pass a single read of the basis; the Hessenberg
-// matrix, Givens rotations and the triangular solve are FP64 in every
-// variant; a cycle ends early when the Givens residual estimate reaches the
-// goal, and convergence is declared only on the explicit FP64 residual.
+// Gram-Schmidt with the re-orthogonalisation of CGS2 (the reference's
+// ortho_method::cgs2) taken from the Gram matrix G = V^T V of the stored
+// basis instead of a second pass over it: with h1 = V^T w, CGS2's second
+// projection is V^T (w - V h1) = h1 - G h1, so h = (2I - G) h1 and
+// w'' = w - V h in a single pass.  G gains one column per step from the
+// same pass that forms h1.  The Hessenberg matrix, Givens rotations, G and
+// the triangular solve are FP64 in every variant; a cycle ends early when
+// the Givens residual estimate reaches the goal, and convergence is declared
+// only on the explicit FP64 residual.
 //
 // Kernels per Arnoldi step j (one CUDA graph per restart cycle):
-//   spmv    v_j = round_basis(src * scale) formed on the fly (src = the
-//           previous unnormalised vector, or r at j = 0) and stored;
-//           w = A D^-1 v_j
-//   dot     h1 = V_{0..j}^T w
-//   orth    w -= V h1;  h2 = V^T w           (one basis read)
-//   orth2   w -= V h2;  ||w||; last block: Hessenberg column, Givens update,
-//           residual estimate, early end of the cycle, back substitution
-// per cycle: update x += D^-1 V y (FP64 accumulate), residual r = b - A x.
+//   prepare v_j = round_basis(src * scale) stored in the basis (src = the
+//           previous unnormalised vector, or r at j = 0); y = D^-1 v_j
+//   spmv    w = A y with the pipelined Csr kernel (values and column
+//           indices of the next row group copied with cp.async while the
+//           current group is summed)
+//   dots    h1 = V_{0..j}^T w and G(:, j) = V_{0..j}^T v_j, eight basis
+//           vectors per pass over the rows; last block: h = (2I - G) h1
+//   update  w'' = w - V h and ||w''||; last block: Hessenberg column,
+//           Givens update, residual estimate, early end of the cycle, back
+//           substitution
+// per cycle: x += D^-1 V y (FP64 accumulate) with r = b, then r -= A x with
+// the pipelined kernel in FP64, then ||r||, ||b|| and the restart check.
+// The serial parts (Givens chain, back substitution, (2I - G) h1) run in
+// the last block on shared-memory copies of the small arrays.
 #include <cuda_bf16.h>
 
+#include "csr_async.cuh"
 #include "solver_common.cuh"
 
 namespace b2s {
 namespace {
 
 constexpr int kMaxKrylov = 32;
+constexpr int kLd = kMaxKrylov + 1;
 
 struct GmresState {
     int done, cycle_done, j, final_iter;
     int total_iter, max_iters, outer_iter, converged;
-    unsigned ticket;
     int krylov_dim;
-    int pad[2];
+    int idle;  // done || cycle_done: the Arnoldi kernels have nothing to do
+    unsigned ticket;
+    int pad;
     double bnorm, rnorm, reduction, inner_reduction, inner_thresh;
     double scale;  // v_j = src * scale: 1/||r|| at j = 0, 1/H(j, j-1) else
-    double h1[kMaxKrylov + 1], h2[kMaxKrylov + 1];
-    double H[kMaxKrylov * (kMaxKrylov + 1)];  // column j at H[j * (M + 1)]
-    double g[kMaxKrylov + 1], cs[kMaxKrylov], sn[kMaxKrylov], y[kMaxKrylov];
+    double minus_one, one;       // alpha, beta of r = b - A x
+    double h[kLd];               // combined projection coefficients of step j
+    double H[kMaxKrylov * kLd];  // column j at H[j * kLd]
+    double G[kLd * kLd];         // Gram matrix of the stored basis
+    double g[kLd], cs[kMaxKrylov], sn[kMaxKrylov], y[kMaxKrylov];
 };
 
 template <typename TB, typename TA>
@@ -72,201 +86,280 @@ __device__ __forceinline__ float from_basis<float, __nv_bfloat16>(__nv_bfloat16 
     return __bfloat162float(v);
 }
 
-// The basis value v_j[c], formed identically wherever it is needed.
+// Step j, part 1: v_j = round_basis(src * scale) stored in the basis and
+// y = D^-1 v_j, the SpMV input (src = the previous unnormalised vector, or
+// r at j = 0).  One pass over n entries.
 template <typename TA, typename TB>
-__device__ __forceinline__ TA basis_value(int j, int64_t c,
-                                          const double* __restrict__ r64,
-                                          const TA* __restrict__ w_src,
-                                          TA scale)
-{
-    const TA src = j == 0 ? TA(r64[c]) : w_src[c];
-    return from_basis<TA>(to_basis<TB>(mul_rn(src, scale)));
-}
-
-template <typename TA, typename TB, int SW>
 __global__ void __launch_bounds__(kSolverBlock)
-    gmres_spmv_kernel(int64_t n, const int32_t* __restrict__ rp,
-                      const int32_t* __restrict__ ci, const TA* __restrict__ v,
-                      const TA* __restrict__ dinv,
-                      const double* __restrict__ r64,
-                      const TA* __restrict__ w_src, TA* __restrict__ w_dst,
-                      TB* __restrict__ V, GmresState* st)
+    gmres_prepare_kernel(int64_t n, const TA* __restrict__ dinv,
+                         const double* __restrict__ r64,
+                         const TA* __restrict__ w_src, TB* __restrict__ V,
+                         TA* __restrict__ y, GmresState* st)
 {
-    if (st->done || st->cycle_done) return;
+    if (st->idle) return;
     const int j = st->j;
     const TA scale = TA(st->scale);
     TB* vj = V + int64_t(j) * n;
-    const int lane = threadIdx.x % SW;
-    const int64_t nsub = int64_t(gridDim.x) * kSolverBlock / SW;
-    // warp-uniform trip count: all lanes of a warp run every iteration, so
-    // the subwarp shuffles below always see the whole warp
-    for (int64_t wbase = (blockIdx.x * int64_t(kSolverBlock) + threadIdx.x) /
-                         kWarp * (kWarp / SW);
-         wbase < n; wbase += nsub) {
-        const int64_t row = wbase + (threadIdx.x % kWarp) / SW;
-        const bool valid = row < n;
-        TA acc = TA(0);
-        const int end = valid ? rp[row + 1] : 0;
-        for (int e = (valid ? rp[row] : end) + lane; e < end; e += SW) {
-            const int64_t c = ci[e];
-            const TA d = dinv ? dinv[c] : TA(1);
-            acc += v[e] * mul_rn(d, basis_value<TA, TB>(j, c, r64, w_src, scale));
-        }
-        acc = subwarp_sum<SW>(acc);
-        if (valid && lane == 0) {
-            vj[row] = to_basis<TB>(basis_value<TA, TB>(j, row, r64, w_src, scale));
-            w_dst[row] = acc;
-        }
+    for (int64_t row = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; row < n;
+         row += int64_t(gridDim.x) * kSolverBlock) {
+        const TA src = j == 0 ? TA(r64[row]) : w_src[row];
+        const TB vb = to_basis<TB>(mul_rn(src, scale));
+        vj[row] = vb;
+        const TA va = from_basis<TA>(vb);
+        y[row] = dinv ? dinv[row] * va : va;
     }
 }
 
-// Loads V[0..j][row] (j < M) into registers.
-template <typename TA, typename TB, int M>
-__device__ __forceinline__ void load_basis_row(const TB* __restrict__ V,
-                                               int64_t n, int j, int64_t row,
-                                               TA (&vb)[M])
+// Sums each of the 16 values v[0..15] over the warp with 16 shuffles (a
+// butterfly that halves the values a lane carries at every level, instead
+// of 16 separate reductions of 5 shuffles each).  Returns, in lane l, the
+// warp total of value l / 2.
+__device__ __forceinline__ double butterfly16(double (&v)[16], int lane)
 {
+    constexpr unsigned kFull = 0xffffffffu;
 #pragma unroll
-    for (int i = 0; i < M; ++i) {
-        vb[i] = i <= j ? from_basis<TA>(V[int64_t(i) * n + row]) : TA(0);
+    for (int half = 8; half >= 1; half /= 2) {
+        const bool up = lane & (2 * half);
+#pragma unroll
+        for (int i = 0; i < half; ++i) {
+            const double send = up ? v[i] : v[i + half];
+            const double keep = up ? v[i + half] : v[i];
+            v[i] = keep + __shfl_xor_sync(kFull, send, 2 * half);
+        }
     }
+    return v[0] + __shfl_xor_sync(kFull, v[0], 1);
 }
 
-// h = V_{0..j}^T w; sums in the last block go to dst (h1 or h2).
-template <typename TA, int M>
-__device__ __forceinline__ void finish_dots(TA (&acc)[M], double* partials,
-                                            GmresState* st, double* dst, int j)
+// Step j, part 3: h1 = V_{0..j}^T w and G(:, j) = V_{0..j}^T v_j, eight
+// basis vectors per pass over the rows (w and v_j stay in L1/L2 between
+// passes), two rows per thread and iteration.  Launched with a few blocks
+// per SM, so the per-pass block reduction is amortised over many rows.
+// Partials: per block 2 * kLd entries.  The last block completes G's row
+// and column j and forms h = (2I - G) h1.
+template <typename TA, typename TB>
+__global__ void __launch_bounds__(kSolverBlock)
+    gmres_dots_kernel(int64_t n, const TB* __restrict__ V,
+                      const TA* __restrict__ w, GmresState* st,
+                      double* __restrict__ partials)
 {
-    __shared__ double red[kSolverBlock / kWarp * M];
-    __shared__ double tot[M];
+    constexpr int C = 8;
+    __shared__ double red[kSolverBlock / kWarp][2 * C];
+    __shared__ double tot[2 * kLd];
+    __shared__ double Gs[kLd * kLd];
     __shared__ int last;
-    double a[M];
+    if (st->idle) return;
+    const int j = st->j;
+    const int lane = threadIdx.x % kWarp, wid = threadIdx.x / kWarp;
+    const TB* vj = V + int64_t(j) * n;
+    double* part = partials + int64_t(blockIdx.x) * 2 * kLd;
+    const int64_t stride = int64_t(gridDim.x) * kSolverBlock;
+    for (int i0 = 0; i0 <= j; i0 += C) {
+        const int nv = j + 1 - i0 < C ? j + 1 - i0 : C;  // vectors this pass
+        TA a[C], g[C];
 #pragma unroll
-    for (int i = 0; i < M; ++i) a[i] = double(acc[i]);
-    block_partials<double, M>(a, partials, red);
+        for (int u = 0; u < C; ++u) a[u] = g[u] = TA(0);
+        int64_t row = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x;
+        for (; row + stride < n; row += 2 * stride) {
+            const int64_t r1 = row + stride;
+            const TA w0 = w[row], w1 = w[r1];
+            const TA v0 = from_basis<TA>(vj[row]), v1 = from_basis<TA>(vj[r1]);
+            TA x0[C], x1[C];
+#pragma unroll
+            for (int u = 0; u < C; ++u) {
+                if (u < nv) {
+                    x0[u] = from_basis<TA>(V[int64_t(i0 + u) * n + row]);
+                    x1[u] = from_basis<TA>(V[int64_t(i0 + u) * n + r1]);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < C; ++u) {
+                if (u < nv) {
+                    a[u] += x0[u] * w0;
+                    g[u] += x0[u] * v0;
+                    a[u] += x1[u] * w1;
+                    g[u] += x1[u] * v1;
+                }
+            }
+        }
+        if (row < n) {
+            const TA w0 = w[row];
+            const TA v0 = from_basis<TA>(vj[row]);
+#pragma unroll
+            for (int u = 0; u < C; ++u) {
+                if (u < nv) {
+                    const TA x0 = from_basis<TA>(V[int64_t(i0 + u) * n + row]);
+                    a[u] += x0 * w0;
+                    g[u] += x0 * v0;
+                }
+            }
+        }
+        double vals[2 * C];
+#pragma unroll
+        for (int u = 0; u < C; ++u) {
+            vals[u] = double(a[u]);
+            vals[C + u] = double(g[u]);
+        }
+        const double t = butterfly16(vals, lane);
+        if ((lane & 1) == 0) red[wid][lane / 2] = t;
+        __syncthreads();
+        if (threadIdx.x < 2 * C) {
+            const int u = threadIdx.x % C;
+            if (u < nv) {
+                double sum = 0.0;
+                for (int k = 0; k < kSolverBlock / kWarp; ++k) sum += red[k][threadIdx.x];
+                part[(threadIdx.x < C ? 0 : kLd) + i0 + u] = sum;
+            }
+        }
+        __syncthreads();
+    }
     if (last_block_done(&st->ticket, &last)) {
-        sum_partials<double, M>(partials, gridDim.x, tot, red);
-        if (threadIdx.x <= j && threadIdx.x < M) dst[threadIdx.x] = tot[threadIdx.x];
+        // block-ordered sums of the 2 (j + 1) used entries
+        for (int e = wid; e < 2 * kLd; e += kSolverBlock / kWarp) {
+            if ((e % kLd) > j) continue;
+            double s = 0.0;
+            for (int b = lane; b < int(gridDim.x); b += kWarp) {
+                s += __ldcg(partials + int64_t(b) * 2 * kLd + e);
+            }
+            s = warp_sum(s);
+            if (lane == 0) tot[e] = s;
+        }
+        // G(0..j-1, 0..j-1) from the earlier steps of this cycle
+        for (int e = threadIdx.x; e < j * kLd; e += kSolverBlock) Gs[e] = st->G[e];
+        __syncthreads();
+        if (threadIdx.x <= j) {
+            const int i = threadIdx.x;
+            const double gij = tot[kLd + i];
+            Gs[i * kLd + j] = gij;
+            Gs[j * kLd + i] = gij;
+            st->G[i * kLd + j] = gij;
+            st->G[j * kLd + i] = gij;
+        }
+        __syncthreads();
+        // h = (2I - G) h1: CGS2's second projection from G
+        if (threadIdx.x <= j) {
+            const int i = threadIdx.x;
+            double gh = 0.0;
+            for (int k = 0; k <= j; ++k) gh += Gs[i * kLd + k] * tot[k];
+            st->h[i] = 2.0 * tot[i] - gh;
+        }
         if (threadIdx.x == 0) st->ticket = 0;
     }
 }
 
-template <typename TA, typename TB, int M>
-__global__ void __launch_bounds__(kSolverBlock)
-    gmres_dot_kernel(int64_t n, const TB* __restrict__ V,
-                     const TA* __restrict__ w, GmresState* st,
-                     double* __restrict__ partials)
+// The end of Arnoldi step j, run by the whole last block of the update
+// kernel: Givens update of column j, residual estimate, cycle bookkeeping
+// and, when the cycle ends, the back substitution y = H \ g.  The small
+// arrays are staged in shared memory, so the serial chain runs at
+// shared-memory latency.
+__device__ void close_step(GmresState* st, double hnorm)
 {
-    if (st->done || st->cycle_done) return;
+    __shared__ double hc[kLd], gS[kLd], csS[kMaxKrylov], snS[kMaxKrylov];
+    __shared__ double Hs[kMaxKrylov * kLd], ts[kMaxKrylov];
+    __shared__ int fin;
     const int j = st->j;
-    TA acc[M];
-#pragma unroll
-    for (int i = 0; i < M; ++i) acc[i] = TA(0);
-    for (int64_t row = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; row < n;
-         row += int64_t(gridDim.x) * kSolverBlock) {
-        TA vb[M];
-        load_basis_row<TA, TB, M>(V, n, j, row, vb);
-        const TA wr = w[row];
-#pragma unroll
-        for (int i = 0; i < M; ++i) acc[i] += vb[i] * wr;
+    for (int i = threadIdx.x; i <= j; i += kSolverBlock) {
+        hc[i] = st->h[i];
+        gS[i] = st->g[i];
     }
-    finish_dots<TA, M>(acc, partials, st, st->h1, j);
-}
-
-template <typename TA, typename TB, int M>
-__global__ void __launch_bounds__(kSolverBlock)
-    gmres_orth_kernel(int64_t n, const TB* __restrict__ V, TA* __restrict__ w,
-                      GmresState* st, double* __restrict__ partials)
-{
-    if (st->done || st->cycle_done) return;
-    const int j = st->j;
-    TA h[M];
-#pragma unroll
-    for (int i = 0; i < M; ++i) h[i] = i <= j ? TA(st->h1[i]) : TA(0);
-    TA acc[M];
-#pragma unroll
-    for (int i = 0; i < M; ++i) acc[i] = TA(0);
-    for (int64_t row = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; row < n;
-         row += int64_t(gridDim.x) * kSolverBlock) {
-        TA vb[M];
-        load_basis_row<TA, TB, M>(V, n, j, row, vb);
-        TA wr = w[row];
-#pragma unroll
-        for (int i = 0; i < M; ++i) wr -= h[i] * vb[i];
-        w[row] = wr;
-#pragma unroll
-        for (int i = 0; i < M; ++i) acc[i] += vb[i] * wr;
+    for (int i = threadIdx.x; i < j; i += kSolverBlock) {
+        csS[i] = st->cs[i];
+        snS[i] = st->sn[i];
     }
-    finish_dots<TA, M>(acc, partials, st, st->h2, j);
-}
-
-// Givens update of column j and the cycle bookkeeping (one thread).
-__device__ void hessenberg_step(GmresState* st, double hnorm)
-{
-    constexpr int LD = kMaxKrylov + 1;
-    const int j = st->j;
-    double* h = st->H + j * LD;
-    for (int i = 0; i <= j; ++i) h[i] = st->h1[i] + st->h2[i];
-    h[j + 1] = hnorm;
-    for (int i = 0; i < j; ++i) {
-        const double t = st->cs[i] * h[i] + st->sn[i] * h[i + 1];
-        h[i + 1] = -st->sn[i] * h[i] + st->cs[i] * h[i + 1];
-        h[i] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        st->ticket = 0;
+        hc[j + 1] = hnorm;
+        for (int i = 0; i < j; ++i) {
+            const double t = csS[i] * hc[i] + snS[i] * hc[i + 1];
+            hc[i + 1] = -snS[i] * hc[i] + csS[i] * hc[i + 1];
+            hc[i] = t;
+        }
+        const double th = hc[j], nh = hc[j + 1];
+        double c, s;
+        if (th == 0.0) {
+            c = 0.0;
+            s = 1.0;
+        } else {
+            const double scale = fabs(th) + fabs(nh);
+            const double a = fabs(th / scale), b = fabs(nh / scale);
+            const double hyp = scale * sqrt(a * a + b * b);
+            c = th / hyp;
+            s = nh / hyp;
+        }
+        hc[j] = c * th + s * nh;
+        hc[j + 1] = 0.0;
+        gS[j + 1] = -s * gS[j];
+        gS[j] = c * gS[j];
+        st->cs[j] = c;
+        st->sn[j] = s;
+        st->g[j] = gS[j];
+        st->g[j + 1] = gS[j + 1];
+        const double est = fabs(gS[j + 1]);
+        const int total = st->total_iter + 1;
+        st->final_iter = j + 1;
+        st->total_iter = total;
+        st->scale = hnorm > 0.0 ? 1.0 / hnorm : 0.0;
+        st->j = j + 1;
+        fin = est <= st->inner_thresh || j + 1 >= st->krylov_dim ||
+              total >= st->max_iters || !(hnorm > 0.0);
+        if (fin) {
+            st->cycle_done = 1;
+            st->idle = 1;
+        }
     }
-    const double th = h[j], nh = h[j + 1];
-    if (th == 0.0) {
-        st->cs[j] = 0.0;
-        st->sn[j] = 1.0;
-    } else {
-        const double scale = fabs(th) + fabs(nh);
-        const double a = fabs(th / scale), b = fabs(nh / scale);
-        const double hyp = scale * sqrt(a * a + b * b);
-        st->cs[j] = th / hyp;
-        st->sn[j] = nh / hyp;
+    __syncthreads();
+    for (int i = threadIdx.x; i <= j + 1; i += kSolverBlock) st->H[j * kLd + i] = hc[i];
+    if (!fin) return;
+    // y = H \ g over the m = j + 1 finished columns: one warp, column by
+    // column from the last (t -= H(:, k) y_k after each y_k)
+    const int m = j + 1;
+    for (int e = threadIdx.x; e < j * kLd; e += kSolverBlock) Hs[e] = st->H[e];
+    for (int i = threadIdx.x; i <= j; i += kSolverBlock) {
+        Hs[j * kLd + i] = hc[i];
+        ts[i] = gS[i];
     }
-    h[j] = st->cs[j] * th + st->sn[j] * nh;
-    h[j + 1] = 0.0;
-    st->g[j + 1] = -st->sn[j] * st->g[j];
-    st->g[j] = st->cs[j] * st->g[j];
-    const double est = fabs(st->g[j + 1]);
-    st->final_iter = j + 1;
-    st->total_iter += 1;
-    st->scale = hnorm > 0.0 ? 1.0 / hnorm : 0.0;
-    st->j = j + 1;
-    if (est <= st->inner_thresh || st->j >= st->krylov_dim ||
-        st->total_iter >= st->max_iters || !(hnorm > 0.0)) {
-        st->cycle_done = 1;
-        // y = H \ g (back substitution over the finished columns)
-        const int m = st->final_iter;
-        for (int i = m - 1; i >= 0; --i) {
-            double t = st->g[i];
-            for (int k = i + 1; k < m; ++k) t -= st->H[k * LD + i] * st->y[k];
-            st->y[i] = t / st->H[i * LD + i];
+    __syncthreads();
+    if (threadIdx.x < kWarp) {
+        const int lane = threadIdx.x;
+        for (int k = m - 1; k >= 0; --k) {
+            const double yk = ts[k] / Hs[k * kLd + k];
+            if (lane == 0) st->y[k] = yk;
+            for (int i = lane; i < k; i += kWarp) ts[i] -= Hs[k * kLd + i] * yk;
+            __syncwarp();
         }
     }
 }
 
-template <typename TA, typename TB, int M>
+// w'' = w - V h, ||w''||; the last block closes the Arnoldi step.
+template <typename TA, typename TB>
 __global__ void __launch_bounds__(kSolverBlock)
-    gmres_orth2_kernel(int64_t n, const TB* __restrict__ V, TA* __restrict__ w,
-                       GmresState* st, double* __restrict__ partials)
+    gmres_update_kernel(int64_t n, const TB* __restrict__ V, TA* __restrict__ w,
+                        GmresState* st, double* __restrict__ partials)
 {
     __shared__ double red[kSolverBlock / kWarp];
     __shared__ double tot[1];
+    __shared__ TA hs[kLd];
     __shared__ int last;
-    if (st->done || st->cycle_done) return;
+    if (st->idle) return;
     const int j = st->j;
-    TA h[M];
-#pragma unroll
-    for (int i = 0; i < M; ++i) h[i] = i <= j ? TA(st->h2[i]) : TA(0);
+    for (int i = threadIdx.x; i <= j; i += kSolverBlock) hs[i] = TA(st->h[i]);
+    __syncthreads();
     double nrm = 0.0;
     for (int64_t row = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; row < n;
          row += int64_t(gridDim.x) * kSolverBlock) {
-        TA vb[M];
-        load_basis_row<TA, TB, M>(V, n, j, row, vb);
         TA wr = w[row];
+        // eight basis loads in flight, subtracted in order i = 0..j
+        for (int i0 = 0; i0 <= j; i0 += 8) {
+            TA x[8];
 #pragma unroll
-        for (int i = 0; i < M; ++i) wr -= h[i] * vb[i];
+            for (int u = 0; u < 8; ++u) {
+                if (i0 + u <= j) x[u] = from_basis<TA>(V[int64_t(i0 + u) * n + row]);
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                if (i0 + u <= j) wr -= hs[i0 + u] * x[u];
+            }
+        }
         w[row] = wr;
         nrm += double(wr) * double(wr);
     }
@@ -274,75 +367,63 @@ __global__ void __launch_bounds__(kSolverBlock)
     block_partials<double, 1>(a, partials, red);
     if (last_block_done(&st->ticket, &last)) {
         sum_partials<double, 1>(partials, gridDim.x, tot, red);
-        if (threadIdx.x == 0) {
-            st->ticket = 0;
-            hessenberg_step(st, sqrt(tot[0]));
-        }
+        close_step(st, sqrt(tot[0]));
     }
 }
 
-// x += D^-1 (V y) over the finished columns, accumulated into FP64 x.
-template <typename TA, typename TB, int M>
+// x += D^-1 (V y) over the finished columns, accumulated into FP64 x, and
+// r = b (the start of r = b - A x).
+template <typename TA, typename TB>
 __global__ void __launch_bounds__(kSolverBlock)
-    gmres_update_kernel(int64_t n, const TB* __restrict__ V,
-                        const TA* __restrict__ dinv, double* __restrict__ x,
-                        GmresState* st)
+    gmres_xupdate_kernel(int64_t n, const TB* __restrict__ V,
+                         const TA* __restrict__ dinv, double* __restrict__ x,
+                         const double* __restrict__ b, double* __restrict__ r,
+                         GmresState* st)
 {
+    __shared__ TA ys[kMaxKrylov];
     if (st->done) return;
     const int m = st->final_iter;
-    if (m == 0) return;
-    TA y[M];
-#pragma unroll
-    for (int i = 0; i < M; ++i) y[i] = i < m ? TA(st->y[i]) : TA(0);
+    for (int i = threadIdx.x; i < m; i += kSolverBlock) ys[i] = TA(st->y[i]);
+    __syncthreads();
     for (int64_t row = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; row < n;
          row += int64_t(gridDim.x) * kSolverBlock) {
-        TA vb[M];
-        load_basis_row<TA, TB, M>(V, n, m - 1, row, vb);
-        TA u = TA(0);
+        if (m > 0) {
+            TA u = TA(0);
+            for (int i0 = 0; i0 < m; i0 += 8) {
+                TA xv[8];
 #pragma unroll
-        for (int i = 0; i < M; ++i) u += y[i] * vb[i];
-        const TA d = dinv ? dinv[row] : TA(1);
-        x[row] += double(d * u);
+                for (int q = 0; q < 8; ++q) {
+                    if (i0 + q < m) xv[q] = from_basis<TA>(V[int64_t(i0 + q) * n + row]);
+                }
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    if (i0 + q < m) u += ys[i0 + q] * xv[q];
+                }
+            }
+            const TA d = dinv ? dinv[row] : TA(1);
+            x[row] += double(d * u);
+        }
+        r[row] = b[row];
     }
 }
 
-// r = b - A x in FP64, ||r||, ||b||; the last block checks convergence and
-// sets up the next cycle (the reference's restart kernel).
-template <int SW>
+// ||r||, ||b|| of r = b - A x; the last block checks convergence and sets up
+// the next cycle (the reference's restart step).
 __global__ void __launch_bounds__(kSolverBlock)
-    gmres_residual_kernel(int64_t n, const int32_t* __restrict__ rp,
-                          const int32_t* __restrict__ ci,
-                          const double* __restrict__ v,
-                          const double* __restrict__ x,
-                          const double* __restrict__ b,
-                          double* __restrict__ r, GmresState* st,
-                          double* __restrict__ partials)
+    gmres_restart_kernel(int64_t n, const double* __restrict__ r,
+                         const double* __restrict__ b, GmresState* st,
+                         double* __restrict__ partials)
 {
     __shared__ double red[kSolverBlock / kWarp * 2];
     __shared__ double tot[2];
     __shared__ int last;
     if (st->done) return;
-    const int lane = threadIdx.x % SW;
-    const int64_t nsub = int64_t(gridDim.x) * kSolverBlock / SW;
     double acc2[2] = {0.0, 0.0};
-    // warp-uniform trip count: all lanes of a warp run every iteration, so
-    // the subwarp shuffles below always see the whole warp
-    for (int64_t wbase = (blockIdx.x * int64_t(kSolverBlock) + threadIdx.x) /
-                         kWarp * (kWarp / SW);
-         wbase < n; wbase += nsub) {
-        const int64_t row = wbase + (threadIdx.x % kWarp) / SW;
-        const bool valid = row < n;
-        double acc = 0.0;
-        const int end = valid ? rp[row + 1] : 0;
-        for (int e = (valid ? rp[row] : end) + lane; e < end; e += SW) acc += v[e] * x[ci[e]];
-        acc = subwarp_sum<SW>(acc);
-        if (valid && lane == 0) {
-            const double bb = b[row];
-            const double rr = bb - acc;
-            r[row] = rr;
-            acc2[0] += rr * rr;
-            acc2[1] += bb * bb;
-        }
+    for (int64_t row = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; row < n;
+         row += int64_t(gridDim.x) * kSolverBlock) {
+        const double rr = r[row], bb = b[row];
+        acc2[0] += rr * rr;
+        acc2[1] += bb * bb;
     }
     block_partials<double, 2>(acc2, partials, red);
     if (last_block_done(&st->ticket, &last)) {
@@ -356,12 +437,15 @@ __global__ void __launch_bounds__(kSolverBlock)
             if (rn <= st->reduction * st->bnorm) {
                 st->converged = 1;
                 st->done = 1;
+                st->idle = 1;
             } else if (st->total_iter >= st->max_iters) {
                 st->done = 1;
+                st->idle = 1;
             } else {
                 st->outer_iter += 1;
                 st->j = 0;
                 st->cycle_done = 0;
+                st->idle = 0;
                 st->g[0] = rn;
                 for (int i = 1; i <= kMaxKrylov; ++i) st->g[i] = 0.0;
                 st->scale = 1.0 / rn;
@@ -380,7 +464,7 @@ __global__ void float_copy_kernel(int64_t n, const double* __restrict__ src,
 }
 
 struct GmresLayout {
-    int64_t bytes, off_st, off_r, off_w0, off_w1, off_v, off_partials,
+    int64_t bytes, off_st, off_r, off_w0, off_w1, off_y, off_v, off_partials,
         off_a32, off_d32;
 };
 
@@ -393,8 +477,9 @@ GmresLayout gmres_layout(int64_t n, int64_t nnz, int d, bool mixed)
     l.off_r = c.take<double>(n);
     l.off_w0 = c.take<TA>(n);
     l.off_w1 = c.take<TA>(n);
+    l.off_y = c.take<TA>(n);
     l.off_v = c.take<TB>((int64_t(d) + 1) * n);
-    l.off_partials = c.take<double>(int64_t(kSolverGrid) * (kMaxKrylov + 1));
+    l.off_partials = c.take<double>(int64_t(kSolverGrid) * 2 * kLd);
     l.off_a32 = mixed ? c.take<float>(nnz) : 0;
     l.off_d32 = mixed ? c.take<float>(n) : 0;
     l.bytes = c.used;
@@ -436,6 +521,7 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
     double* r = reinterpret_cast<double*>(w + lay.off_r);
     TA* wv[2] = {reinterpret_cast<TA*>(w + lay.off_w0),
                  reinterpret_cast<TA*>(w + lay.off_w1)};
+    TA* y = reinterpret_cast<TA*>(w + lay.off_y);
     TB* V = reinterpret_cast<TB*>(w + lay.off_v);
     double* partials = reinterpret_cast<double*>(w + lay.off_partials);
     const TA* va;
@@ -463,47 +549,56 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
     h.reduction = reduction;
     h.inner_reduction = inner_reduction;
     h.cycle_done = 1;
+    h.idle = 1;
+    h.minus_one = -1.0;
+    h.one = 1.0;
     B2S_CUDA_TRY(cudaMemcpyAsync(gs, &h, sizeof(h), cudaMemcpyHostToDevice, st));
 
-    const int sw = solver_subwarp(max_row_nnz);
-    const int grid_spmv = int(std::min<int64_t>(
-        std::max<int64_t>(1, ceildiv(n * sw, kSolverBlock)), kSolverGrid));
     const int grid_vec = int(std::min<int64_t>(
         std::max<int64_t>(1, ceildiv(n, kSolverBlock)), kSolverGrid));
-    constexpr int M = kMaxKrylov;
-    // first residual outside the graph
-    B2S_DISPATCH_SW(sw, {
-        gmres_residual_kernel<SW><<<grid_spmv, kSolverBlock, 0, st>>>(
-            n, rp, ci, v64, x, b, r, gs, partials);
-    });
+    const int grid_dots = int(std::min<int64_t>(
+        std::max<int64_t>(1, ceildiv(n, 2 * kSolverBlock)), int64_t(kNumSMs) * 2));
+    // pipelined SpMV: persistent grid, as many blocks as fit at once
+    const int lpr = async_lanes_per_row(max_row_nnz);
+    const int64_t async_need = ceildiv(ceildiv(n, kWarp / lpr), kAsyncBlock / kWarp);
+    // x += D^-1 V y and r = b; r -= A x (FP64); ||r||, ||b|| and the check
+    auto restart = [&](cudaStream_t cs) {
+        gmres_xupdate_kernel<TA, TB><<<grid_vec, kSolverBlock, 0, cs>>>(n, V, da, x, b,
+                                                                        r, gs);
+        with_async_kernel<double, 1, false>(lpr, [&](auto kernel) {
+            const int64_t grid = std::min<int64_t>(async_need, async_resident_blocks(kernel));
+            kernel<<<grid, kAsyncBlock, 0, cs>>>(n, rp, ci, v64, x, 1, r, 1,
+                                                 &gs->minus_one, &gs->one, &gs->done);
+        });
+        gmres_restart_kernel<<<grid_vec, kSolverBlock, 0, cs>>>(n, r, b, gs, partials);
+    };
+    // first residual outside the graph (final_iter = 0: x is not touched)
+    restart(st);
     B2S_LAUNCH_CHECK();
     auto capture = [&](cudaStream_t cs) -> int {
         for (int j = 0; j < krylov_dim; ++j) {
             TA* src = wv[(j + 1) % 2];
             TA* dst = wv[j % 2];
-            B2S_DISPATCH_SW(sw, {
-                gmres_spmv_kernel<TA, TB, SW><<<grid_spmv, kSolverBlock, 0, cs>>>(
-                    n, rp, ci, va, da, r, src, dst, V, gs);
+            gmres_prepare_kernel<TA, TB><<<grid_vec, kSolverBlock, 0, cs>>>(
+                n, da, r, src, V, y, gs);
+            with_async_kernel<TA, 1, false>(lpr, [&](auto kernel) {
+                const int64_t grid = std::min<int64_t>(async_need,
+                                                       async_resident_blocks(kernel));
+                kernel<<<grid, kAsyncBlock, 0, cs>>>(n, rp, ci, va, y, 1, dst, 1,
+                                                     nullptr, nullptr, &gs->idle);
             });
-            gmres_dot_kernel<TA, TB, M><<<grid_vec, kSolverBlock, 0, cs>>>(
+            gmres_dots_kernel<TA, TB><<<grid_dots, kSolverBlock, 0, cs>>>(
                 n, V, dst, gs, partials);
-            gmres_orth_kernel<TA, TB, M><<<grid_vec, kSolverBlock, 0, cs>>>(
-                n, V, dst, gs, partials);
-            gmres_orth2_kernel<TA, TB, M><<<grid_vec, kSolverBlock, 0, cs>>>(
+            gmres_update_kernel<TA, TB><<<grid_vec, kSolverBlock, 0, cs>>>(
                 n, V, dst, gs, partials);
             B2S_LAUNCH_CHECK();
         }
-        gmres_update_kernel<TA, TB, M><<<grid_vec, kSolverBlock, 0, cs>>>(
-            n, V, da, x, gs);
-        B2S_DISPATCH_SW(sw, {
-            gmres_residual_kernel<SW><<<grid_spmv, kSolverBlock, 0, cs>>>(
-                n, rp, ci, v64, x, b, r, gs, partials);
-        });
+        restart(cs);
         B2S_LAUNCH_CHECK();
         return B2S_OK;
     };
-    // the spmv of step j reads the vector written at step j - 1: the graph
-    // alternates w buffers inside a cycle and every cycle restarts from r
+    // the spmv of step j reads the vector prepared at step j; the update of
+    // step j - 1 wrote the other w buffer, which prepare reads
     cudaStream_t cap;
     B2S_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
     cudaGraph_t graph = nullptr;
@@ -520,13 +615,13 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
         if (e != cudaSuccess) { set_error("instantiate: %s", cudaGetErrorString(e)); rc = B2S_ERR_CUDA; break; }
         // each cycle either finishes or advances >= 1 iteration
         const int64_t max_cycles = max_iters + 2;
-        GmresState hs;
+        int done = 0;
         for (int64_t cyc = 0; cyc < max_cycles; ++cyc) {
-            e = cudaMemcpyAsync(&hs.done, &gs->done, sizeof(int),
+            e = cudaMemcpyAsync(&done, &gs->done, sizeof(int),
                                 cudaMemcpyDeviceToHost, st);
             if (e == cudaSuccess) e = cudaStreamSynchronize(st);
             if (e != cudaSuccess) { set_error("replay: %s", cudaGetErrorString(e)); rc = B2S_ERR_CUDA; break; }
-            if (hs.done) break;
+            if (done) break;
             e = cudaGraphLaunch(exec, st);
             if (e != cudaSuccess) { set_error("replay: %s", cudaGetErrorString(e)); rc = B2S_ERR_CUDA; break; }
         }

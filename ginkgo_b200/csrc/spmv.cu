@@ -9,6 +9,7 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "csr_async.cuh"
 
 namespace b2s {
 namespace {
@@ -376,91 +377,6 @@ __global__ void __launch_bounds__(kBlock)
 }
 
 // ---------------------------------------------------------------------------
-// Csr, one and two right-hand sides: each warp owns 32 consecutive rows and
-// streams their entries [rp[r0], rp[r0 + 32]) with fully coalesced loads into
-// shared memory as products val * b(col, :); every lane then sums its own row
-// in order, so a row is reduced exactly as the reference's sequential loop
-// does (reference/matrix/csr_kernels.cpp:65-74).  A group with more than CAP
-// entries (long rows) is reduced row by row by the whole warp.
-// ---------------------------------------------------------------------------
-template <typename T, int K, bool VEC>
-__global__ void __launch_bounds__(kBlock)
-    csr_stream_kernel(int64_t n, const int32_t* __restrict__ rp,
-                      const int32_t* __restrict__ ci, const T* __restrict__ v,
-                      const T* __restrict__ b, int64_t ldb, T* __restrict__ c,
-                      int64_t ldc, const T* __restrict__ alpha,
-                      const T* __restrict__ beta)
-{
-    constexpr int CAP = 256 / K;   // staged entries per warp
-    constexpr int PER = CAP / kWarp;
-    constexpr unsigned kFull = 0xffffffffu;
-    __shared__ T prod[kBlock / kWarp][CAP * K];
-    const int lane = threadIdx.x % kWarp, wid = threadIdx.x / kWarp;
-    const int64_t row0 = (blockIdx.x * int64_t(kBlock)) + wid * kWarp;
-    const int64_t row = row0 + lane;
-    const int rs = __ldg(rp + (row < n ? row : n));
-    int re = __shfl_down_sync(kFull, rs, 1);
-    if (lane == kWarp - 1) re = __ldg(rp + (row0 + kWarp < n ? row0 + kWarp : n));
-    const int start = __shfl_sync(kFull, rs, 0);
-    const int cnt = __shfl_sync(kFull, re, kWarp - 1) - start;
-    T acc[K];
-#pragma unroll
-    for (int j = 0; j < K; ++j) acc[j] = T(0);
-    if (cnt <= CAP) {
-        T* pw = prod[wid];
-        T vals[PER];
-        int32_t cols[PER];
-#pragma unroll
-        for (int q = 0; q < PER; ++q) {
-            const int i = lane + q * kWarp;
-            if (i < cnt) {
-                vals[q] = ld_stream(v + start + i);
-                cols[q] = ld_stream(ci + start + i);
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < PER; ++q) {
-            const int i = lane + q * kWarp;
-            if (i < cnt) {
-                T xr[K];
-                RowLoad<T, K, VEC>::load(b + int64_t(cols[q]) * ldb, xr);
-#pragma unroll
-                for (int j = 0; j < K; ++j) pw[i * K + j] = vals[q] * xr[j];
-            }
-        }
-        __syncwarp();
-        for (int i = rs - start; i < re - start; ++i) {
-#pragma unroll
-            for (int j = 0; j < K; ++j) acc[j] += pw[i * K + j];
-        }
-    } else {
-        for (int l = 0; l < kWarp; ++l) {
-            const int s = __shfl_sync(kFull, rs, l), e = __shfl_sync(kFull, re, l);
-            T a[K];
-#pragma unroll
-            for (int j = 0; j < K; ++j) a[j] = T(0);
-            for (int ee = s + lane; ee < e; ee += kWarp) {
-                const T val = ld_stream(v + ee);
-                T xr[K];
-                RowLoad<T, K, VEC>::load(b + int64_t(ld_stream(ci + ee)) * ldb, xr);
-#pragma unroll
-                for (int j = 0; j < K; ++j) a[j] += val * xr[j];
-            }
-#pragma unroll
-            for (int j = 0; j < K; ++j) {
-                a[j] = warp_sum(a[j]);
-                if (lane == l) acc[j] = a[j];
-            }
-        }
-    }
-    if (row < n) {
-        T* dst = c + row * ldc;
-#pragma unroll
-        for (int j = 0; j < K; ++j) dst[j] = combine(acc[j], alpha, beta, dst + j);
-    }
-}
-
-// ---------------------------------------------------------------------------
 // Four or more right-hand sides: KL = K / VW lanes share one row and each
 // owns VW consecutive columns (one 16-byte vector), so the lanes of a row
 // read one contiguous stretch of b(col, :) and write one of c(row, :); the
@@ -698,16 +614,21 @@ int csr_spmv(int strategy, int64_t n, int64_t num_cols, const int32_t* rp,
                                       ldb, cc, ldc, alpha, beta, st);
             });
         } else if (kk <= 2) {
-            const int64_t grid = ceildiv(n, kBlock);
+            // persistent: as many blocks as fit on the SMs at once; rows of
+            // the longest length share a stage 32 / lpr at a time
+            const int lpr = async_lanes_per_row(max_row_nnz);
+            const int64_t need = ceildiv(ceildiv(n, kWarp / lpr), kAsyncBlock / kWarp);
+            auto launch = [&](auto kernel) {
+                const int64_t grid = std::min<int64_t>(need, async_resident_blocks(kernel));
+                kernel<<<grid, kAsyncBlock, 0, st>>>(n, rp, ci, v, bb, ldb, cc, ldc,
+                                                     alpha, beta, nullptr);
+            };
             if (kk == 2 && vec) {
-                csr_stream_kernel<T, 2, true><<<grid, kBlock, 0, st>>>(
-                    n, rp, ci, v, bb, ldb, cc, ldc, alpha, beta);
+                with_async_kernel<T, 2, true>(lpr, launch);
             } else if (kk == 2) {
-                csr_stream_kernel<T, 2, false><<<grid, kBlock, 0, st>>>(
-                    n, rp, ci, v, bb, ldb, cc, ldc, alpha, beta);
+                with_async_kernel<T, 2, false>(lpr, launch);
             } else {
-                csr_stream_kernel<T, 1, false><<<grid, kBlock, 0, st>>>(
-                    n, rp, ci, v, bb, ldb, cc, ldc, alpha, beta);
+                with_async_kernel<T, 1, false>(lpr, launch);
             }
         } else {
             B2S_DISPATCH_K(kk, VEC, {

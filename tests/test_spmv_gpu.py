@@ -95,6 +95,31 @@ def test_random_power_law_matches_oracle(exe, fmt, dt, k):
                       alpha=0.5, beta_y=2.0 * y0.astype(np.float64))
 
 
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+@pytest.mark.parametrize("k", [1, 2])
+def test_classical_every_group_width(exe, dt, k):
+    # The pipelined kernel groups 32 / lpr rows per warp, lpr chosen from
+    # the longest row; the row-length bound handed to it only changes the
+    # grouping, so every width (and groups that overflow a stage) must give
+    # the same result.  Rows of 0..60 entries, a few of 400.
+    rng = np.random.default_rng(21 + k)
+    n = 30001
+    lens = rng.integers(0, 61, n)
+    lens[rng.choice(n, 20, replace=False)] = 400
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    ci = np.concatenate([rng.choice(n, l, replace=False) for l in lens]).astype(np.int32)
+    v = rng.standard_normal(int(rp[-1])).astype(NP[dt])
+    x = rng.standard_normal((n, k)).astype(NP[dt])
+    ref = orc.csr_spmv(rp, ci, v, x)
+    A = Csr.read(exe, rp, ci, v, dtype=dt)
+    xd = torch.from_numpy(x).cuda()
+    for bound in (1, 8, 16, 32, 64, 128, 256, 400):
+        A._max_row_nnz = bound
+        y = torch.full((n, k), float("nan"), dtype=dt, device="cuda")
+        A.apply(xd, y)
+        assert_spmv_close(rp, ci, v, x, y.cpu().numpy(), ref, TOL[dt])
+
+
 @pytest.mark.parametrize("fmt", ["classical", "load_balance"])
 def test_empty_rows_and_single_long_row(exe, fmt):
     n = 9000
