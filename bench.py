@@ -193,10 +193,16 @@ def main():
                     help="also time every format / precision / k on matrix A")
     ap.add_argument("--no-solve", action="store_true",
                     help="skip the time-to-1e-10 mixed vs FP64 GMRES section")
+    ap.add_argument("--solve-case", choices=["f64", "ir_f32", "ir_bf16"],
+                    help="profiling aid: run one GMRES variant on the 27-point "
+                    "operator for --solve-iters iterations and exit")
+    ap.add_argument("--solve-iters", type=int, default=60)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
+    if args.solve_case:
+        return solve_case(args.solve_case, args.solve_iters)
 
     import torch
     world, rank, local = dist_env()
@@ -306,6 +312,46 @@ def main():
         torch.distributed.destroy_process_group()
 
 
+def gmres_variants(max_iters):
+    """GMRES(30) + scalar Jacobi to 1e-10: plain FP64, and iterative
+    refinement around an FP32 / BF16-basis inner cycle."""
+    from ginkgo_b200.solver import Gmres, Ir, Iteration, Jacobi, ResidualNorm
+    crit = (Iteration.build().with_max_iters(max_iters),
+            ResidualNorm.build().with_reduction_factor(1e-10))
+    jac = Jacobi.build().with_max_block_size(1)
+    return {
+        "f64": Gmres.build().with_krylov_dim(30).with_criteria(*crit)
+        .with_preconditioner(jac),
+        "ir_f32": Ir.build().with_criteria(*crit).with_solver(
+            Gmres.build().with_krylov_dim(30).with_storage_precision("f32")
+            .with_preconditioner(jac)),
+        "ir_bf16": Ir.build().with_criteria(*crit).with_solver(
+            Gmres.build().with_krylov_dim(30).with_storage_precision("bf16")
+            .with_preconditioner(jac)),
+    }
+
+
+def solve_case(name, iters, grid=96):
+    """One capped solve of one variant on the 27-point operator, untimed:
+    the workload of the GMRES kernel profiles."""
+    import torch
+    from ginkgo_b200 import stencils
+    from ginkgo_b200.matrix import Csr, CudaExecutor
+    exe = CudaExecutor.create(0)
+    rp, ci, v = stencils.anisotropic_27pt(grid)
+    n = len(rp) - 1
+    A = Csr.read(exe, rp, ci, v)
+    b = torch.from_numpy(np.random.default_rng(3).standard_normal(n)).cuda()
+    s = gmres_variants(iters)[name].on(exe).generate(A)
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    s.apply(b, x)
+    torch.cuda.synchronize()
+    print(json.dumps({"solve_case": name, "workload": f"aniso27_{grid}",
+                      "iterations": s.logger.num_iterations,
+                      "residual_norm": np.asarray(s.logger.residual_norm,
+                                                 dtype=float).tolist()}))
+
+
 def ir_gmres_section(exe, stream, grid=96, reps=3):
     """Time to a relative residual of 1e-10 (verified on the explicit FP64
     residual) on the 3D 27-point anisotropic operator (96^3, coefficients
@@ -316,24 +362,11 @@ def ir_gmres_section(exe, stream, grid=96, reps=3):
     import torch
     from ginkgo_b200 import stencils
     from ginkgo_b200.matrix import Csr
-    from ginkgo_b200.solver import Gmres, Ir, Iteration, Jacobi, ResidualNorm
     rp, ci, v = stencils.anisotropic_27pt(grid)
     n = len(rp) - 1
     A = Csr.read(exe, rp, ci, v)
     b = torch.from_numpy(np.random.default_rng(3).standard_normal(n)).cuda()
-    crit = (Iteration.build().with_max_iters(20000),
-            ResidualNorm.build().with_reduction_factor(1e-10))
-    jac = Jacobi.build().with_max_block_size(1)
-    variants = {
-        "f64": Gmres.build().with_krylov_dim(30).with_criteria(*crit)
-        .with_preconditioner(jac),
-        "ir_f32": Ir.build().with_criteria(*crit).with_solver(
-            Gmres.build().with_krylov_dim(30).with_storage_precision("f32")
-            .with_preconditioner(jac)),
-        "ir_bf16": Ir.build().with_criteria(*crit).with_solver(
-            Gmres.build().with_krylov_dim(30).with_storage_precision("bf16")
-            .with_preconditioner(jac)),
-    }
+    variants = gmres_variants(20000)
     out = {"workload": f"aniso27_{grid}", "n": n, "nnz": len(ci),
            "krylov_dim": 30, "goal": 1e-10}
     sols = {}
