@@ -29,8 +29,9 @@
 //   spmv    w = A y with the pipelined Csr kernel (values and column
 //           indices of the next row group copied with cp.async while the
 //           current group is summed)
-//   dots    h1 = V_{0..j}^T w and G(:, j) = V_{0..j}^T v_j, eight basis
-//           vectors per pass over the rows; last block: h = (2I - G) h1
+//   dots    h1 = V_{0..j}^T w and G(:, j) = V_{0..j}^T v_j in one pass over
+//           the basis (all sums of a thread in registers); last block:
+//           h = (2I - G) h1
 //   update  w'' = w - V h and ||w''||; last block: Hessenberg column,
 //           Givens update, residual estimate, early end of the cycle, back
 //           substitution
@@ -86,145 +87,271 @@ __device__ __forceinline__ float from_basis<float, __nv_bfloat16>(__nv_bfloat16 
     return __bfloat162float(v);
 }
 
+// Row groups: every streamed vector (basis, w, y) has a leading dimension
+// that is a multiple of 64 rows, so the R = 16 / sizeof(TB) rows of a group
+// start on a 16-byte boundary and move as 16-byte vector loads.  The group
+// that holds row n - 1 may be partial and is read element by element.
+template <typename T, int R>
+__device__ __forceinline__ void load_rows(const T* p, T (&o)[R])
+{
+    static_assert((R * sizeof(T)) % 16 == 0, "whole 16-byte vectors");
+    constexpr int NV = int(R * sizeof(T) / 16);
+    uint4 buf[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) buf[k] = reinterpret_cast<const uint4*>(p)[k];
+    const T* q = reinterpret_cast<const T*>(buf);
+#pragma unroll
+    for (int r = 0; r < R; ++r) o[r] = q[r];
+}
+template <typename T, int R>
+__device__ __forceinline__ void store_rows(T* p, const T (&v)[R])
+{
+    constexpr int NV = int(R * sizeof(T) / 16);
+    uint4 buf[NV];
+    T* q = reinterpret_cast<T*>(buf);
+#pragma unroll
+    for (int r = 0; r < R; ++r) q[r] = v[r];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) reinterpret_cast<uint4*>(p)[k] = buf[k];
+}
+// rows r < valid of the group, zero past the end
+template <typename T, int R>
+__device__ __forceinline__ void load_rows(const T* p, T (&o)[R], int valid)
+{
+    if (valid >= R) {
+        load_rows<T, R>(p, o);
+    } else {
+#pragma unroll
+        for (int r = 0; r < R; ++r) o[r] = r < valid ? p[r] : T(0);
+    }
+}
+template <typename T, int R>
+__device__ __forceinline__ void store_rows(T* p, const T (&v)[R], int valid)
+{
+    if (valid >= R) {
+        store_rows<T, R>(p, v);
+    } else {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            if (r < valid) p[r] = v[r];
+        }
+    }
+}
+// basis rows converted to the arithmetic type
+template <typename TA, typename TB, int R>
+__device__ __forceinline__ void load_basis(const TB* p, TA (&o)[R], int valid)
+{
+    TB b[R];
+    load_rows<TB, R>(p, b, valid);
+#pragma unroll
+    for (int r = 0; r < R; ++r) o[r] = from_basis<TA>(b[r]);
+}
+
+template <typename TB>
+__host__ __device__ constexpr int rows_per_group()
+{
+    return int(16 / sizeof(TB));
+}
+
 // Step j, part 1: v_j = round_basis(src * scale) stored in the basis and
 // y = D^-1 v_j, the SpMV input (src = the previous unnormalised vector, or
-// r at j = 0).  One pass over n entries.
+// r at j = 0).  One row group per thread and iteration.
 template <typename TA, typename TB>
 __global__ void __launch_bounds__(kSolverBlock)
-    gmres_prepare_kernel(int64_t n, const TA* __restrict__ dinv,
+    gmres_prepare_kernel(int64_t n, int64_t ldv, const TA* __restrict__ dinv,
                          const double* __restrict__ r64,
                          const TA* __restrict__ w_src, TB* __restrict__ V,
                          TA* __restrict__ y, GmresState* st)
 {
+    constexpr int R = rows_per_group<TB>();
     if (st->idle) return;
     const int j = st->j;
     const TA scale = TA(st->scale);
-    TB* vj = V + int64_t(j) * n;
-    for (int64_t row = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; row < n;
-         row += int64_t(gridDim.x) * kSolverBlock) {
-        const TA src = j == 0 ? TA(r64[row]) : w_src[row];
-        const TB vb = to_basis<TB>(mul_rn(src, scale));
-        vj[row] = vb;
-        const TA va = from_basis<TA>(vb);
-        y[row] = dinv ? dinv[row] * va : va;
+    TB* vj = V + int64_t(j) * ldv;
+    const int64_t groups = ceildiv(n, R);
+    for (int64_t q = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; q < groups;
+         q += int64_t(gridDim.x) * kSolverBlock) {
+        const int64_t r0 = q * R;
+        const int valid = n - r0 < R ? int(n - r0) : R;
+        TA src[R], d[R];
+        if (j == 0) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) src[r] = r < valid ? TA(r64[r0 + r]) : TA(0);
+        } else {
+            load_rows<TA, R>(w_src + r0, src, valid);
+        }
+        if (dinv) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) d[r] = r < valid ? dinv[r0 + r] : TA(0);
+        }
+        TB vb[R];
+        TA yv[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            vb[r] = to_basis<TB>(mul_rn(src[r], scale));
+            const TA va = from_basis<TA>(vb[r]);
+            yv[r] = dinv ? d[r] * va : va;
+        }
+        store_rows<TB, R>(vj + r0, vb, valid);
+        store_rows<TA, R>(y + r0, yv, valid);
     }
 }
 
-// Sums each of the 16 values v[0..15] over the warp with 16 shuffles (a
-// butterfly that halves the values a lane carries at every level, instead
-// of 16 separate reductions of 5 shuffles each).  Returns, in lane l, the
-// warp total of value l / 2.
-__device__ __forceinline__ double butterfly16(double (&v)[16], int lane)
+// Sums each of the N values v[0..N) (N = 32 P) over the warp with N - P
+// shuffles: every level of the butterfly hands half of the values a lane
+// carries to its partner.  On return lane l holds the totals of values
+// l P + k in v[k], k < P.
+template <typename T, int N>
+__device__ __forceinline__ void warp_multi_sum(T (&v)[N], int lane)
 {
+    static_assert(N % 32 == 0, "32 P values");
     constexpr unsigned kFull = 0xffffffffu;
 #pragma unroll
-    for (int half = 8; half >= 1; half /= 2) {
-        const bool up = lane & (2 * half);
+    for (int lvl = 0; lvl < 5; ++lvl) {
+        const int m = 16 >> lvl;
+        const int half = N >> (lvl + 1);
+        const bool up = lane & m;
 #pragma unroll
         for (int i = 0; i < half; ++i) {
-            const double send = up ? v[i] : v[i + half];
-            const double keep = up ? v[i + half] : v[i];
-            v[i] = keep + __shfl_xor_sync(kFull, send, 2 * half);
+            const T send = up ? v[i] : v[i + half];
+            const T keep = up ? v[i + half] : v[i];
+            v[i] = keep + __shfl_xor_sync(kFull, send, m);
         }
     }
-    return v[0] + __shfl_xor_sync(kFull, v[0], 1);
 }
 
-// Step j, part 3: h1 = V_{0..j}^T w and G(:, j) = V_{0..j}^T v_j, eight
-// basis vectors per pass over the rows (w and v_j stay in L1/L2 between
-// passes), two rows per thread and iteration.  Launched with a few blocks
-// per SM, so the per-pass block reduction is amortised over many rows.
-// Partials: per block 2 * kLd entries.  The last block completes G's row
-// and column j and forms h = (2I - G) h1.
+// One pass of the dots kernel over C basis vectors i0 .. i0 + C - 1 (C a
+// compile-time count, so the C 16-byte loads of a row group are issued
+// back to back without predicates): acc[u] += V_{i0+u}^T w and
+// acc[16 + u] += V_{i0+u}^T v_j over this thread's row groups.
+template <typename TA, typename TB, int C>
+__device__ __forceinline__ void dots_pass(int64_t n, int64_t ldv,
+                                          const TB* __restrict__ V,
+                                          const TA* __restrict__ w,
+                                          const TB* __restrict__ vj, int i0,
+                                          TA (&acc)[32])
+{
+    constexpr int R = rows_per_group<TB>();
+    const int64_t groups = ceildiv(n, R);
+    for (int64_t grp = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; grp < groups;
+         grp += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t r0 = grp * R;
+        const int valid = n - r0 < R ? int(n - r0) : R;
+        TA wr[R], vr[R];
+        load_rows<TA, R>(w + r0, wr, valid);
+        load_basis<TA, TB, R>(vj + r0, vr, valid);
+#pragma unroll
+        for (int u = 0; u < C; ++u) {
+            TA x[R];
+            load_basis<TA, TB, R>(V + int64_t(i0 + u) * ldv + r0, x, valid);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                acc[u] += x[r] * wr[r];
+                acc[16 + u] += x[r] * vr[r];
+            }
+        }
+    }
+}
+
+constexpr int kDotsBlock = 512;
+constexpr int kDotsMaxGrid = 160;  // the final reduction reads 20 per lane
+
+// In the last block: out[c] = sum over b < B of part[e(c) * B + b] for the
+// E values c < E (e(c) = c for c < half, kLd + c - half after), in a fixed
+// order: lane k of an 8-lane group sums b = k, k + 8, ... with all of its
+// loads in flight at once, then the group combines its 8 sums.
+__device__ __forceinline__ void reduce_value_major(const double* part, int B, int E,
+                                                   int half, double* out)
+{
+    const int sub = threadIdx.x % 8, grp = threadIdx.x / 8;
+    const int ngrp = blockDim.x / 8;
+    for (int c0 = 0; c0 < E; c0 += ngrp) {
+        const int c = c0 + grp;
+        double s = 0.0;
+        if (c < E) {
+            const int e = c < half ? c : kLd + c - half;
+            const double* p = part + int64_t(e) * B;
+            double v[kDotsMaxGrid / 8];
+#pragma unroll
+            for (int k = 0; k < kDotsMaxGrid / 8; ++k) {
+                const int b = sub + 8 * k;
+                v[k] = b < B ? __ldcg(p + b) : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < kDotsMaxGrid / 8; ++k) s += v[k];
+        }
+        s = subwarp_sum<8>(s);
+        if (sub == 0 && c < E) out[c] = s;
+    }
+}
+
+// Step j, part 3: h1 = V_{0..j}^T w and G(:, j) = V_{0..j}^T v_j: passes of
+// up to CMAX basis vectors (16 for FP32 arithmetic, 8 for FP64), a thread
+// taking one row group per iteration with all sums of the pass in
+// registers; one block of 512 threads per SM.  Per pass one multi-value
+// warp reduction and one block reduction; partials are value-major
+// (partials[e * gridDim.x + block], e < 2 kLd).  The last block reduces
+// them, completes G's row and column j and forms h = (2I - G) h1.
 template <typename TA, typename TB>
-__global__ void __launch_bounds__(kSolverBlock)
-    gmres_dots_kernel(int64_t n, const TB* __restrict__ V,
+__global__ void __launch_bounds__(kDotsBlock, 1)
+    gmres_dots_kernel(int64_t n, int64_t ldv, const TB* __restrict__ V,
                       const TA* __restrict__ w, GmresState* st,
                       double* __restrict__ partials)
 {
-    constexpr int C = 8;
-    __shared__ double red[kSolverBlock / kWarp][2 * C];
+    constexpr int CMAX = sizeof(TA) == 8 ? 8 : 16;
+    constexpr int W = kDotsBlock / kWarp;
+    __shared__ double red[W][32];
     __shared__ double tot[2 * kLd];
     __shared__ double Gs[kLd * kLd];
     __shared__ int last;
     if (st->idle) return;
     const int j = st->j;
+    const int nvec = j + 1;
     const int lane = threadIdx.x % kWarp, wid = threadIdx.x / kWarp;
-    const TB* vj = V + int64_t(j) * n;
-    double* part = partials + int64_t(blockIdx.x) * 2 * kLd;
-    const int64_t stride = int64_t(gridDim.x) * kSolverBlock;
-    for (int i0 = 0; i0 <= j; i0 += C) {
-        const int nv = j + 1 - i0 < C ? j + 1 - i0 : C;  // vectors this pass
-        TA a[C], g[C];
+    const TB* vj = V + int64_t(j) * ldv;
+    const int B = gridDim.x;
+    for (int i0 = 0; i0 < nvec; i0 += CMAX) {
+        const int c = nvec - i0 < CMAX ? nvec - i0 : CMAX;
+        TA acc[32];
 #pragma unroll
-        for (int u = 0; u < C; ++u) a[u] = g[u] = TA(0);
-        int64_t row = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x;
-        for (; row + stride < n; row += 2 * stride) {
-            const int64_t r1 = row + stride;
-            const TA w0 = w[row], w1 = w[r1];
-            const TA v0 = from_basis<TA>(vj[row]), v1 = from_basis<TA>(vj[r1]);
-            TA x0[C], x1[C];
-#pragma unroll
-            for (int u = 0; u < C; ++u) {
-                if (u < nv) {
-                    x0[u] = from_basis<TA>(V[int64_t(i0 + u) * n + row]);
-                    x1[u] = from_basis<TA>(V[int64_t(i0 + u) * n + r1]);
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < C; ++u) {
-                if (u < nv) {
-                    a[u] += x0[u] * w0;
-                    g[u] += x0[u] * v0;
-                    a[u] += x1[u] * w1;
-                    g[u] += x1[u] * v1;
-                }
-            }
+        for (int u = 0; u < 32; ++u) acc[u] = TA(0);
+        switch (c) {
+#define B2S_DOTS_CASE(K)                                                          \
+    case K:                                                                       \
+        if constexpr (K <= CMAX) dots_pass<TA, TB, K>(n, ldv, V, w, vj, i0, acc); \
+        break;
+            B2S_DOTS_CASE(1) B2S_DOTS_CASE(2) B2S_DOTS_CASE(3) B2S_DOTS_CASE(4)
+            B2S_DOTS_CASE(5) B2S_DOTS_CASE(6) B2S_DOTS_CASE(7) B2S_DOTS_CASE(8)
+            B2S_DOTS_CASE(9) B2S_DOTS_CASE(10) B2S_DOTS_CASE(11) B2S_DOTS_CASE(12)
+            B2S_DOTS_CASE(13) B2S_DOTS_CASE(14) B2S_DOTS_CASE(15) B2S_DOTS_CASE(16)
+#undef B2S_DOTS_CASE
+        default: break;
         }
-        if (row < n) {
-            const TA w0 = w[row];
-            const TA v0 = from_basis<TA>(vj[row]);
-#pragma unroll
-            for (int u = 0; u < C; ++u) {
-                if (u < nv) {
-                    const TA x0 = from_basis<TA>(V[int64_t(i0 + u) * n + row]);
-                    a[u] += x0 * w0;
-                    g[u] += x0 * v0;
-                }
-            }
-        }
-        double vals[2 * C];
-#pragma unroll
-        for (int u = 0; u < C; ++u) {
-            vals[u] = double(a[u]);
-            vals[C + u] = double(g[u]);
-        }
-        const double t = butterfly16(vals, lane);
-        if ((lane & 1) == 0) red[wid][lane / 2] = t;
+        warp_multi_sum<TA, 32>(acc, lane);
+        red[wid][lane] = double(acc[0]);  // lane l: value l
         __syncthreads();
-        if (threadIdx.x < 2 * C) {
-            const int u = threadIdx.x % C;
-            if (u < nv) {
-                double sum = 0.0;
-                for (int k = 0; k < kSolverBlock / kWarp; ++k) sum += red[k][threadIdx.x];
-                part[(threadIdx.x < C ? 0 : kLd) + i0 + u] = sum;
+        if (threadIdx.x < 32) {
+            const int u = threadIdx.x % 16;
+            if (u < c) {
+                double s = 0.0;
+                for (int k = 0; k < W; ++k) s += red[k][threadIdx.x];
+                const int e = (threadIdx.x < 16 ? 0 : kLd) + i0 + u;
+                partials[int64_t(e) * B + blockIdx.x] = s;
             }
         }
         __syncthreads();
     }
     if (last_block_done(&st->ticket, &last)) {
-        // block-ordered sums of the 2 (j + 1) used entries
-        for (int e = wid; e < 2 * kLd; e += kSolverBlock / kWarp) {
-            if ((e % kLd) > j) continue;
-            double s = 0.0;
-            for (int b = lane; b < int(gridDim.x); b += kWarp) {
-                s += __ldcg(partials + int64_t(b) * 2 * kLd + e);
-            }
-            s = warp_sum(s);
-            if (lane == 0) tot[e] = s;
+        // tot[0..nvec): h1, tot[kLd + i]: G(i, j)
+        double* tv = Gs;  // scratch for the 2 nvec sums before Gs is staged
+        reduce_value_major(partials, B, 2 * nvec, nvec, tv);
+        __syncthreads();
+        for (int c = threadIdx.x; c < 2 * nvec; c += kDotsBlock) {
+            tot[c < nvec ? c : kLd + c - nvec] = tv[c];
         }
+        __syncthreads();
         // G(0..j-1, 0..j-1) from the earlier steps of this cycle
-        for (int e = threadIdx.x; e < j * kLd; e += kSolverBlock) Gs[e] = st->G[e];
+        for (int e = threadIdx.x; e < j * kLd; e += kDotsBlock) Gs[e] = st->G[e];
         __syncthreads();
         if (threadIdx.x <= j) {
             const int i = threadIdx.x;
@@ -330,12 +457,16 @@ __device__ void close_step(GmresState* st, double hnorm)
     }
 }
 
-// w'' = w - V h, ||w''||; the last block closes the Arnoldi step.
+// w'' = w - V h, ||w''||, one row group per thread and iteration (16-byte
+// basis loads, subtracted in order i = 0..j); the last block closes the
+// Arnoldi step.
 template <typename TA, typename TB>
 __global__ void __launch_bounds__(kSolverBlock)
-    gmres_update_kernel(int64_t n, const TB* __restrict__ V, TA* __restrict__ w,
-                        GmresState* st, double* __restrict__ partials)
+    gmres_update_kernel(int64_t n, int64_t ldv, const TB* __restrict__ V,
+                        TA* __restrict__ w, GmresState* st,
+                        double* __restrict__ partials)
 {
+    constexpr int R = rows_per_group<TB>();
     __shared__ double red[kSolverBlock / kWarp];
     __shared__ double tot[1];
     __shared__ TA hs[kLd];
@@ -344,24 +475,25 @@ __global__ void __launch_bounds__(kSolverBlock)
     const int j = st->j;
     for (int i = threadIdx.x; i <= j; i += kSolverBlock) hs[i] = TA(st->h[i]);
     __syncthreads();
+    const int64_t groups = ceildiv(n, R);
     double nrm = 0.0;
-    for (int64_t row = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; row < n;
-         row += int64_t(gridDim.x) * kSolverBlock) {
-        TA wr = w[row];
-        // eight basis loads in flight, subtracted in order i = 0..j
-        for (int i0 = 0; i0 <= j; i0 += 8) {
-            TA x[8];
+    for (int64_t grp = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; grp < groups;
+         grp += int64_t(gridDim.x) * kSolverBlock) {
+        const int64_t r0 = grp * R;
+        const int valid = n - r0 < R ? int(n - r0) : R;
+        TA wr[R];
+        load_rows<TA, R>(w + r0, wr, valid);
+#pragma unroll 4
+        for (int i = 0; i <= j; ++i) {
+            TA x[R];
+            load_basis<TA, TB, R>(V + int64_t(i) * ldv + r0, x, valid);
+            const TA hi = hs[i];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                if (i0 + u <= j) x[u] = from_basis<TA>(V[int64_t(i0 + u) * n + row]);
-            }
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                if (i0 + u <= j) wr -= hs[i0 + u] * x[u];
-            }
+            for (int r = 0; r < R; ++r) wr[r] -= hi * x[r];
         }
-        w[row] = wr;
-        nrm += double(wr) * double(wr);
+        store_rows<TA, R>(w + r0, wr, valid);
+#pragma unroll
+        for (int r = 0; r < R; ++r) nrm += double(wr[r]) * double(wr[r]);
     }
     double a[1] = {nrm};
     block_partials<double, 1>(a, partials, red);
@@ -371,39 +503,50 @@ __global__ void __launch_bounds__(kSolverBlock)
     }
 }
 
-// x += D^-1 (V y) over the finished columns, accumulated into FP64 x, and
-// r = b (the start of r = b - A x).
+// x += D^-1 (V y) over the m finished columns, accumulated into FP64 x, and
+// r = b (the start of r = b - A x); one row group per thread and iteration.
 template <typename TA, typename TB>
 __global__ void __launch_bounds__(kSolverBlock)
-    gmres_xupdate_kernel(int64_t n, const TB* __restrict__ V,
+    gmres_xupdate_kernel(int64_t n, int64_t ldv, const TB* __restrict__ V,
                          const TA* __restrict__ dinv, double* __restrict__ x,
                          const double* __restrict__ b, double* __restrict__ r,
                          GmresState* st)
 {
+    constexpr int R = rows_per_group<TB>();
     __shared__ TA ys[kMaxKrylov];
     if (st->done) return;
     const int m = st->final_iter;
     for (int i = threadIdx.x; i < m; i += kSolverBlock) ys[i] = TA(st->y[i]);
     __syncthreads();
-    for (int64_t row = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; row < n;
-         row += int64_t(gridDim.x) * kSolverBlock) {
+    const int64_t groups = ceildiv(n, R);
+    for (int64_t grp = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; grp < groups;
+         grp += int64_t(gridDim.x) * kSolverBlock) {
+        const int64_t r0 = grp * R;
+        const int valid = n - r0 < R ? int(n - r0) : R;
         if (m > 0) {
-            TA u = TA(0);
-            for (int i0 = 0; i0 < m; i0 += 8) {
-                TA xv[8];
+            TA u[R];
 #pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    if (i0 + q < m) xv[q] = from_basis<TA>(V[int64_t(i0 + q) * n + row]);
-                }
+            for (int k = 0; k < R; ++k) u[k] = TA(0);
+#pragma unroll 4
+            for (int i = 0; i < m; ++i) {
+                TA xv[R];
+                load_basis<TA, TB, R>(V + int64_t(i) * ldv + r0, xv, valid);
+                const TA yi = ys[i];
 #pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    if (i0 + q < m) u += ys[i0 + q] * xv[q];
+                for (int k = 0; k < R; ++k) u[k] += yi * xv[k];
+            }
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+                if (k < valid) {
+                    const TA d = dinv ? dinv[r0 + k] : TA(1);
+                    x[r0 + k] += double(d * u[k]);
                 }
             }
-            const TA d = dinv ? dinv[row] : TA(1);
-            x[row] += double(d * u);
         }
-        r[row] = b[row];
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            if (k < valid) r[r0 + k] = b[r0 + k];
+        }
     }
 }
 
@@ -463,6 +606,9 @@ __global__ void float_copy_kernel(int64_t n, const double* __restrict__ src,
     if (i < n) dst[i] = float(src[i]);
 }
 
+// Leading dimension of the streamed vectors: a multiple of 64 rows.
+inline int64_t gmres_ld(int64_t n) { return ceildiv(n, 64) * 64; }
+
 struct GmresLayout {
     int64_t bytes, off_st, off_r, off_w0, off_w1, off_y, off_v, off_partials,
         off_a32, off_d32;
@@ -475,10 +621,11 @@ GmresLayout gmres_layout(int64_t n, int64_t nnz, int d, bool mixed)
     GmresLayout l;
     l.off_st = c.take<GmresState>(1);
     l.off_r = c.take<double>(n);
-    l.off_w0 = c.take<TA>(n);
-    l.off_w1 = c.take<TA>(n);
-    l.off_y = c.take<TA>(n);
-    l.off_v = c.take<TB>((int64_t(d) + 1) * n);
+    const int64_t ldv = gmres_ld(n);
+    l.off_w0 = c.take<TA>(ldv);
+    l.off_w1 = c.take<TA>(ldv);
+    l.off_y = c.take<TA>(ldv);
+    l.off_v = c.take<TB>((int64_t(d) + 1) * ldv);
     l.off_partials = c.take<double>(int64_t(kSolverGrid) * 2 * kLd);
     l.off_a32 = mixed ? c.take<float>(nnz) : 0;
     l.off_d32 = mixed ? c.take<float>(n) : 0;
@@ -516,6 +663,9 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
                   (long long)lay.bytes);
         return B2S_ERR_WORKSPACE;
     }
+    B2S_CHECK_ARG(reinterpret_cast<uintptr_t>(workspace) % 256 == 0,
+                  "GMRES workspace must be 256-byte aligned");
+    const int64_t ldv = gmres_ld(n);
     char* w = static_cast<char*>(workspace);
     auto* gs = reinterpret_cast<GmresState*>(w + lay.off_st);
     double* r = reinterpret_cast<double*>(w + lay.off_r);
@@ -557,14 +707,15 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
     const int grid_vec = int(std::min<int64_t>(
         std::max<int64_t>(1, ceildiv(n, kSolverBlock)), kSolverGrid));
     const int grid_dots = int(std::min<int64_t>(
-        std::max<int64_t>(1, ceildiv(n, 2 * kSolverBlock)), int64_t(kNumSMs) * 2));
+        std::max<int64_t>(1, ceildiv(ceildiv(n, rows_per_group<TB>()), kDotsBlock)),
+        std::min(kNumSMs, kDotsMaxGrid)));
     // pipelined SpMV: persistent grid, as many blocks as fit at once
     const int lpr = async_lanes_per_row(max_row_nnz);
     const int64_t async_need = ceildiv(ceildiv(n, kWarp / lpr), kAsyncBlock / kWarp);
     // x += D^-1 V y and r = b; r -= A x (FP64); ||r||, ||b|| and the check
     auto restart = [&](cudaStream_t cs) {
-        gmres_xupdate_kernel<TA, TB><<<grid_vec, kSolverBlock, 0, cs>>>(n, V, da, x, b,
-                                                                        r, gs);
+        gmres_xupdate_kernel<TA, TB><<<grid_vec, kSolverBlock, 0, cs>>>(n, ldv, V, da, x,
+                                                                        b, r, gs);
         with_async_kernel<double, 1, false>(lpr, [&](auto kernel) {
             const int64_t grid = std::min<int64_t>(async_need, async_resident_blocks(kernel));
             kernel<<<grid, kAsyncBlock, 0, cs>>>(n, rp, ci, v64, x, 1, r, 1,
@@ -580,17 +731,17 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
             TA* src = wv[(j + 1) % 2];
             TA* dst = wv[j % 2];
             gmres_prepare_kernel<TA, TB><<<grid_vec, kSolverBlock, 0, cs>>>(
-                n, da, r, src, V, y, gs);
+                n, ldv, da, r, src, V, y, gs);
             with_async_kernel<TA, 1, false>(lpr, [&](auto kernel) {
                 const int64_t grid = std::min<int64_t>(async_need,
                                                        async_resident_blocks(kernel));
                 kernel<<<grid, kAsyncBlock, 0, cs>>>(n, rp, ci, va, y, 1, dst, 1,
                                                      nullptr, nullptr, &gs->idle);
             });
-            gmres_dots_kernel<TA, TB><<<grid_dots, kSolverBlock, 0, cs>>>(
-                n, V, dst, gs, partials);
+            gmres_dots_kernel<TA, TB><<<grid_dots, kDotsBlock, 0, cs>>>(
+                n, ldv, V, dst, gs, partials);
             gmres_update_kernel<TA, TB><<<grid_vec, kSolverBlock, 0, cs>>>(
-                n, V, dst, gs, partials);
+                n, ldv, V, dst, gs, partials);
             B2S_LAUNCH_CHECK();
         }
         restart(cs);

@@ -193,6 +193,30 @@ def test_mixed_precision_ir_reaches_fp64_accuracy(exe, basis):
     assert s.logger.restarts >= 2
 
 
+@pytest.mark.parametrize("basis", [None, "f32", "bf16"])
+def test_gmres_ragged_row_count(exe, basis):
+    # 15^3 = 3375 rows: the last 16-byte row group of every basis vector is
+    # partial for each basis type (2, 4 or 8 rows per group)
+    rp, ci, v, n, b = _aniso(15)
+    A = Csr.read(exe, rp, ci, v)
+    g = (Gmres.build().with_krylov_dim(30)
+         .with_preconditioner(Jacobi.build().with_max_block_size(1)))
+    if basis is None:
+        s = g.with_criteria(*crit(3000, 1e-10)).on(exe).generate(A)
+    else:
+        s = (Ir.build().with_solver(g.with_storage_precision(basis))
+             .with_criteria(*crit(5000, 1e-10)).on(exe).generate(A))
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    s.apply(torch.from_numpy(b).cuda(), x)
+    assert s.logger.has_converged
+    assert explicit_rel_res(rp, ci, v, x.cpu().numpy(), b)[0] <= 1e-10
+    xo, _, _, conv_o = orc.gmres(rp, ci, v, b, krylov_dim=30, max_iters=3000,
+                                 reduction=1e-10)
+    assert conv_o
+    np.testing.assert_allclose(x.cpu().numpy(), xo, rtol=0,
+                               atol=1e-8 * np.abs(xo).max())
+
+
 def test_gmres_nonzero_initial_guess_and_exact_start(exe):
     rp, ci, v, n, b = _aniso(8)
     A = Csr.read(exe, rp, ci, v)
