@@ -1,0 +1,103 @@
+// Column-major (Ell-layout) SpMV with R consecutive rows per thread: the
+// values and column indices of entry k of rows r0 .. r0 + R - 1 are one
+// vector load each (16 bytes of values), so a warp moves 32 R entries per
+// instruction and the gathers of x for neighbouring rows stay coalesced for
+// banded matrices.  Used by the GMRES engine on its column-major copy of A.
+#pragma once
+
+#include <cstring>
+
+#include "common.cuh"
+
+namespace b2s {
+
+// R consecutive elements of 4, 8, 16 or 32 bytes in total, evict-first.
+template <typename T, int R>
+__device__ __forceinline__ void load_stream_rows(const T* p, T (&o)[R])
+{
+    constexpr int kBytes = int(R * sizeof(T));
+    static_assert(kBytes == 4 || kBytes == 8 || kBytes % 16 == 0, "vector width");
+    if constexpr (kBytes == 4) {
+        const unsigned u = __ldcs(reinterpret_cast<const unsigned*>(p));
+        memcpy(o, &u, 4);
+    } else if constexpr (kBytes == 8) {
+        const uint2 u = __ldcs(reinterpret_cast<const uint2*>(p));
+        memcpy(o, &u, 8);
+    } else {
+        uint4 u[kBytes / 16];
+#pragma unroll
+        for (int k = 0; k < kBytes / 16; ++k) u[k] = __ldcs(reinterpret_cast<const uint4*>(p) + k);
+        memcpy(o, u, kBytes);
+    }
+}
+
+// y(rows) = A x over an Ell-layout copy: entry k of row r at k * ld + r
+// (ld a multiple of R, every row group 16-byte aligned), padding entries
+// with column -1 and value 0.  Entries are summed in stored order.  A
+// launch whose *skip is non-zero returns at once.
+template <typename T, int R>
+__global__ void __launch_bounds__(256)
+    ell_rows_kernel(int64_t n, int width, int64_t ld,
+                    const int32_t* __restrict__ cols, const T* __restrict__ vals,
+                    const T* __restrict__ x, T* __restrict__ y,
+                    const int* __restrict__ skip)
+{
+    if (skip != nullptr && *skip) return;
+    const int64_t groups = (n + R - 1) / R;
+    for (int64_t grp = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; grp < groups;
+         grp += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t r0 = grp * R;
+        T acc[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) acc[r] = T(0);
+        const int32_t* cp = cols + r0;
+        const T* vp = vals + r0;
+#pragma unroll 4
+        for (int k = 0; k < width; ++k) {
+            int32_t c[R];
+            T v[R];
+            load_stream_rows<int32_t, R>(cp + int64_t(k) * ld, c);
+            load_stream_rows<T, R>(vp + int64_t(k) * ld, v);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const T xv = c[r] >= 0 ? __ldg(x + c[r]) : T(0);
+                acc[r] += v[r] * xv;
+            }
+        }
+        const int valid = n - r0 < R ? int(n - r0) : R;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            if (r < valid) y[r0 + r] = acc[r];
+        }
+    }
+}
+
+// Fills the Ell-layout copy (ld >= n rows, width entries per row) from Csr,
+// converting the values to T; rows n .. ld - 1 and the tail of shorter rows
+// are padding.  A row longer than width sets *too_long.
+template <typename T>
+__global__ void ell_fill_kernel(int64_t n, int64_t ld, int width,
+                                const int32_t* __restrict__ rp,
+                                const int32_t* __restrict__ ci,
+                                const double* __restrict__ v,
+                                int32_t* __restrict__ cols, T* __restrict__ vals,
+                                int* too_long)
+{
+    const int64_t row = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+    if (row >= ld) return;
+    const int rs = row < n ? rp[row] : 0;
+    const int len = row < n ? rp[row + 1] - rs : 0;
+    if (len > width) *too_long = 1;
+    for (int k = 0; k < width; ++k) {
+        const int64_t idx = int64_t(k) * ld + row;
+        if (k < len) {
+            cols[idx] = ci[rs + k];
+            vals[idx] = T(v[rs + k]);
+        } else {
+            cols[idx] = -1;
+            vals[idx] = T(0);
+        }
+    }
+}
+
+}  // namespace b2s

@@ -26,9 +26,9 @@
 // Kernels per Arnoldi step j (one CUDA graph per restart cycle):
 //   prepare v_j = round_basis(src * scale) stored in the basis (src = the
 //           previous unnormalised vector, or r at j = 0); y = D^-1 v_j
-//   spmv    w = A y with the pipelined Csr kernel (values and column
-//           indices of the next row group copied with cp.async while the
-//           current group is summed)
+//   spmv    w = A y on a column-major (Ell) copy of A in the Arnoldi type,
+//           16 bytes of rows per thread, when its padding stays within a
+//           quarter of nnz; else the pipelined Csr kernel on A
 //   dots    h1 = V_{0..j}^T w and G(:, j) = V_{0..j}^T v_j in one pass over
 //           the basis (all sums of a thread in registers); last block:
 //           h = (2I - G) h1
@@ -42,6 +42,7 @@
 #include <cuda_bf16.h>
 
 #include "csr_async.cuh"
+#include "ell_rows.cuh"
 #include "solver_common.cuh"
 
 namespace b2s {
@@ -56,7 +57,7 @@ struct GmresState {
     int krylov_dim;
     int idle;  // done || cycle_done: the Arnoldi kernels have nothing to do
     unsigned ticket;
-    int pad;
+    int too_long;  // a row is longer than the Ell copy's width
     double bnorm, rnorm, reduction, inner_reduction, inner_thresh;
     double scale;  // v_j = src * scale: 1/||r|| at j = 0, 1/H(j, j-1) else
     double minus_one, one;       // alpha, beta of r = b - A x
@@ -609,13 +610,24 @@ __global__ void float_copy_kernel(int64_t n, const double* __restrict__ src,
 // Leading dimension of the streamed vectors: a multiple of 64 rows.
 inline int64_t gmres_ld(int64_t n) { return ceildiv(n, 64) * 64; }
 
+// Width of the column-major (Ell) copy of A that the Arnoldi SpMV runs on,
+// or 0 when its padding would exceed a quarter of nnz (then the Csr kernel
+// runs on A itself).
+inline int gmres_ell_width(int64_t n, int64_t nnz, int64_t max_row_nnz)
+{
+    if (max_row_nnz < 1 || max_row_nnz > (int64_t(1) << 20)) return 0;
+    const int64_t padded = max_row_nnz * gmres_ld(n);
+    return padded <= nnz + nnz / 4 ? int(max_row_nnz) : 0;
+}
+
 struct GmresLayout {
     int64_t bytes, off_st, off_r, off_w0, off_w1, off_y, off_v, off_partials,
-        off_a32, off_d32;
+        off_a32, off_d32, off_ell_c, off_ell_v;
+    int ell_width;
 };
 
 template <typename TA, typename TB>
-GmresLayout gmres_layout(int64_t n, int64_t nnz, int d, bool mixed)
+GmresLayout gmres_layout(int64_t n, int64_t nnz, int64_t max_row_nnz, int d, bool mixed)
 {
     Carver c{nullptr};
     GmresLayout l;
@@ -627,8 +639,11 @@ GmresLayout gmres_layout(int64_t n, int64_t nnz, int d, bool mixed)
     l.off_y = c.take<TA>(ldv);
     l.off_v = c.take<TB>((int64_t(d) + 1) * ldv);
     l.off_partials = c.take<double>(int64_t(kSolverGrid) * 2 * kLd);
-    l.off_a32 = mixed ? c.take<float>(nnz) : 0;
+    l.ell_width = gmres_ell_width(n, nnz, max_row_nnz);
+    l.off_a32 = mixed && l.ell_width == 0 ? c.take<float>(nnz) : 0;
     l.off_d32 = mixed ? c.take<float>(n) : 0;
+    l.off_ell_c = l.ell_width ? c.take<int32_t>(int64_t(l.ell_width) * ldv) : 0;
+    l.off_ell_v = l.ell_width ? c.take<TA>(int64_t(l.ell_width) * ldv) : 0;
     l.bytes = c.used;
     return l;
 }
@@ -657,7 +672,7 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
         B2S_CUDA_TRY(cudaStreamSynchronize(st));
         nnz = h_nnz;
     }
-    const GmresLayout lay = gmres_layout<TA, TB>(n, nnz, krylov_dim, kMixed);
+    const GmresLayout lay = gmres_layout<TA, TB>(n, nnz, max_row_nnz, krylov_dim, kMixed);
     if (workspace_bytes < lay.bytes) {
         set_error("workspace of %lld bytes < %lld", (long long)workspace_bytes,
                   (long long)lay.bytes);
@@ -679,7 +694,7 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
     if constexpr (kMixed) {
         float* a32 = reinterpret_cast<float*>(w + lay.off_a32);
         float* d32 = reinterpret_cast<float*>(w + lay.off_d32);
-        if (nnz > 0) {
+        if (nnz > 0 && lay.ell_width == 0) {
             float_copy_kernel<<<ceildiv(nnz, 256), 256, 0, st>>>(nnz, v64, a32);
             B2S_LAUNCH_CHECK();
         }
@@ -703,6 +718,23 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
     h.minus_one = -1.0;
     h.one = 1.0;
     B2S_CUDA_TRY(cudaMemcpyAsync(gs, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+    const int ell_w = lay.ell_width;
+    int32_t* ell_c = reinterpret_cast<int32_t*>(w + lay.off_ell_c);
+    TA* ell_v = reinterpret_cast<TA*>(w + lay.off_ell_v);
+    if (ell_w > 0) {
+        ell_fill_kernel<TA><<<ceildiv(ldv, 256), 256, 0, st>>>(n, ldv, ell_w, rp, ci, v64,
+                                                               ell_c, ell_v, &gs->too_long);
+        B2S_LAUNCH_CHECK();
+        int too_long = 0;
+        B2S_CUDA_TRY(cudaMemcpyAsync(&too_long, &gs->too_long, sizeof(int),
+                                     cudaMemcpyDeviceToHost, st));
+        B2S_CUDA_TRY(cudaStreamSynchronize(st));
+        B2S_CHECK_ARG(!too_long, "max_row_nnz (%lld) is smaller than the longest row",
+                      (long long)max_row_nnz);
+    }
+    constexpr int kEllRows = int(16 / sizeof(TA));
+    const int grid_ell = int(std::min<int64_t>(
+        std::max<int64_t>(1, ceildiv(ceildiv(n, kEllRows), 256)), int64_t(kNumSMs) * 8));
 
     const int grid_vec = int(std::min<int64_t>(
         std::max<int64_t>(1, ceildiv(n, kSolverBlock)), kSolverGrid));
@@ -732,12 +764,17 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
             TA* dst = wv[j % 2];
             gmres_prepare_kernel<TA, TB><<<grid_vec, kSolverBlock, 0, cs>>>(
                 n, ldv, da, r, src, V, y, gs);
-            with_async_kernel<TA, 1, false>(lpr, [&](auto kernel) {
-                const int64_t grid = std::min<int64_t>(async_need,
-                                                       async_resident_blocks(kernel));
-                kernel<<<grid, kAsyncBlock, 0, cs>>>(n, rp, ci, va, y, 1, dst, 1,
-                                                     nullptr, nullptr, &gs->idle);
-            });
+            if (ell_w > 0) {
+                ell_rows_kernel<TA, kEllRows><<<grid_ell, 256, 0, cs>>>(
+                    n, ell_w, ldv, ell_c, ell_v, y, dst, &gs->idle);
+            } else {
+                with_async_kernel<TA, 1, false>(lpr, [&](auto kernel) {
+                    const int64_t grid = std::min<int64_t>(async_need,
+                                                           async_resident_blocks(kernel));
+                    kernel<<<grid, kAsyncBlock, 0, cs>>>(n, rp, ci, va, y, 1, dst, 1,
+                                                         nullptr, nullptr, &gs->idle);
+                });
+            }
             gmres_dots_kernel<TA, TB><<<grid_dots, kDotsBlock, 0, cs>>>(
                 n, ldv, V, dst, gs, partials);
             gmres_update_kernel<TA, TB><<<grid_vec, kSolverBlock, 0, cs>>>(
@@ -799,16 +836,20 @@ using namespace b2s;
 extern "C" {
 
 int64_t b2s_gmres_workspace_bytes(int64_t num_rows, int64_t nnz,
-                                  int64_t krylov_dim, int variant)
+                                  int64_t max_row_nnz, int64_t krylov_dim,
+                                  int variant)
 {
     if (num_rows < 1 || krylov_dim < 1 || krylov_dim > kMaxKrylov) return -1;
     switch (variant) {
     case B2S_GMRES_F64:
-        return gmres_layout<double, double>(num_rows, nnz, int(krylov_dim), false).bytes;
+        return gmres_layout<double, double>(num_rows, nnz, max_row_nnz, int(krylov_dim),
+                                            false).bytes;
     case B2S_GMRES_MIXED_F32:
-        return gmres_layout<float, float>(num_rows, nnz, int(krylov_dim), true).bytes;
+        return gmres_layout<float, float>(num_rows, nnz, max_row_nnz, int(krylov_dim),
+                                          true).bytes;
     case B2S_GMRES_MIXED_BF16:
-        return gmres_layout<float, __nv_bfloat16>(num_rows, nnz, int(krylov_dim), true).bytes;
+        return gmres_layout<float, __nv_bfloat16>(num_rows, nnz, max_row_nnz,
+                                                  int(krylov_dim), true).bytes;
     default:
         return -1;
     }

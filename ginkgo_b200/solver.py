@@ -225,7 +225,8 @@ class _Solver:
         if b2.shape[1] != 1 or not x2.is_contiguous() or not b2.is_contiguous():
             raise NotImplementedError("GMRES here takes one contiguous right-hand side")
         variant = {None: 0, "f64": 0, "f32": 1, "bf16": 2}[self.f.storage_precision]
-        nbytes = lib().b2s_gmres_workspace_bytes(n, A.nnz, self.f.krylov_dim, variant)
+        nbytes = lib().b2s_gmres_workspace_bytes(n, A.nnz, A.max_row_nnz,
+                                                 self.f.krylov_dim, variant)
         ws = self._workspace(nbytes)
         it, rs = C.c_int64(0), C.c_int64(0)
         rn, conv = C.c_double(0), C.c_int(0)

@@ -451,9 +451,14 @@ int b2s_bicgstab_solve_f32(int64_t num_rows, const int32_t* row_ptrs,
  * triangular solve are FP64 in all variants.  max_iters bounds the total
  * Arnoldi steps; reduction_factor is the goal on the explicit FP64 residual
  * relative to ||b||; inner_reduction ends an inner cycle early once its
- * estimate falls below inner_reduction * ||r||.  *restarts counts cycles. */
+ * estimate falls below inner_reduction * ||r||.  *restarts counts cycles.
+ * max_row_nnz must be at least the longest row (the workspace holds a
+ * column-major copy of A in the Arnoldi type when its padding stays within
+ * a quarter of nnz; a longer row makes the solve return
+ * B2S_ERR_INVALID_ARG). */
 int64_t b2s_gmres_workspace_bytes(int64_t num_rows, int64_t nnz,
-                                  int64_t krylov_dim, int variant);
+                                  int64_t max_row_nnz, int64_t krylov_dim,
+                                  int variant);
 int b2s_gmres_solve(int variant, int64_t num_rows, const int32_t* row_ptrs,
                     const int32_t* col_idxs, const double* values,
                     int64_t max_row_nnz, const double* inv_diag,

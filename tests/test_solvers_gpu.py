@@ -284,3 +284,16 @@ def test_bicgstab_multi_rhs(exe):
     s.apply(torch.from_numpy(b).cuda(), x)
     assert s.logger.has_converged
     assert np.all(explicit_rel_res(rp, ci, v, x.cpu().numpy(), b) <= 3e-9)
+
+
+def test_gmres_rejects_row_bound_below_longest_row(exe):
+    # the column-major copy of A is sized by max_row_nnz: a bound below the
+    # longest row is an argument error, not a silently truncated matrix
+    rp, ci, v, n, b = _aniso(8)
+    A = Csr.read(exe, rp, ci, v)
+    A._max_row_nnz = 20  # rows have up to 27 entries
+    s = (Gmres.build().with_krylov_dim(10).with_criteria(*crit(50, 1e-8))
+         .on(exe).generate(A))
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    with pytest.raises(RuntimeError, match="longest row"):
+        s.apply(torch.from_numpy(b).cuda(), x)
