@@ -50,6 +50,9 @@ namespace {
 
 constexpr int kMaxKrylov = 32;
 constexpr int kLd = kMaxKrylov + 1;
+constexpr int kDotsMaxGrid = kNumSMs * 3;  // resident at 3 blocks per SM
+constexpr int kDotsGroup = 32;  // blocks folded by one group's last block
+constexpr int kDotsMaxGroups = (kDotsMaxGrid + kDotsGroup - 1) / kDotsGroup;
 
 struct GmresState {
     int done, cycle_done, j, final_iter;
@@ -58,6 +61,7 @@ struct GmresState {
     int idle;  // done || cycle_done: the Arnoldi kernels have nothing to do
     unsigned ticket;
     int too_long;  // a row is longer than the Ell copy's width
+    unsigned gticket[kDotsMaxGroups + 1];  // dots: per group of 32 blocks
     double bnorm, rnorm, reduction, inner_reduction, inner_thresh;
     double scale;  // v_j = src * scale: 1/||r|| at j = 0, 1/H(j, j-1) else
     double minus_one, one;       // alpha, beta of r = b - A x
@@ -198,25 +202,30 @@ __global__ void __launch_bounds__(kSolverBlock)
     }
 }
 
-// Sums each of the N values v[0..N) (N = 32 P) over the warp with N - P
-// shuffles: every level of the butterfly hands half of the values a lane
-// carries to its partner.  On return lane l holds the totals of values
-// l P + k in v[k], k < P.
+// Sums each of the N values v[0..N) (N = 16 or 32 P) over the warp: every
+// level of the butterfly hands half of the values a lane carries to its
+// partner (N - 1 shuffles for N = 16, N - P for N = 32 P).  On return lane
+// l holds the total of value l * P + k in v[k] (N = 32 P), or of value
+// l / 2 in v[0] (N = 16).
 template <typename T, int N>
 __device__ __forceinline__ void warp_multi_sum(T (&v)[N], int lane)
 {
-    static_assert(N % 32 == 0, "32 P values");
+    static_assert(N == 16 || N % 32 == 0, "16 or 32 P values");
     constexpr unsigned kFull = 0xffffffffu;
 #pragma unroll
     for (int lvl = 0; lvl < 5; ++lvl) {
         const int m = 16 >> lvl;
         const int half = N >> (lvl + 1);
-        const bool up = lane & m;
+        if (half == 0) {
+            v[0] += __shfl_xor_sync(kFull, v[0], m);
+        } else {
+            const bool up = lane & m;
 #pragma unroll
-        for (int i = 0; i < half; ++i) {
-            const T send = up ? v[i] : v[i + half];
-            const T keep = up ? v[i + half] : v[i];
-            v[i] = keep + __shfl_xor_sync(kFull, send, m);
+            for (int i = 0; i < half; ++i) {
+                const T send = up ? v[i] : v[i + half];
+                const T keep = up ? v[i + half] : v[i];
+                v[i] = keep + __shfl_xor_sync(kFull, send, m);
+            }
         }
     }
 }
@@ -224,13 +233,13 @@ __device__ __forceinline__ void warp_multi_sum(T (&v)[N], int lane)
 // One pass of the dots kernel over C basis vectors i0 .. i0 + C - 1 (C a
 // compile-time count, so the C 16-byte loads of a row group are issued
 // back to back without predicates): acc[u] += V_{i0+u}^T w and
-// acc[16 + u] += V_{i0+u}^T v_j over this thread's row groups.
+// acc[8 + u] += V_{i0+u}^T v_j over this thread's row groups.
 template <typename TA, typename TB, int C>
 __device__ __forceinline__ void dots_pass(int64_t n, int64_t ldv,
                                           const TB* __restrict__ V,
                                           const TA* __restrict__ w,
                                           const TB* __restrict__ vj, int i0,
-                                          TA (&acc)[32])
+                                          TA (&acc)[16])
 {
     constexpr int R = rows_per_group<TB>();
     const int64_t groups = ceildiv(n, R);
@@ -248,60 +257,75 @@ __device__ __forceinline__ void dots_pass(int64_t n, int64_t ldv,
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 acc[u] += x[r] * wr[r];
-                acc[16 + u] += x[r] * vr[r];
+                acc[8 + u] += x[r] * vr[r];
             }
         }
     }
 }
 
-constexpr int kDotsBlock = 512;
-constexpr int kDotsMaxGrid = 160;  // the final reduction reads 20 per lane
-
-// In the last block: out[c] = sum over b < B of part[e(c) * B + b] for the
-// E values c < E (e(c) = c for c < half, kLd + c - half after), in a fixed
-// order: lane k of an 8-lane group sums b = k, k + 8, ... with all of its
-// loads in flight at once, then the group combines its 8 sums.
-__device__ __forceinline__ void reduce_value_major(const double* part, int B, int E,
-                                                   int half, double* out)
+// compact value index c < 2 nvec -> partial row e (h1 at e < kLd, G after)
+__device__ __forceinline__ int dots_row(int c, int nvec)
 {
-    const int sub = threadIdx.x % 8, grp = threadIdx.x / 8;
-    const int ngrp = blockDim.x / 8;
-    for (int c0 = 0; c0 < E; c0 += ngrp) {
-        const int c = c0 + grp;
-        double s = 0.0;
-        if (c < E) {
-            const int e = c < half ? c : kLd + c - half;
-            const double* p = part + int64_t(e) * B;
-            double v[kDotsMaxGrid / 8];
+    return c < nvec ? c : kLd + c - nvec;
+}
+
+// Ticket of `count` arrivals; true in the last one to arrive (the caller's
+// writes are fenced first), which resets the ticket.
+__device__ __forceinline__ bool last_of(unsigned* ticket, unsigned count, int* flag_sm)
+{
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned t = atomicAdd(ticket, 1u);
+        *flag_sm = (t == count - 1);
+        if (t == count - 1) *ticket = 0;
+    }
+    __syncthreads();
+    const bool last = *flag_sm;
+    if (last) __threadfence();
+    return last;
+}
+
+// In one block: for the 2 nvec values c, the sum over the L partials
+// src[dots_row(c) * ld + base + k], k < L <= 32, one warp load per value
+// (warp w takes c = w, w + 8, ...; all loads issued before the sums).
+__device__ __forceinline__ void fold32(const double* src, int64_t ld, int base, int L,
+                                       int nvec, double* dst, int64_t dst_ld, int dst_col)
+{
+    const int lane = threadIdx.x % kWarp, wid = threadIdx.x / kWarp;
+    constexpr int K = (2 * kLd + 7) / 8;
+    double v[K];
 #pragma unroll
-            for (int k = 0; k < kDotsMaxGrid / 8; ++k) {
-                const int b = sub + 8 * k;
-                v[k] = b < B ? __ldcg(p + b) : 0.0;
-            }
+    for (int k = 0; k < K; ++k) {
+        const int c = wid + 8 * k;
+        v[k] = c < 2 * nvec && lane < L ? __ldcg(src + dots_row(c, nvec) * ld + base + lane)
+                                        : 0.0;
+    }
 #pragma unroll
-            for (int k = 0; k < kDotsMaxGrid / 8; ++k) s += v[k];
-        }
-        s = subwarp_sum<8>(s);
-        if (sub == 0 && c < E) out[c] = s;
+    for (int k = 0; k < K; ++k) {
+        const int c = wid + 8 * k;
+        const double s = warp_sum(v[k]);
+        if (lane == 0 && c < 2 * nvec) dst[dots_row(c, nvec) * dst_ld + dst_col] = s;
     }
 }
 
 // Step j, part 3: h1 = V_{0..j}^T w and G(:, j) = V_{0..j}^T v_j: passes of
-// up to CMAX basis vectors (16 for FP32 arithmetic, 8 for FP64), a thread
-// taking one row group per iteration with all sums of the pass in
-// registers; one block of 512 threads per SM.  Per pass one multi-value
-// warp reduction and one block reduction; partials are value-major
-// (partials[e * gridDim.x + block], e < 2 kLd).  The last block reduces
-// them, completes G's row and column j and forms h = (2I - G) h1.
+// up to 8 basis vectors, a thread taking one row group per iteration with
+// the 16 sums of the pass in registers (3 blocks per SM).  Per pass
+// one multi-value warp reduction and one block reduction into value-major
+// partials (partials[e * gridDim.x + block]).  The last block of every 32
+// blocks folds its group's partials; the last group to finish folds the
+// groups, completes G's row and column j and forms h = (2I - G) h1.  The
+// summation order is fixed: the result does not depend on scheduling.
 template <typename TA, typename TB>
-__global__ void __launch_bounds__(kDotsBlock, 1)
+__global__ void __launch_bounds__(kSolverBlock, 3)
     gmres_dots_kernel(int64_t n, int64_t ldv, const TB* __restrict__ V,
                       const TA* __restrict__ w, GmresState* st,
-                      double* __restrict__ partials)
+                      double* __restrict__ partials, double* __restrict__ gpart)
 {
-    constexpr int CMAX = sizeof(TA) == 8 ? 8 : 16;
-    constexpr int W = kDotsBlock / kWarp;
-    __shared__ double red[W][32];
+    constexpr int CMAX = 8;
+    constexpr int W = kSolverBlock / kWarp;
+    __shared__ double redv[W][16];
     __shared__ double tot[2 * kLd];
     __shared__ double Gs[kLd * kLd];
     __shared__ int last;
@@ -313,64 +337,62 @@ __global__ void __launch_bounds__(kDotsBlock, 1)
     const int B = gridDim.x;
     for (int i0 = 0; i0 < nvec; i0 += CMAX) {
         const int c = nvec - i0 < CMAX ? nvec - i0 : CMAX;
-        TA acc[32];
+        TA acc[16];
 #pragma unroll
-        for (int u = 0; u < 32; ++u) acc[u] = TA(0);
+        for (int u = 0; u < 16; ++u) acc[u] = TA(0);
         switch (c) {
-#define B2S_DOTS_CASE(K)                                                          \
-    case K:                                                                       \
-        if constexpr (K <= CMAX) dots_pass<TA, TB, K>(n, ldv, V, w, vj, i0, acc); \
-        break;
-            B2S_DOTS_CASE(1) B2S_DOTS_CASE(2) B2S_DOTS_CASE(3) B2S_DOTS_CASE(4)
-            B2S_DOTS_CASE(5) B2S_DOTS_CASE(6) B2S_DOTS_CASE(7) B2S_DOTS_CASE(8)
-            B2S_DOTS_CASE(9) B2S_DOTS_CASE(10) B2S_DOTS_CASE(11) B2S_DOTS_CASE(12)
-            B2S_DOTS_CASE(13) B2S_DOTS_CASE(14) B2S_DOTS_CASE(15) B2S_DOTS_CASE(16)
-#undef B2S_DOTS_CASE
-        default: break;
+        case 1: dots_pass<TA, TB, 1>(n, ldv, V, w, vj, i0, acc); break;
+        case 2: dots_pass<TA, TB, 2>(n, ldv, V, w, vj, i0, acc); break;
+        case 3: dots_pass<TA, TB, 3>(n, ldv, V, w, vj, i0, acc); break;
+        case 4: dots_pass<TA, TB, 4>(n, ldv, V, w, vj, i0, acc); break;
+        case 5: dots_pass<TA, TB, 5>(n, ldv, V, w, vj, i0, acc); break;
+        case 6: dots_pass<TA, TB, 6>(n, ldv, V, w, vj, i0, acc); break;
+        case 7: dots_pass<TA, TB, 7>(n, ldv, V, w, vj, i0, acc); break;
+        default: dots_pass<TA, TB, 8>(n, ldv, V, w, vj, i0, acc); break;
         }
-        warp_multi_sum<TA, 32>(acc, lane);
-        red[wid][lane] = double(acc[0]);  // lane l: value l
+        warp_multi_sum<TA, 16>(acc, lane);
+        // lane l holds value l / 2: the h1 sum of vector i0 + l / 2 for
+        // l < 16, the G sum of vector i0 + l / 2 - 8 after
+        if ((lane & 1) == 0) redv[wid][lane / 2] = double(acc[0]);
         __syncthreads();
-        if (threadIdx.x < 32) {
-            const int u = threadIdx.x % 16;
+        if (threadIdx.x < 16) {
+            const int u = threadIdx.x % 8;
             if (u < c) {
                 double s = 0.0;
-                for (int k = 0; k < W; ++k) s += red[k][threadIdx.x];
-                const int e = (threadIdx.x < 16 ? 0 : kLd) + i0 + u;
+                for (int k = 0; k < W; ++k) s += redv[k][threadIdx.x];
+                const int e = (threadIdx.x < 8 ? 0 : kLd) + i0 + u;
                 partials[int64_t(e) * B + blockIdx.x] = s;
             }
         }
         __syncthreads();
     }
-    if (last_block_done(&st->ticket, &last)) {
-        // tot[0..nvec): h1, tot[kLd + i]: G(i, j)
-        double* tv = Gs;  // scratch for the 2 nvec sums before Gs is staged
-        reduce_value_major(partials, B, 2 * nvec, nvec, tv);
-        __syncthreads();
-        for (int c = threadIdx.x; c < 2 * nvec; c += kDotsBlock) {
-            tot[c < nvec ? c : kLd + c - nvec] = tv[c];
-        }
-        __syncthreads();
-        // G(0..j-1, 0..j-1) from the earlier steps of this cycle
-        for (int e = threadIdx.x; e < j * kLd; e += kDotsBlock) Gs[e] = st->G[e];
-        __syncthreads();
-        if (threadIdx.x <= j) {
-            const int i = threadIdx.x;
-            const double gij = tot[kLd + i];
-            Gs[i * kLd + j] = gij;
-            Gs[j * kLd + i] = gij;
-            st->G[i * kLd + j] = gij;
-            st->G[j * kLd + i] = gij;
-        }
-        __syncthreads();
-        // h = (2I - G) h1: CGS2's second projection from G
-        if (threadIdx.x <= j) {
-            const int i = threadIdx.x;
-            double gh = 0.0;
-            for (int k = 0; k <= j; ++k) gh += Gs[i * kLd + k] * tot[k];
-            st->h[i] = 2.0 * tot[i] - gh;
-        }
-        if (threadIdx.x == 0) st->ticket = 0;
+    const int g = blockIdx.x / kDotsGroup;
+    const int ngroups = (B + kDotsGroup - 1) / kDotsGroup;
+    const int gsize = B - g * kDotsGroup < kDotsGroup ? B - g * kDotsGroup : kDotsGroup;
+    if (!last_of(&st->gticket[g], unsigned(gsize), &last)) return;
+    fold32(partials, B, g * kDotsGroup, gsize, nvec, gpart, kDotsMaxGroups, g);
+    if (!last_of(&st->ticket, unsigned(ngroups), &last)) return;
+    // tot[0..nvec): h1, tot[kLd + i]: G(i, j)
+    fold32(gpart, kDotsMaxGroups, 0, ngroups, nvec, tot, 1, 0);
+    __syncthreads();
+    // G(0..j-1, 0..j-1) from the earlier steps of this cycle
+    for (int e = threadIdx.x; e < j * kLd; e += kSolverBlock) Gs[e] = st->G[e];
+    __syncthreads();
+    if (threadIdx.x <= j) {
+        const int i = threadIdx.x;
+        const double gij = tot[kLd + i];
+        Gs[i * kLd + j] = gij;
+        Gs[j * kLd + i] = gij;
+        st->G[i * kLd + j] = gij;
+        st->G[j * kLd + i] = gij;
+    }
+    __syncthreads();
+    // h = (2I - G) h1: CGS2's second projection from G
+    if (threadIdx.x <= j) {
+        const int i = threadIdx.x;
+        double gh = 0.0;
+        for (int k = 0; k <= j; ++k) gh += Gs[i * kLd + k] * tot[k];
+        st->h[i] = 2.0 * tot[i] - gh;
     }
 }
 
@@ -622,7 +644,7 @@ inline int gmres_ell_width(int64_t n, int64_t nnz, int64_t max_row_nnz)
 
 struct GmresLayout {
     int64_t bytes, off_st, off_r, off_w0, off_w1, off_y, off_v, off_partials,
-        off_a32, off_d32, off_ell_c, off_ell_v;
+        off_a32, off_d32, off_ell_c, off_ell_v, off_gpart;
     int ell_width;
 };
 
@@ -639,6 +661,7 @@ GmresLayout gmres_layout(int64_t n, int64_t nnz, int64_t max_row_nnz, int d, boo
     l.off_y = c.take<TA>(ldv);
     l.off_v = c.take<TB>((int64_t(d) + 1) * ldv);
     l.off_partials = c.take<double>(int64_t(kSolverGrid) * 2 * kLd);
+    l.off_gpart = c.take<double>(int64_t(kDotsMaxGroups) * 2 * kLd);
     l.ell_width = gmres_ell_width(n, nnz, max_row_nnz);
     l.off_a32 = mixed && l.ell_width == 0 ? c.take<float>(nnz) : 0;
     l.off_d32 = mixed ? c.take<float>(n) : 0;
@@ -689,6 +712,7 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
     TA* y = reinterpret_cast<TA*>(w + lay.off_y);
     TB* V = reinterpret_cast<TB*>(w + lay.off_v);
     double* partials = reinterpret_cast<double*>(w + lay.off_partials);
+    double* gpart = reinterpret_cast<double*>(w + lay.off_gpart);
     const TA* va;
     const TA* da;
     if constexpr (kMixed) {
@@ -739,8 +763,8 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
     const int grid_vec = int(std::min<int64_t>(
         std::max<int64_t>(1, ceildiv(n, kSolverBlock)), kSolverGrid));
     const int grid_dots = int(std::min<int64_t>(
-        std::max<int64_t>(1, ceildiv(ceildiv(n, rows_per_group<TB>()), kDotsBlock)),
-        std::min(kNumSMs, kDotsMaxGrid)));
+        std::max<int64_t>(1, ceildiv(ceildiv(n, rows_per_group<TB>()), kSolverBlock)),
+        kDotsMaxGrid));
     // pipelined SpMV: persistent grid, as many blocks as fit at once
     const int lpr = async_lanes_per_row(max_row_nnz);
     const int64_t async_need = ceildiv(ceildiv(n, kWarp / lpr), kAsyncBlock / kWarp);
@@ -775,8 +799,8 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
                                                          nullptr, nullptr, &gs->idle);
                 });
             }
-            gmres_dots_kernel<TA, TB><<<grid_dots, kDotsBlock, 0, cs>>>(
-                n, ldv, V, dst, gs, partials);
+            gmres_dots_kernel<TA, TB><<<grid_dots, kSolverBlock, 0, cs>>>(
+                n, ldv, V, dst, gs, partials, gpart);
             gmres_update_kernel<TA, TB><<<grid_vec, kSolverBlock, 0, cs>>>(
                 n, ldv, V, dst, gs, partials);
             B2S_LAUNCH_CHECK();
