@@ -16,8 +16,9 @@ namespace b2s {
 // Csr, persistent and pipelined: every warp walks groups of R = 32 / LPR
 // consecutive rows with a stride of the grid's warp count.  The values and
 // column indices of the next group are copied into shared memory with
-// cp.async while the current group is reduced, so the matrix stream never
-// waits for the x gathers or the row-pointer loads of the group in hand.
+// cp.async while the current group is reduced, and the row pointers of the
+// group after that are loaded at the same time, so neither the matrix
+// stream nor the next copy waits for a row-pointer load or an x gather.
 // Each row is then summed from shared memory by LPR lanes (LPR = 1: each
 // lane sums its own row in order, the reference's sequential row sum of
 // reference/matrix/csr_kernels.cpp:65-74).  Groups with more than kAsyncCap
@@ -48,6 +49,10 @@ int async_resident_blocks(Kern kernel)
     for (const auto& e : cache) {
         if (e.first == key) return e.second;
     }
+    // four 48 KB blocks per SM leave the rest of the unified L1 (about a
+    // fifth) for the x gathers; a larger shared-memory carveout measured
+    // slower on the 7-point matrix
+    (void)cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 80);
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kAsyncBlock, 0) !=
             cudaSuccess ||
@@ -104,12 +109,16 @@ __global__ void __launch_bounds__(kAsyncBlock)
     const int64_t ngroups = (n + R - 1) / R;
     const int64_t nwarps = int64_t(gridDim.x) * (kAsyncBlock / kWarp);
     AsyncStage<T>* st = stages[wid];
-    // row span [rs, re) of this lane's row in group g, group start and count
-    auto desc = [&](int64_t g, int& rs, int& re, int& start, int& cnt) {
+    // row pointers of group g: lane l holds rp[row0 + l], pe = rp[row0 + R]
+    // (clamped at n); loaded one group before they are needed
+    auto load_ptrs = [&](int64_t g, int& p, int& pe) {
         const int64_t row0 = g * R;
         const int64_t pl = row0 + lane;
-        const int p = __ldg(rp + (pl < n ? pl : n));
-        const int pe = __ldg(rp + (row0 + R < n ? row0 + R : n));
+        p = __ldg(rp + (pl < n ? pl : n));
+        pe = __ldg(rp + (row0 + R < n ? row0 + R : n));
+    };
+    // row span [rs, re) of this lane's row, group start and count
+    auto desc = [&](int p, int pe, int& rs, int& re, int& start, int& cnt) {
         rs = __shfl_sync(kFull, p, myrow);
         const int nx = __shfl_sync(kFull, p, myrow + 1 < kWarp ? myrow + 1 : kWarp - 1);
         re = myrow + 1 < R ? nx : pe;
@@ -125,17 +134,22 @@ __global__ void __launch_bounds__(kAsyncBlock)
     if (skip != nullptr && *skip) return;  // whole grid (solver idle)
     int64_t g = blockIdx.x * int64_t(kAsyncBlock / kWarp) + wid;
     if (g >= ngroups) return;  // whole warp
-    int rs, re, start, cnt;
-    desc(g, rs, re, start, cnt);
+    int rs, re, start, cnt, p, pe;
+    load_ptrs(g, p, pe);
+    desc(p, pe, rs, re, start, cnt);
     if (cnt <= kAsyncCap) issue(0, start, cnt);
     cp_async_commit();
+    // pointers of the group after the next
+    int pn = 0, pen = 0;
+    if (g + nwarps < ngroups) load_ptrs(g + nwarps, pn, pen);
     int s = 0;
     for (; g < ngroups; g += nwarps) {
         const int64_t gn = g + nwarps;
         int nrs = 0, nre = 0, nstart = 0, ncnt = 0;
         if (gn < ngroups) {
-            desc(gn, nrs, nre, nstart, ncnt);
+            desc(pn, pen, nrs, nre, nstart, ncnt);
             if (ncnt <= kAsyncCap) issue(s ^ 1, nstart, ncnt);
+            if (gn + nwarps < ngroups) load_ptrs(gn + nwarps, pn, pen);
         }
         cp_async_commit();
         cp_async_wait_one();
@@ -146,6 +160,7 @@ __global__ void __launch_bounds__(kAsyncBlock)
         const int64_t row = g * R + myrow;
         if (cnt <= kAsyncCap) {
             const AsyncStage<T>& cur = st[s];
+#pragma unroll 4
             for (int i = rs - start + sub; i < re - start; i += LPR) {
                 T xr[K];
                 RowLoad<T, K, VEC>::load(b + int64_t(cur.cols[i]) * ldb, xr);
