@@ -2,7 +2,8 @@
 // values and column indices of entry k of rows r0 .. r0 + R - 1 are one
 // vector load each (16 bytes of values), so a warp moves 32 R entries per
 // instruction and the gathers of x for neighbouring rows stay coalesced for
-// banded matrices.  Used by the GMRES engine on its column-major copy of A.
+// banded matrices.  Used for Ell SpMV with one right-hand side and by the
+// GMRES engine on its column-major copy of A.
 #pragma once
 
 #include <cstring>
@@ -31,22 +32,27 @@ __device__ __forceinline__ void load_stream_rows(const T* p, T (&o)[R])
     }
 }
 
-// y(rows) = A x over an Ell-layout copy: entry k of row r at k * ld + r
-// (ld a multiple of R, every row group 16-byte aligned), padding entries
-// with column -1 and value 0.  Entries are summed in stored order.  A
-// launch whose *skip is non-zero returns at once.
+// y = A x (or alpha A x + beta y) over an Ell layout: entry k of row r at
+// k * ld + r (ld a multiple of R, every row group 16-byte aligned), padding
+// entries with column -1; the slots of rows n .. ld - 1 are never gathered
+// through.  x and y are strided by ldx and ldy.  Entries are
+// summed in stored order.  A launch whose *skip is non-zero returns at once.
 template <typename T, int R>
 __global__ void __launch_bounds__(256)
     ell_rows_kernel(int64_t n, int width, int64_t ld,
                     const int32_t* __restrict__ cols, const T* __restrict__ vals,
-                    const T* __restrict__ x, T* __restrict__ y,
-                    const int* __restrict__ skip)
+                    const T* __restrict__ x, int64_t ldx, T* __restrict__ y,
+                    int64_t ldy, const T* __restrict__ alpha,
+                    const T* __restrict__ beta, const int* __restrict__ skip)
 {
     if (skip != nullptr && *skip) return;
     const int64_t groups = (n + R - 1) / R;
     for (int64_t grp = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; grp < groups;
          grp += int64_t(gridDim.x) * blockDim.x) {
         const int64_t r0 = grp * R;
+        // slots of rows n .. ld - 1 may hold anything: they are loaded with
+        // the group but never used as gather indices
+        const int valid = n - r0 < R ? int(n - r0) : R;
         T acc[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) acc[r] = T(0);
@@ -60,16 +66,26 @@ __global__ void __launch_bounds__(256)
             load_stream_rows<T, R>(vp + int64_t(k) * ld, v);
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                const T xv = c[r] >= 0 ? __ldg(x + c[r]) : T(0);
+                const T xv = r < valid && c[r] >= 0 ? __ldg(x + int64_t(c[r]) * ldx) : T(0);
                 acc[r] += v[r] * xv;
             }
         }
-        const int valid = n - r0 < R ? int(n - r0) : R;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            if (r < valid) y[r0 + r] = acc[r];
+            if (r < valid) {
+                T* dst = y + (r0 + r) * ldy;
+                *dst = combine(acc[r], alpha, beta, dst);
+            }
         }
     }
+}
+
+// Rows per thread: 16 bytes of values, except one FP64 row per thread for
+// rows wider than 16 entries (measured faster on the 27-point matrix).
+template <typename T>
+inline int ell_rows_per_thread(int64_t width)
+{
+    return sizeof(T) == 8 && width > 16 ? 1 : int(16 / sizeof(T));
 }
 
 // Fills the Ell-layout copy (ld >= n rows, width entries per row) from Csr,

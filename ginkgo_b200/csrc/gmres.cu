@@ -757,8 +757,9 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
                       (long long)max_row_nnz);
     }
     constexpr int kEllRows = int(16 / sizeof(TA));
+    const int ell_r = ell_rows_per_thread<TA>(ell_w);
     const int grid_ell = int(std::min<int64_t>(
-        std::max<int64_t>(1, ceildiv(ceildiv(n, kEllRows), 256)), int64_t(kNumSMs) * 8));
+        std::max<int64_t>(1, ceildiv(ceildiv(n, ell_r), 256)), int64_t(kNumSMs) * 8));
 
     const int grid_vec = int(std::min<int64_t>(
         std::max<int64_t>(1, ceildiv(n, kSolverBlock)), kSolverGrid));
@@ -789,8 +790,15 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
             gmres_prepare_kernel<TA, TB><<<grid_vec, kSolverBlock, 0, cs>>>(
                 n, ldv, da, r, src, V, y, gs);
             if (ell_w > 0) {
-                ell_rows_kernel<TA, kEllRows><<<grid_ell, 256, 0, cs>>>(
-                    n, ell_w, ldv, ell_c, ell_v, y, dst, &gs->idle);
+                if (ell_r == kEllRows) {
+                    ell_rows_kernel<TA, kEllRows><<<grid_ell, 256, 0, cs>>>(
+                        n, ell_w, ldv, ell_c, ell_v, y, 1, dst, 1, nullptr, nullptr,
+                        &gs->idle);
+                } else {
+                    ell_rows_kernel<TA, 1><<<grid_ell, 256, 0, cs>>>(
+                        n, ell_w, ldv, ell_c, ell_v, y, 1, dst, 1, nullptr, nullptr,
+                        &gs->idle);
+                }
             } else {
                 with_async_kernel<TA, 1, false>(lpr, [&](auto kernel) {
                     const int64_t grid = std::min<int64_t>(async_need,

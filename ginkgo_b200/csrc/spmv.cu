@@ -10,6 +10,7 @@
 
 #include "common.cuh"
 #include "csr_async.cuh"
+#include "ell_rows.cuh"
 
 namespace b2s {
 namespace {
@@ -662,6 +663,20 @@ int ell_spmv(int64_t n, int64_t num_cols, int64_t width, int64_t stride,
     if (n == 0 || k == 0) return B2S_OK;
     cudaStream_t st = as_stream(stream);
     const int64_t grid = ceildiv(n, kBlock);
+    constexpr int RV = int(16 / sizeof(T));
+    const int R = ell_rows_per_thread<T>(width);
+    if (k == 1 && R == RV && stride % R == 0 && reinterpret_cast<uintptr_t>(ci) % 16 == 0 &&
+        reinterpret_cast<uintptr_t>(v) % 16 == 0 && width <= INT32_MAX) {
+        // one right-hand side: R rows per thread, 16-byte loads of values
+        // (wide FP64 rows stay on the row-per-thread kernel below, which
+        // measured faster there)
+        const int64_t g = std::min<int64_t>(ceildiv(ceildiv(n, R), kBlock),
+                                            int64_t(kNumSMs) * 16);
+        ell_rows_kernel<T, RV><<<g, kBlock, 0, st>>>(n, int(width), stride, ci, v, b, ldb,
+                                                     c, ldc, alpha, beta, nullptr);
+        B2S_LAUNCH_CHECK();
+        return B2S_OK;
+    }
     for (int64_t col0 = 0; col0 < k;) {
         const int kk = rhs_chunk(k - col0);
         const bool vec = vec_ok(b, ldb, col0, kk);

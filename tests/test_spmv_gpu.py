@@ -148,6 +148,31 @@ def test_empty_matrix(exe, fmt):
     op.apply(x, y)
 
 
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+def test_ell_one_rhs_row_groups_and_odd_stride(exe, dt):
+    # one right-hand side runs R = 16 / sizeof(value) rows per thread when
+    # the stride allows 16-byte loads (3376), element by element otherwise
+    # (3375); both against the oracle, plain and advanced
+    rp, ci, v = stencils.anisotropic_27pt(15)
+    n = len(rp) - 1
+    v = v.astype(NP[dt])
+    rng = np.random.default_rng(9)
+    x = rng.standard_normal((n, 1)).astype(NP[dt])
+    y0 = rng.standard_normal((n, 1)).astype(NP[dt])
+    ref = orc.csr_spmv(rp, ci, v, x)
+    ref2 = orc.csr_spmv(rp, ci, v, x, y0, 0.5, -1.5)
+    A = Csr.read(exe, rp, ci, v, dtype=dt)
+    for stride in (n, n + 1):
+        E = A.convert_to_ell(stride=stride)
+        y = torch.full((n, 1), float("nan"), dtype=dt, device="cuda")
+        E.apply(torch.from_numpy(x).cuda(), y)
+        assert_spmv_close(rp, ci, v, x, y.cpu().numpy(), ref, TOL[dt])
+        y2 = torch.from_numpy(y0).cuda()
+        E.apply(0.5, torch.from_numpy(x).cuda(), -1.5, y2)
+        assert_spmv_close(rp, ci, v, x, y2.cpu().numpy(), ref2, TOL[dt] * 4,
+                          alpha=0.5, beta_y=1.5 * y0.astype(np.float64))
+
+
 def test_conversions_bit_exact(exe, known):
     rp, ci, v = stencils.power_law(5000, seed=2, mu=1.8, max_len=400)
     A = Csr.read(exe, rp, ci, v)
