@@ -2,8 +2,8 @@
 // values and column indices of entry k of rows r0 .. r0 + R - 1 are one
 // vector load each (16 bytes of values), so a warp moves 32 R entries per
 // instruction and the gathers of x for neighbouring rows stay coalesced for
-// banded matrices.  Used for Ell SpMV with one right-hand side and by the
-// GMRES engine on its column-major copy of A.
+// banded matrices.  Used for Ell and Sellp SpMV with one right-hand side
+// and by the GMRES engine on its column-major copy of A.
 #pragma once
 
 #include <cstring>
@@ -36,8 +36,9 @@ __device__ __forceinline__ void load_stream_rows(const T* p, T (&o)[R])
 // k * ld + r (ld a multiple of R, every row group 16-byte aligned), padding
 // entries with column -1; the slots of rows n .. ld - 1 are never gathered
 // through.  x and y are strided by ldx and ldy.  Entries are
-// summed in stored order.  A launch whose *skip is non-zero returns at once.
-template <typename T, int R>
+// summed in stored order.  PLAIN: unit strides and y = A x (no alpha/beta).
+// A launch whose *skip is non-zero returns at once.
+template <typename T, int R, bool PLAIN = false>
 __global__ void __launch_bounds__(256)
     ell_rows_kernel(int64_t n, int width, int64_t ld,
                     const int32_t* __restrict__ cols, const T* __restrict__ vals,
@@ -66,6 +67,76 @@ __global__ void __launch_bounds__(256)
             load_stream_rows<T, R>(vp + int64_t(k) * ld, v);
 #pragma unroll
             for (int r = 0; r < R; ++r) {
+                const int64_t xo = PLAIN ? int64_t(c[r]) : int64_t(c[r]) * ldx;
+                const T xv = r < valid && c[r] >= 0 ? __ldg(x + xo) : T(0);
+                acc[r] += v[r] * xv;
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            if (r < valid) {
+                if constexpr (PLAIN) {
+                    y[r0 + r] = acc[r];
+                } else {
+                    T* dst = y + (r0 + r) * ldy;
+                    *dst = combine(acc[r], alpha, beta, dst);
+                }
+            }
+        }
+    }
+}
+
+// Sellp with R consecutive rows of one slice per thread (slice_size a
+// multiple of R): entry k of local rows l .. l + R - 1 of slice s sits at
+// (slice_sets[s] + k) * slice_size + l, one vector load of values and one
+// of column indices.  Padding entries (column -1) and rows past n are not
+// gathered through.
+template <typename T, int R, bool PREFETCH>
+__global__ void __launch_bounds__(256)
+    sellp_rows_kernel(int n, int slice_size, int slice_shift,
+                      const uint64_t* __restrict__ slice_sets,
+                      const uint64_t* __restrict__ slice_lengths,
+                      const int32_t* __restrict__ cols, const T* __restrict__ vals,
+                      const T* __restrict__ x, int64_t ldx, T* __restrict__ y,
+                      int64_t ldy, const T* __restrict__ alpha,
+                      const T* __restrict__ beta)
+{
+    // PREFETCH: grid-stride over row groups, the slice length and start of
+    // the next group loaded while the current one is summed; else one group
+    // per thread (the grid covers every group).  32-bit slice
+    // arithmetic (n < 2^31), a shift when the slice size is a power of two
+    // (slice_shift >= 0).
+    const unsigned groups = unsigned((int64_t(n) + R - 1) / R);
+    const unsigned stride = gridDim.x * blockDim.x;
+    unsigned grp = blockIdx.x * blockDim.x + threadIdx.x;
+    if (grp >= groups) return;
+    auto lookup = [&](unsigned g, int& len, int64_t& base) {
+        const unsigned r0 = g * unsigned(R);
+        const unsigned slice = slice_shift >= 0 ? r0 >> slice_shift : r0 / unsigned(slice_size);
+        const unsigned local = r0 - slice * unsigned(slice_size);
+        len = int(__ldg(slice_lengths + slice));
+        base = int64_t(__ldg(slice_sets + slice)) * slice_size + local;
+    };
+    int len;
+    int64_t base;
+    lookup(grp, len, base);
+    for (; grp < groups; grp += stride) {
+        int len_n = 0;
+        int64_t base_n = 0;
+        if (PREFETCH && grp + stride < groups) lookup(grp + stride, len_n, base_n);
+        const unsigned r0 = grp * unsigned(R);
+        const int valid = n - int(r0) < R ? n - int(r0) : R;
+        T acc[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) acc[r] = T(0);
+#pragma unroll 4
+        for (int k = 0; k < len; ++k) {
+            int32_t c[R];
+            T v[R];
+            load_stream_rows<int32_t, R>(cols + base + int64_t(k) * slice_size, c);
+            load_stream_rows<T, R>(vals + base + int64_t(k) * slice_size, v);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
                 const T xv = r < valid && c[r] >= 0 ? __ldg(x + int64_t(c[r]) * ldx) : T(0);
                 acc[r] += v[r] * xv;
             }
@@ -73,10 +144,13 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             if (r < valid) {
-                T* dst = y + (r0 + r) * ldy;
+                T* dst = y + (int64_t(r0) + r) * ldy;
                 *dst = combine(acc[r], alpha, beta, dst);
             }
         }
+        if (!PREFETCH) break;  // one group per thread: the grid covers all
+        len = len_n;
+        base = base_n;
     }
 }
 

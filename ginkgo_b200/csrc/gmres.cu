@@ -50,7 +50,7 @@ namespace {
 
 constexpr int kMaxKrylov = 32;
 constexpr int kLd = kMaxKrylov + 1;
-constexpr int kDotsMaxGrid = kNumSMs * 3;  // resident at 3 blocks per SM
+constexpr int kDotsMaxGrid = kNumSMs * 4;  // resident at 4 blocks per SM
 constexpr int kDotsGroup = 32;  // blocks folded by one group's last block
 constexpr int kDotsMaxGroups = (kDotsMaxGrid + kDotsGroup - 1) / kDotsGroup;
 
@@ -202,15 +202,14 @@ __global__ void __launch_bounds__(kSolverBlock)
     }
 }
 
-// Sums each of the N values v[0..N) (N = 16 or 32 P) over the warp: every
-// level of the butterfly hands half of the values a lane carries to its
-// partner (N - 1 shuffles for N = 16, N - P for N = 32 P).  On return lane
-// l holds the total of value l * P + k in v[k] (N = 32 P), or of value
-// l / 2 in v[0] (N = 16).
+// Sums each of the N values v[0..N) (N = 8, 16 or 32 P) over the warp:
+// every level of the butterfly hands half of the values a lane carries to
+// its partner.  On return lane l holds the total of value l * P + k in v[k]
+// (N = 32 P), or of value l / (32 / N) in v[0] (N = 8, 16).
 template <typename T, int N>
 __device__ __forceinline__ void warp_multi_sum(T (&v)[N], int lane)
 {
-    static_assert(N == 16 || N % 32 == 0, "16 or 32 P values");
+    static_assert(N == 8 || N == 16 || N % 32 == 0, "8, 16 or 32 P values");
     constexpr unsigned kFull = 0xffffffffu;
 #pragma unroll
     for (int lvl = 0; lvl < 5; ++lvl) {
@@ -233,34 +232,37 @@ __device__ __forceinline__ void warp_multi_sum(T (&v)[N], int lane)
 // One pass of the dots kernel over C basis vectors i0 .. i0 + C - 1 (C a
 // compile-time count, so the C 16-byte loads of a row group are issued
 // back to back without predicates): acc[u] += V_{i0+u}^T w and
-// acc[8 + u] += V_{i0+u}^T v_j over this thread's row groups.
+// acc[4 + u] += V_{i0+u}^T v_j over this thread's row groups.  Full groups
+// take the unconditional vector loads; the one partial group at the end is
+// read element by element by the thread it falls to.
 template <typename TA, typename TB, int C>
 __device__ __forceinline__ void dots_pass(int64_t n, int64_t ldv,
                                           const TB* __restrict__ V,
                                           const TA* __restrict__ w,
                                           const TB* __restrict__ vj, int i0,
-                                          TA (&acc)[16])
+                                          TA (&acc)[8])
 {
     constexpr int R = rows_per_group<TB>();
-    const int64_t groups = ceildiv(n, R);
-    for (int64_t grp = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; grp < groups;
-         grp += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t r0 = grp * R;
-        const int valid = n - r0 < R ? int(n - r0) : R;
+    auto group = [&](int64_t r0, int valid) {
         TA wr[R], vr[R];
         load_rows<TA, R>(w + r0, wr, valid);
         load_basis<TA, TB, R>(vj + r0, vr, valid);
+        TA x[C][R];
+#pragma unroll
+        for (int u = 0; u < C; ++u) load_basis<TA, TB, R>(V + int64_t(i0 + u) * ldv + r0, x[u], valid);
 #pragma unroll
         for (int u = 0; u < C; ++u) {
-            TA x[R];
-            load_basis<TA, TB, R>(V + int64_t(i0 + u) * ldv + r0, x, valid);
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                acc[u] += x[r] * wr[r];
-                acc[8 + u] += x[r] * vr[r];
+                acc[u] += x[u][r] * wr[r];
+                acc[4 + u] += x[u][r] * vr[r];
             }
         }
-    }
+    };
+    const int64_t full = n / R;
+    int64_t grp = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+    for (; grp < full; grp += int64_t(gridDim.x) * blockDim.x) group(grp * R, R);
+    if (grp == full && n % R != 0) group(full * R, int(n % R));
 }
 
 // compact value index c < 2 nvec -> partial row e (h1 at e < kLd, G after)
@@ -310,22 +312,22 @@ __device__ __forceinline__ void fold32(const double* src, int64_t ld, int base, 
 }
 
 // Step j, part 3: h1 = V_{0..j}^T w and G(:, j) = V_{0..j}^T v_j: passes of
-// up to 8 basis vectors, a thread taking one row group per iteration with
-// the 16 sums of the pass in registers (3 blocks per SM).  Per pass
+// up to 4 basis vectors, a thread taking one row group per iteration with
+// the 8 sums of the pass in registers (4 blocks per SM).  Per pass
 // one multi-value warp reduction and one block reduction into value-major
 // partials (partials[e * gridDim.x + block]).  The last block of every 32
 // blocks folds its group's partials; the last group to finish folds the
 // groups, completes G's row and column j and forms h = (2I - G) h1.  The
 // summation order is fixed: the result does not depend on scheduling.
 template <typename TA, typename TB>
-__global__ void __launch_bounds__(kSolverBlock, 3)
+__global__ void __launch_bounds__(kSolverBlock, 4)
     gmres_dots_kernel(int64_t n, int64_t ldv, const TB* __restrict__ V,
                       const TA* __restrict__ w, GmresState* st,
                       double* __restrict__ partials, double* __restrict__ gpart)
 {
-    constexpr int CMAX = 8;
+    constexpr int CMAX = 4;
     constexpr int W = kSolverBlock / kWarp;
-    __shared__ double redv[W][16];
+    __shared__ double redv[W][8];
     __shared__ double tot[2 * kLd];
     __shared__ double Gs[kLd * kLd];
     __shared__ int last;
@@ -337,30 +339,26 @@ __global__ void __launch_bounds__(kSolverBlock, 3)
     const int B = gridDim.x;
     for (int i0 = 0; i0 < nvec; i0 += CMAX) {
         const int c = nvec - i0 < CMAX ? nvec - i0 : CMAX;
-        TA acc[16];
+        TA acc[8];
 #pragma unroll
-        for (int u = 0; u < 16; ++u) acc[u] = TA(0);
+        for (int u = 0; u < 8; ++u) acc[u] = TA(0);
         switch (c) {
         case 1: dots_pass<TA, TB, 1>(n, ldv, V, w, vj, i0, acc); break;
         case 2: dots_pass<TA, TB, 2>(n, ldv, V, w, vj, i0, acc); break;
         case 3: dots_pass<TA, TB, 3>(n, ldv, V, w, vj, i0, acc); break;
-        case 4: dots_pass<TA, TB, 4>(n, ldv, V, w, vj, i0, acc); break;
-        case 5: dots_pass<TA, TB, 5>(n, ldv, V, w, vj, i0, acc); break;
-        case 6: dots_pass<TA, TB, 6>(n, ldv, V, w, vj, i0, acc); break;
-        case 7: dots_pass<TA, TB, 7>(n, ldv, V, w, vj, i0, acc); break;
-        default: dots_pass<TA, TB, 8>(n, ldv, V, w, vj, i0, acc); break;
+        default: dots_pass<TA, TB, 4>(n, ldv, V, w, vj, i0, acc); break;
         }
-        warp_multi_sum<TA, 16>(acc, lane);
-        // lane l holds value l / 2: the h1 sum of vector i0 + l / 2 for
-        // l < 16, the G sum of vector i0 + l / 2 - 8 after
-        if ((lane & 1) == 0) redv[wid][lane / 2] = double(acc[0]);
+        warp_multi_sum<TA, 8>(acc, lane);
+        // lane l holds value l / 4: the h1 sum of vector i0 + l / 4 for
+        // l < 16, the G sum of vector i0 + l / 4 - 4 after
+        if ((lane & 3) == 0) redv[wid][lane / 4] = double(acc[0]);
         __syncthreads();
-        if (threadIdx.x < 16) {
-            const int u = threadIdx.x % 8;
+        if (threadIdx.x < 8) {
+            const int u = threadIdx.x % 4;
             if (u < c) {
                 double s = 0.0;
                 for (int k = 0; k < W; ++k) s += redv[k][threadIdx.x];
-                const int e = (threadIdx.x < 8 ? 0 : kLd) + i0 + u;
+                const int e = (threadIdx.x < 4 ? 0 : kLd) + i0 + u;
                 partials[int64_t(e) * B + blockIdx.x] = s;
             }
         }
@@ -498,15 +496,12 @@ __global__ void __launch_bounds__(kSolverBlock)
     const int j = st->j;
     for (int i = threadIdx.x; i <= j; i += kSolverBlock) hs[i] = TA(st->h[i]);
     __syncthreads();
-    const int64_t groups = ceildiv(n, R);
     double nrm = 0.0;
-    for (int64_t grp = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; grp < groups;
-         grp += int64_t(gridDim.x) * kSolverBlock) {
-        const int64_t r0 = grp * R;
-        const int valid = n - r0 < R ? int(n - r0) : R;
+    auto group = [&](int64_t r0, int valid) {
         TA wr[R];
         load_rows<TA, R>(w + r0, wr, valid);
-#pragma unroll 4
+        // more loads in flight for the 4- and 8-row groups (fewer groups)
+#pragma unroll(R == 2 ? 8 : 16)
         for (int i = 0; i <= j; ++i) {
             TA x[R];
             load_basis<TA, TB, R>(V + int64_t(i) * ldv + r0, x, valid);
@@ -517,7 +512,12 @@ __global__ void __launch_bounds__(kSolverBlock)
         store_rows<TA, R>(w + r0, wr, valid);
 #pragma unroll
         for (int r = 0; r < R; ++r) nrm += double(wr[r]) * double(wr[r]);
-    }
+    };
+    // full row groups on the vector path; the partial one by its thread
+    const int64_t full = n / R;
+    int64_t grp = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x;
+    for (; grp < full; grp += int64_t(gridDim.x) * kSolverBlock) group(grp * R, R);
+    if (grp == full && n % R != 0) group(full * R, int(n % R));
     double a[1] = {nrm};
     block_partials<double, 1>(a, partials, red);
     if (last_block_done(&st->ticket, &last)) {
@@ -791,11 +791,11 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
                 n, ldv, da, r, src, V, y, gs);
             if (ell_w > 0) {
                 if (ell_r == kEllRows) {
-                    ell_rows_kernel<TA, kEllRows><<<grid_ell, 256, 0, cs>>>(
+                    ell_rows_kernel<TA, kEllRows, true><<<grid_ell, 256, 0, cs>>>(
                         n, ell_w, ldv, ell_c, ell_v, y, 1, dst, 1, nullptr, nullptr,
                         &gs->idle);
                 } else {
-                    ell_rows_kernel<TA, 1><<<grid_ell, 256, 0, cs>>>(
+                    ell_rows_kernel<TA, 1, true><<<grid_ell, 256, 0, cs>>>(
                         n, ell_w, ldv, ell_c, ell_v, y, 1, dst, 1, nullptr, nullptr,
                         &gs->idle);
                 }

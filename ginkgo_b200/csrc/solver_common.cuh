@@ -123,9 +123,26 @@ __device__ __forceinline__ void sum_partials(const T* partials, int nblocks,
     T acc[M];
 #pragma unroll
     for (int j = 0; j < M; ++j) acc[j] = T(0);
-    for (int b = threadIdx.x; b < nblocks; b += kSolverBlock) {
+    constexpr int kPer = (kSolverGrid + kSolverBlock - 1) / kSolverBlock;
+    if (M * kPer <= 32 && nblocks <= kSolverGrid) {
+        // every load of this thread in flight at once, summed in block order
+        T v[kPer][M];
 #pragma unroll
-        for (int j = 0; j < M; ++j) acc[j] += __ldcg(partials + b * M + j);
+        for (int q = 0; q < kPer; ++q) {
+            const int b = threadIdx.x + q * kSolverBlock;
+#pragma unroll
+            for (int j = 0; j < M; ++j) v[q][j] = b < nblocks ? __ldcg(partials + b * M + j) : T(0);
+        }
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+#pragma unroll
+            for (int j = 0; j < M; ++j) acc[j] += v[q][j];
+        }
+    } else {
+        for (int b = threadIdx.x; b < nblocks; b += kSolverBlock) {
+#pragma unroll
+            for (int j = 0; j < M; ++j) acc[j] += __ldcg(partials + b * M + j);
+        }
     }
 #pragma unroll
     for (int j = 0; j < M; ++j) acc[j] = warp_sum(acc[j]);

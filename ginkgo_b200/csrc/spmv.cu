@@ -724,6 +724,32 @@ int sellp_spmv(int64_t n, int64_t num_cols, int64_t slice_size,
     if (n == 0 || k == 0) return B2S_OK;
     cudaStream_t st = as_stream(stream);
     const int64_t grid = ceildiv(n, kBlock);
+    constexpr int R = int(16 / sizeof(T));
+    if (k == 1 && slice_size % R == 0 && reinterpret_cast<uintptr_t>(ci) % 16 == 0 &&
+        reinterpret_cast<uintptr_t>(v) % 16 == 0) {
+        // one right-hand side: R rows of a slice per thread, 16-byte loads
+        int shift = -1;
+        if ((slice_size & (slice_size - 1)) == 0) {
+            shift = 0;
+            while ((int64_t(1) << shift) < slice_size) ++shift;
+        }
+        // FP64 (2-row groups): a persistent grid, so most slice lookups
+        // are prefetched; FP32 (4-row groups): one group per thread (each
+        // measured faster on the 7-point matrix)
+        const int64_t groups_blocks = ceildiv(ceildiv(n, R), kBlock);
+        if constexpr (sizeof(T) == 8) {
+            sellp_rows_kernel<T, R, true>
+                <<<std::min<int64_t>(groups_blocks, int64_t(kNumSMs) * 6), kBlock, 0, st>>>(
+                    int(n), int(slice_size), shift, slice_sets, slice_lengths, ci, v, b, ldb,
+                    c, ldc, alpha, beta);
+        } else {
+            sellp_rows_kernel<T, R, false><<<groups_blocks, kBlock, 0, st>>>(
+                int(n), int(slice_size), shift, slice_sets, slice_lengths, ci, v, b, ldb, c,
+                ldc, alpha, beta);
+        }
+        B2S_LAUNCH_CHECK();
+        return B2S_OK;
+    }
     for (int64_t col0 = 0; col0 < k;) {
         const int kk = rhs_chunk(k - col0);
         const bool vec = vec_ok(b, ldb, col0, kk);

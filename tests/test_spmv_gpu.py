@@ -149,10 +149,10 @@ def test_empty_matrix(exe, fmt):
 
 
 @pytest.mark.parametrize("dt", [torch.float64, torch.float32])
-def test_ell_one_rhs_row_groups_and_odd_stride(exe, dt):
+def test_ell_sellp_one_rhs_row_groups(exe, dt):
     # one right-hand side runs R = 16 / sizeof(value) rows per thread when
-    # the stride allows 16-byte loads (3376), element by element otherwise
-    # (3375); both against the oracle, plain and advanced
+    # the layout allows 16-byte loads, the row-per-thread kernel otherwise;
+    # all against the oracle, plain and advanced
     rp, ci, v = stencils.anisotropic_27pt(15)
     n = len(rp) - 1
     v = v.astype(NP[dt])
@@ -162,8 +162,12 @@ def test_ell_one_rhs_row_groups_and_odd_stride(exe, dt):
     ref = orc.csr_spmv(rp, ci, v, x)
     ref2 = orc.csr_spmv(rp, ci, v, x, y0, 0.5, -1.5)
     A = Csr.read(exe, rp, ci, v, dtype=dt)
-    for stride in (n, n + 1):
-        E = A.convert_to_ell(stride=stride)
+    # Ell with an odd and an even stride; Sellp with a slice size that is
+    # not a multiple of the row group (7) and two that are (32, 64; the last
+    # slice partial)
+    ops = [A.convert_to_ell(stride=n), A.convert_to_ell(stride=n + 1)]
+    ops += [A.convert_to_sellp(ss, sf) for ss, sf in ((7, 1), (32, 1), (64, 2))]
+    for E in ops:
         y = torch.full((n, 1), float("nan"), dtype=dt, device="cuda")
         E.apply(torch.from_numpy(x).cuda(), y)
         assert_spmv_close(rp, ci, v, x, y.cpu().numpy(), ref, TOL[dt])
