@@ -12,13 +12,17 @@
 
 namespace b2s {
 
-// R consecutive elements of 4, 8, 16 or 32 bytes in total, evict-first.
+// R consecutive elements of 2, 4, 8, 16 or 32 bytes in total, evict-first.
 template <typename T, int R>
 __device__ __forceinline__ void load_stream_rows(const T* p, T (&o)[R])
 {
     constexpr int kBytes = int(R * sizeof(T));
-    static_assert(kBytes == 4 || kBytes == 8 || kBytes % 16 == 0, "vector width");
-    if constexpr (kBytes == 4) {
+    static_assert(kBytes == 2 || kBytes == 4 || kBytes == 8 || kBytes % 16 == 0,
+                  "vector width");
+    if constexpr (kBytes == 2) {
+        const unsigned short u = __ldcs(reinterpret_cast<const unsigned short*>(p));
+        memcpy(o, &u, 2);
+    } else if constexpr (kBytes == 4) {
         const unsigned u = __ldcs(reinterpret_cast<const unsigned*>(p));
         memcpy(o, &u, 4);
     } else if constexpr (kBytes == 8) {
@@ -32,16 +36,19 @@ __device__ __forceinline__ void load_stream_rows(const T* p, T (&o)[R])
     }
 }
 
+// Padding marker of the 16-bit offset layout (offsets lie in -32767..32767).
+constexpr int16_t kEllPad16 = INT16_MIN;
+
 // y = A x (or alpha A x + beta y) over an Ell layout: entry k of row r at
 // k * ld + r (ld a multiple of R, every row group 16-byte aligned), padding
 // entries with column -1; the slots of rows n .. ld - 1 are never gathered
 // through.  x and y are strided by ldx and ldy.  Entries are
 // summed in stored order.  PLAIN: unit strides and y = A x (no alpha/beta).
 // A launch whose *skip is non-zero returns at once.
-template <typename T, int R, bool PLAIN = false>
+template <typename T, int R, bool PLAIN = false, typename IT = int32_t>
 __global__ void __launch_bounds__(256)
     ell_rows_kernel(int64_t n, int width, int64_t ld,
-                    const int32_t* __restrict__ cols, const T* __restrict__ vals,
+                    const IT* __restrict__ cols, const T* __restrict__ vals,
                     const T* __restrict__ x, int64_t ldx, T* __restrict__ y,
                     int64_t ldy, const T* __restrict__ alpha,
                     const T* __restrict__ beta, const int* __restrict__ skip)
@@ -57,18 +64,28 @@ __global__ void __launch_bounds__(256)
         T acc[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) acc[r] = T(0);
-        const int32_t* cp = cols + r0;
+        const IT* cp = cols + r0;
         const T* vp = vals + r0;
 #pragma unroll 4
         for (int k = 0; k < width; ++k) {
-            int32_t c[R];
+            IT c[R];
             T v[R];
-            load_stream_rows<int32_t, R>(cp + int64_t(k) * ld, c);
+            load_stream_rows<IT, R>(cp + int64_t(k) * ld, c);
             load_stream_rows<T, R>(vp + int64_t(k) * ld, v);
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                const int64_t xo = PLAIN ? int64_t(c[r]) : int64_t(c[r]) * ldx;
-                const T xv = r < valid && c[r] >= 0 ? __ldg(x + xo) : T(0);
+                // 16-bit entries are offsets from the row, kEllPad16 padding
+                int64_t col;
+                bool used;
+                if constexpr (sizeof(IT) == 2) {
+                    col = r0 + r + c[r];
+                    used = c[r] != kEllPad16;
+                } else {
+                    col = c[r];
+                    used = c[r] >= 0;
+                }
+                const int64_t xo = PLAIN ? col : col * ldx;
+                const T xv = r < valid && used ? __ldg(x + xo) : T(0);
                 acc[r] += v[r] * xv;
             }
         }
@@ -185,6 +202,36 @@ __global__ void ell_fill_kernel(int64_t n, int64_t ld, int width,
             vals[idx] = T(v[rs + k]);
         } else {
             cols[idx] = -1;
+            vals[idx] = T(0);
+        }
+    }
+}
+
+// The same copy with 16-bit column offsets col - row (a quarter less
+// traffic for FP32 values); an offset outside -32767..32767 sets
+// *too_far and the caller falls back to ell_fill_kernel.
+template <typename T>
+__global__ void ell_fill16_kernel(int64_t n, int64_t ld, int width,
+                                  const int32_t* __restrict__ rp,
+                                  const int32_t* __restrict__ ci,
+                                  const double* __restrict__ v,
+                                  int16_t* __restrict__ cols, T* __restrict__ vals,
+                                  int* too_long, int* too_far)
+{
+    const int64_t row = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+    if (row >= ld) return;
+    const int rs = row < n ? rp[row] : 0;
+    const int len = row < n ? rp[row + 1] - rs : 0;
+    if (len > width) *too_long = 1;
+    for (int k = 0; k < width; ++k) {
+        const int64_t idx = int64_t(k) * ld + row;
+        if (k < len) {
+            const int64_t d = int64_t(ci[rs + k]) - row;
+            if (d < -32767 || d > 32767) *too_far = 1;
+            cols[idx] = int16_t(d < -32767 || d > 32767 ? 0 : d);
+            vals[idx] = T(v[rs + k]);
+        } else {
+            cols[idx] = kEllPad16;
             vals[idx] = T(0);
         }
     }

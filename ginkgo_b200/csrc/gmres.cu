@@ -26,9 +26,10 @@
 // Kernels per Arnoldi step j (one CUDA graph per restart cycle):
 //   prepare v_j = round_basis(src * scale) stored in the basis (src = the
 //           previous unnormalised vector, or r at j = 0); y = D^-1 v_j
-//   spmv    w = A y on a column-major (Ell) copy of A in the Arnoldi type,
-//           16 bytes of rows per thread, when its padding stays within a
-//           quarter of nnz; else the pipelined Csr kernel on A
+//   spmv    w = A y on a column-major (Ell) copy of A in the Arnoldi type
+//           with 16-bit column offsets (32-bit columns when an offset does
+//           not fit), when its padding stays within a quarter of nnz; else
+//           the pipelined Csr kernel on A
 //   dots    h1 = V_{0..j}^T w and G(:, j) = V_{0..j}^T v_j in one pass over
 //           the basis (all sums of a thread in registers); last block:
 //           h = (2I - G) h1
@@ -61,6 +62,7 @@ struct GmresState {
     int idle;  // done || cycle_done: the Arnoldi kernels have nothing to do
     unsigned ticket;
     int too_long;  // a row is longer than the Ell copy's width
+    int too_far;   // a column offset does not fit 16 bits
     unsigned gticket[kDotsMaxGroups + 1];  // dots: per group of 32 blocks
     double bnorm, rnorm, reduction, inner_reduction, inner_thresh;
     double scale;  // v_j = src * scale: 1/||r|| at j = 0, 1/H(j, j-1) else
@@ -745,16 +747,25 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
     const int ell_w = lay.ell_width;
     int32_t* ell_c = reinterpret_cast<int32_t*>(w + lay.off_ell_c);
     TA* ell_v = reinterpret_cast<TA*>(w + lay.off_ell_v);
+    // 16-bit column offsets when every |col - row| fits, else 32-bit columns
+    bool ell16 = false;
     if (ell_w > 0) {
-        ell_fill_kernel<TA><<<ceildiv(ldv, 256), 256, 0, st>>>(n, ldv, ell_w, rp, ci, v64,
-                                                               ell_c, ell_v, &gs->too_long);
+        ell_fill16_kernel<TA><<<ceildiv(ldv, 256), 256, 0, st>>>(
+            n, ldv, ell_w, rp, ci, v64, reinterpret_cast<int16_t*>(ell_c), ell_v,
+            &gs->too_long, &gs->too_far);
         B2S_LAUNCH_CHECK();
-        int too_long = 0;
-        B2S_CUDA_TRY(cudaMemcpyAsync(&too_long, &gs->too_long, sizeof(int),
+        int flags[2] = {0, 0};  // too_long, too_far
+        B2S_CUDA_TRY(cudaMemcpyAsync(flags, &gs->too_long, sizeof(flags),
                                      cudaMemcpyDeviceToHost, st));
         B2S_CUDA_TRY(cudaStreamSynchronize(st));
-        B2S_CHECK_ARG(!too_long, "max_row_nnz (%lld) is smaller than the longest row",
+        B2S_CHECK_ARG(!flags[0], "max_row_nnz (%lld) is smaller than the longest row",
                       (long long)max_row_nnz);
+        ell16 = !flags[1];
+        if (!ell16) {
+            ell_fill_kernel<TA><<<ceildiv(ldv, 256), 256, 0, st>>>(
+                n, ldv, ell_w, rp, ci, v64, ell_c, ell_v, &gs->too_long);
+            B2S_LAUNCH_CHECK();
+        }
     }
     constexpr int kEllRows = int(16 / sizeof(TA));
     const int ell_r = ell_rows_per_thread<TA>(ell_w);
@@ -790,10 +801,17 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
             gmres_prepare_kernel<TA, TB><<<grid_vec, kSolverBlock, 0, cs>>>(
                 n, ldv, da, r, src, V, y, gs);
             if (ell_w > 0) {
-                if (ell_r == kEllRows) {
+                const int16_t* c16 = reinterpret_cast<const int16_t*>(ell_c);
+                if (ell_r == kEllRows && ell16) {
+                    ell_rows_kernel<TA, kEllRows, true, int16_t><<<grid_ell, 256, 0, cs>>>(
+                        n, ell_w, ldv, c16, ell_v, y, 1, dst, 1, nullptr, nullptr, &gs->idle);
+                } else if (ell_r == kEllRows) {
                     ell_rows_kernel<TA, kEllRows, true><<<grid_ell, 256, 0, cs>>>(
                         n, ell_w, ldv, ell_c, ell_v, y, 1, dst, 1, nullptr, nullptr,
                         &gs->idle);
+                } else if (ell16) {
+                    ell_rows_kernel<TA, 1, true, int16_t><<<grid_ell, 256, 0, cs>>>(
+                        n, ell_w, ldv, c16, ell_v, y, 1, dst, 1, nullptr, nullptr, &gs->idle);
                 } else {
                     ell_rows_kernel<TA, 1, true><<<grid_ell, 256, 0, cs>>>(
                         n, ell_w, ldv, ell_c, ell_v, y, 1, dst, 1, nullptr, nullptr,

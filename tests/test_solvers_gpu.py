@@ -297,3 +297,33 @@ def test_gmres_rejects_row_bound_below_longest_row(exe):
     x = torch.zeros(n, dtype=torch.float64, device="cuda")
     with pytest.raises(RuntimeError, match="longest row"):
         s.apply(torch.from_numpy(b).cuda(), x)
+
+
+@pytest.mark.parametrize("basis", [None, "f32"])
+def test_gmres_far_columns_fall_back_to_32bit_offsets(exe, basis):
+    # the solver's column-major copy stores col - row in 16 bits when every
+    # offset fits; a coupling 35000 rows away forces 32-bit columns
+    n = 40000
+    rows, cols, vals = [], [], []
+    for i in range(n):
+        for j, a in ((i - 1, -1.0), (i, 4.0), (i + 1, -1.0), ((i + 35000) % n, 0.5)):
+            if 0 <= j < n:
+                rows.append(i), cols.append(j), vals.append(a)
+    order = np.lexsort((np.array(cols), np.array(rows)))
+    r = np.array(rows)[order]
+    ci = np.array(cols, dtype=np.int32)[order]
+    v = np.array(vals)[order]
+    rp = np.concatenate([[0], np.cumsum(np.bincount(r, minlength=n))]).astype(np.int32)
+    b = np.random.default_rng(4).standard_normal(n)
+    A = Csr.read(exe, rp, ci, v)
+    g = (Gmres.build().with_krylov_dim(20)
+         .with_preconditioner(Jacobi.build().with_max_block_size(1)))
+    if basis is None:
+        s = g.with_criteria(*crit(500, 1e-10)).on(exe).generate(A)
+    else:
+        s = (Ir.build().with_solver(g.with_storage_precision(basis))
+             .with_criteria(*crit(500, 1e-10)).on(exe).generate(A))
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    s.apply(torch.from_numpy(b).cuda(), x)
+    assert s.logger.has_converged
+    assert explicit_rel_res(rp, ci, v, x.cpu().numpy(), b)[0] <= 1e-10
