@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(256)
         for (int r = 0; r < R; ++r) acc[r] = T(0);
         const IT* cp = cols + r0;
         const T* vp = vals + r0;
-#pragma unroll 4
+#pragma unroll(sizeof(T) == 4 ? 8 : 4)
         for (int k = 0; k < width; ++k) {
             IT c[R];
             T v[R];

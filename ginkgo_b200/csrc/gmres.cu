@@ -23,9 +23,12 @@
 // the Givens residual estimate reaches the goal, and convergence is declared
 // only on the explicit FP64 residual.
 //
+// The basis is stored unnormalised: V_i = round_basis(w''_{i-1}) (V_0 =
+// round_basis(r)) with v_i = sigma_i V_i, sigma_i = 1 / ||w''_{i-1}||, and
+// the sigmas are folded into the projection coefficients, so the vector
+// that enters step j + 1 is written by step j's update pass itself.
+//
 // Kernels per Arnoldi step j (one CUDA graph per restart cycle):
-//   prepare v_j = round_basis(src * scale) stored in the basis (src = the
-//           previous unnormalised vector, or r at j = 0); y = D^-1 v_j
 //   spmv    w = A y on a column-major (Ell) copy of A in the Arnoldi type
 //           with 16-bit column offsets (32-bit columns when an offset does
 //           not fit), when its padding stays within a quarter of nnz; else
@@ -33,11 +36,13 @@
 //   dots    h1 = V_{0..j}^T w and G(:, j) = V_{0..j}^T v_j in one pass over
 //           the basis (all sums of a thread in registers); last block:
 //           h = (2I - G) h1
-//   update  w'' = w - V h and ||w''||; last block: Hessenberg column,
-//           Givens update, residual estimate, early end of the cycle, back
-//           substitution
-// per cycle: x += D^-1 V y (FP64 accumulate) with r = b, then r -= A x with
-// the pipelined kernel in FP64, then ||r||, ||b|| and the restart check.
+//   update  w'' = sigma_j w - V (sigma h) and ||w''||, V_{j+1} and the next
+//           SpMV input y = D^-1 V_{j+1} in the same pass; last block:
+//           Hessenberg column, Givens update, residual estimate, early end
+//           of the cycle, back substitution
+// per cycle: x += D^-1 V (sigma y) (FP64 accumulate) with r = b, then
+// r -= A x with the pipelined kernel in FP64, then ||r||, ||b||, V_0, the
+// first SpMV input and the restart check.
 // The serial parts (Givens chain, back substitution, (2I - G) h1) run in
 // the last block on shared-memory copies of the small arrays.
 #include <cuda_bf16.h>
@@ -65,7 +70,7 @@ struct GmresState {
     int too_far;   // a column offset does not fit 16 bits
     unsigned gticket[kDotsMaxGroups + 1];  // dots: per group of 32 blocks
     double bnorm, rnorm, reduction, inner_reduction, inner_thresh;
-    double scale;  // v_j = src * scale: 1/||r|| at j = 0, 1/H(j, j-1) else
+    double sigma[kLd];  // stored basis vector i is v_i / sigma[i] (unnormalised)
     double minus_one, one;       // alpha, beta of r = b - A x
     double h[kLd];               // combined projection coefficients of step j
     double H[kMaxKrylov * kLd];  // column j at H[j * kLd]
@@ -158,50 +163,6 @@ template <typename TB>
 __host__ __device__ constexpr int rows_per_group()
 {
     return int(16 / sizeof(TB));
-}
-
-// Step j, part 1: v_j = round_basis(src * scale) stored in the basis and
-// y = D^-1 v_j, the SpMV input (src = the previous unnormalised vector, or
-// r at j = 0).  One row group per thread and iteration.
-template <typename TA, typename TB>
-__global__ void __launch_bounds__(kSolverBlock)
-    gmres_prepare_kernel(int64_t n, int64_t ldv, const TA* __restrict__ dinv,
-                         const double* __restrict__ r64,
-                         const TA* __restrict__ w_src, TB* __restrict__ V,
-                         TA* __restrict__ y, GmresState* st)
-{
-    constexpr int R = rows_per_group<TB>();
-    if (st->idle) return;
-    const int j = st->j;
-    const TA scale = TA(st->scale);
-    TB* vj = V + int64_t(j) * ldv;
-    const int64_t groups = ceildiv(n, R);
-    for (int64_t q = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; q < groups;
-         q += int64_t(gridDim.x) * kSolverBlock) {
-        const int64_t r0 = q * R;
-        const int valid = n - r0 < R ? int(n - r0) : R;
-        TA src[R], d[R];
-        if (j == 0) {
-#pragma unroll
-            for (int r = 0; r < R; ++r) src[r] = r < valid ? TA(r64[r0 + r]) : TA(0);
-        } else {
-            load_rows<TA, R>(w_src + r0, src, valid);
-        }
-        if (dinv) {
-#pragma unroll
-            for (int r = 0; r < R; ++r) d[r] = r < valid ? dinv[r0 + r] : TA(0);
-        }
-        TB vb[R];
-        TA yv[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            vb[r] = to_basis<TB>(mul_rn(src[r], scale));
-            const TA va = from_basis<TA>(vb[r]);
-            yv[r] = dinv ? d[r] * va : va;
-        }
-        store_rows<TB, R>(vj + r0, vb, valid);
-        store_rows<TA, R>(y + r0, yv, valid);
-    }
 }
 
 // Sums each of the N values v[0..N) (N = 8, 16 or 32 P) over the warp:
@@ -372,8 +333,15 @@ __global__ void __launch_bounds__(kSolverBlock, 4)
     if (!last_of(&st->gticket[g], unsigned(gsize), &last)) return;
     fold32(partials, B, g * kDotsGroup, gsize, nvec, gpart, kDotsMaxGroups, g);
     if (!last_of(&st->ticket, unsigned(ngroups), &last)) return;
-    // tot[0..nvec): h1, tot[kLd + i]: G(i, j)
+    // tot[0..nvec): h1, tot[kLd + i]: G(i, j), of the stored (unnormalised)
+    // vectors; scaled to the normalised basis by sigma_i sigma_j
     fold32(gpart, kDotsMaxGroups, 0, ngroups, nvec, tot, 1, 0);
+    __syncthreads();
+    if (threadIdx.x <= j) {
+        const double sc = st->sigma[threadIdx.x] * st->sigma[j];
+        tot[threadIdx.x] *= sc;
+        tot[kLd + threadIdx.x] *= sc;
+    }
     __syncthreads();
     // G(0..j-1, 0..j-1) from the earlier steps of this cycle
     for (int e = threadIdx.x; e < j * kLd; e += kSolverBlock) Gs[e] = st->G[e];
@@ -448,7 +416,7 @@ __device__ void close_step(GmresState* st, double hnorm)
         const int total = st->total_iter + 1;
         st->final_iter = j + 1;
         st->total_iter = total;
-        st->scale = hnorm > 0.0 ? 1.0 / hnorm : 0.0;
+        st->sigma[j + 1] = hnorm > 0.0 ? 1.0 / hnorm : 0.0;
         st->j = j + 1;
         fin = est <= st->inner_thresh || j + 1 >= st->krylov_dim ||
               total >= st->max_iters || !(hnorm > 0.0);
@@ -480,13 +448,17 @@ __device__ void close_step(GmresState* st, double hnorm)
     }
 }
 
-// w'' = w - V h, ||w''||, one row group per thread and iteration (16-byte
-// basis loads, subtracted in order i = 0..j); the last block closes the
-// Arnoldi step.
+// w'' = sigma_j w - sum_i (h_i sigma_i) V_i (the stored vectors are
+// unnormalised), ||w''||, one row group per thread and iteration (16-byte
+// basis loads, subtracted in order i = 0..j).  The same pass stores the
+// next basis vector V_{j+1} = round_basis(w'') and the next SpMV input
+// y = D^-1 V_{j+1}; its scale sigma_{j+1} = 1 / ||w''|| is set by the last
+// block, which closes the Arnoldi step.
 template <typename TA, typename TB>
 __global__ void __launch_bounds__(kSolverBlock)
-    gmres_update_kernel(int64_t n, int64_t ldv, const TB* __restrict__ V,
-                        TA* __restrict__ w, GmresState* st,
+    gmres_update_kernel(int64_t n, int64_t ldv, TB* __restrict__ V,
+                        const TA* __restrict__ w, const TA* __restrict__ dinv,
+                        TA* __restrict__ y, GmresState* st,
                         double* __restrict__ partials)
 {
     constexpr int R = rows_per_group<TB>();
@@ -496,12 +468,16 @@ __global__ void __launch_bounds__(kSolverBlock)
     __shared__ int last;
     if (st->idle) return;
     const int j = st->j;
-    for (int i = threadIdx.x; i <= j; i += kSolverBlock) hs[i] = TA(st->h[i]);
+    for (int i = threadIdx.x; i <= j; i += kSolverBlock) hs[i] = TA(st->h[i] * st->sigma[i]);
+    const TA sj = TA(st->sigma[j]);
     __syncthreads();
+    TB* vnext = V + int64_t(j + 1) * ldv;
     double nrm = 0.0;
     auto group = [&](int64_t r0, int valid) {
         TA wr[R];
         load_rows<TA, R>(w + r0, wr, valid);
+#pragma unroll
+        for (int r = 0; r < R; ++r) wr[r] *= sj;
         // more loads in flight for the 4- and 8-row groups (fewer groups)
 #pragma unroll(R == 2 ? 8 : 16)
         for (int i = 0; i <= j; ++i) {
@@ -511,9 +487,19 @@ __global__ void __launch_bounds__(kSolverBlock)
 #pragma unroll
             for (int r = 0; r < R; ++r) wr[r] -= hi * x[r];
         }
-        store_rows<TA, R>(w + r0, wr, valid);
+        TB vb[R];
+        TA yv[R];
+        TA d[R];
+        if (dinv) load_rows<TA, R>(dinv + r0, d, valid);
 #pragma unroll
-        for (int r = 0; r < R; ++r) nrm += double(wr[r]) * double(wr[r]);
+        for (int r = 0; r < R; ++r) {
+            vb[r] = to_basis<TB>(wr[r]);
+            const TA va = from_basis<TA>(vb[r]);
+            yv[r] = dinv ? d[r] * va : va;
+            nrm += double(wr[r]) * double(wr[r]);
+        }
+        store_rows<TB, R>(vnext + r0, vb, valid);
+        store_rows<TA, R>(y + r0, yv, valid);
     };
     // full row groups on the vector path; the partial one by its thread
     const int64_t full = n / R;
@@ -541,7 +527,7 @@ __global__ void __launch_bounds__(kSolverBlock)
     __shared__ TA ys[kMaxKrylov];
     if (st->done) return;
     const int m = st->final_iter;
-    for (int i = threadIdx.x; i < m; i += kSolverBlock) ys[i] = TA(st->y[i]);
+    for (int i = threadIdx.x; i < m; i += kSolverBlock) ys[i] = TA(st->y[i] * st->sigma[i]);
     __syncthreads();
     const int64_t groups = ceildiv(n, R);
     for (int64_t grp = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; grp < groups;
@@ -575,12 +561,15 @@ __global__ void __launch_bounds__(kSolverBlock)
     }
 }
 
-// ||r||, ||b|| of r = b - A x; the last block checks convergence and sets up
-// the next cycle (the reference's restart step).
+// ||r||, ||b|| of r = b - A x, and V_0 = round_basis(r), y = D^-1 V_0 for
+// the next cycle; the last block checks convergence and sets up the next
+// cycle (the reference's restart step).
+template <typename TA, typename TB>
 __global__ void __launch_bounds__(kSolverBlock)
     gmres_restart_kernel(int64_t n, const double* __restrict__ r,
-                         const double* __restrict__ b, GmresState* st,
-                         double* __restrict__ partials)
+                         const double* __restrict__ b, TB* __restrict__ V0,
+                         const TA* __restrict__ dinv, TA* __restrict__ y,
+                         GmresState* st, double* __restrict__ partials)
 {
     __shared__ double red[kSolverBlock / kWarp * 2];
     __shared__ double tot[2];
@@ -592,6 +581,12 @@ __global__ void __launch_bounds__(kSolverBlock)
         const double rr = r[row], bb = b[row];
         acc2[0] += rr * rr;
         acc2[1] += bb * bb;
+        // the first basis vector of the next cycle, unnormalised
+        // (sigma_0 = 1 / ||r||), and the first SpMV input
+        const TB vb = to_basis<TB>(TA(rr));
+        V0[row] = vb;
+        const TA va = from_basis<TA>(vb);
+        y[row] = dinv ? dinv[row] * va : va;
     }
     block_partials<double, 2>(acc2, partials, red);
     if (last_block_done(&st->ticket, &last)) {
@@ -616,7 +611,7 @@ __global__ void __launch_bounds__(kSolverBlock)
                 st->idle = 0;
                 st->g[0] = rn;
                 for (int i = 1; i <= kMaxKrylov; ++i) st->g[i] = 0.0;
-                st->scale = 1.0 / rn;
+                st->sigma[0] = 1.0 / rn;
                 st->inner_thresh = fmax(st->inner_reduction * rn,
                                         st->reduction * st->bnorm);
             }
@@ -645,7 +640,7 @@ inline int gmres_ell_width(int64_t n, int64_t nnz, int64_t max_row_nnz)
 }
 
 struct GmresLayout {
-    int64_t bytes, off_st, off_r, off_w0, off_w1, off_y, off_v, off_partials,
+    int64_t bytes, off_st, off_r, off_w, off_y, off_v, off_partials,
         off_a32, off_d32, off_ell_c, off_ell_v, off_gpart;
     int ell_width;
 };
@@ -658,8 +653,7 @@ GmresLayout gmres_layout(int64_t n, int64_t nnz, int64_t max_row_nnz, int d, boo
     l.off_st = c.take<GmresState>(1);
     l.off_r = c.take<double>(n);
     const int64_t ldv = gmres_ld(n);
-    l.off_w0 = c.take<TA>(ldv);
-    l.off_w1 = c.take<TA>(ldv);
+    l.off_w = c.take<TA>(ldv);
     l.off_y = c.take<TA>(ldv);
     l.off_v = c.take<TB>((int64_t(d) + 1) * ldv);
     l.off_partials = c.take<double>(int64_t(kSolverGrid) * 2 * kLd);
@@ -709,8 +703,7 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
     char* w = static_cast<char*>(workspace);
     auto* gs = reinterpret_cast<GmresState*>(w + lay.off_st);
     double* r = reinterpret_cast<double*>(w + lay.off_r);
-    TA* wv[2] = {reinterpret_cast<TA*>(w + lay.off_w0),
-                 reinterpret_cast<TA*>(w + lay.off_w1)};
+    TA* wbuf = reinterpret_cast<TA*>(w + lay.off_w);
     TA* y = reinterpret_cast<TA*>(w + lay.off_y);
     TB* V = reinterpret_cast<TB*>(w + lay.off_v);
     double* partials = reinterpret_cast<double*>(w + lay.off_partials);
@@ -789,17 +782,17 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
             kernel<<<grid, kAsyncBlock, 0, cs>>>(n, rp, ci, v64, x, 1, r, 1,
                                                  &gs->minus_one, &gs->one, &gs->done);
         });
-        gmres_restart_kernel<<<grid_vec, kSolverBlock, 0, cs>>>(n, r, b, gs, partials);
+        gmres_restart_kernel<TA, TB><<<grid_vec, kSolverBlock, 0, cs>>>(n, r, b, V, da, y,
+                                                                        gs, partials);
     };
     // first residual outside the graph (final_iter = 0: x is not touched)
     restart(st);
     B2S_LAUNCH_CHECK();
     auto capture = [&](cudaStream_t cs) -> int {
         for (int j = 0; j < krylov_dim; ++j) {
-            TA* src = wv[(j + 1) % 2];
-            TA* dst = wv[j % 2];
-            gmres_prepare_kernel<TA, TB><<<grid_vec, kSolverBlock, 0, cs>>>(
-                n, ldv, da, r, src, V, y, gs);
+            // y (the SpMV input) was written by the restart kernel (j = 0)
+            // or by the previous step's update
+            TA* dst = wbuf;
             if (ell_w > 0) {
                 const int16_t* c16 = reinterpret_cast<const int16_t*>(ell_c);
                 if (ell_r == kEllRows && ell16) {
@@ -828,15 +821,14 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
             gmres_dots_kernel<TA, TB><<<grid_dots, kSolverBlock, 0, cs>>>(
                 n, ldv, V, dst, gs, partials, gpart);
             gmres_update_kernel<TA, TB><<<grid_vec, kSolverBlock, 0, cs>>>(
-                n, ldv, V, dst, gs, partials);
+                n, ldv, V, dst, da, y, gs, partials);
             B2S_LAUNCH_CHECK();
         }
         restart(cs);
         B2S_LAUNCH_CHECK();
         return B2S_OK;
     };
-    // the spmv of step j reads the vector prepared at step j; the update of
-    // step j - 1 wrote the other w buffer, which prepare reads
+    // every step: y -> spmv -> w -> dots, update -> V_{j+1}, y
     cudaStream_t cap;
     B2S_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
     cudaGraph_t graph = nullptr;
