@@ -14,10 +14,15 @@
 //               ResidualNorm(rhs_norm) checks  (step_2 + precond + 2 dots +
 //               residual_norm check)
 //
+// With four or more right-hand sides (FP64; eight or more in FP32) the same
+// two passes run with lanes owning 16-byte column slices of each row.
+//
 // z is never stored.  Per-column stopping status uses the reference's bit
 // layout; stopped columns are frozen as in the reference.  The host replays
 // a CUDA graph of `check_every` iterations and reads the stop flag once per
 // replay.
+#include <cstring>
+
 #include "solver_common.cuh"
 
 namespace b2s {
@@ -231,6 +236,215 @@ __global__ void __launch_bounds__(kSolverBlock)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Four or more right-hand sides: lanes own columns.  A row's KL = K / VW
+// lanes each hold VW = 16 / sizeof(T) consecutive columns (one 16-byte
+// vector of the row-major n x K blocks), so the gathers of r(c, :) and
+// p(c, :) are contiguous 16-byte loads across the row's lanes and no
+// shuffle reduction runs per row.  Stopped columns are computed along
+// (their results are never used: the update pass freezes them).
+// ---------------------------------------------------------------------------
+template <typename T, int R>
+__device__ __forceinline__ void ld_vec(const T* p, T (&o)[R])
+{
+    static_assert(R * sizeof(T) == 16, "one 16-byte vector");
+    const uint4 u = *reinterpret_cast<const uint4*>(p);
+    memcpy(o, &u, 16);
+}
+template <typename T, int R>
+__device__ __forceinline__ void st_vec(T* p, const T (&v)[R])
+{
+    uint4 u;
+    memcpy(&u, v, 16);
+    *reinterpret_cast<uint4*>(p) = u;
+}
+
+template <typename T, int K>
+__global__ void __launch_bounds__(kSolverBlock)
+    cg_spmv_lanes_kernel(int64_t n, const int32_t* __restrict__ rp,
+                         const int32_t* __restrict__ ci, const T* __restrict__ v,
+                         const T* __restrict__ dinv, const T* __restrict__ r,
+                         const T* __restrict__ p_old, T* __restrict__ p_new,
+                         T* __restrict__ q, SolveCtl* ctl, CgScalars<T>* sc,
+                         T* __restrict__ partials)
+{
+    constexpr int VW = int(16 / sizeof(T));
+    constexpr int KL = K / VW;         // lanes per row
+    constexpr int RPW = kWarp / KL;    // rows per warp
+    constexpr int W = kSolverBlock / kWarp;
+    __shared__ T red[W][K];
+    __shared__ T tot[K];
+    __shared__ int last;
+    if (ctl->all_stopped) return;
+    const int lane = threadIdx.x % kWarp, wid = threadIdx.x / kWarp;
+    const int col0 = (lane % KL) * VW;
+    bool from_z[VW];
+    T beta[VW];
+#pragma unroll
+    for (int u = 0; u < VW; ++u) {
+        const T pr = sc->prev_rho[col0 + u];
+        from_z[u] = pr == T(0);
+        beta[u] = from_z[u] ? T(0) : sc->rho[col0 + u] / pr;
+    }
+    T dot[VW];
+#pragma unroll
+    for (int u = 0; u < VW; ++u) dot[u] = T(0);
+    const int64_t nwarps = int64_t(gridDim.x) * W;
+    for (int64_t g = blockIdx.x * int64_t(W) + wid; g * RPW < n; g += nwarps) {
+        const int64_t row = g * RPW + lane / KL;
+        if (row < n) {
+            T acc[VW];
+#pragma unroll
+            for (int u = 0; u < VW; ++u) acc[u] = T(0);
+            const int end = rp[row + 1];
+            for (int e = rp[row]; e < end; ++e) {
+                const T a = v[e];
+                const int64_t c = ci[e];
+                const T d = dinv ? dinv[c] : T(1);
+                T rr[VW], pp[VW];
+                ld_vec<T, VW>(r + c * K + col0, rr);
+                ld_vec<T, VW>(p_old + c * K + col0, pp);
+#pragma unroll
+                for (int u = 0; u < VW; ++u) acc[u] += a * cg_p(d, rr[u], beta[u], pp[u], from_z[u]);
+            }
+            const T d = dinv ? dinv[row] : T(1);
+            T rr[VW], pp[VW], pn[VW];
+            ld_vec<T, VW>(r + row * K + col0, rr);
+            ld_vec<T, VW>(p_old + row * K + col0, pp);
+#pragma unroll
+            for (int u = 0; u < VW; ++u) {
+                pn[u] = cg_p(d, rr[u], beta[u], pp[u], from_z[u]);
+                dot[u] += pn[u] * acc[u];
+            }
+            st_vec<T, VW>(p_new + row * K + col0, pn);
+            st_vec<T, VW>(q + row * K + col0, acc);
+        }
+    }
+    // lanes with the same columns: xor over the row bits of the lane index
+#pragma unroll
+    for (int off = KL; off < kWarp; off *= 2) {
+#pragma unroll
+        for (int u = 0; u < VW; ++u) dot[u] += __shfl_xor_sync(0xffffffffu, dot[u], off);
+    }
+    if (lane < KL) {
+#pragma unroll
+        for (int u = 0; u < VW; ++u) red[wid][col0 + u] = dot[u];
+    }
+    __syncthreads();
+    if (threadIdx.x < K) {
+        T s = T(0);
+        for (int k = 0; k < W; ++k) s += red[k][threadIdx.x];
+        partials[blockIdx.x * K + threadIdx.x] = s;
+    }
+    if (last_block_done(&ctl->ticket, &last)) {
+        sum_partials<T, K>(partials, gridDim.x, tot, reinterpret_cast<T*>(red));
+        if (threadIdx.x < K) {
+            const T pq = tot[threadIdx.x];
+            sc->alpha[threadIdx.x] = pq != T(0) ? sc->rho[threadIdx.x] / pq : T(0);
+        }
+        if (threadIdx.x == 0) ctl->ticket = 0;
+    }
+}
+
+// x += alpha p, r -= alpha q over the row-major n x K blocks as one flat
+// array of 16-byte vectors (a thread keeps the same VW columns: the grid
+// stride is a multiple of K); rho' = dot(r, D^-1 r) and ||r||^2 per column.
+template <typename T, int K>
+__global__ void __launch_bounds__(kSolverBlock)
+    cg_update_lanes_kernel(int64_t n, const T* __restrict__ dinv, T* __restrict__ x,
+                           int64_t ldx, T* __restrict__ r, const T* __restrict__ p,
+                           const T* __restrict__ q, SolveCtl* ctl, CgScalars<T>* sc,
+                           T* __restrict__ partials)
+{
+    constexpr int VW = int(16 / sizeof(T));
+    constexpr int KL = K / VW;
+    constexpr int W = kSolverBlock / kWarp;
+    __shared__ T red[W][2 * K];
+    __shared__ T tot[2 * K];
+    __shared__ int last;
+    if (ctl->all_stopped) return;
+    const int lane = threadIdx.x % kWarp, wid = threadIdx.x / kWarp;
+    const int64_t t0 = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x;
+    const int col0 = int((t0 * VW) % K);
+    bool active[VW];
+    T alpha[VW];
+#pragma unroll
+    for (int u = 0; u < VW; ++u) {
+        active[u] = !has_stopped(ctl->status[col0 + u]);
+        alpha[u] = sc->alpha[col0 + u];
+    }
+    T acc[2 * VW];
+#pragma unroll
+    for (int u = 0; u < 2 * VW; ++u) acc[u] = T(0);
+    const int64_t nvec = n * K / VW;
+    for (int64_t t = t0; t < nvec; t += int64_t(gridDim.x) * kSolverBlock) {
+        const int64_t i = t * VW / K;
+        const T d = dinv ? dinv[i] : T(1);
+        T pv[VW], qv[VW], rv[VW];
+        ld_vec<T, VW>(p + t * VW, pv);
+        ld_vec<T, VW>(q + t * VW, qv);
+        ld_vec<T, VW>(r + t * VW, rv);
+#pragma unroll
+        for (int u = 0; u < VW; ++u) {
+            if (active[u]) {
+                x[i * ldx + col0 + u] += alpha[u] * pv[u];
+                const T rr = rv[u] - alpha[u] * qv[u];
+                rv[u] = rr;
+                acc[u] += rr * mul_rn(d, rr);
+                acc[VW + u] += rr * rr;
+            }
+        }
+        st_vec<T, VW>(r + t * VW, rv);
+    }
+#pragma unroll
+    for (int off = KL; off < kWarp; off *= 2) {
+#pragma unroll
+        for (int u = 0; u < 2 * VW; ++u) acc[u] += __shfl_xor_sync(0xffffffffu, acc[u], off);
+    }
+    if (lane < KL) {
+#pragma unroll
+        for (int u = 0; u < VW; ++u) {
+            red[wid][col0 + u] = acc[u];
+            red[wid][K + col0 + u] = acc[VW + u];
+        }
+    }
+    __syncthreads();
+    // partials: rho parts [block][K], then ||r||^2 parts [block][K] (two
+    // K-wide sums keep the last block's register use low)
+    if (threadIdx.x < 2 * K) {
+        T s = T(0);
+        for (int k = 0; k < W; ++k) s += red[k][threadIdx.x];
+        const int j = threadIdx.x % K;
+        partials[(threadIdx.x < K ? 0 : int64_t(gridDim.x) * K) + blockIdx.x * K + j] = s;
+    }
+    if (last_block_done(&ctl->ticket, &last)) {
+        sum_partials<T, K>(partials, gridDim.x, tot, reinterpret_cast<T*>(red));
+        sum_partials<T, K>(partials + int64_t(gridDim.x) * K, gridDim.x, tot + K,
+                           reinterpret_cast<T*>(red));
+        if (threadIdx.x == 0) {
+            ctl->ticket = 0;
+            const int iter = ctl->iter + 1;
+            ctl->iter = iter;
+            int all = 1;
+            for (int j = 0; j < K; ++j) {
+                uint8_t s = ctl->status[j];
+                if (!has_stopped(s)) {
+                    sc->prev_rho[j] = sc->rho[j];
+                    sc->rho[j] = tot[j];
+                    sc->tau[j] = sqrt(tot[K + j]);
+                    if (double(sc->tau[j]) <= ctl->reduction * double(sc->start[j])) {
+                        converge_status(s, kResidualId, true);
+                    }
+                    if (iter >= ctl->max_iters) stop_status(s, kIterationId, true);
+                    ctl->status[j] = s;
+                }
+                all &= has_stopped(s);
+            }
+            ctl->all_stopped = all;
+        }
+    }
+}
+
 struct CgLayout {
     int64_t bytes;
     int64_t off_ctl, off_sc, off_r, off_p0, off_p1, off_q, off_partials;
@@ -308,12 +522,27 @@ int cg_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
             T* po = p[it % 2];
             T* pn = p[(it + 1) % 2];
             B2S_DISPATCH_RHS(K, {
-                B2S_DISPATCH_SW(sw, {
-                    cg_spmv_kernel<T, SW, K><<<grid_spmv, kSolverBlock, 0, cs>>>(
+                if constexpr (K * sizeof(T) >= 32) {
+                    // lanes own 16-byte column slices of a row
+                    constexpr int VW = int(16 / sizeof(T));
+                    constexpr int RPW = kWarp / (K / VW);
+                    const int gs = int(std::min<int64_t>(
+                        std::max<int64_t>(1, ceildiv(n, RPW * (kSolverBlock / kWarp))),
+                        kSolverGrid));
+                    const int gu = int(std::min<int64_t>(
+                        std::max<int64_t>(1, ceildiv(n * K / VW, kSolverBlock)), kSolverGrid));
+                    cg_spmv_lanes_kernel<T, K><<<gs, kSolverBlock, 0, cs>>>(
                         n, rp, ci, v, dinv, r, po, pn, q, ctl, sc, partials);
-                });
-                cg_update_kernel<T, K><<<grid_vec, kSolverBlock, 0, cs>>>(
-                    n, dinv, x, ldx, r, pn, q, ctl, sc, partials);
+                    cg_update_lanes_kernel<T, K><<<gu, kSolverBlock, 0, cs>>>(
+                        n, dinv, x, ldx, r, pn, q, ctl, sc, partials);
+                } else {
+                    B2S_DISPATCH_SW(sw, {
+                        cg_spmv_kernel<T, SW, K><<<grid_spmv, kSolverBlock, 0, cs>>>(
+                            n, rp, ci, v, dinv, r, po, pn, q, ctl, sc, partials);
+                    });
+                    cg_update_kernel<T, K><<<grid_vec, kSolverBlock, 0, cs>>>(
+                        n, dinv, x, ldx, r, pn, q, ctl, sc, partials);
+                }
             });
             B2S_LAUNCH_CHECK();
         }
