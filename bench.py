@@ -307,7 +307,8 @@ def main():
         result["ir_gmres"] = solve
         result["gpu_launches"] += solve.pop("gpu_launches")
     if not args.no_extra:
-        for key, fn in (("batch_bicgstab", batch_section), ("autograd", autograd_section)):
+        for key, fn in (("cg", cg_section), ("batch_bicgstab", batch_section),
+                        ("autograd", autograd_section)):
             try:
                 result[key] = fn(exe, stream)
             except Exception as e:  # a failed optional section is reported, not fatal
@@ -430,6 +431,35 @@ def _event_ms(fn, stream, reps=3):
     return float(np.median(times))
 
 
+def cg_section(exe, stream, grid=256):
+    """The reference's CPU-runnable case on the GPU: CG + scalar Jacobi on
+    the 2D 5-point Poisson matrix (256^2), b = A x_true with x_true ~
+    U[-1, 1] drawn as the reference run drew it (mt19937(1234)), to a
+    relative residual of 1e-10 or 1000 iterations.  The reference executors
+    take 710 iterations to 9.777e-11 on this system."""
+    import torch
+    from ginkgo_b200 import stencils
+    from ginkgo_b200.matrix import Csr
+    from ginkgo_b200.solver import Cg, Iteration, Jacobi, ResidualNorm
+    rp, ci, v = stencils.poisson_2d_5pt(grid)
+    n = len(rp) - 1
+    A = Csr.read(exe, rp, ci, v)
+    xt = torch.from_numpy(stencils.std_uniform(1234, n, -1.0, 1.0)).cuda()
+    b = torch.empty_like(xt)
+    A.apply(xt, b)
+    s = (Cg.build().with_criteria(Iteration.build().with_max_iters(1000),
+                                  ResidualNorm.build().with_reduction_factor(1e-10))
+         .with_preconditioner(Jacobi.build().with_max_block_size(1)).on(exe).generate(A))
+    x = torch.zeros_like(b)
+    ms = _event_ms(lambda: (x.zero_(), s.apply(b, x)), stream)
+    r = b.clone()
+    A.apply(-1.0, x, 1.0, r)
+    return {"workload": f"poisson2d_5pt_{grid}", "n": n, "nnz": len(ci), "ms": round(ms, 3),
+            "iterations": s.logger.num_iterations,
+            "explicit_rel_residual": float(r.norm() / b.norm()),
+            "reference_iterations": 710}
+
+
 def batch_section(exe, stream, num_systems=8192, seed=3):
     """Batched BiCGStab + scalar Jacobi over 8192 convection-diffusion
     systems of n ~ U[32, 1024] rows (batch Ell, ragged), relative tolerance
@@ -449,7 +479,7 @@ def batch_section(exe, stream, num_systems=8192, seed=3):
              .with_tolerance_type("relative").with_preconditioner("jacobi")
              .on(exe).generate(A))
         x = torch.zeros_like(b)
-        s.tune(b, x)
+        table = s.tune(b, x)
         ms = _event_ms(lambda: (x.zero_(), s.apply(b, x)), stream)
         it = s.logger.iterations.double()
         bn = torch.zeros(A.num_systems, dtype=torch.float64, device=b.device)
@@ -457,7 +487,16 @@ def batch_section(exe, stream, num_systems=8192, seed=3):
                                       torch.from_numpy(np.diff(A.host_row_offsets)).cuda())
         bn.index_add_(0, seg, b.double() ** 2)
         rel = s.logger.residual_norms / bn.sqrt()
+        vb = 8 if dt == torch.float64 else 4
+        # two matrix reads per iteration (5 slots per row, value + index)
+        mat_bytes = float((it * torch.from_numpy(np.diff(A.host_row_offsets)).cuda()
+                           .double()).sum()) * 2 * 5 * (vb + 4)
+        buckets = {f"<={1 << k}": {"threads_per_system": int(table[2 * k]),
+                                   "vectors_in_smem": bool(table[2 * k + 1])}
+                   for k in range(12) if table[2 * k] > 0}
         out[name] = {"ms": round(ms, 3), "systems_per_s": round(A.num_systems / ms * 1e3, 1),
+                     "matrix_gbs": round(mat_bytes / (ms * 1e-3) / 1e9, 1),
+                     "tuned_buckets": buckets,
                      "total_rows": int(A.total_rows),
                      "mean_iterations": round(float(it.mean()), 1),
                      "max_iterations": int(it.max()),
@@ -496,34 +535,60 @@ def autograd_section(exe, stream, nx=64, k=16, seed=5):
             "grad_norm": float(theta.grad.norm())}
 
 
-def sweep(exe, rp, ci, v, time_op):
+def sweep(exe, rp, ci, v, time_op, include_b=True):
+    """Every format x precision x k in {1, 4, 16} on matrix A (the 7-point
+    128^3 Poisson matrix) and matrix B (power-law, n = 4M, row lengths
+    round(lognormal(2.5, 1)) clipped to [1, 4096], seed 0).  gbs counts the
+    bytes of the format as stored (padding included), useful_gbs the Csr
+    bytes of the same product; Ell on B is not built (its padding would
+    need n * max_row slots)."""
     import torch
+    from ginkgo_b200 import stencils
     from ginkgo_b200.matrix import Csr
-    n, nnz = len(rp) - 1, len(ci)
+    peak, _ = measured_peaks()
     out = {}
+    mats = [("A", rp, ci, v)]
+    if include_b:
+        mats.append(("B",) + stencils.power_law(4_000_000, seed=0, mu=2.5, sigma=1.0,
+                                                max_len=4096))
     rng = np.random.default_rng(1)
-    for dt, vb in ((torch.float64, 8), (torch.float32, 4)):
-        A = Csr.read(exe, rp, ci, v, dtype=dt)
-        E = A.convert_to_ell()
-        S = A.convert_to_sellp(32, 1)
-        for k in (1, 4, 16):
-            x = torch.from_numpy(rng.standard_normal((n, k))).to(dt).cuda()
-            y = torch.empty((n, k), dtype=dt, device="cuda")
-            for name, op, mat_bytes in (
-                    ("csr_classical", A.set_strategy("classical"), None),
-                    ("csr_load_balance", A.set_strategy("load_balance"), None),
-                    ("ell", E, E.width * E.stride * (vb + 4)),
-                    ("sellp32", S, S.num_stored_elements * (vb + 4) +
-                     (S.slice_sets.numel() + S.slice_lengths.numel()) * 8)):
-                if name.startswith("csr"):
-                    A.set_strategy(name[4:])
-                    op = A
-                    nb = csr_bytes(n, nnz, k, vb)
-                else:
-                    nb = mat_bytes + k * n * 2 * vb
-                t = time_op(lambda: op.apply(x, y), 20, 3)
-                out[f"{name}_{'f64' if vb == 8 else 'f32'}_k{k}"] = {
-                    "ms": round(t * 1e3, 5), "gbs": round(nb / t / 1e9, 1)}
+    for mname, mrp, mci, mv in mats:
+        n, nnz = len(mrp) - 1, len(mci)
+        out[f"{mname}_shape"] = {"n": n, "nnz": nnz}
+        for dt, vb in ((torch.float64, 8), (torch.float32, 4)):
+            A = Csr.read(exe, mrp, mci, mv, dtype=dt)
+            ops = [("csr_classical", None), ("csr_load_balance", None)]
+            width = A.max_row_nnz
+            if mname == "A":
+                ops.append(("ell", A.convert_to_ell()))
+            else:
+                out[f"{mname}_ell_{'f64' if vb == 8 else 'f32'}"] = {
+                    "not_applicable": f"storage: {n} x {width} slots = "
+                                      f"{n * width * (vb + 4) / 1e9:.0f} GB"}
+            S = A.convert_to_sellp(32, 1)
+            ops.append(("sellp32", S))
+            for k in (1, 4, 16):
+                x = torch.from_numpy(rng.standard_normal((n, k))).to(dt).cuda()
+                y = torch.empty((n, k), dtype=dt, device="cuda")
+                useful = csr_bytes(n, nnz, k, vb)
+                for name, op in ops:
+                    if name.startswith("csr"):
+                        A.set_strategy(name[4:])
+                        op, nb = A, useful
+                    elif name == "ell":
+                        nb = op.width * op.stride * (vb + 4) + k * n * 2 * vb
+                    else:
+                        nb = (op.num_stored_elements * (vb + 4) +
+                              (op.slice_sets.numel() + op.slice_lengths.numel()) * 8 +
+                              k * n * 2 * vb)
+                    t = time_op(lambda: op.apply(x, y), 20, 3)
+                    out[f"{mname}_{name}_{'f64' if vb == 8 else 'f32'}_k{k}"] = {
+                        "ms": round(t * 1e3, 5), "gbs": round(nb / t / 1e9, 1),
+                        "useful_gbs": round(useful / t / 1e9, 1),
+                        "frac_of_measured": round(nb / t / 1e9 / peak, 3)}
+                del x, y
+            del A, S, ops
+            torch.cuda.empty_cache()
     return out
 
 
