@@ -29,11 +29,13 @@ constexpr int kAsyncCap = 256;  // staged entries per group and stage
 constexpr int kAsyncBlock = 256;
 
 // Lanes per row: the fewest that keep a group of 32 / LPR rows of the
-// longest length within one stage.
+// longest length within one stage, at most 4 (groups of 8 rows): with
+// longer rows the groups that overflow a stage take the row-by-row path,
+// and the short rows of an irregular matrix still share warps.
 inline int async_lanes_per_row(int64_t max_row_nnz)
 {
     int lpr = 1;
-    while (lpr < 32 && (32 / lpr) * max_row_nnz > kAsyncCap) lpr *= 2;
+    while (lpr < 4 && (32 / lpr) * max_row_nnz > kAsyncCap) lpr *= 2;
     return lpr;
 }
 
@@ -209,17 +211,14 @@ __global__ void __launch_bounds__(kAsyncBlock)
 }
 
 // Calls f(csr_async_kernel<T, K, VEC, LPR>) for the runtime lanes-per-row
-// value lpr (a power of two <= 32).
+// value lpr (1, 2 or 4, from async_lanes_per_row).
 template <typename T, int K, bool VEC, typename F>
 void with_async_kernel(int lpr, F&& f)
 {
     switch (lpr) {
     case 1: f(csr_async_kernel<T, K, VEC, 1>); break;
     case 2: f(csr_async_kernel<T, K, VEC, 2>); break;
-    case 4: f(csr_async_kernel<T, K, VEC, 4>); break;
-    case 8: f(csr_async_kernel<T, K, VEC, 8>); break;
-    case 16: f(csr_async_kernel<T, K, VEC, 16>); break;
-    default: f(csr_async_kernel<T, K, VEC, 32>); break;
+    default: f(csr_async_kernel<T, K, VEC, 4>); break;
     }
 }
 

@@ -98,10 +98,10 @@ def test_random_power_law_matches_oracle(exe, fmt, dt, k):
 @pytest.mark.parametrize("dt", [torch.float64, torch.float32])
 @pytest.mark.parametrize("k", [1, 2])
 def test_classical_every_group_width(exe, dt, k):
-    # The pipelined kernel groups 32 / lpr rows per warp, lpr chosen from
-    # the longest row; the row-length bound handed to it only changes the
-    # grouping, so every width (and groups that overflow a stage) must give
-    # the same result.  Rows of 0..60 entries, a few of 400.
+    # The pipelined kernel groups 32 / lpr rows per warp (lpr 1, 2 or 4),
+    # chosen from the longest row; the row-length bound handed to it only
+    # changes the grouping, so every width (and groups that overflow a
+    # stage) must give the same result.  Rows of 0..60 entries, a few of 400.
     rng = np.random.default_rng(21 + k)
     n = 30001
     lens = rng.integers(0, 61, n)
