@@ -146,16 +146,50 @@ __global__ void __launch_bounds__(256)
         T acc[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) acc[r] = T(0);
+        if constexpr (R <= 2) {
 #pragma unroll 4
-        for (int k = 0; k < len; ++k) {
-            int32_t c[R];
-            T v[R];
-            load_stream_rows<int32_t, R>(cols + base + int64_t(k) * slice_size, c);
-            load_stream_rows<T, R>(vals + base + int64_t(k) * slice_size, v);
+            for (int k = 0; k < len; ++k) {
+                int32_t c[R];
+                T v[R];
+                load_stream_rows<int32_t, R>(cols + base + int64_t(k) * slice_size, c);
+                load_stream_rows<T, R>(vals + base + int64_t(k) * slice_size, v);
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const T xv = r < valid && c[r] >= 0 ? __ldg(x + int64_t(c[r]) * ldx) : T(0);
-                acc[r] += v[r] * xv;
+                for (int r = 0; r < R; ++r) {
+                    const T xv = r < valid && c[r] >= 0 ? __ldg(x + int64_t(c[r]) * ldx) : T(0);
+                    acc[r] += v[r] * xv;
+                }
+            }
+        } else {
+            // 4-row groups (FP32): chunks of CH entries with predicated loads,
+            // so a short slice issues all its loads at once instead of
+            // finishing in a serial remainder loop (measured faster; in FP64
+            // the extra registers cost more than they gain)
+            constexpr int CH = 4;
+            for (int k0 = 0; k0 < len; k0 += CH) {
+                int32_t c[CH][R];
+                T v[CH][R];
+#pragma unroll
+                for (int u = 0; u < CH; ++u) {
+                    if (k0 + u < len) {
+                        load_stream_rows<int32_t, R>(cols + base + int64_t(k0 + u) * slice_size, c[u]);
+                        load_stream_rows<T, R>(vals + base + int64_t(k0 + u) * slice_size, v[u]);
+                    } else {
+#pragma unroll
+                        for (int r = 0; r < R; ++r) {
+                            c[u][r] = -1;
+                            v[u][r] = T(0);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < CH; ++u) {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        const T xv = r < valid && c[u][r] >= 0 ? __ldg(x + int64_t(c[u][r]) * ldx)
+                                                               : T(0);
+                        acc[r] += v[u][r] * xv;
+                    }
+                }
             }
         }
 #pragma unroll
