@@ -199,12 +199,18 @@ def main():
                     help="profiling aid: run one GMRES variant on the 27-point "
                     "operator for --solve-iters iterations and exit")
     ap.add_argument("--solve-iters", type=int, default=60)
+    ap.add_argument("--profile-tour", action="store_true",
+                    help="profiling aid: one capped invocation of every kernel "
+                    "family (SpMV formats, conversions, CG, BiCGStab, batch, "
+                    "transpose + SDDMM) and exit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
     if args.solve_case:
         return solve_case(args.solve_case, args.solve_iters)
+    if args.profile_tour:
+        return profile_tour()
 
     import torch
     world, rank, local = dist_env()
@@ -359,6 +365,55 @@ def solve_case(name, iters, grid=96):
                       "iterations": s.logger.num_iterations,
                       "residual_norm": np.asarray(s.logger.residual_norm,
                                                  dtype=float).tolist()}))
+
+
+def profile_tour():
+    """One capped invocation of every kernel family on inputs larger than
+    L2, for an ncu launch list with DRAM byte counters: SpMV in every
+    format (FP64, one and four right-hand sides) on the 7-point 128^3
+    matrix, the Ell and Sellp conversions, 20 CG and 20 BiCGStab iterations
+    (one and sixteen right-hand sides), the batched BiCGStab on 1024
+    systems, and the transpose + SDDMM of the differentiable solve."""
+    import torch
+    from ginkgo_b200 import stencils
+    from ginkgo_b200._lib import call
+    from ginkgo_b200.batch import BatchBicgstab, convection_diffusion_batch
+    from ginkgo_b200.matrix import Csr, CudaExecutor, _p, _stream
+    from ginkgo_b200.solver import Bicgstab, Cg, Iteration, Jacobi, ResidualNorm
+    exe = CudaExecutor.create(0)
+    rp, ci, v = stencils.poisson_3d_7pt(128)
+    n = len(rp) - 1
+    A = Csr.read(exe, rp, ci, v)
+    E = A.convert_to_ell()
+    S = A.convert_to_sellp(32, 1)
+    rng = np.random.default_rng(0)
+    for k in (1, 4):
+        x = torch.from_numpy(rng.standard_normal((n, k))).cuda()
+        y = torch.empty((n, k), dtype=torch.float64, device="cuda")
+        for op in (A.set_strategy("classical"), A.set_strategy("load_balance"), E, S):
+            op.apply(x, y)
+    A.set_strategy("classical")
+    crit = (Iteration.build().with_max_iters(20), ResidualNorm.build().with_reduction_factor(1e-14))
+    jac = Jacobi.build().with_max_block_size(1)
+    for k in (1, 16):
+        b = torch.from_numpy(rng.standard_normal((n, k))).cuda()
+        for fac in (Cg, Bicgstab):
+            s = fac.build().with_criteria(*crit).with_preconditioner(jac).on(exe).generate(A)
+            x = torch.zeros_like(b)
+            s.apply(b, x)
+    Ab, _ = convection_diffusion_batch(exe, 1024, lo=32, hi=1024, seed=3)
+    bb = torch.from_numpy(rng.standard_normal(Ab.total_rows)).cuda()
+    sb = (BatchBicgstab.build().with_max_iterations(500).with_tolerance(1e-8)
+          .with_tolerance_type("relative").with_preconditioner("jacobi").on(exe).generate(Ab))
+    sb.apply(bb, torch.zeros_like(bb))
+    At = A.transpose()
+    lam = torch.from_numpy(rng.standard_normal((n, 16))).cuda()
+    xx = torch.from_numpy(rng.standard_normal((n, 16))).cuda()
+    g = torch.empty_like(A.values)
+    call("b2s_csr_sddmm_f64", n, _p(At.row_ptrs), _p(At.col_idxs), At.max_row_nnz, _p(lam),
+         lam.stride(0), _p(xx), xx.stride(0), 16, -1.0, _p(g), _stream(g))
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_tour": "done", "n": n}))
 
 
 def ir_gmres_section(exe, stream, grid=96, reps=3):
