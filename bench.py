@@ -390,7 +390,8 @@ def profile_tour():
     for k in (1, 4):
         x = torch.from_numpy(rng.standard_normal((n, k))).cuda()
         y = torch.empty((n, k), dtype=torch.float64, device="cuda")
-        for op in (A.set_strategy("classical"), A.set_strategy("load_balance"), E, S):
+        for name in ("classical", "load_balance", "ell", "sellp"):
+            op = E if name == "ell" else S if name == "sellp" else A.set_strategy(name)
             op.apply(x, y)
     A.set_strategy("classical")
     crit = (Iteration.build().with_max_iters(20), ResidualNorm.build().with_reduction_factor(1e-14))
