@@ -15,7 +15,9 @@
 //               residual_norm check)
 //
 // With four or more right-hand sides (FP64; eight or more in FP32) the same
-// two passes run with lanes owning 16-byte column slices of each row.
+// two passes run with lanes owning 16-byte column slices of each row; with
+// one right-hand side on a system of 2^19 rows or more the SpMV pass is
+// split so that the matrix streams through the pipelined Csr kernel.
 //
 // z is never stored.  Per-column stopping status uses the reference's bit
 // layout; stopped columns are frozen as in the reference.  The host replays
@@ -23,6 +25,7 @@
 // replay.
 #include <cstring>
 
+#include "csr_async.cuh"
 #include "solver_common.cuh"
 
 namespace b2s {
@@ -445,6 +448,60 @@ __global__ void __launch_bounds__(kSolverBlock)
     }
 }
 
+// ---------------------------------------------------------------------------
+// One right-hand side on a large system: the SpMV pass is split in three so
+// the matrix streams through the pipelined Csr kernel (one x gather per
+// stored entry instead of forming p' = D^-1 r + beta p at every gathered
+// column, which triples the gathers once the vectors no longer sit in L2):
+//   cg_pupdate_kernel  p' = cg_p(...)   (the same rounding as the fused pass)
+//   csr_async_kernel   q = A p'
+//   cg_pq_kernel       dot(p', q); the last block sets alpha
+// ---------------------------------------------------------------------------
+constexpr int64_t kCgSplitRows = int64_t(1) << 19;
+
+template <typename T>
+__global__ void __launch_bounds__(kSolverBlock)
+    cg_pupdate_kernel(int64_t n, const T* __restrict__ dinv, const T* __restrict__ r,
+                      const T* __restrict__ p_old, T* __restrict__ p_new,
+                      SolveCtl* ctl, CgScalars<T>* sc)
+{
+    if (ctl->all_stopped) return;
+    const T pr = sc->prev_rho[0];
+    const bool from_z = pr == T(0);
+    const T beta = from_z ? T(0) : sc->rho[0] / pr;
+    for (int64_t i = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * kSolverBlock) {
+        const T d = dinv ? dinv[i] : T(1);
+        p_new[i] = cg_p(d, r[i], beta, p_old[i], from_z);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSolverBlock)
+    cg_pq_kernel(int64_t n, const T* __restrict__ p, const T* __restrict__ q,
+                 SolveCtl* ctl, CgScalars<T>* sc, T* __restrict__ partials)
+{
+    __shared__ T red[kSolverBlock / kWarp];
+    __shared__ T tot[1];
+    __shared__ int last;
+    if (ctl->all_stopped) return;
+    T acc[1] = {T(0)};
+    for (int64_t i = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * kSolverBlock) {
+        acc[0] += p[i] * q[i];
+    }
+    block_partials<T, 1>(acc, partials, red);
+    if (last_block_done(&ctl->ticket, &last)) {
+        sum_partials<T, 1>(partials, gridDim.x, tot, red);
+        if (threadIdx.x == 0) {
+            const T pq = tot[0];
+            // step_2 skips the update when dot(p, q) == 0
+            sc->alpha[0] = pq != T(0) ? sc->rho[0] / pq : T(0);
+            ctl->ticket = 0;
+        }
+    }
+}
+
 struct CgLayout {
     int64_t bytes;
     int64_t off_ctl, off_sc, off_r, off_p0, off_p1, off_q, off_partials;
@@ -517,10 +574,29 @@ int cg_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
             n, dinv, b, ldb, int(k), r, p[0], ctl, sc, partials);
         B2S_LAUNCH_CHECK();
     });
+    // the split single-RHS pass (large systems)
+    const int lpr = async_lanes_per_row(max_row_nnz);
+    const int64_t async_need = ceildiv(ceildiv(n, kWarp / lpr), kAsyncBlock / kWarp);
+    auto launch_split = [&](cudaStream_t cs, T* po, T* pn) {
+        cg_pupdate_kernel<T><<<grid_vec, kSolverBlock, 0, cs>>>(n, dinv, r, po, pn, ctl, sc);
+        with_async_kernel<T, 1, false>(lpr, [&](auto kernel) {
+            const int64_t grid = std::min<int64_t>(async_need, async_resident_blocks(kernel));
+            kernel<<<grid, kAsyncBlock, 0, cs>>>(n, rp, ci, v, pn, 1, q, 1, nullptr, nullptr,
+                                                 &ctl->all_stopped);
+        });
+        cg_pq_kernel<T><<<grid_vec, kSolverBlock, 0, cs>>>(n, pn, q, ctl, sc, partials);
+        cg_update_kernel<T, 1><<<grid_vec, kSolverBlock, 0, cs>>>(n, dinv, x, ldx, r, pn, q,
+                                                                  ctl, sc, partials);
+    };
     auto capture = [&](cudaStream_t cs) -> int {
         for (int it = 0; it < chunk; ++it) {
             T* po = p[it % 2];
             T* pn = p[(it + 1) % 2];
+            if (K == 1 && n >= kCgSplitRows) {
+                launch_split(cs, po, pn);
+                B2S_LAUNCH_CHECK();
+                continue;
+            }
             B2S_DISPATCH_RHS(K, {
                 if constexpr (K * sizeof(T) >= 32) {
                     // lanes own 16-byte column slices of a row

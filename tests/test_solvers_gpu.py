@@ -327,3 +327,23 @@ def test_gmres_far_columns_fall_back_to_32bit_offsets(exe, basis):
     s.apply(torch.from_numpy(b).cuda(), x)
     assert s.logger.has_converged
     assert explicit_rel_res(rp, ci, v, x.cpu().numpy(), b)[0] <= 1e-10
+
+
+def test_cg_large_single_rhs_split_pass_matches_oracle(exe):
+    # 96^3 = 884,736 rows: one right-hand side on a system this large runs the
+    # split SpMV pass (p update, pipelined Csr SpMV, dot); 40 iterations of it
+    # against 40 of the oracle's CG
+    rp, ci, v = stencils.poisson_3d_7pt(96)
+    n = len(rp) - 1
+    b = np.random.default_rng(6).standard_normal(n)
+    A = Csr.read(exe, rp, ci, v)
+    s = (Cg.build().with_criteria(*crit(40, 1e-14))
+         .with_preconditioner(Jacobi.build().with_max_block_size(1))
+         .on(exe).generate(A))
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    s.apply(torch.from_numpy(b).cuda(), x)
+    xo, it_o, res_o, conv_o = orc.cg(rp, ci, v, b, max_iters=40, reduction=1e-14)
+    assert s.logger.num_iterations == 40 == it_o
+    assert not s.logger.has_converged
+    np.testing.assert_allclose(x.cpu().numpy(), xo[:, 0] if xo.ndim == 2 else xo,
+                               rtol=1e-9, atol=1e-11 * np.abs(xo).max())
