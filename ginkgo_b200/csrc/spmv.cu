@@ -738,10 +738,16 @@ int sellp_spmv(int64_t n, int64_t num_cols, int64_t slice_size,
         // measured faster on the 7-point matrix)
         const int64_t groups_blocks = ceildiv(ceildiv(n, R), kBlock);
         if constexpr (sizeof(T) == 8) {
-            sellp_rows_kernel<T, R, true>
-                <<<std::min<int64_t>(groups_blocks, int64_t(kNumSMs) * 16), kBlock, 0, st>>>(
+            const int64_t g = std::min<int64_t>(groups_blocks, int64_t(kNumSMs) * 16);
+            if (alpha == nullptr && ldb == 1 && ldc == 1) {
+                sellp_rows_kernel<T, R, true, true><<<g, kBlock, 0, st>>>(
                     int(n), int(slice_size), shift, slice_sets, slice_lengths, ci, v, b, ldb,
                     c, ldc, alpha, beta);
+            } else {
+                sellp_rows_kernel<T, R, true><<<g, kBlock, 0, st>>>(
+                    int(n), int(slice_size), shift, slice_sets, slice_lengths, ci, v, b, ldb,
+                    c, ldc, alpha, beta);
+            }
         } else {
             sellp_rows_kernel<T, R, false><<<groups_blocks, kBlock, 0, st>>>(
                 int(n), int(slice_size), shift, slice_sets, slice_lengths, ci, v, b, ldb, c,
