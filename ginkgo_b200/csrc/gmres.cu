@@ -796,17 +796,17 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
             if (ell_w > 0) {
                 const int16_t* c16 = reinterpret_cast<const int16_t*>(ell_c);
                 if (ell_r == kEllRows && ell16) {
-                    ell_rows_kernel<TA, kEllRows, true, int16_t><<<grid_ell, 256, 0, cs>>>(
+                    ell_rows_kernel_for<TA, kEllRows, true, int16_t>()<<<grid_ell, 256, 0, cs>>>(
                         n, ell_w, ldv, c16, ell_v, y, 1, dst, 1, nullptr, nullptr, &gs->idle);
                 } else if (ell_r == kEllRows) {
-                    ell_rows_kernel<TA, kEllRows, true><<<grid_ell, 256, 0, cs>>>(
+                    ell_rows_kernel_for<TA, kEllRows, true>()<<<grid_ell, 256, 0, cs>>>(
                         n, ell_w, ldv, ell_c, ell_v, y, 1, dst, 1, nullptr, nullptr,
                         &gs->idle);
                 } else if (ell16) {
-                    ell_rows_kernel<TA, 1, true, int16_t><<<grid_ell, 256, 0, cs>>>(
+                    ell_rows_kernel_for<TA, 1, true, int16_t>()<<<grid_ell, 256, 0, cs>>>(
                         n, ell_w, ldv, c16, ell_v, y, 1, dst, 1, nullptr, nullptr, &gs->idle);
                 } else {
-                    ell_rows_kernel<TA, 1, true><<<grid_ell, 256, 0, cs>>>(
+                    ell_rows_kernel_for<TA, 1, true>()<<<grid_ell, 256, 0, cs>>>(
                         n, ell_w, ldv, ell_c, ell_v, y, 1, dst, 1, nullptr, nullptr,
                         &gs->idle);
                 }

@@ -672,8 +672,8 @@ int ell_spmv(int64_t n, int64_t num_cols, int64_t width, int64_t stride,
         // measured faster there)
         const int64_t g = std::min<int64_t>(ceildiv(ceildiv(n, R), kBlock),
                                             int64_t(kNumSMs) * 16);
-        ell_rows_kernel<T, RV><<<g, kBlock, 0, st>>>(n, int(width), stride, ci, v, b, ldb,
-                                                     c, ldc, alpha, beta, nullptr);
+        ell_rows_kernel_for<T, RV>()<<<g, kBlock, 0, st>>>(
+            n, int(width), stride, ci, v, b, ldb, c, ldc, alpha, beta, nullptr);
         B2S_LAUNCH_CHECK();
         return B2S_OK;
     }
