@@ -120,6 +120,17 @@ def dist_env():
     return world, rank, local
 
 
+def max_over_ranks(values, device):
+    """Each per-rank time replaced by its maximum over all ranks of the
+    default process group (every rank gets the result): the whole job is as
+    slow as its slowest rank."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
 def build_matrix():
     from ginkgo_b200 import stencils
     rp, ci, v = stencils.poisson_3d_7pt(GRID)
@@ -266,9 +277,7 @@ def main():
             yh.copy_(y, non_blocking=True)
         t_e2e = time_op(e2e_step, max(args.steps // 4, 5), 3)
     if world > 1:
-        t = torch.tensor([t_step, t_e2e], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        t_step, t_e2e = float(t[0]), float(t[1])
+        t_step, t_e2e = max_over_ranks([t_step, t_e2e], "cuda")
 
     nbytes = csr_bytes(n, nnz, 1, 8)
     gbs = nbytes / t_step / 1e9
