@@ -36,6 +36,10 @@ def _headers():
             glob.glob(os.path.join(ROOT, "include", "*.h")))
 
 
+def _obj(src):
+    return os.path.join(OBJ, os.path.splitext(os.path.basename(src))[0] + ".o")
+
+
 def _stale(src, obj, hdr_mtime):
     if not os.path.exists(obj):
         return True
@@ -46,11 +50,14 @@ def _stale(src, obj, hdr_mtime):
 def build(force: bool = False, verbose: bool = False, extra=()) -> str:
     os.makedirs(OBJ, exist_ok=True)
     nvcc = _nvcc()
-    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    # CUDA sources and host-only C++ sources (nvcc hands the latter to the
+    # host compiler)
+    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) +
+                  glob.glob(os.path.join(CSRC, "*.cpp")))
     hdr_mtime = max([os.path.getmtime(h) for h in _headers()] + [0])
     jobs = []
     for s in srcs:
-        o = os.path.join(OBJ, os.path.basename(s)[:-3] + ".o")
+        o = _obj(s)
         if force or _stale(s, o, hdr_mtime):
             cmd = [nvcc, *ARCH, *FLAGS, *extra, "-c", s, "-o", o]
             if verbose:
@@ -71,7 +78,7 @@ def build(force: bool = False, verbose: bool = False, extra=()) -> str:
                 failed.append(s)
     if failed:
         raise RuntimeError("nvcc failed for: " + ", ".join(failed))
-    objs = [os.path.join(OBJ, os.path.basename(s)[:-3] + ".o") for s in srcs]
+    objs = [_obj(s) for s in srcs]
     if jobs or not os.path.exists(LIB):
         cmd = [nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart_static",
                "-ldl", "-lrt", "-lpthread"]

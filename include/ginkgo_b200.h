@@ -542,6 +542,63 @@ int b2s_batch_ell_bicgstab_tune_f32(
     void* workspace, int64_t workspace_bytes, int32_t* iterations,
     double* residual_norms, int32_t* tune_table_out, void* stream);
 
+/* ------------------------------------------ MatrixMarket and binary I/O -- */
+/* Host-side matrix data I/O: every pointer here is a HOST pointer and no
+ * CUDA call is made.  Matrix data is the reference's matrix_data: a size
+ * (rows x cols) and a list of (row, column, value) entries, 0-based.
+ *
+ * b2s_mtx_read parses num_bytes bytes as
+ *   B2S_MTX_TEXT     MatrixMarket text: read_raw (core/base/mtx_io.cpp:
+ *                    747-751, parser :53-742): layouts coordinate/array,
+ *                    fields real/integer/pattern (complex is rejected for
+ *                    real value types), modifiers general/symmetric/
+ *                    skew-symmetric/hermitian expanded to both triangles;
+ *   B2S_MTX_BINARY   the reference's binary format: read_binary_raw
+ *                    (:882-927): a 32-byte header (magic "GINKGO" + value
+ *                    and index type letters, rows, cols, entries as uint64)
+ *                    then (row, col, value) records; file values double,
+ *                    float, half or bfloat16, indices int32 or int64;
+ *   B2S_MTX_GENERIC  text when the first byte is '%', else binary
+ *                    (read_generic_raw, :930-941);
+ * into value_type (B2S_MTX_F64 / B2S_MTX_F32) and index_type (B2S_MTX_I32 /
+ * B2S_MTX_I64) entries sorted by (row, column) (matrix_data::
+ * sort_row_major; entries with equal coordinates keep their file order).
+ * *(void**)handle_out receives a handle that owns the result.
+ *
+ * b2s_mtx_write formats num_entries entries (in the given order) as
+ *   B2S_MTX_COORDINATE  "%%MatrixMarket matrix coordinate real general",
+ *   B2S_MTX_ARRAY       "%%MatrixMarket matrix array real general" (column-
+ *                       major, absent entries written as 0),
+ *   B2S_MTX_BINARY      the binary format (write_binary_raw, :943-978),
+ * with text values printed as the reference's default stream format (six
+ * significant digits); write_raw :980-1004.
+ *
+ * b2s_mtx_sizes writes int64[4] = {rows, cols, entries, bytes} of a handle
+ * (bytes: the formatted output of a write, 0 after a read); b2s_mtx_copy
+ * copies the entries (row_idxs/col_idxs of the handle's index type, values
+ * of its value type) and/or the formatted bytes into caller arrays (any may
+ * be NULL); b2s_mtx_free releases a handle.  Errors (malformed input, the
+ * reference's StreamError cases) return B2S_ERR_INVALID_ARG with the
+ * reference's message in b2s_last_error(). */
+#define B2S_MTX_TEXT 0
+#define B2S_MTX_BINARY 1
+#define B2S_MTX_GENERIC 2
+#define B2S_MTX_COORDINATE 3
+#define B2S_MTX_ARRAY 4
+#define B2S_MTX_F64 0
+#define B2S_MTX_F32 1
+#define B2S_MTX_I32 0
+#define B2S_MTX_I64 1
+int b2s_mtx_read(const void* bytes, int64_t num_bytes, int format, int value_type,
+                 int index_type, void* handle_out);
+int b2s_mtx_write(int64_t num_rows, int64_t num_cols, int64_t num_entries,
+                  const void* row_idxs, const void* col_idxs, const void* values,
+                  int value_type, int index_type, int format, void* handle_out);
+int b2s_mtx_sizes(const void* handle, int64_t* sizes_out);
+int b2s_mtx_copy(const void* handle, void* row_idxs, void* col_idxs, void* values,
+                 void* bytes);
+int b2s_mtx_free(void* handle);
+
 #ifdef __cplusplus
 }
 #endif
