@@ -17,6 +17,7 @@
 // pass, no per-token allocation.
 #include <algorithm>
 #include <cctype>
+#include <charconv>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -27,6 +28,8 @@
 #include <new>
 #include <numeric>
 #include <string>
+#include <system_error>
+#include <thread>
 #include <vector>
 
 #include "../../include/ginkgo_b200.h"
@@ -58,6 +61,78 @@ struct MtxError {
 double round_to(int value_type, double x)
 {
     return value_type == B2S_MTX_F32 ? double(float(x)) : x;
+}
+
+inline bool is_digit(char ch) { return ch >= '0' && ch <= '9'; }
+
+// A signed decimal integer at p (no leading whitespace) within [lo, hi];
+// all its digits are consumed even when it overflows.
+bool scan_int(const char*& p, const char* end, int64_t lo, int64_t hi, int64_t& out)
+{
+    const char* q = p;
+    bool neg = false;
+    if (q < end && (*q == '+' || *q == '-')) neg = *q++ == '-';
+    if (q >= end || !is_digit(*q)) return false;
+    // magnitude up to 2^63 (the most negative int64)
+    const uint64_t lim = uint64_t(std::numeric_limits<int64_t>::max()) + (neg ? 1 : 0);
+    uint64_t mag = 0;
+    bool over = false;
+    for (; q < end && is_digit(*q); ++q) {
+        const unsigned d = unsigned(*q - '0');
+        if (mag > (lim - d) / 10) over = true;
+        else mag = mag * 10 + d;
+    }
+    p = q;
+    if (over) return false;
+    const int64_t val = neg ? (mag == (uint64_t(1) << 63) ? std::numeric_limits<int64_t>::min()
+                                                        : -int64_t(mag))
+                            : int64_t(mag);
+    if (val < lo || val > hi) return false;
+    out = val;
+    return true;
+}
+
+// A double at p (no leading whitespace) with the stream's grammar:
+// [sign] digits [. digits] [(e|E) [sign] digits], at least one mantissa
+// digit.  An exponent marker without digits fails, and so does a value that
+// overflows to infinity (the stream's conversion sets failbit for both,
+// LWG 23); an underflow gives the correctly rounded tiny value or zero.
+bool scan_double(const char*& p, const char* end, double& out)
+{
+    const char* s = p;
+    const char* q = p;
+    bool plus = false;
+    if (q < end && (*q == '+' || *q == '-')) plus = *q++ == '+';
+    bool digits = false;
+    while (q < end && is_digit(*q)) ++q, digits = true;
+    if (q < end && *q == '.') {
+        ++q;
+        while (q < end && is_digit(*q)) ++q, digits = true;
+    }
+    if (!digits) {
+        p = q;
+        return false;
+    }
+    if (q < end && (*q == 'e' || *q == 'E')) {
+        const char* e = q + 1;
+        if (e < end && (*e == '+' || *e == '-')) ++e;
+        if (e >= end || !is_digit(*e)) {
+            p = e;
+            return false;
+        }
+        while (e < end && is_digit(*e)) ++e;
+        q = e;
+    }
+    p = q;
+    // from_chars takes no leading '+'; it is correctly rounded, as strtod
+    const char* f = plus ? s + 1 : s;
+    const auto r = std::from_chars(f, q, out);
+    if (r.ec == std::errc()) return true;
+    const std::string t(f, q);
+    const double x = std::strtod(t.c_str(), nullptr);
+    if (std::isinf(x)) return false;
+    out = x;
+    return true;
 }
 
 // Cursor over the input with the extraction rules of a C++ stream in the
@@ -97,27 +172,7 @@ struct Cursor {
     bool read_int(int64_t lo, int64_t hi, int64_t& out)
     {
         skip_ws();
-        const char* q = p;
-        bool neg = false;
-        if (q < end && (*q == '+' || *q == '-')) neg = *q++ == '-';
-        if (q >= end || *q < '0' || *q > '9') return false;
-        // magnitude up to 2^63 (the most negative int64)
-        const uint64_t lim = uint64_t(std::numeric_limits<int64_t>::max()) + (neg ? 1 : 0);
-        uint64_t mag = 0;
-        bool over = false;
-        for (; q < end && *q >= '0' && *q <= '9'; ++q) {
-            const unsigned d = unsigned(*q - '0');
-            if (mag > (lim - d) / 10) over = true;
-            else mag = mag * 10 + d;
-        }
-        p = q;
-        if (over) return false;
-        const int64_t val = neg ? (mag == (uint64_t(1) << 63) ? std::numeric_limits<int64_t>::min()
-                                                            : -int64_t(mag))
-                                : int64_t(mag);
-        if (val < lo || val > hi) return false;
-        out = val;
-        return true;
+        return scan_int(p, end, lo, hi, out);
     }
     // unsigned decimal size (a leading '-' is rejected)
     bool read_size(int64_t& out)
@@ -126,52 +181,10 @@ struct Cursor {
         if (p < end && *p == '-') return false;
         return read_int(0, std::numeric_limits<int64_t>::max(), out);
     }
-    // [sign] digits [. digits] [(e|E) [sign] digits], at least one mantissa
-    // digit; an exponent marker without digits fails, as the stream's
-    // conversion does
     bool read_double(double& out)
     {
         skip_ws();
-        const char* s = p;
-        const char* q = p;
-        if (q < end && (*q == '+' || *q == '-')) ++q;
-        bool digits = false;
-        while (q < end && *q >= '0' && *q <= '9') ++q, digits = true;
-        if (q < end && *q == '.') {
-            ++q;
-            while (q < end && *q >= '0' && *q <= '9') ++q, digits = true;
-        }
-        if (!digits) {
-            p = q;
-            return false;
-        }
-        if (q < end && (*q == 'e' || *q == 'E')) {
-            const char* e = q + 1;
-            if (e < end && (*e == '+' || *e == '-')) ++e;
-            if (e >= end || *e < '0' || *e > '9') {
-                p = e;
-                return false;
-            }
-            while (e < end && *e >= '0' && *e <= '9') ++e;
-            q = e;
-        }
-        // strtod on the matched text alone: correctly rounded, the same
-        // value the stream produces
-        char buf[128];
-        std::string big;
-        const size_t len = size_t(q - s);
-        const char* z;
-        if (len < sizeof(buf)) {
-            std::memcpy(buf, s, len);
-            buf[len] = '\0';
-            z = buf;
-        } else {
-            big.assign(s, q);
-            z = big.c_str();
-        }
-        out = std::strtod(z, nullptr);
-        p = q;
-        return true;
+        return scan_double(p, end, out);
     }
 };
 
@@ -264,6 +277,29 @@ struct Reader {
     }
 };
 
+// Threads for a host pass over `bytes` bytes: at most the hardware threads
+// (64 at most), at least 4 MiB each.
+unsigned io_threads(size_t bytes)
+{
+    unsigned hw = std::thread::hardware_concurrency();
+    hw = hw == 0 ? 1 : std::min(hw, 64u);
+    return std::max(1u, std::min<unsigned>(hw, unsigned(std::min<size_t>(bytes >> 22, 64))));
+}
+
+// Runs f(0) .. f(T - 1), on T threads when T > 1.
+template <typename F>
+void parallel_for(unsigned T, F&& f)
+{
+    std::vector<std::thread> pool;
+    pool.reserve(T);
+    for (unsigned t = 1; t < T; ++t) pool.emplace_back(f, t);
+    f(0u);
+    for (auto& th : pool) th.join();
+}
+
+// matrix_data::sort_row_major with equal coordinates kept in input order:
+// a counting sort by row (rows inside [0, rows) and not far more rows than
+// entries), then each row by column; otherwise a comparison sort.
 void sort_row_major(MtxData& d)
 {
     const size_t n = d.r.size();
@@ -272,21 +308,177 @@ void sort_row_major(MtxData& d)
         sorted = d.r[i - 1] < d.r[i] || (d.r[i - 1] == d.r[i] && d.c[i - 1] <= d.c[i]);
     }
     if (sorted) return;
-    std::vector<size_t> perm(n);
-    std::iota(perm.begin(), perm.end(), size_t(0));
-    std::stable_sort(perm.begin(), perm.end(), [&](size_t a, size_t b) {
-        return d.r[a] < d.r[b] || (d.r[a] == d.r[b] && d.c[a] < d.c[b]);
-    });
+    bool counting = d.rows <= int64_t(4 * n + 1024);
+    for (size_t i = 0; i < n && counting; ++i) counting = d.r[i] >= 0 && d.r[i] < d.rows;
     std::vector<int64_t> r(n), c(n);
     std::vector<double> v(n);
-    for (size_t i = 0; i < n; ++i) {
-        r[i] = d.r[perm[i]];
-        c[i] = d.c[perm[i]];
-        v[i] = d.v[perm[i]];
+    if (counting) {
+        std::vector<int64_t> start(size_t(d.rows) + 1, 0);
+        for (size_t i = 0; i < n; ++i) ++start[size_t(d.r[i]) + 1];
+        for (size_t k = 1; k < start.size(); ++k) start[k] += start[k - 1];
+        std::vector<int64_t> pos(start.begin(), start.end() - 1);
+        for (size_t i = 0; i < n; ++i) {
+            const size_t k = size_t(pos[size_t(d.r[i])]++);
+            r[k] = d.r[i];
+            c[k] = d.c[i];
+            v[k] = d.v[i];
+        }
+        // each row by column, stable: insertion sort (rows are short), or a
+        // stable sort of an index range for long rows
+        for (int64_t row = 0; row < d.rows; ++row) {
+            const size_t b = size_t(start[row]), e = size_t(start[row + 1]);
+            if (e - b < 2) continue;
+            if (e - b <= 64) {
+                for (size_t i = b + 1; i < e; ++i) {
+                    const int64_t ci = c[i];
+                    const double vi = v[i];
+                    size_t j = i;
+                    while (j > b && c[j - 1] > ci) {
+                        c[j] = c[j - 1];
+                        v[j] = v[j - 1];
+                        --j;
+                    }
+                    c[j] = ci;
+                    v[j] = vi;
+                }
+            } else {
+                std::vector<size_t> perm(e - b);
+                std::iota(perm.begin(), perm.end(), b);
+                std::stable_sort(perm.begin(), perm.end(),
+                                 [&](size_t x, size_t y) { return c[x] < c[y]; });
+                std::vector<int64_t> cc(e - b);
+                std::vector<double> vv(e - b);
+                for (size_t k = 0; k < perm.size(); ++k) {
+                    cc[k] = c[perm[k]];
+                    vv[k] = v[perm[k]];
+                }
+                std::copy(cc.begin(), cc.end(), c.begin() + b);
+                std::copy(vv.begin(), vv.end(), v.begin() + b);
+            }
+        }
+    } else {
+        std::vector<size_t> perm(n);
+        std::iota(perm.begin(), perm.end(), size_t(0));
+        std::stable_sort(perm.begin(), perm.end(), [&](size_t a, size_t b) {
+            return d.r[a] < d.r[b] || (d.r[a] == d.r[b] && d.c[a] < d.c[b]);
+        });
+        for (size_t i = 0; i < n; ++i) {
+            r[i] = d.r[perm[i]];
+            c[i] = d.c[perm[i]];
+            v[i] = d.v[perm[i]];
+        }
     }
     d.r.swap(r);
     d.c.swap(c);
     d.v.swap(v);
+}
+
+inline bool line_space(char ch)
+{
+    return ch == ' ' || ch == '\t' || ch == '\r' || ch == '\v' || ch == '\f';
+}
+
+// Coordinate entries of a large file, speculatively in parallel: the text
+// after the dimension line is cut at line starts, every chunk counts its
+// non-blank lines, then parses them as one entry per line ("row col
+// [value] [anything]").  Valid only when each of the first nnz entries sits
+// on its own line; otherwise (a token on the next line, a malformed or
+// missing entry) it returns false and the serial reader, which follows the
+// stream's rules exactly, runs instead.  Blank lines are skipped by both.
+bool read_coordinate_parallel(const char* p, const char* end, int64_t nnz, const Reader& rd,
+                              MtxData& d)
+{
+    const size_t bytes = size_t(end - p);
+    const unsigned T = io_threads(bytes);
+    if (T < 2 || nnz < (int64_t(1) << 16)) return false;
+    std::vector<const char*> cut(T + 1);
+    cut[0] = p;
+    cut[T] = end;
+    for (unsigned t = 1; t < T; ++t) {
+        const char* q = std::max(p + bytes * t / T, cut[t - 1]);
+        const void* nl = q < end ? std::memchr(q, '\n', size_t(end - q)) : nullptr;
+        cut[t] = nl ? static_cast<const char*>(nl) + 1 : end;
+    }
+    std::vector<int64_t> count(T, 0);
+    parallel_for(T, [&](unsigned t) {
+        int64_t k = 0;
+        bool blank = true;
+        for (const char* q = cut[t]; q < cut[t + 1]; ++q) {
+            if (*q == '\n') {
+                k += !blank;
+                blank = true;
+            } else if (!line_space(*q)) {
+                blank = false;
+            }
+        }
+        count[t] = k + !blank;
+    });
+    std::vector<int64_t> first(T + 1, 0);
+    for (unsigned t = 0; t < T; ++t) first[t + 1] = first[t] + count[t];
+    if (first[T] < nnz) return false;
+    struct Part {
+        std::vector<int64_t> r, c;
+        std::vector<double> v;
+        bool ok = true;
+    };
+    std::vector<Part> part(T);
+    const bool pattern = rd.field == Field::pattern;
+    const bool general = rd.modifier == Modifier::general;
+    const bool skew = rd.modifier == Modifier::skew_symmetric;
+    parallel_for(T, [&](unsigned t) {
+        int64_t idx = first[t];
+        if (idx >= nnz) return;
+        Part& o = part[t];
+        const size_t want = size_t(std::min(nnz, first[t + 1]) - idx) * (general ? 1 : 2);
+        o.r.reserve(want);
+        o.c.reserve(want);
+        o.v.reserve(want);
+        const char* q = cut[t];
+        const char* e = cut[t + 1];
+        while (q < e && idx < nnz) {
+            const void* nl = std::memchr(q, '\n', size_t(e - q));
+            const char* le = nl ? static_cast<const char*>(nl) : e;
+            const char* x = q;
+            q = nl ? le + 1 : e;
+            while (x < le && line_space(*x)) ++x;
+            if (x == le) continue;
+            int64_t row, col;
+            if (!scan_int(x, le, rd.ilo, rd.ihi, row)) return void(o.ok = false);
+            while (x < le && line_space(*x)) ++x;
+            if (!scan_int(x, le, rd.ilo, rd.ihi, col)) return void(o.ok = false);
+            double val = 1.0;
+            if (!pattern) {
+                while (x < le && line_space(*x)) ++x;
+                if (!scan_double(x, le, val)) return void(o.ok = false);
+                val = round_to(rd.d.value_type, val);
+            }
+            --row;
+            --col;
+            o.r.push_back(row);
+            o.c.push_back(col);
+            o.v.push_back(val);
+            if (!general && row != col) {
+                o.r.push_back(col);
+                o.c.push_back(row);
+                o.v.push_back(skew ? -val : val);
+            }
+            ++idx;
+        }
+    });
+    for (const auto& o : part) {
+        if (!o.ok) return false;
+    }
+    std::vector<size_t> off(T + 1, 0);
+    for (unsigned t = 0; t < T; ++t) off[t + 1] = off[t] + part[t].r.size();
+    d.r.resize(off[T]);
+    d.c.resize(off[T]);
+    d.v.resize(off[T]);
+    parallel_for(T, [&](unsigned t) {
+        std::copy(part[t].r.begin(), part[t].r.end(), d.r.begin() + off[t]);
+        std::copy(part[t].c.begin(), part[t].c.end(), d.c.begin() + off[t]);
+        std::copy(part[t].v.begin(), part[t].v.end(), d.v.begin() + off[t]);
+    });
+    return true;
 }
 
 void read_text(const char* buf, int64_t len, MtxData& d)
@@ -317,6 +509,11 @@ void read_text(const char* buf, int64_t len, MtxData& d)
         int64_t nnz;
         if (!dc.read_size(d.rows) || !dc.read_size(d.cols) || !dc.read_size(nnz)) {
             fail("error when determining matrix size, expected: rows cols nnz");
+        }
+        if (field != Field::complex &&
+            read_coordinate_parallel(cur.p, cur.end, nnz, rd, d)) {
+            sort_row_major(d);
+            return;
         }
         // reserve no more than the text can hold (two bytes per entry at least)
         const int64_t mult = modifier == Modifier::general ? 1 : 2;
@@ -445,19 +642,20 @@ void read_binary(const char* buf, int64_t len, MtxData& d)
     sort_row_major(d);
 }
 
-// the stream's default floating-point format: %g with six digits
-void put_value(std::string& out, double v)
+// The stream's default floating-point format is printf's %g with six
+// significant digits; to_chars with chars_format::general and precision 6
+// is specified to produce exactly that text.
+inline char* put_value(char* b, char* e, double v)
 {
-    char b[40];
-    const int n = std::snprintf(b, sizeof(b), "%g", v);
-    out.append(b, size_t(n));
+    return std::to_chars(b, e, v, std::chars_format::general, 6).ptr;
 }
 
-void put_int(std::string& out, int64_t v)
+inline char* put_int(char* b, char* e, int64_t v) { return std::to_chars(b, e, v).ptr; }
+
+void append_int(std::string& o, int64_t v)
 {
     char b[24];
-    const int n = std::snprintf(b, sizeof(b), "%lld", (long long)v);
-    out.append(b, size_t(n));
+    o.append(b, size_t(put_int(b, b + sizeof(b), v) - b));
 }
 
 void write_text(MtxData& d, bool array)
@@ -467,20 +665,34 @@ void write_text(MtxData& d, bool array)
               : "%%MatrixMarket matrix coordinate real general\n";
     const size_t n = d.r.size();
     if (!array) {
-        put_int(o, d.rows);
+        append_int(o, d.rows);
         o += ' ';
-        put_int(o, d.cols);
+        append_int(o, d.cols);
         o += ' ';
-        put_int(o, int64_t(n));
+        append_int(o, int64_t(n));
         o += '\n';
-        for (size_t i = 0; i < n; ++i) {
-            put_int(o, d.r[i] + 1);
-            o += ' ';
-            put_int(o, d.c[i] + 1);
-            o += ' ';
-            put_value(o, d.v[i]);
-            o += '\n';
-        }
+        // entries in the given order; ranges formatted on separate threads
+        const unsigned T = io_threads(n * 24);
+        std::vector<std::string> part(T);
+        parallel_for(T, [&](unsigned t) {
+            const size_t b = n * t / T, e = n * (t + 1) / T;
+            std::string& s = part[t];
+            s.reserve((e - b) * 24);
+            char line[96];
+            for (size_t i = b; i < e; ++i) {
+                char* q = put_int(line, line + 24, d.r[i] + 1);
+                *q++ = ' ';
+                q = put_int(q, q + 24, d.c[i] + 1);
+                *q++ = ' ';
+                q = put_value(q, q + 40, d.v[i]);
+                *q++ = '\n';
+                s.append(line, size_t(q - line));
+            }
+        });
+        size_t total = o.size();
+        for (const auto& s : part) total += s.size();
+        o.reserve(total);
+        for (const auto& s : part) o += s;
         return;
     }
     // column-major walk over every position; entries in (column, row) order
@@ -489,20 +701,23 @@ void write_text(MtxData& d, bool array)
     std::stable_sort(perm.begin(), perm.end(), [&](size_t a, size_t b) {
         return d.c[a] < d.c[b] || (d.c[a] == d.c[b] && d.r[a] < d.r[b]);
     });
-    put_int(o, d.rows);
+    append_int(o, d.rows);
     o += ' ';
-    put_int(o, d.cols);
+    append_int(o, d.cols);
     o += '\n';
     size_t pos = 0;
+    char line[48];
     for (int64_t j = 0; j < d.cols; ++j) {
         for (int64_t i = 0; i < d.rows; ++i) {
+            char* q;
             if (pos >= n || d.r[perm[pos]] != i || d.c[perm[pos]] != j) {
-                put_value(o, 0.0);
+                q = put_value(line, line + 40, 0.0);
             } else {
-                put_value(o, d.v[perm[pos]]);
+                q = put_value(line, line + 40, d.v[perm[pos]]);
                 ++pos;
             }
-            o += '\n';
+            *q++ = '\n';
+            o.append(line, size_t(q - line));
         }
     }
 }

@@ -83,10 +83,9 @@ def _read(src, fmt, value_type, index_type):
     vt, it = np.dtype(value_type), np.dtype(index_type)
     if vt not in _VT or it not in _IT:
         raise TypeError("value type float64/float32 and index type int32/int64 only")
-    data = _bytes(src)
-    buf = C.create_string_buffer(data, len(data))
+    data = _bytes(src)  # ctypes hands a bytes object's own buffer to void*
     h = C.c_void_p()
-    call("b2s_mtx_read", buf, len(data), fmt, _VT[vt], _IT[it], C.addressof(h))
+    call("b2s_mtx_read", data, len(data), fmt, _VT[vt], _IT[it], C.addressof(h))
     size, r, c, v, _ = _take(h, vt, it)
     return MatrixData(size, r, c, v)
 

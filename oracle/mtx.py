@@ -12,6 +12,7 @@ reference's StreamError message.
 """
 from __future__ import annotations
 
+import math
 import re
 import struct
 
@@ -34,7 +35,10 @@ _IRANGE = {"i32": (-2**31, 2**31 - 1), "i64": (-2**63, 2**63 - 1)}
 
 
 def _round(x, value_type):
-    return float(np.float32(x)) if value_type == "f32" else float(x)
+    if value_type != "f32":
+        return float(x)
+    with np.errstate(over="ignore"):  # a cast to float32 may overflow to inf
+        return float(np.float32(x))
 
 
 class _Stream:
@@ -80,7 +84,10 @@ class _Stream:
         if not m:
             return None
         self.i = m.end()
-        return float(m.group())
+        v = float(m.group())
+        # a decimal that overflows sets failbit in the stream (LWG 23);
+        # an underflow keeps the correctly rounded tiny value or zero
+        return None if math.isinf(v) else v
 
 
 def read_raw(text, value_type="f64", index_type="i32"):

@@ -293,3 +293,110 @@ def test_csr_arrays_from_matrix_data():
     with pytest.raises(ValueError):
         M.data_to_csr_arrays(M.read_raw(
             "%%MatrixMarket matrix coordinate real general\n2 2 1\n3 1 1.0\n"))
+
+
+@pytest.mark.parametrize("value,ok", [
+    ("1e400", False), ("-1e400", False), ("1.8e308", False), ("1.7e308", True),
+    ("1e-400", True), ("4.9e-324", True), ("2.4e-324", True), ("-2.5e-324", True),
+    ("+.5", True), ("5.", True), ("007", True), ("-0", True)])
+def test_overflow_fails_and_underflow_rounds_like_the_stream(value, ok):
+    text = f"%%MatrixMarket matrix coordinate real general\n1 1 1\n1 1 {value}\n"
+    if not ok:
+        with pytest.raises(O.MtxError):
+            O.read_raw(text)
+        with pytest.raises(GinkgoError):
+            M.read_raw(text)
+        return
+    exp = O.read_raw(text)[1]
+    got = M.read_raw(text).nonzeros
+    assert got == exp and np.signbit(got[0][2]) == np.signbit(exp[0][2])
+    # FP32 storage rounds the double (1.7e308 becomes inf there, as a cast does)
+    assert M.read_raw(text, np.float32).nonzeros == O.read_raw(text, "f32")[1]
+
+
+def _big_coordinate_text(rng, n, per_row, symmetric=False):
+    """A coordinate file of about n * per_row entries (> 8 MB, so the reader
+    takes its parallel path), rows shuffled."""
+    rows, cols = [], []
+    for k in range(per_row):
+        r = np.arange(n)
+        c = (r + k * 7919) % n if not symmetric else np.maximum(r - k, 0)
+        rows.append(r)
+        cols.append(c)
+    r = np.concatenate(rows)
+    c = np.concatenate(cols)
+    keep = np.ones(len(r), bool)
+    if symmetric:  # unique lower-triangle positions
+        key = r * n + c
+        _, first = np.unique(key, return_index=True)
+        keep[:] = False
+        keep[first] = True
+    r, c = r[keep], c[keep]
+    perm = rng.permutation(len(r))
+    r, c = r[perm], c[perm]
+    v = rng.standard_normal(len(r)) * 10.0 ** rng.integers(-5, 6, len(r))
+    body = "\n".join(f"{a + 1} {b + 1} {x!r}" for a, b, x in zip(r.tolist(), c.tolist(), v.tolist()))
+    kind = "symmetric" if symmetric else "general"
+    return f"%%MatrixMarket matrix coordinate real {kind}\n{n} {n} {len(r)}\n{body}\n"
+
+
+@pytest.mark.parametrize("symmetric", [False, True])
+def test_large_file_parallel_path_matches_oracle(symmetric):
+    rng = np.random.default_rng(7 + symmetric)
+    text = _big_coordinate_text(rng, 50_000, 9, symmetric)
+    assert len(text) > 9 << 20
+    size, entries = O.read_raw(text)
+    d = M.read_raw(text)
+    assert d.size == size
+    assert np.array_equal(d.row_idxs, [e[0] for e in entries])
+    assert np.array_equal(d.col_idxs, [e[1] for e in entries])
+    assert np.array_equal(d.values, [e[2] for e in entries])
+
+
+def test_large_file_irregular_lines_fall_back_to_the_stream_rules():
+    rng = np.random.default_rng(11)
+    base = _big_coordinate_text(rng, 40_000, 9)
+    head, dims, body = base.split("\n", 2)
+    lines = body.split("\n")
+    nnz = int(dims.split()[2])
+    mid = len(lines) // 2
+    variants = {
+        # the value of one entry on the next line: still valid for a stream
+        "split": lines[:mid] + [" ".join(lines[mid].split()[:2]), lines[mid].split()[2]]
+        + lines[mid + 1:],
+        # blank lines between entries
+        "blank": lines[:mid] + ["", "   \t"] + lines[mid:],
+        # garbage after the last entry is never read
+        "tail": lines[:nnz] + ["not an entry", "%"],
+        # a comment line in the middle is an error
+        "comment": lines[:mid] + ["% comment"] + lines[mid:],
+        # one entry too few
+        "short": lines[:nnz - 1],
+    }
+    for name, ls in variants.items():
+        text = f"{head}\n{dims}\n" + "\n".join(ls) + "\n"
+        try:
+            size, entries = O.read_raw(text)
+        except O.MtxError:
+            with pytest.raises(GinkgoError):
+                M.read_raw(text)
+            assert name in ("comment", "short")
+            continue
+        assert name in ("split", "blank", "tail")
+        d = M.read_raw(text)
+        assert d.size == size
+        assert np.array_equal(d.values, [e[2] for e in entries]), name
+        assert np.array_equal(d.row_idxs, [e[0] for e in entries]), name
+        assert np.array_equal(d.col_idxs, [e[1] for e in entries]), name
+
+
+def test_large_write_matches_oracle_format():
+    rng = np.random.default_rng(5)
+    n = 300_000
+    r = np.sort(rng.integers(0, 100_000, n)).astype(np.int32)
+    c = rng.integers(0, 100_000, n).astype(np.int32)
+    v = rng.standard_normal(n) * 10.0 ** rng.integers(-8, 9, n)
+    data = M.MatrixData((100_000, 100_000), r, c, v)
+    text = M.write_raw(data)
+    ent = list(zip(r.tolist(), c.tolist(), v.tolist()))
+    assert text == O.write_raw((100_000, 100_000), ent)
