@@ -17,7 +17,7 @@ def _symmetric_lower_text(rp, ci, v, n):
     for r in range(n):
         for k in range(rp[r], rp[r + 1]):
             if ci[k] <= r:
-                lines.append(f"{r + 1} {ci[k] + 1} {v[k]!r}")
+                lines.append(f"{r + 1} {int(ci[k]) + 1} {float(v[k])!r}")
     return ("%%MatrixMarket matrix coordinate real symmetric\n% 7-point 6^3\n"
             f"{n} {n} {len(lines)}\n" + "\n".join(lines) + "\n")
 
