@@ -214,8 +214,13 @@ def main():
                     help="profiling aid: one capped invocation of every kernel "
                     "family (SpMV formats, conversions, CG, BiCGStab, batch, "
                     "transpose + SDDMM) and exit")
+    ap.add_argument("--mtx", action="store_true",
+                    help="host-side matrix I/O: MatrixMarket text and binary "
+                    "read/write of the 128^3 matrix (no GPU needed) and exit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.mtx:
+        return mtx_section(args.steps if "--steps" in sys.argv else 3)
     if args.impl == "reference":
         return run_reference(args)
     if args.solve_case:
@@ -374,6 +379,65 @@ def solve_case(name, iters, grid=96):
                       "iterations": s.logger.num_iterations,
                       "residual_norm": np.asarray(s.logger.residual_norm,
                                                  dtype=float).tolist()}))
+
+
+def mtx_section(steps):
+    """Host-side matrix I/O on the 7-point 128^3 matrix (14.6M entries): the
+    library's MatrixMarket text and binary readers and writers through the
+    Python API (bytes in and out, numpy arrays), best of `steps` runs each,
+    checked bit-exact against the source arrays; and the oracle
+    restatement on a bounded sample as the CPU-port baseline."""
+    from ginkgo_b200 import mtx_io as M
+    from oracle import mtx as O
+    rp, ci, v = build_matrix()
+    n = len(rp) - 1
+    rows = np.repeat(np.arange(n, dtype=np.int32), np.diff(rp))
+    data = M.MatrixData((n, n), rows, np.asarray(ci, np.int32), np.asarray(v, np.float64))
+    lower = np.asarray(ci) <= rows
+    perm = np.random.default_rng(SEED).permutation(int(lower.sum()))
+    sym = M.MatrixData((n, n), rows[lower][perm], np.asarray(ci, np.int32)[lower][perm],
+                       np.asarray(v, np.float64)[lower][perm])
+
+    def best(f):
+        ts = []
+        for _ in range(max(steps, 1)):
+            t0 = time.perf_counter()
+            out = f()
+            ts.append(time.perf_counter() - t0)
+        return min(ts), out
+
+    t_w, text = best(lambda: M.write_raw(data).encode())
+    t_r, back = best(lambda: M.read_raw(text))
+    t_bw, binary = best(lambda: M.write_binary_raw(data))
+    t_br, bback = best(lambda: M.read_binary_raw(binary))
+    sym_text = M.write_raw(sym).replace("real general", "real symmetric", 1).encode()
+    t_s, sback = best(lambda: M.read_raw(sym_text))
+    for d in (back, bback, sback):
+        assert np.array_equal(d.row_idxs, rows) and np.array_equal(d.col_idxs, ci) \
+            and np.array_equal(d.values, v), "matrix I/O round trip differs"
+    k = 200_000
+    sample = M.write_raw(M.MatrixData((n, n), rows[:k], np.asarray(ci[:k], np.int32),
+                                      np.asarray(v[:k], np.float64)))
+    t0 = time.perf_counter()
+    O.read_raw(sample)
+    t_o = time.perf_counter() - t0
+    nnz = len(ci)
+    mb = lambda nbytes, t: round(nbytes / t / 1e6, 1)  # noqa: E731
+    print(json.dumps({
+        "mtx_io": {"workload": "poisson3d_7pt_128", "entries": nnz,
+                   "host_threads": os.cpu_count(),
+                   "text_bytes": len(text), "binary_bytes": len(binary),
+                   "read_text_s": round(t_r, 3), "read_text_mb_s": mb(len(text), t_r),
+                   "read_text_mentries_s": round(nnz / t_r / 1e6, 2),
+                   "write_text_s": round(t_w, 3), "write_text_mb_s": mb(len(text), t_w),
+                   "read_binary_s": round(t_br, 3), "read_binary_mb_s": mb(len(binary), t_br),
+                   "write_binary_s": round(t_bw, 3),
+                   "read_symmetric_shuffled_s": round(t_s, 3),
+                   "symmetric_text_bytes": len(sym_text),
+                   "cpu_baseline": {"kind": "port", "cores": 1,
+                                    "value": round(k / t_o / 1e6, 3), "unit": "M entries/s",
+                                    "sample": f"oracle read of the first {k} entries"},
+                   "steps": steps}}), flush=True)
 
 
 def profile_tour():

@@ -297,6 +297,39 @@ void parallel_for(unsigned T, F&& f)
     for (auto& th : pool) th.join();
 }
 
+// Stable sort of entries [b, e) of one row by column: insertion sort for
+// short rows, a stable sort of an index range for long ones.
+void sort_row_by_column(std::vector<int64_t>& c, std::vector<double>& v, size_t b, size_t e)
+{
+    if (e - b < 2) return;
+    if (e - b <= 64) {
+        for (size_t i = b + 1; i < e; ++i) {
+            const int64_t ci = c[i];
+            const double vi = v[i];
+            size_t j = i;
+            while (j > b && c[j - 1] > ci) {
+                c[j] = c[j - 1];
+                v[j] = v[j - 1];
+                --j;
+            }
+            c[j] = ci;
+            v[j] = vi;
+        }
+        return;
+    }
+    std::vector<size_t> perm(e - b);
+    std::iota(perm.begin(), perm.end(), b);
+    std::stable_sort(perm.begin(), perm.end(), [&](size_t x, size_t y) { return c[x] < c[y]; });
+    std::vector<int64_t> cc(e - b);
+    std::vector<double> vv(e - b);
+    for (size_t k = 0; k < perm.size(); ++k) {
+        cc[k] = c[perm[k]];
+        vv[k] = v[perm[k]];
+    }
+    std::copy(cc.begin(), cc.end(), c.begin() + b);
+    std::copy(vv.begin(), vv.end(), v.begin() + b);
+}
+
 // matrix_data::sort_row_major with equal coordinates kept in input order:
 // a counting sort by row (rows inside [0, rows) and not far more rows than
 // entries), then each row by column; otherwise a comparison sort.
@@ -313,49 +346,64 @@ void sort_row_major(MtxData& d)
     std::vector<int64_t> r(n), c(n);
     std::vector<double> v(n);
     if (counting) {
-        std::vector<int64_t> start(size_t(d.rows) + 1, 0);
-        for (size_t i = 0; i < n; ++i) ++start[size_t(d.r[i]) + 1];
-        for (size_t k = 1; k < start.size(); ++k) start[k] += start[k - 1];
-        std::vector<int64_t> pos(start.begin(), start.end() - 1);
-        for (size_t i = 0; i < n; ++i) {
-            const size_t k = size_t(pos[size_t(d.r[i])]++);
-            r[k] = d.r[i];
-            c[k] = d.c[i];
-            v[k] = d.v[i];
-        }
-        // each row by column, stable: insertion sort (rows are short), or a
-        // stable sort of an index range for long rows
-        for (int64_t row = 0; row < d.rows; ++row) {
-            const size_t b = size_t(start[row]), e = size_t(start[row + 1]);
-            if (e - b < 2) continue;
-            if (e - b <= 64) {
-                for (size_t i = b + 1; i < e; ++i) {
-                    const int64_t ci = c[i];
-                    const double vi = v[i];
-                    size_t j = i;
-                    while (j > b && c[j - 1] > ci) {
-                        c[j] = c[j - 1];
-                        v[j] = v[j - 1];
-                        --j;
-                    }
-                    c[j] = ci;
-                    v[j] = vi;
-                }
-            } else {
-                std::vector<size_t> perm(e - b);
-                std::iota(perm.begin(), perm.end(), b);
-                std::stable_sort(perm.begin(), perm.end(),
-                                 [&](size_t x, size_t y) { return c[x] < c[y]; });
-                std::vector<int64_t> cc(e - b);
-                std::vector<double> vv(e - b);
-                for (size_t k = 0; k < perm.size(); ++k) {
-                    cc[k] = c[perm[k]];
-                    vv[k] = v[perm[k]];
-                }
-                std::copy(cc.begin(), cc.end(), c.begin() + b);
-                std::copy(vv.begin(), vv.end(), v.begin() + b);
+        // two stable passes on T threads: entries into B buckets of
+        // consecutive rows (each thread's range in order), then a counting
+        // sort by row inside each bucket and a column sort of every row
+        const unsigned T = io_threads(n * 24);
+        const uint64_t R = uint64_t(d.rows);
+        const uint64_t B = std::min<uint64_t>(4096, R);
+        auto bucket = [&](int64_t row) { return size_t(uint64_t(row) * B / R); };
+        std::vector<size_t> off(size_t(T) * B, 0);
+        parallel_for(T, [&](unsigned t) {
+            size_t* cnt = &off[size_t(t) * B];
+            for (size_t i = n * t / T; i < n * (t + 1) / T; ++i) ++cnt[bucket(d.r[i])];
+        });
+        std::vector<size_t> bstart(B + 1, 0);
+        size_t run = 0;
+        for (size_t b = 0; b < B; ++b) {
+            bstart[b] = run;
+            for (unsigned t = 0; t < T; ++t) {
+                const size_t k = off[size_t(t) * B + b];
+                off[size_t(t) * B + b] = run;
+                run += k;
             }
         }
+        bstart[B] = run;
+        std::vector<int64_t> tr(n), tc(n);
+        std::vector<double> tv(n);
+        parallel_for(T, [&](unsigned t) {
+            size_t* pos = &off[size_t(t) * B];
+            for (size_t i = n * t / T; i < n * (t + 1) / T; ++i) {
+                const size_t k = pos[bucket(d.r[i])]++;
+                tr[k] = d.r[i];
+                tc[k] = d.c[i];
+                tv[k] = d.v[i];
+            }
+        });
+        parallel_for(T, [&](unsigned t) {
+            std::vector<size_t> start;
+            for (size_t b = B * t / T; b < B * (t + 1) / T; ++b) {
+                // rows of bucket b: [ceil(b R / B), ceil((b + 1) R / B))
+                const int64_t lo = int64_t((b * R + B - 1) / B);
+                const int64_t hi = int64_t(((b + 1) * R + B - 1) / B);
+                start.assign(size_t(hi - lo) + 1, 0);
+                for (size_t i = bstart[b]; i < bstart[b + 1]; ++i) ++start[size_t(tr[i] - lo) + 1];
+                for (size_t k = 1; k < start.size(); ++k) start[k] += start[k - 1];
+                for (size_t i = bstart[b]; i < bstart[b + 1]; ++i) {
+                    const size_t k = bstart[b] + start[size_t(tr[i] - lo)]++;
+                    r[k] = tr[i];
+                    c[k] = tc[i];
+                    v[k] = tv[i];
+                }
+                // each row by column, stable (start[] now holds row ends)
+                size_t rb = bstart[b];
+                for (int64_t row = lo; row < hi; ++row) {
+                    const size_t re = bstart[b] + start[size_t(row - lo)];
+                    sort_row_by_column(c, v, rb, re);
+                    rb = re;
+                }
+            }
+        });
     } else {
         std::vector<size_t> perm(n);
         std::iota(perm.begin(), perm.end(), size_t(0));

@@ -185,3 +185,45 @@ def write(csr, layout: str | None = None) -> str:
     if layout is None:
         layout = "array" if len(rows) >= n * m // 4 else "coordinate"
     return write_raw(data, layout)
+
+
+def read_dense(src, exec_=None, dtype=None):
+    """gko::read<Dense>(stream, exec): the file as a dense rows x cols torch
+    tensor (row-major, the layout of the right-hand sides and solutions on
+    this path), zero where the file has no entry; an entry given twice keeps
+    the later one (Dense::read, core/matrix/dense.cpp:1064-1072).  On
+    exec_'s device when one is given, else on the host."""
+    import torch
+    dtype = torch.float64 if dtype is None else dtype
+    vt = np.float64 if dtype == torch.float64 else np.float32
+    data = read_generic_raw(src, vt, np.int64)
+    n, m = data.size
+    r, c = data.row_idxs, data.col_idxs
+    if len(r) and (r.min() < 0 or r.max() >= n or c.min() < 0 or c.max() >= m):
+        raise ValueError("matrix data has an entry outside its size")
+    out = np.zeros((n, m), dtype=vt)
+    # the entries come sorted by (row, column) with a repeated position in
+    # file order, so the last of each run is the later value
+    last = np.ones(len(r), dtype=bool)
+    last[:-1] = (r[1:] != r[:-1]) | (c[1:] != c[:-1])
+    out[r[last], c[last]] = data.values[last]
+    t = torch.from_numpy(out)
+    return t.to(exec_.device) if exec_ is not None else t
+
+
+def write_dense(tensor, layout: str | None = None) -> str:
+    """gko::write(stream, Dense): the nonzero entries in row-major order
+    (Dense::write, core/matrix/dense.cpp:1119-1132), array layout when at
+    least a quarter of the entries are nonzero, else coordinate
+    (mtx_io.cpp:1043-1047).  A 1-D tensor is one column."""
+    a = tensor.detach().cpu().numpy()
+    if a.ndim == 1:
+        a = a[:, None]
+    if a.dtype not in (np.float64, np.float32):
+        a = a.astype(np.float64)
+    n, m = a.shape
+    r, c = np.nonzero(a)  # NaN counts as nonzero, as is_nonzero does
+    data = MatrixData((n, m), r.astype(np.int64), c.astype(np.int64), a[r, c])
+    if layout is None:
+        layout = "array" if len(r) >= n * m // 4 else "coordinate"
+    return write_raw(data, layout)

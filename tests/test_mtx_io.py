@@ -400,3 +400,25 @@ def test_large_write_matches_oracle_format():
     text = M.write_raw(data)
     ent = list(zip(r.tolist(), c.tolist(), v.tolist()))
     assert text == O.write_raw((100_000, 100_000), ent)
+
+
+def test_dense_read_and_write_follow_dense_read_write():
+    import torch
+    text = ("%%MatrixMarket matrix coordinate real general\n3 2 4\n"
+            "1 1 1.5\n3 2 -2\n1 1 7\n2 1 0.25\n")
+    t = M.read_dense(text)
+    size, entries = O.read_raw(text)
+    exp = np.zeros(size)
+    for r, c, v in entries:  # Dense::read assigns in order: the later 1 1 wins
+        exp[r, c] = v
+    assert t.dtype == torch.float64 and np.array_equal(t.numpy(), exp)
+    assert M.read_dense(text, dtype=torch.float32).dtype == torch.float32
+    # write: nonzeros row-major; array once a quarter is nonzero
+    a = torch.zeros(8, 3, dtype=torch.float64)
+    a[1, 2], a[5, 0] = 3.5, -1.0
+    ent = [(1, 2, 3.5), (5, 0, -1.0)]
+    assert M.write_dense(a) == O.write_raw((8, 3), ent, "coordinate")
+    a[:3, :] = 1.0
+    ent = [(i, j, float(a[i, j])) for i in range(8) for j in range(3) if a[i, j] != 0]
+    assert M.write_dense(a) == O.write_raw((8, 3), ent, "array")
+    assert np.array_equal(M.read_dense(M.write_dense(a)).numpy(), a.numpy())
