@@ -2,6 +2,10 @@
 
 Submodules:
   matrix        Csr / Ell / Sellp and the CudaExecutor (SpMV, conversions)
+  solver        Cg / Bicgstab / Gmres / Ir factories over the fused solvers
+  batch         batched BiCGStab on ragged batch Ell with its autotuner
+  autograd      differentiable sparse solve (adjoint CG + SDDMM)
+  mtx_io        MatrixMarket and binary matrix I/O (host code)
   stencils      seeded synthetic matrices of the benchmark workloads
   build         nvcc build of libginkgo_b200.so (sm_100a)
 
