@@ -209,3 +209,83 @@ class BatchBicgstab:
     @staticmethod
     def build():
         return _Builder()
+
+
+# --------------------------------------------------------- multi-GPU ------
+
+def shard_bounds(row_offsets, world: int) -> np.ndarray:
+    """Split of the systems into `world` contiguous shards of about equal
+    rows (the work of an iteration is proportional to rows): rank k owns
+    systems [bounds[k], bounds[k + 1]).  Each shard's rows are within one
+    system of total / world; ranks beyond the number of systems get none."""
+    offs = np.asarray(row_offsets, dtype=np.int64)
+    total = int(offs[-1])
+    targets = np.array([total * k / world for k in range(world + 1)])
+    bounds = np.searchsorted(offs, targets, side="left").astype(np.int64)
+    bounds[0], bounds[-1] = 0, len(offs) - 1
+    return np.maximum.accumulate(bounds)
+
+
+def slice_systems(A: BatchEll, s0: int, s1: int, exec_) -> BatchEll:
+    """Systems [s0, s1) of A as a batch on exec_ (their storage is one
+    contiguous slice: system s owns entries from width * row_offsets[s])."""
+    o0, o1 = int(A.host_row_offsets[s0]), int(A.host_row_offsets[s1])
+    w = A.width
+    return BatchEll(exec_, A.host_row_offsets[s0:s1 + 1] - o0, w,
+                    A.col_idxs[w * o0:w * o1], A.values[w * o0:w * o1])
+
+
+def _all_gather_segments(local, lengths, group):
+    """Concatenation over ranks of each rank's 1-D segment (lengths known on
+    every rank): one all-gather of segments padded to the longest."""
+    import torch.distributed as dist
+    world = len(lengths)
+    m = max(int(n) for n in lengths)
+    if m == 0:
+        return local[:0]
+    pad = torch.zeros(m, dtype=local.dtype, device=local.device)
+    pad[:local.numel()] = local
+    parts = [torch.empty_like(pad) for _ in range(world)]
+    dist.all_gather(parts, pad, group=group)
+    return torch.cat([p[:int(n)] for p, n in zip(parts, lengths)])
+
+
+def solve_sharded(A: BatchEll, b, x, exec_, factory=None, group=None, local_solve=None):
+    """Solves the independent systems of A across the ranks of `group` (the
+    default process group when None): rank k solves its contiguous shard
+    (shard_bounds) on exec_, its own device, and every rank receives the
+    whole solution, the iteration counts and the residual norms through one
+    all-gather each; there is no other communication.  A, b and x hold the
+    whole batch (host or device); x is overwritten with the solution.
+    factory: a BatchBicgstab builder (the .build()....with_*() chain), used
+    on exec_; local_solve(A_local, b_local, x_local) -> (x, iterations,
+    residual_norms) replaces it (a host solver in tests).  Returns
+    (x, iterations, residual_norms)."""
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    bounds = shard_bounds(A.host_row_offsets, world)
+    s0, s1 = int(bounds[rank]), int(bounds[rank + 1])
+    offs = A.host_row_offsets
+    o0, o1 = int(offs[s0]), int(offs[s1])
+    A_loc = slice_systems(A, s0, s1, exec_)
+    dev = exec_.device
+    b_loc = b[o0:o1].to(dev).contiguous()
+    x_loc = x[o0:o1].to(dev).contiguous()
+    if local_solve is None:
+        if s1 > s0:
+            solver = factory.on(exec_).generate(A_loc)
+            solver.apply(b_loc, x_loc)
+            iters, res = solver.logger.iterations, solver.logger.residual_norms
+        else:
+            iters = torch.zeros(0, dtype=torch.int32, device=dev)
+            res = torch.zeros(0, dtype=torch.float64, device=dev)
+    else:
+        x_loc, iters, res = local_solve(A_loc, b_loc, x_loc)
+    row_len = [int(offs[bounds[k + 1]] - offs[bounds[k]]) for k in range(world)]
+    sys_len = [int(bounds[k + 1] - bounds[k]) for k in range(world)]
+    x_all = _all_gather_segments(x_loc.reshape(-1), row_len, group)
+    it_all = _all_gather_segments(iters.to(dev, torch.int64).reshape(-1), sys_len, group)
+    res_all = _all_gather_segments(res.to(dev, torch.float64).reshape(-1), sys_len, group)
+    x.copy_(x_all.to(x.device))
+    return x, it_all, res_all
