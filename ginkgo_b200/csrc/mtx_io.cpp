@@ -286,13 +286,19 @@ unsigned io_threads(size_t bytes)
     return std::max(1u, std::min<unsigned>(hw, unsigned(std::min<size_t>(bytes >> 22, 64))));
 }
 
-// Runs f(0) .. f(T - 1), on T threads when T > 1.
+// Runs f(0) .. f(T - 1), on T threads when T > 1; parts whose thread
+// cannot be started run on the calling thread.
 template <typename F>
 void parallel_for(unsigned T, F&& f)
 {
     std::vector<std::thread> pool;
     pool.reserve(T);
-    for (unsigned t = 1; t < T; ++t) pool.emplace_back(f, t);
+    unsigned t = 1;
+    try {
+        for (; t < T; ++t) pool.emplace_back(f, t);
+    } catch (const std::system_error&) {
+        for (; t < T; ++t) f(t);
+    }
     f(0u);
     for (auto& th : pool) th.join();
 }
