@@ -892,6 +892,9 @@ int64_t b2s_gmres_workspace_bytes(int64_t num_rows, int64_t nnz,
     case B2S_GMRES_MIXED_BF16:
         return gmres_layout<float, __nv_bfloat16>(num_rows, nnz, max_row_nnz,
                                                   int(krylov_dim), true).bytes;
+    case B2S_GMRES_CB_F32:
+        return gmres_layout<double, float>(num_rows, nnz, max_row_nnz, int(krylov_dim),
+                                           false).bytes;
     default:
         return -1;
     }
@@ -926,6 +929,15 @@ int b2s_gmres_solve(int variant, int64_t num_rows, const int32_t* row_ptrs,
             int(krylov_dim), max_iters, reduction_factor, inner_reduction,
             workspace, workspace_bytes, iterations, restarts, residual_norm,
             converged, stream);
+    case B2S_GMRES_CB_F32:
+        // FP64 arithmetic over an FP32 basis: the plain (non-refinement)
+        // engine; its row groups follow the basis type (4 rows, 16 bytes
+        // of basis and 32 of FP64 vectors per load)
+        return gmres_engine<double, float>(
+            num_rows, row_ptrs, col_idxs, values, max_row_nnz, inv_diag, b, x,
+            int(krylov_dim), max_iters, reduction_factor, 0.0, workspace,
+            workspace_bytes, iterations, restarts, residual_norm, converged,
+            stream);
     default:
         set_error("unknown GMRES variant %d", variant);
         return B2S_ERR_INVALID_ARG;

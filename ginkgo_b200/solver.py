@@ -187,7 +187,7 @@ class _Solver:
         kind = self.f.kind
         if kind in ("cg", "bicgstab"):
             return self._apply_cg(b, x)
-        if kind in ("gmres", "ir"):
+        if kind in ("gmres", "ir", "cb_gmres"):
             return self._apply_gmres(b, x)
         raise NotImplementedError(kind)
 
@@ -224,7 +224,14 @@ class _Solver:
         x2 = _check_dense(x, n, A.dtype, "x")
         if b2.shape[1] != 1 or not x2.is_contiguous() or not b2.is_contiguous():
             raise NotImplementedError("GMRES here takes one contiguous right-hand side")
-        variant = {None: 0, "f64": 0, "f32": 1, "bf16": 2}[self.f.storage_precision]
+        if self.f.kind == "cb_gmres":
+            sp = self.f.storage_precision or "reduce1"
+            if sp not in ("keep", "reduce1"):
+                raise NotImplementedError(
+                    f"CbGmres storage_precision {sp!r}: keep and reduce1 are on this path")
+            variant = 0 if sp == "keep" else 3
+        else:
+            variant = {None: 0, "f64": 0, "f32": 1, "bf16": 2}[self.f.storage_precision]
         nbytes = lib().b2s_gmres_workspace_bytes(n, A.nnz, A.max_row_nnz,
                                                  self.f.krylov_dim, variant)
         ws = self._workspace(nbytes)
@@ -250,6 +257,10 @@ class _BicgstabFactory(_SolverFactory):
 
 class _GmresFactory(_SolverFactory):
     kind = "gmres"
+
+
+class _CbGmresFactory(_SolverFactory):
+    kind = "cb_gmres"
 
 
 class _IrFactory(_SolverFactory):
@@ -289,6 +300,18 @@ class Gmres:
     @staticmethod
     def build():
         return _Builder(_GmresFactory, krylov_dim=30)
+
+
+class CbGmres:
+    """solver::CbGmres (core/solver/cb_gmres.cpp): restarted GMRES with FP64
+    arithmetic and the Krylov basis stored in a reduced format;
+    with_storage_precision("reduce1") (the default here, an FP32 basis) or
+    "keep" (FP64).  krylov_dim <= 32 (the reference default of 100 is
+    capped)."""
+
+    @staticmethod
+    def build():
+        return _Builder(_CbGmresFactory, krylov_dim=30, storage_precision="reduce1")
 
 
 class Ir:

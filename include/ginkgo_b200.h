@@ -440,6 +440,7 @@ int b2s_bicgstab_solve_f32(int64_t num_rows, const int32_t* row_ptrs,
 #define B2S_GMRES_F64 0
 #define B2S_GMRES_MIXED_F32 1
 #define B2S_GMRES_MIXED_BF16 2
+#define B2S_GMRES_CB_F32 3
 
 /* Restarted GMRES(krylov_dim <= 32), right scalar-Jacobi preconditioning,
  * one right-hand side, FP64 matrix/b/x/inv_diag.  variant B2S_GMRES_F64 is
@@ -448,7 +449,11 @@ int b2s_bicgstab_solve_f32(int64_t num_rows, const int32_t* row_ptrs,
  * core/solver/ir.cpp:191-257) whose every outer step computes r = b - A x
  * and ||r|| in FP64 and runs one GMRES cycle on an FP32 copy of A with FP32
  * vectors and an FP32 or BF16 Krylov basis.  Hessenberg, Givens and the
- * triangular solve are FP64 in all variants.  max_iters bounds the total
+ * triangular solve are FP64 in all variants.  B2S_GMRES_CB_F32 is
+ * compressed-basis GMRES (CbGmres<double> with storage_precision reduce1,
+ * core/solver/cb_gmres.cpp): FP64 matrix, vectors and arithmetic, the
+ * Krylov basis stored in FP32 and read back for the orthogonalisation and
+ * the solution update.  max_iters bounds the total
  * Arnoldi steps; reduction_factor is the goal on the explicit FP64 residual
  * relative to ||b||; inner_reduction ends an inner cycle early once its
  * estimate falls below inner_reduction * ||r||.  *restarts counts cycles.

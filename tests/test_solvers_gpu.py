@@ -6,6 +6,8 @@ Solves are checked by what they must achieve: the explicit FP64 residual
 close to the oracle's for the same stopping rule, and the known solutions of
 the reference tests within their tolerances.
 """
+import os
+
 import numpy as np
 import pytest
 import torch
@@ -347,3 +349,57 @@ def test_cg_large_single_rhs_split_pass_matches_oracle(exe):
     assert not s.logger.has_converged
     np.testing.assert_allclose(x.cpu().numpy(), xo[:, 0] if xo.ndim == 2 else xo,
                                rtol=1e-9, atol=1e-11 * np.abs(xo).max())
+
+
+def _cb_cases():
+    import json
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                           "cb_gmres_cases.json")) as f:
+        return [c for c in json.load(f)["cases"] if "block_jacobi" not in c]
+
+
+@pytest.mark.parametrize("case", _cb_cases(), ids=lambda c: c["name"])
+@pytest.mark.parametrize("storage", ["keep", "reduce1"])
+def test_cb_gmres_meets_reference_known_answers(exe, case, storage):
+    # reference/test/solver/cb_gmres_kernels.cpp: reduction 10 eps(double)
+    # from the initial residual; the solution to tol_factor x assert_precision
+    # (10 eps of the storage type; its square root for the restart case)
+    from ginkgo_b200.solver import CbGmres
+    A_d = np.array(case["A"])
+    rp, ci, v = dense_to_csr(case["A"])
+    A = Csr.read(exe, rp, ci, v)
+    eps = 10 * np.finfo(np.float64).eps
+    prec = eps if storage == "keep" else 10 * np.finfo(np.float32).eps
+    tol = np.sqrt(prec) if case.get("tol_sqrt") else case["tol_factor"] * prec
+    s = (CbGmres.build().with_krylov_dim(min(case["krylov_dim"], 32))
+         .with_storage_precision(storage)
+         .with_criteria(*crit(case["max_iters"], eps)).on(exe).generate(A))
+    B = np.array(case["b"])
+    for col in range(B.shape[1]):
+        b = torch.tensor(B[:, col], dtype=torch.float64, device="cuda")
+        x = torch.zeros_like(b)
+        s.apply(b, x)
+        got, exp = x.cpu().numpy(), np.array(case["x"])[:, col]
+        err = np.linalg.norm(got - exp) / max(np.linalg.norm(got), np.linalg.norm(exp))
+        assert err <= tol, (case["name"], storage, err, tol)
+        assert np.linalg.norm(A_d @ got - B[:, col]) <= 1e-6 * np.linalg.norm(B[:, col])
+
+
+@pytest.mark.parametrize("nx", [16, 15])
+def test_cb_gmres_fp32_basis_reaches_fp64_accuracy(exe, nx):
+    # 15^3 rows leave a partial 4-row group at the end of every basis vector
+    from ginkgo_b200.solver import CbGmres
+    rp, ci, v, n, b = _aniso(nx)
+    A = Csr.read(exe, rp, ci, v)
+    runs = {}
+    for storage in ("keep", "reduce1"):
+        s = (CbGmres.build().with_krylov_dim(30).with_storage_precision(storage)
+             .with_criteria(*crit(3000, 1e-10))
+             .with_preconditioner(Jacobi.build().with_max_block_size(1))
+             .on(exe).generate(A))
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        s.apply(torch.from_numpy(b).cuda(), x)
+        assert s.logger.has_converged, storage
+        assert explicit_rel_res(rp, ci, v, x.cpu().numpy(), b)[0] <= 1e-10, storage
+        runs[storage] = s.logger.num_iterations
+    assert runs["reduce1"] <= 1.5 * runs["keep"] + 30, runs
