@@ -206,7 +206,7 @@ def main():
                     help="skip the time-to-1e-10 mixed vs FP64 GMRES section")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the batched BiCGStab and differentiable-solve sections")
-    ap.add_argument("--solve-case", choices=["f64", "ir_f32", "ir_bf16"],
+    ap.add_argument("--solve-case", choices=["f64", "ir_f32", "ir_bf16", "cb_f32"],
                     help="profiling aid: run one GMRES variant on the 27-point "
                     "operator for --solve-iters iterations and exit")
     ap.add_argument("--solve-iters", type=int, default=60)
@@ -342,9 +342,10 @@ def main():
 
 
 def gmres_variants(max_iters):
-    """GMRES(30) + scalar Jacobi to 1e-10: plain FP64, and iterative
-    refinement around an FP32 / BF16-basis inner cycle."""
-    from ginkgo_b200.solver import Gmres, Ir, Iteration, Jacobi, ResidualNorm
+    """GMRES(30) + scalar Jacobi to 1e-10: plain FP64, iterative refinement
+    around an FP32 / BF16-basis inner cycle, and compressed-basis GMRES
+    (FP64 arithmetic over an FP32 basis)."""
+    from ginkgo_b200.solver import CbGmres, Gmres, Ir, Iteration, Jacobi, ResidualNorm
     crit = (Iteration.build().with_max_iters(max_iters),
             ResidualNorm.build().with_reduction_factor(1e-10))
     jac = Jacobi.build().with_max_block_size(1)
@@ -357,6 +358,8 @@ def gmres_variants(max_iters):
         "ir_bf16": Ir.build().with_criteria(*crit).with_solver(
             Gmres.build().with_krylov_dim(30).with_storage_precision("bf16")
             .with_preconditioner(jac)),
+        "cb_f32": CbGmres.build().with_krylov_dim(30).with_storage_precision("reduce1")
+        .with_criteria(*crit).with_preconditioner(jac),
     }
 
 
@@ -535,7 +538,7 @@ def ir_gmres_section(exe, stream, grid=96, reps=3):
                      "iterations": it, "restarts": s.logger.restarts,
                      "converged": s.logger.has_converged,
                      "explicit_rel_residual": rel}
-    for name in ("ir_f32", "ir_bf16"):
+    for name in ("ir_f32", "ir_bf16", "cb_f32"):
         out[name]["error_vs_f64"] = float((sols[name] - sols["f64"]).norm() /
                                           sols["f64"].norm())
         out[name]["speedup_vs_f64"] = round(out["f64"]["ms"] / out[name]["ms"], 3)
