@@ -272,18 +272,3 @@ def solve(A, b, x0=None, value_type="f64", storage="keep", krylov_dim=100,
     x = (x + _apply_prec(preconditioner, before)).astype(vt)
     return (x[:, 0] if one_col else x), total_iter
 
-
-def block_jacobi(A, block_ptrs, value_type="f64"):
-    """A block-diagonal preconditioner with the given block starts: M v
-    applies the inverse of each diagonal block (preconditioner::Jacobi with
-    full-precision blocks)."""
-    vt = _FLOAT[value_type]
-    A = np.asarray(A, dtype=np.float64)
-    inv = [np.linalg.inv(A[s:e, s:e]).astype(vt) for s, e in zip(block_ptrs[:-1], block_ptrs[1:])]
-
-    def apply(v):
-        out = np.zeros_like(v)
-        for (s, e), B in zip(zip(block_ptrs[:-1], block_ptrs[1:]), inv):
-            out[s:e] = (B @ v[s:e]).astype(vt)
-        return out
-    return apply

@@ -40,7 +40,15 @@ PARAMS = [(c, vt, st) for c in G["cases"] for vt in ("f64", "f32") for st in G["
 def test_cb_gmres_oracle_meets_reference_known_answers(case, vt, storage):
     prec = None
     if "block_jacobi" in case:
-        prec = CB.block_jacobi(case["A"], case["block_jacobi"], vt)
+        # Jacobi with max_block_size 3 (:508-510): blocks detected on the
+        # Csr of A, the inverted blocks applied in the value type
+        from oracle import jacobi as J
+        A = np.array(case["A"])
+        rp = np.arange(0, A.size + 1, A.shape[1])
+        ci = np.tile(np.arange(A.shape[1]), A.shape[0])
+        assert J.find_blocks(rp, ci, 3) == case["block_jacobi"]
+        jac = J.generate(rp, ci, A.ravel(), 3, dtype=CB._FLOAT[vt])
+        prec = lambda v: J.apply(jac, v)  # noqa: E731
     x, iters = CB.solve(case["A"], np.array(case["b"]), value_type=vt, storage=storage,
                         krylov_dim=case["krylov_dim"], max_iters=case["max_iters"],
                         preconditioner=prec)
