@@ -110,23 +110,144 @@ class Jacobi:
              _p(A.row_ptrs), _p(A.col_idxs), _p(A.values), _p(self.inv_diag),
              _stream(self.inv_diag))
 
-    def apply(self, b, x):
+    def apply(self, *args):
+        """apply(b, x) or apply(alpha, b, beta, x)."""
+        if len(args) == 2:
+            (b, x), alpha, beta = args, None, None
+        else:
+            a, b, be, x = args
+            dev = self.A.values.device
+            alpha = torch.as_tensor(a, dtype=self.A.dtype, device=dev).reshape(1)
+            beta = torch.as_tensor(be, dtype=self.A.dtype, device=dev).reshape(1)
         b2 = _check_dense(b, self.A.shape[0], self.A.dtype, "b")
         x2 = _check_dense(x, self.A.shape[0], self.A.dtype, "x")
         call(f"b2s_jacobi_apply_{_SFX[self.A.dtype]}", b2.shape[0], b2.shape[1],
              _p(self.inv_diag), _p(b2), b2.stride(0), _p(x2), x2.stride(0),
-             None, None, _stream(x2))
+             _p(alpha), _p(beta), _stream(x2))
         return x
 
 
+def find_blocks(row_ptrs, col_idxs, max_block_size):
+    """Block pointers of the diagonal blocks (jacobi::find_blocks,
+    reference/preconditioner/jacobi_kernels.cpp:28-98): runs of consecutive
+    rows with equal column patterns up to max_block_size rows (natural
+    blocks), then neighbouring natural blocks merged while they fit.  Host
+    set-up on the Csr arrays (numpy)."""
+    rp = np.asarray(row_ptrs, dtype=np.int64)
+    ci = np.asarray(col_idxs)
+    n = len(rp) - 1
+    if n == 0:
+        return np.zeros(1, dtype=np.int32)
+    lens = np.diff(rp)
+    # same pattern as the previous row: same length and same columns
+    same = np.zeros(n, dtype=bool)
+    eq_len = lens[1:] == lens[:-1]
+    for i in np.nonzero(eq_len)[0] + 1:
+        same[i] = np.array_equal(ci[rp[i]:rp[i + 1]], ci[rp[i - 1]:rp[i]])
+    natural = [0]
+    size = 1
+    for i in range(1, n):
+        if size < max_block_size and same[i]:
+            size += 1
+        else:
+            natural.append(natural[-1] + size)
+            size = 1
+    natural.append(natural[-1] + size)
+    out = [0]
+    cur = natural[1] - natural[0]
+    for i in range(1, len(natural) - 1):
+        bs = natural[i + 1] - natural[i]
+        if cur + bs <= max_block_size:
+            cur += bs
+        else:
+            out.append(natural[i])
+            cur = bs
+    out.append(natural[-1])
+    return np.array(out, dtype=np.int32)
+
+
+class BlockJacobi:
+    """preconditioner::Jacobi with max_block_size 2..32 and full-precision
+    blocks (core/preconditioner/jacobi.cpp:370-420): the diagonal blocks
+    inverted on the device (b2s_jacobi_block_generate_*), applied as
+    x = D^-1 b or alpha D^-1 b + beta x.  Not fused into the solvers here
+    (they take scalar Jacobi)."""
+
+    def __init__(self, A: Csr, max_block_size: int, block_pointers=None):
+        self.A = A
+        self.max_block_size = int(max_block_size)
+        if not 1 <= self.max_block_size <= 32:
+            raise ValueError("max_block_size must be 1..32")
+        if block_pointers is None:
+            block_pointers = find_blocks(A.row_ptrs.cpu().numpy(), A.col_idxs.cpu().numpy(),
+                                         self.max_block_size)
+        bp = np.asarray(block_pointers, dtype=np.int32)
+        sizes = np.diff(bp)
+        if bp[0] != 0 or bp[-1] != A.shape[0] or np.any(sizes < 0) or \
+                np.any(sizes > self.max_block_size):
+            raise ValueError("block pointers must run from 0 to num_rows in steps of "
+                             "0..max_block_size")
+        dev = A.values.device
+        self.block_pointers = bp
+        self.num_blocks = len(bp) - 1
+        self._ptrs = torch.from_numpy(bp).to(dev)
+        m = self.max_block_size
+        self.blocks = torch.zeros(max(self.num_blocks, 1) * m * m, dtype=A.dtype, device=dev)
+        call(f"b2s_jacobi_block_generate_{_SFX[A.dtype]}", A.shape[0], _p(A.row_ptrs),
+             _p(A.col_idxs), _p(A.values), self.num_blocks, _p(self._ptrs), m,
+             _p(self.blocks), _stream(self.blocks))
+
+    @property
+    def inv_diag(self):
+        raise NotImplementedError("the solvers here fuse scalar Jacobi only "
+                                  "(with_max_block_size(1))")
+
+    def apply(self, *args):
+        """apply(b, x) or apply(alpha, b, beta, x)."""
+        n = self.A.shape[0]
+        if len(args) == 2:
+            (b, x), alpha, beta = args, None, None
+        else:
+            a, b, be, x = args
+            dev = self.A.values.device
+            alpha = torch.as_tensor(a, dtype=self.A.dtype, device=dev).reshape(1)
+            beta = torch.as_tensor(be, dtype=self.A.dtype, device=dev).reshape(1)
+        b2 = _check_dense(b, n, self.A.dtype, "b")
+        x2 = _check_dense(x, n, self.A.dtype, "x")
+        call(f"b2s_jacobi_block_apply_{_SFX[self.A.dtype]}", n, self.num_blocks,
+             _p(self._ptrs), self.max_block_size, _p(self.blocks), _p(b2), b2.stride(0),
+             _p(x2), x2.stride(0), b2.shape[1], _p(alpha), _p(beta), _stream(x2))
+        return x
+
+    def to_dense(self):
+        """The block-diagonal inverse as a dense host array."""
+        n, m = self.A.shape[0], self.max_block_size
+        blk = self.blocks.cpu().numpy()
+        out = np.zeros((n, n), dtype=blk.dtype)
+        for i, (s, e) in enumerate(zip(self.block_pointers[:-1], self.block_pointers[1:])):
+            bs = e - s
+            slot = blk[i * m * m:(i + 1) * m * m].reshape(m, m)  # [col][row]
+            out[s:e, s:e] = slot[:bs, :bs].T
+        return out
+
+    def transpose(self):
+        """Jacobi::transpose: the same blocks, each transposed."""
+        t = BlockJacobi.__new__(BlockJacobi)
+        t.__dict__.update(self.__dict__)
+        m = self.max_block_size
+        t.blocks = (self.blocks.reshape(-1, m, m).transpose(1, 2).contiguous().reshape(-1))
+        return t
+
+
 class JacobiFactory:
-    def __init__(self, exec_, max_block_size=32):
-        if int(max_block_size) != 1:
-            raise NotImplementedError(
-                "this path provides scalar Jacobi only: use with_max_block_size(1)")
+    def __init__(self, exec_, max_block_size=32, block_pointers=None):
+        self.max_block_size = int(max_block_size)
+        self.block_pointers = block_pointers
 
     def generate(self, A):
-        return Jacobi(A)
+        if self.max_block_size == 1:
+            return Jacobi(A)
+        return BlockJacobi(A, self.max_block_size, self.block_pointers)
 
 
 # ---------------------------------------------------------------- logging --

@@ -226,6 +226,37 @@ int b2s_jacobi_apply_f32(int64_t num_rows, int64_t num_rhs,
                          float* x, int64_t ldx, const float* alpha,
                          const float* beta, void* stream);
 
+/* Block Jacobi with full-precision blocks of at most max_block_size <= 32
+ * rows.  block_ptrs (device, num_blocks + 1 entries, from 0 to num_rows)
+ * delimit the diagonal blocks; a block with a bad extent is skipped.  Block
+ * b's inverse is stored at blocks + b * max_block_size^2, entry (i, j) at
+ * i + j * max_block_size (column-major), as the reference's storage with a
+ * stride of max_block_size.  Generate: Gauss-Jordan with partial pivoting
+ * in place (the first row of largest magnitude is the pivot; a zero pivot
+ * ends the elimination of that block, as the reference's invert_block
+ * does); replaces jacobi::generate (core/preconditioner/jacobi_kernels.hpp,
+ * reference/preconditioner/jacobi_kernels.cpp:310-395) without adaptive
+ * precision.  Apply: x = D^-1 b or alpha D^-1 b + beta x (beta == 0 ignores
+ * x); replaces jacobi::simple_apply / apply. */
+int b2s_jacobi_block_generate_f64(int64_t num_rows, const int32_t* row_ptrs,
+                                  const int32_t* col_idxs, const double* values,
+                                  int64_t num_blocks, const int32_t* block_ptrs,
+                                  int max_block_size, double* blocks, void* stream);
+int b2s_jacobi_block_generate_f32(int64_t num_rows, const int32_t* row_ptrs,
+                                  const int32_t* col_idxs, const float* values,
+                                  int64_t num_blocks, const int32_t* block_ptrs,
+                                  int max_block_size, float* blocks, void* stream);
+int b2s_jacobi_block_apply_f64(int64_t num_rows, int64_t num_blocks,
+                               const int32_t* block_ptrs, int max_block_size,
+                               const double* blocks, const double* b, int64_t ldb,
+                               double* x, int64_t ldx, int64_t num_rhs,
+                               const double* alpha, const double* beta, void* stream);
+int b2s_jacobi_block_apply_f32(int64_t num_rows, int64_t num_blocks,
+                               const int32_t* block_ptrs, int max_block_size,
+                               const float* blocks, const float* b, int64_t ldb,
+                               float* x, int64_t ldx, int64_t num_rhs,
+                               const float* alpha, const float* beta, void* stream);
+
 /* ------------------------------------------------ Krylov step kernels -- */
 
 /* Kernel-level stand-ins for a caller that keeps the reference's solver

@@ -65,7 +65,9 @@ def invert_block(blk):
     """invert_block (:223-240) with choose_pivot, swap_rows and
     apply_gauss_jordan_transform (:128-170), then permute_and_transpose_block
     (:203-220): in-place Gauss-Jordan with partial pivoting.  Returns the
-    inverse (row-major), or None for a singular block."""
+    inverse (row-major).  A zero pivot ends the elimination and the block is
+    stored as far as it got, as the reference's generate does (it does not
+    check invert_block's result)."""
     b = np.array(blk, copy=True)
     dt = b.dtype.type
     n = b.shape[0]
@@ -79,7 +81,7 @@ def invert_block(blk):
         perm[k], perm[cp] = perm[cp], perm[k]
         d = b[k, k]
         if d == 0:
-            return None
+            break
         for i in range(n):
             b[i, k] = dt(b[i, k] / -d)
         b[k, k] = 0

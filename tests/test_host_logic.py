@@ -82,10 +82,39 @@ def test_solver_factory_parameters():
     assert (m, r) == (50, 1e-8)
     with pytest.raises(ValueError):
         _criteria((ResidualNorm.build().with_reduction_factor(1e-8),))
-    with pytest.raises(NotImplementedError):
-        Jacobi.build().with_max_block_size(4).on(None)
+    assert Jacobi.build().with_max_block_size(4).on(None).max_block_size == 4
     f = (Gmres.build().with_krylov_dim(100)
          .with_criteria(Iteration.build().with_max_iters(5)).on(None))
     assert f.krylov_dim == 32  # capped by the device Hessenberg
     f = Cg.build().with_criteria(Iteration.build().with_max_iters(3)).on(None)
     assert f.kind == "cg" and f.max_iters == 3 and f.reduction == 0.0
+
+
+def test_block_detection_matches_the_oracle():
+    import json
+    import os
+
+    from ginkgo_b200.solver import find_blocks
+    from oracle import jacobi as J
+    here = os.path.dirname(os.path.abspath(__file__))
+    with open(os.path.join(here, "golden", "jacobi_cases.json")) as f:
+        cases = json.load(f)["blocks"]
+    for c in cases:
+        if "block_ptrs" in c:
+            continue
+        m = c["matrix"]
+        got = find_blocks(m["row_ptrs"], m["col_idxs"], c["max_block_size"])
+        assert got.tolist() == c["expected"], c["name"]
+    rng = np.random.default_rng(0)
+    for _ in range(30):
+        # runs of rows sharing a pattern, of random lengths
+        n, rows = 0, []
+        while n < 300:
+            run = int(rng.integers(1, 12))
+            cols = np.sort(rng.choice(400, size=int(rng.integers(1, 6)), replace=False))
+            rows += [cols] * run
+            n += run
+        rp = np.concatenate([[0], np.cumsum([len(r) for r in rows])])
+        ci = np.concatenate(rows)
+        for mbs in (1, 3, 8, 32):
+            assert find_blocks(rp, ci, mbs).tolist() == J.find_blocks(rp, ci, mbs)

@@ -1,0 +1,131 @@
+"""Block Jacobi on the GPU (b2s_jacobi_block_generate/apply) against the
+reference's known answers (tests/golden/jacobi_cases.json, from
+reference/test/preconditioner/jacobi_kernels.cpp) and against the oracle's
+restatement on seeded random block patterns, pivoting and singular blocks
+included."""
+import json
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from ginkgo_b200.matrix import Csr, CudaExecutor
+from ginkgo_b200.solver import BlockJacobi, Jacobi
+from oracle import jacobi as J
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+with open(os.path.join(ROOT, "tests", "golden", "jacobi_cases.json")) as f:
+    G = json.load(f)
+DT = [(torch.float64, np.float64), (torch.float32, np.float32)]
+
+
+@pytest.fixture(scope="module")
+def exe():
+    return CudaExecutor.create(0)
+
+
+def _csr(exe, m, dt):
+    return Csr.read(exe, m["row_ptrs"], m["col_idxs"], m["values"], dtype=dt)
+
+
+@pytest.mark.parametrize("dt,npdt", DT)
+@pytest.mark.parametrize("case", [c for c in G["dense"] if not c.get("aggregate_l1")],
+                         ids=lambda c: c["name"])
+def test_inverted_blocks_known_answers(exe, case, dt, npdt):
+    A = _csr(exe, case["matrix"], dt)
+    bj = BlockJacobi(A, case["max_block_size"], case.get("block_ptrs"))
+    if case.get("transpose"):
+        bj = bj.transpose()
+    got = bj.to_dense()
+    assert np.abs(got - np.array(case["expected"])).max() <= 10 * np.finfo(npdt).eps
+
+
+@pytest.mark.parametrize("dt,npdt", DT)
+@pytest.mark.parametrize("case", G["apply"], ids=lambda c: c["name"])
+def test_apply_known_answers(exe, case, dt, npdt):
+    A = _csr(exe, G["dense"][0]["matrix"], dt)
+    if case["max_block_size"] == 1:
+        p = Jacobi(A)
+    else:
+        p = BlockJacobi(A, case["max_block_size"], case.get("block_ptrs"))
+    b = torch.tensor(case["b"], dtype=dt, device="cuda")
+    x = torch.tensor(case["x"], dtype=dt, device="cuda")
+    if "alpha" in case:
+        p.apply(case["alpha"], b, case["beta"], x)
+    else:
+        p.apply(b, x)
+    got, exp = x.cpu().double().numpy(), np.array(case["expected"])
+    err = np.linalg.norm(got - exp) / max(np.linalg.norm(got), np.linalg.norm(exp))
+    assert err <= 10 * np.finfo(npdt).eps, (case["name"], err)
+
+
+def _random_blocks(seed, n_target=600, max_run=9, pivoting=False, singular=False):
+    """Csr with runs of rows sharing a pattern: each run's columns are the
+    run itself plus a few far columns; diagonally dominant values, or (with
+    pivoting) zero diagonals in some runs; one run singular when asked."""
+    rng = np.random.default_rng(seed)
+    if pivoting:
+        max_run = 4  # a run never straddles blocks of 4 or more rows
+    runs, n = [], 0
+    while n < n_target:
+        r = int(rng.integers(1, max_run + 1))
+        runs.append((n, r))
+        n += r
+    rows = []
+    for k, (s, r) in enumerate(runs):
+        # far columns at least 40 rows away, so they never fall inside a
+        # (merged) block: every block stays block-diagonal in its runs
+        pool = np.setdiff1d(np.arange(n), np.arange(max(0, s - 40), s + r + 40))
+        far = rng.choice(pool, size=3, replace=False)
+        cols = np.unique(np.concatenate([np.arange(s, s + r), far]))
+        for i in range(r):
+            vals = rng.uniform(-1, 1, len(cols))
+            row = s + i
+            if pivoting and k % 3 == 0:
+                # zero diagonal, the strong entry one column to the right
+                # (cyclically): every elimination step must swap rows
+                vals[cols == row] = 0.0
+                vals[cols == s + (i + 1) % r] = 2.0 * r + 4.0
+            else:
+                vals[cols == row] = 2.0 * r + 4.0
+            if singular and k == 1:
+                vals[cols == s] = 0.0  # first column of the block is all zero
+            rows.append((cols, vals))
+    rp = np.concatenate([[0], np.cumsum([len(c) for c, _ in rows])]).astype(np.int32)
+    ci = np.concatenate([c for c, _ in rows]).astype(np.int32)
+    v = np.concatenate([v for _, v in rows])
+    return rp, ci, v
+
+
+@pytest.mark.parametrize("dt,npdt", DT)
+@pytest.mark.parametrize("mbs", [4, 13, 32])
+@pytest.mark.parametrize("kind", ["dominant", "pivoting", "singular"])
+def test_random_blocks_match_oracle(exe, dt, npdt, mbs, kind):
+    rp, ci, v = _random_blocks(mbs * 10 + len(kind), pivoting=kind == "pivoting",
+                               singular=kind == "singular")
+    n = len(rp) - 1
+    A = Csr.read(exe, rp, ci, v, dtype=dt)
+    bj = BlockJacobi(A, mbs)
+    assert bj.block_pointers.tolist() == J.find_blocks(rp, ci, mbs)
+    ref = J.generate(rp, ci, v.astype(npdt), mbs, dtype=npdt)
+    got = bj.to_dense()
+    exp = J.to_dense(ref, n)
+    tol = 1e-11 if npdt == np.float64 else 2e-4
+    scale = max(1.0, np.abs(exp).max())
+    assert np.abs(got - exp).max() <= tol * scale
+    # apply, 3 right-hand sides, plain and alpha/beta
+    rng = np.random.default_rng(mbs)
+    b = rng.standard_normal((n, 3)).astype(npdt)
+    x0 = rng.standard_normal((n, 3)).astype(npdt)
+    bd = torch.from_numpy(b).cuda()
+    xd = torch.from_numpy(x0.copy()).cuda()
+    bj.apply(bd, xd)
+    np.testing.assert_allclose(xd.cpu().numpy(), J.apply(ref, b), rtol=0,
+                               atol=tol * scale * np.abs(b).max() * 40)
+    xd = torch.from_numpy(x0.copy()).cuda()
+    bj.apply(-0.5, bd, 2.0, xd)
+    np.testing.assert_allclose(xd.cpu().numpy(), J.apply(ref, b, x0, -0.5, 2.0), rtol=0,
+                               atol=tol * scale * np.abs(b).max() * 40 + tol * 4)
