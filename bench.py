@@ -328,7 +328,8 @@ def main():
         result["gpu_launches"] += solve.pop("gpu_launches")
     if not args.no_extra:
         for key, fn in (("cg", cg_section), ("batch_bicgstab", batch_section),
-                        ("autograd", autograd_section)):
+                        ("autograd", autograd_section),
+                        ("block_jacobi", block_jacobi_section)):
             try:
                 result[key] = fn(exe, stream)
             except Exception as e:  # a failed optional section is reported, not fatal
@@ -544,6 +545,32 @@ def ir_gmres_section(exe, stream, grid=96, reps=3):
         out[name]["speedup_vs_f64"] = round(out["f64"]["ms"] / out[name]["ms"], 3)
     out["gpu_launches"] = launches
     return out
+
+
+def block_jacobi_section(exe, stream, block_size=8):
+    """Block Jacobi on the 7-point 128^3 matrix: blocks of up to block_size
+    rows (consecutive single-row natural blocks merged), device generate
+    (pivoted Gauss-Jordan per block) and apply with one right-hand side.
+    Apply bytes: the stored blocks (block_size^2 values each) + b + x +
+    the block pointers."""
+    import torch
+    from ginkgo_b200.matrix import Csr
+    from ginkgo_b200.solver import BlockJacobi
+    rp, ci, v = build_matrix()
+    n = len(rp) - 1
+    A = Csr.read(exe, rp, ci, v)
+    bj = BlockJacobi(A, block_size)
+    gen_ms = _event_ms(lambda: BlockJacobi(A, block_size, bj.block_pointers), stream)
+    b = torch.from_numpy(np.random.default_rng(SEED).standard_normal(n)).cuda()
+    x = torch.empty_like(b)
+    apply_ms = _event_ms(lambda: bj.apply(b, x), stream, reps=20)
+    nbytes = bj.num_blocks * block_size * block_size * 8 + 2 * n * 8 + (bj.num_blocks + 1) * 4
+    peak, _ = measured_peaks()
+    return {"workload": "poisson3d_7pt_128", "max_block_size": block_size,
+            "num_blocks": bj.num_blocks, "generate_ms": round(gen_ms, 3),
+            "apply_ms": round(apply_ms, 4),
+            "apply_gbs": round(nbytes / (apply_ms * 1e-3) / 1e9, 1),
+            "apply_frac_of_measured": round(nbytes / (apply_ms * 1e-3) / 1e9 / peak, 3)}
 
 
 def _event_ms(fn, stream, reps=3):

@@ -111,6 +111,10 @@ __global__ void __launch_bounds__(kJacobiWarps * kWarp)
     }
 }
 
+// Apply: floor(32 / max_bs) blocks per warp, lane = (block in warp, row),
+// so small blocks keep the whole warp busy.  Every lane runs the same
+// max_bs broadcast steps (full-mask shuffles); lanes outside a valid row
+// only pass values along.
 template <typename T>
 __global__ void __launch_bounds__(kJacobiWarps * kWarp)
     jacobi_block_apply_kernel(int64_t n, int64_t num_blocks, const int32_t* __restrict__ ptrs,
@@ -120,23 +124,29 @@ __global__ void __launch_bounds__(kJacobiWarps * kWarp)
                               const T* __restrict__ beta)
 {
     const int lane = threadIdx.x % kWarp, w = threadIdx.x / kWarp;
-    const int64_t blk = int64_t(blockIdx.x) * kJacobiWarps + w;
-    if (blk >= num_blocks) return;
-    int s, bs;
-    if (!block_extent(ptrs, blk, n, max_bs, s, bs)) return;
-    const T* inv = blocks + blk * int64_t(max_bs) * max_bs;
+    const int per_warp = kWarp / max_bs;
+    const int sub = lane / max_bs, r = lane % max_bs;
+    const int64_t warp = int64_t(blockIdx.x) * kJacobiWarps + w;
+    const int64_t blk = warp * per_warp + sub;
+    if (warp * per_warp >= num_blocks) return;  // the whole warp: uniform
+    int s = 0, bs = 0;
+    const bool in_block = sub < per_warp && blk < num_blocks &&
+                          block_extent(ptrs, blk, n, max_bs, s, bs);
+    const bool active = in_block && r < bs;
+    const T* inv = blocks + (in_block ? blk : 0) * int64_t(max_bs) * max_bs;
     const T a = alpha ? *alpha : T(1);
     const T be = beta ? *beta : T(0);
+    const int base = sub * max_bs;  // first lane of this lane's block
     for (int64_t col = 0; col < k; ++col) {
-        const T bv = lane < bs ? b[(s + lane) * ldb + col] : T(0);
+        const T bv = active ? b[(s + r) * ldb + col] : T(0);
         T acc = T(0);
-        if (lane < bs && be != T(0)) acc = x[(s + lane) * ldx + col] * be;
+        if (active && be != T(0)) acc = x[(s + r) * ldx + col] * be;
         // apply_block: x(row) += alpha * inv(row, inner) * b(inner), inner in order
-        for (int inner = 0; inner < bs; ++inner) {
-            const T bi = __shfl_sync(0xffffffffu, bv, inner);
-            if (lane < bs) acc += a * inv[lane + int64_t(inner) * max_bs] * bi;
+        for (int inner = 0; inner < max_bs; ++inner) {
+            const T bi = __shfl_sync(0xffffffffu, bv, (base + inner) % kWarp);
+            if (active && inner < bs) acc += a * inv[r + int64_t(inner) * max_bs] * bi;
         }
-        if (lane < bs) x[(s + lane) * ldx + col] = acc;
+        if (active) x[(s + r) * ldx + col] = acc;
     }
 }
 
@@ -166,7 +176,8 @@ int block_apply(int64_t n, int64_t num_blocks, const int32_t* ptrs, int max_bs,
                   "alpha and beta must both be given or both be null");
     B2S_CHECK_ARG(k == 0 || (ldb >= k && ldx >= k), "leading dimension < num_rhs");
     if (num_blocks == 0 || k == 0) return B2S_OK;
-    jacobi_block_apply_kernel<T><<<ceildiv(num_blocks, kJacobiWarps), kJacobiWarps * kWarp,
+    const int64_t warps = ceildiv(num_blocks, kWarp / max_bs);
+    jacobi_block_apply_kernel<T><<<ceildiv(warps, kJacobiWarps), kJacobiWarps * kWarp,
                                    0, as_stream(stream)>>>(n, num_blocks, ptrs, max_bs,
                                                            blocks, b, ldb, x, ldx, k,
                                                            alpha, beta);
