@@ -132,38 +132,16 @@ def find_blocks(row_ptrs, col_idxs, max_block_size):
     reference/preconditioner/jacobi_kernels.cpp:28-98): runs of consecutive
     rows with equal column patterns up to max_block_size rows (natural
     blocks), then neighbouring natural blocks merged while they fit.  Host
-    set-up on the Csr arrays (numpy)."""
-    rp = np.asarray(row_ptrs, dtype=np.int64)
-    ci = np.asarray(col_idxs)
+    set-up in the library (b2s_jacobi_find_blocks) on host Csr arrays."""
+    rp = np.ascontiguousarray(row_ptrs, dtype=np.int32)
+    ci = np.ascontiguousarray(col_idxs, dtype=np.int32)
     n = len(rp) - 1
-    if n == 0:
-        return np.zeros(1, dtype=np.int32)
-    lens = np.diff(rp)
-    # same pattern as the previous row: same length and same columns
-    same = np.zeros(n, dtype=bool)
-    eq_len = lens[1:] == lens[:-1]
-    for i in np.nonzero(eq_len)[0] + 1:
-        same[i] = np.array_equal(ci[rp[i]:rp[i + 1]], ci[rp[i - 1]:rp[i]])
-    natural = [0]
-    size = 1
-    for i in range(1, n):
-        if size < max_block_size and same[i]:
-            size += 1
-        else:
-            natural.append(natural[-1] + size)
-            size = 1
-    natural.append(natural[-1] + size)
-    out = [0]
-    cur = natural[1] - natural[0]
-    for i in range(1, len(natural) - 1):
-        bs = natural[i + 1] - natural[i]
-        if cur + bs <= max_block_size:
-            cur += bs
-        else:
-            out.append(natural[i])
-            cur = bs
-    out.append(natural[-1])
-    return np.array(out, dtype=np.int32)
+    out = np.zeros(n + 1, dtype=np.int32)
+    if len(ci) == 0:
+        ci = np.zeros(1, dtype=np.int32)  # rows without entries: any valid buffer
+    nb = call("b2s_jacobi_find_blocks", n, rp.ctypes.data, ci.ctypes.data,
+              int(max_block_size), out.ctypes.data)
+    return out[:nb + 1].copy()
 
 
 class BlockJacobi:

@@ -238,6 +238,16 @@ int b2s_jacobi_apply_f32(int64_t num_rows, int64_t num_rhs,
  * reference/preconditioner/jacobi_kernels.cpp:310-395) without adaptive
  * precision.  Apply: x = D^-1 b or alpha D^-1 b + beta x (beta == 0 ignores
  * x); replaces jacobi::simple_apply / apply. */
+/* Block pointers for block Jacobi, computed on the host from HOST arrays:
+ * runs of consecutive rows with identical column patterns, cut at
+ * max_block_size rows (natural blocks), then neighbouring natural blocks
+ * merged while the sum stays within max_block_size; jacobi::find_blocks
+ * (reference/preconditioner/jacobi_kernels.cpp:28-98).  block_ptrs_out
+ * holds num_rows + 1 entries; returns the number of blocks, or a negative
+ * B2S_ERR_* code. */
+int64_t b2s_jacobi_find_blocks(int64_t num_rows, const int32_t* row_ptrs,
+                               const int32_t* col_idxs, int max_block_size,
+                               int32_t* block_ptrs_out);
 int b2s_jacobi_block_generate_f64(int64_t num_rows, const int32_t* row_ptrs,
                                   const int32_t* col_idxs, const double* values,
                                   int64_t num_blocks, const int32_t* block_ptrs,
