@@ -9,6 +9,12 @@ measured HBM copy bandwidth.  The matrix and vectors (217 MB) exceed the
 126 MB L2, so no flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                  [--sweep] [--no-solve] [--no-extra] [--mtx] [--profile-tour]
+
+The same line carries the time-to-1e-10 GMRES section (FP64, IR+FP32,
+IR+BF16, CB-GMRES with an FP32 basis) and, unless --no-extra, the CG,
+batched BiCGStab, differentiable-solve and block Jacobi sections.  --mtx
+times the host matrix I/O instead (no GPU).
 
 --impl reference times the CPU restatement of the reference executor's
 SpMV (oracle/, OpenMP over all host cores) on the same workload.  Under
