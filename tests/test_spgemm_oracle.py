@@ -143,3 +143,23 @@ def test_hybrid_strategies_and_round_trip_on_random_rows():
             back = S.hybrid_to_csr(h)
             assert back[0].tolist() == rp.tolist() and back[1].tolist() == ci.tolist()
             assert np.array_equal(back[2], v)
+
+
+@pytest.mark.parametrize("strategy,kw,width,ell_c,ell_v,coo", [
+    # core/test/matrix/hybrid.cpp:170-200 (automatic), :203-211 with
+    # assert_equal_to_original_mtx :62-86 (column_limit 2), :214-244 (imbalance 0.4)
+    ("automatic", {}, 0, [], [], ([0, 0, 0, 1], [0, 1, 2, 1], [1.0, 0.0, 2.0, 5.0])),
+    ("column_limit", {"num_columns": 2}, 2, [0, 1, 1, -1], [1.0, 5.0, 0.0, 0.0],
+     ([0], [2], [2.0])),
+    ("imbalance_limit", {"percent": 0.4}, 1, [0, 1], [1.0, 5.0],
+     ([0, 0], [1, 2], [0.0, 2.0])),
+])
+def test_hybrid_read_known_answers(strategy, kw, width, ell_c, ell_v, coo):
+    # matrix data {(0,0,1), (0,1,0), (0,2,2), (1,1,5)}: the explicit zero is stored
+    rp, ci, v = np.array([0, 3, 4]), np.array([0, 1, 2, 1]), np.array([1.0, 0.0, 2.0, 5.0])
+    w = S.hybrid_width(np.diff(rp), strategy, **kw)
+    h = S.csr_to_hybrid(rp, ci, v, w)
+    assert w == width and h["stride"] == 2
+    assert h["ell_col_idxs"].tolist() == ell_c and h["ell_values"].tolist() == ell_v
+    assert (h["coo_row_idxs"].tolist(), h["coo_col_idxs"].tolist(),
+            h["coo_values"].tolist()) == coo
