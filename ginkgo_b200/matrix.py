@@ -260,3 +260,31 @@ class Sellp(_SparseBase):
              _p(self.col_idxs), _p(self.values), _p(b2), b2.stride(0), _p(x2),
              x2.stride(0), x2.shape[1], _p(alpha), _p(beta), _stream(x2))
         return args[-1]
+
+
+_HYBRID = {"column_limit": 0, "imbalance_limit": 1, "imbalance_bounded_limit": 2,
+           "minimal_storage_limit": 3, "automatic": 4}
+
+
+def hybrid_config(row_nnz, strategy="automatic", num_columns=None, percent=None,
+                  ratio=None, value_bytes=8, index_bytes=4):
+    """(Ell width, Coo entries) of a Hybrid matrix with these row lengths
+    under one of the reference's strategies (matrix::Hybrid::strategy_type,
+    include/ginkgo/core/matrix/hybrid.hpp:103-360): column_limit(num_columns),
+    imbalance_limit(percent=0.8), imbalance_bounded_limit(percent=0.8,
+    ratio=0.0001), minimal_storage_limit(), automatic().  Host set-up in the
+    library (b2s_hybrid_config)."""
+    if strategy not in _HYBRID:
+        raise ValueError(f"unknown Hybrid strategy {strategy!r}")
+    p1 = {"column_limit": num_columns,
+          "imbalance_limit": 0.8 if percent is None else percent,
+          "imbalance_bounded_limit": 0.8 if percent is None else percent}.get(strategy, 0.0)
+    p2 = 0.0001 if ratio is None else ratio
+    if strategy == "column_limit" and num_columns is None:
+        raise ValueError("column_limit needs num_columns")
+    nnz = np.ascontiguousarray(row_nnz, dtype=np.int64)
+    buf = nnz if len(nnz) else np.zeros(1, dtype=np.int64)
+    out = np.zeros(2, dtype=np.int64)
+    call("b2s_hybrid_config", len(nnz), buf.ctypes.data, _HYBRID[strategy], float(p1),
+         float(p2), int(value_bytes), int(index_bytes), out.ctypes.data)
+    return int(out[0]), int(out[1])

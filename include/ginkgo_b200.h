@@ -588,6 +588,29 @@ int b2s_batch_ell_bicgstab_tune_f32(
     void* workspace, int64_t workspace_bytes, int32_t* iterations,
     double* residual_norms, int32_t* tune_table_out, void* stream);
 
+/* ------------------------------------------------------- Hybrid set-up -- */
+/* Ell width and Coo entry count of a Hybrid matrix (Ell + Coo) from its row
+ * lengths, a HOST array, as the strategy classes compute them on the host
+ * (include/ginkgo/core/matrix/hybrid.hpp:103-360, compute_hybrid_config):
+ *   B2S_HYBRID_COLUMN_LIMIT          width = param1 (columns)
+ *   B2S_HYBRID_IMBALANCE_LIMIT       the sorted row length at
+ *                                    floor(rows * param1), param1 clamped to
+ *                                    [0, 1] (the longest for 1)
+ *   B2S_HYBRID_IMBALANCE_BOUNDED     min(imbalance_limit(param1),
+ *                                    floor(rows * param2))
+ *   B2S_HYBRID_MINIMAL_STORAGE       imbalance_limit(index_bytes /
+ *                                    (value_bytes + 2 index_bytes))
+ *   B2S_HYBRID_AUTOMATIC             imbalance_bounded(1/3, 0.001)
+ * config_out: int64[2] = {width, coo entries}. */
+#define B2S_HYBRID_COLUMN_LIMIT 0
+#define B2S_HYBRID_IMBALANCE_LIMIT 1
+#define B2S_HYBRID_IMBALANCE_BOUNDED 2
+#define B2S_HYBRID_MINIMAL_STORAGE 3
+#define B2S_HYBRID_AUTOMATIC 4
+int b2s_hybrid_config(int64_t num_rows, const int64_t* row_nnz, int strategy,
+                      double param1, double param2, int value_bytes,
+                      int index_bytes, int64_t* config_out);
+
 /* ------------------------------------------ MatrixMarket and binary I/O -- */
 /* Host-side matrix data I/O: every pointer here is a HOST pointer and no
  * CUDA call is made.  Matrix data is the reference's matrix_data: a size

@@ -118,3 +118,25 @@ def test_block_detection_matches_the_oracle():
         ci = np.concatenate(rows)
         for mbs in (1, 3, 8, 32):
             assert find_blocks(rp, ci, mbs).tolist() == J.find_blocks(rp, ci, mbs)
+
+
+def test_hybrid_config_matches_the_oracle():
+    from ginkgo_b200.matrix import hybrid_config
+    from oracle import spgemm as S
+    # the reference's own cases (core/test/matrix/hybrid.cpp:170-244)
+    assert hybrid_config([3, 1], "automatic") == (0, 4)
+    assert hybrid_config([3, 2], "column_limit", num_columns=2) == (2, 1)
+    assert hybrid_config([3, 1], "imbalance_limit", percent=0.4) == (1, 2)
+    assert hybrid_config([], "automatic") == (0, 0)
+    rng = np.random.default_rng(2)
+    cases = [("automatic", {}), ("imbalance_limit", {"percent": 0.3}),
+             ("imbalance_limit", {"percent": 1.0}), ("imbalance_limit", {"percent": 1.7}),
+             ("imbalance_bounded_limit", {"percent": 0.9, "ratio": 0.02}),
+             ("minimal_storage_limit", {}), ("column_limit", {"num_columns": 5})]
+    for _ in range(25):
+        lens = rng.integers(0, 40, size=int(rng.integers(1, 3000)))
+        for strat, kw in cases:
+            w = S.hybrid_width(lens, strat, **kw)
+            assert hybrid_config(lens, strat, **kw) == (w, int(np.maximum(lens - w, 0).sum()))
+    with pytest.raises(ValueError):
+        hybrid_config([1, 2], "column_limit")
