@@ -42,17 +42,25 @@ __device__ __forceinline__ void group_sync(int group)
     }
 }
 
-// Sum over the G threads of a group, M values at once; every thread gets
-// the totals.  red: [2][G/32][M] per group, alternating between calls.
+// Sum over the G threads of a group, M <= kMaxSums values at once; every
+// thread gets the totals.  red: [2][G/32][kMaxSums] per group; consecutive
+// calls alternate between the two halves.  The halves have a fixed size
+// whatever M is, so a call never writes entries that the previous call (on
+// the other half) may still be reading: a warp reaches call c + 2's writes
+// only after call c + 1's barrier, which every warp passes after its reads
+// of call c.
+constexpr int kMaxSums = 2;
+
 template <typename T, int G, int M>
 __device__ __forceinline__ void group_sum(T (&v)[M], T* red, int& parity,
                                           int group)
 {
+    static_assert(M <= kMaxSums, "group_sum: too many values");
 #pragma unroll
     for (int m = 0; m < M; ++m) v[m] = warp_sum(v[m]);
     if constexpr (G > 32) {
         constexpr int W = G / 32;
-        T* slot = red + parity * W * M;
+        T* slot = red + parity * W * kMaxSums;
         const int lane = threadIdx.x % 32, wig = (threadIdx.x % G) / 32;
         if (lane == 0) {
 #pragma unroll
@@ -96,10 +104,10 @@ __global__ void __launch_bounds__(kBatchBlock, 1)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int group = threadIdx.x / G;
     const int t = threadIdx.x % G;
-    T* red = reinterpret_cast<T*>(smem_raw) + group * 2 * (G / 32 > 0 ? G / 32 : 1) * 2;
+    T* red = reinterpret_cast<T*>(smem_raw) + group * 2 * (G / 32) * kMaxSums;
     T* vecs;
     if constexpr (SMEM) {
-        vecs = reinterpret_cast<T*>(smem_raw) + GPB * 2 * (G / 32) * 2 +
+        vecs = reinterpret_cast<T*>(smem_raw) + GPB * 2 * (G / 32) * kMaxSums +
                group * 2 * NMAX;
     } else {
         vecs = gscratch + (int64_t(blockIdx.x) * GPB + group) * 2 * NMAX;
@@ -265,7 +273,7 @@ template <typename T, int G, int RPT>
 size_t batch_smem_bytes(bool smem_vecs)
 {
     constexpr int GPB = kBatchBlock / G;
-    size_t bytes = size_t(GPB) * 2 * (G / 32) * 2 * sizeof(T);
+    size_t bytes = size_t(GPB) * 2 * (G / 32) * kMaxSums * sizeof(T);
     if (smem_vecs) bytes += size_t(GPB) * 2 * G * RPT * sizeof(T);
     return bytes;
 }
@@ -296,7 +304,7 @@ int launch_bucket(const BatchConfig& cfg, const BatchArgs& a,
             int per_sm = 0;                                                    \
             B2S_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(        \
                 &per_sm, k, kBatchBlock, sm));                                 \
-            grid = std::max(1, std::min(need, std::max(per_sm, 1) * kNumSMs)); \
+            grid = std::max(1, std::min(need, std::max(per_sm, 1) * num_sms())); \
             k<<<grid, kBatchBlock, sm, st>>>(a, ci, val, b, x, gscratch);      \
         } else {                                                               \
             auto k = batch_bicgstab_kernel<T, GG, RR, false>;                  \
@@ -304,7 +312,7 @@ int launch_bucket(const BatchConfig& cfg, const BatchArgs& a,
             int per_sm = 0;                                                    \
             B2S_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(        \
                 &per_sm, k, kBatchBlock, sm));                                 \
-            grid = std::max(1, std::min(need, std::max(per_sm, 1) * kNumSMs)); \
+            grid = std::max(1, std::min(need, std::max(per_sm, 1) * num_sms())); \
             const int64_t need_scratch = int64_t(grid) * GPB * 2 * GG * RR;    \
             if (need_scratch > gscratch_entries) {                             \
                 grid = int(gscratch_entries / (int64_t(GPB) * 2 * GG * RR));   \

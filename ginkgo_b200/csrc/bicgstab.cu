@@ -398,9 +398,9 @@ int bicgstab_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
     B2S_CUDA_TRY(cudaMemcpyAsync(ctl, &h, sizeof(h), cudaMemcpyHostToDevice, st));
     const int sw = solver_subwarp(max_row_nnz);
     const int grid_spmv = int(std::min<int64_t>(
-        std::max<int64_t>(1, ceildiv(n * sw, kSolverBlock)), kSolverGrid));
+        std::max<int64_t>(1, ceildiv(n * sw, kSolverBlock)), solver_grid()));
     const int grid_vec = int(std::min<int64_t>(
-        std::max<int64_t>(1, ceildiv(n, kSolverBlock)), kSolverGrid));
+        std::max<int64_t>(1, ceildiv(n, kSolverBlock)), solver_grid()));
     const int chunk = int(std::max<int64_t>(2, (check_every + 1) / 2 * 2));
     B2S_DISPATCH_RHS(K, {
         B2S_DISPATCH_SW(sw, {

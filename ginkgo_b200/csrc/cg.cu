@@ -559,9 +559,9 @@ int cg_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
     B2S_CUDA_TRY(cudaMemcpyAsync(ctl, &h, sizeof(h), cudaMemcpyHostToDevice, st));
     const int sw = solver_subwarp(max_row_nnz);
     const int64_t row_blocks = std::max<int64_t>(1, ceildiv(n * sw, kSolverBlock));
-    const int grid_spmv = int(std::min<int64_t>(row_blocks, kSolverGrid));
+    const int grid_spmv = int(std::min<int64_t>(row_blocks, solver_grid()));
     const int grid_vec = int(std::min<int64_t>(
-        std::max<int64_t>(1, ceildiv(n, kSolverBlock)), kSolverGrid));
+        std::max<int64_t>(1, ceildiv(n, kSolverBlock)), solver_grid()));
     const int chunk = int(std::max<int64_t>(2, (check_every + 1) / 2 * 2));
 
     B2S_DISPATCH_RHS(K, {
@@ -604,9 +604,9 @@ int cg_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
                     constexpr int RPW = kWarp / (K / VW);
                     const int gs = int(std::min<int64_t>(
                         std::max<int64_t>(1, ceildiv(n, RPW * (kSolverBlock / kWarp))),
-                        kSolverGrid));
+                        solver_grid()));
                     const int gu = int(std::min<int64_t>(
-                        std::max<int64_t>(1, ceildiv(n * K / VW, kSolverBlock)), kSolverGrid));
+                        std::max<int64_t>(1, ceildiv(n * K / VW, kSolverBlock)), solver_grid()));
                     cg_spmv_lanes_kernel<T, K><<<gs, kSolverBlock, 0, cs>>>(
                         n, rp, ci, v, dinv, r, po, pn, q, ctl, sc, partials);
                     cg_update_lanes_kernel<T, K><<<gu, kSolverBlock, 0, cs>>>(

@@ -11,7 +11,14 @@
 namespace b2s {
 
 constexpr int kWarp = 32;
-constexpr int kNumSMs = 148;  // B200: 2 dies x 74 SMs
+// Upper bound on the SM count for the grid bounds that size partial-sum
+// buffers (B200: 148 SMs on two dies); launches use the device's own count
+// from num_sms(), capped at this bound where a buffer is sized by it.
+constexpr int kMaxSMs = 148;
+
+// Multiprocessors of the current device (cudaDevAttrMultiProcessorCount),
+// looked up once per device; kMaxSMs when the query fails.
+int num_sms();
 
 // Thread-local last-error message, read through b2s_last_error().
 void set_error(const char* fmt, ...);

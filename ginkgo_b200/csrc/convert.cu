@@ -318,7 +318,7 @@ int b2s_csr_max_row_nnz(int64_t num_rows, const int32_t* row_ptrs,
     auto* w = static_cast<unsigned long long*>(workspace);
     B2S_CUDA_TRY(cudaMemsetAsync(w, 0, sizeof(*w), st));
     if (num_rows > 0) {
-        const int64_t grid = std::min<int64_t>(ceildiv(num_rows, kBlock), 4 * kNumSMs);
+        const int64_t grid = std::min<int64_t>(ceildiv(num_rows, kBlock), 4 * num_sms());
         max_row_nnz_kernel<<<grid, kBlock, 0, st>>>(num_rows, row_ptrs, w);
         B2S_LAUNCH_CHECK();
     }
@@ -344,6 +344,9 @@ int b2s_sellp_compute_slice_sets(int64_t num_rows, const int32_t* row_ptrs,
 {
     B2S_CHECK_ARG(num_rows >= 0 && slice_size >= 1 && stride_factor >= 1,
                   "bad Sellp parameters");
+    B2S_CHECK_ARG(slice_sets != nullptr, "null slice_sets");
+    B2S_CHECK_ARG(num_rows == 0 || (row_ptrs != nullptr && slice_lengths != nullptr),
+                  "null row_ptrs or slice_lengths");
     const int64_t need = b2s_sellp_slice_sets_workspace_bytes(num_rows, slice_size);
     if (workspace_bytes < need) {
         set_error("workspace of %lld bytes < %lld", (long long)workspace_bytes,
@@ -430,7 +433,7 @@ int64_t b2s_csr_transpose_workspace_bytes(int64_t num_rows, int64_t num_cols,
         B2S_CUDA_TRY(cudaMemsetAsync(counts, 0, (num_cols + 1) * 4, st));      \
         if (nnz > 0) {                                                         \
             const int64_t grid =                                               \
-                std::min<int64_t>(ceildiv(nnz, kBlock), 16 * kNumSMs);         \
+                std::min<int64_t>(ceildiv(nnz, kBlock), 16 * num_sms());        \
             count_cols_kernel<<<grid, kBlock, 0, st>>>(nnz, col_idxs, counts); \
             B2S_LAUNCH_CHECK();                                                \
         }                                                                      \
@@ -513,6 +516,8 @@ void* g_noalloc_scratch[kNoAllocMaxDevices] = {};
 
 // Device address of the scratch array on the current device, looked up once
 // per device (the name is only a host-side stand-in for the device symbol).
+// The cached address is not refreshed after a device reset; the header says
+// so to callers.
 int noalloc_scratch(void** out)
 {
     int dev = -1;
@@ -549,6 +554,8 @@ extern "C" int b2s_sellp_compute_slice_sets_noalloc(
         return B2S_ERR_INVALID_ARG;
     }
     B2S_CHECK_ARG(slice_sets != nullptr, "null slice_sets");
+    B2S_CHECK_ARG(num_rows == 0 || (row_ptrs != nullptr && slice_lengths != nullptr),
+                  "null row_ptrs or slice_lengths");
     void* scratch = nullptr;
     const int rc = noalloc_scratch(&scratch);
     if (rc != B2S_OK) return rc;

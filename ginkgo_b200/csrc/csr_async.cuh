@@ -49,7 +49,7 @@ int async_resident_blocks(Kern kernel)
     std::lock_guard<std::mutex> lock(m);
     const void* key = reinterpret_cast<const void*>(kernel);
     for (const auto& e : cache) {
-        if (e.first == key) return e.second;
+        if (e.first == key) return e.second * num_sms();
     }
     // four 48 KB blocks per SM leave the rest of the unified L1 (about a
     // fifth) for the x gathers; a larger shared-memory carveout measured
@@ -62,8 +62,8 @@ int async_resident_blocks(Kern kernel)
         (void)cudaGetLastError();
         per_sm = 1;
     }
-    cache.emplace_back(key, per_sm * kNumSMs);
-    return per_sm * kNumSMs;
+    cache.emplace_back(key, per_sm);
+    return per_sm * num_sms();
 }
 
 // One element copy of 4 or 8 bytes (the element's own size and alignment).

@@ -56,7 +56,7 @@ namespace {
 
 constexpr int kMaxKrylov = 32;
 constexpr int kLd = kMaxKrylov + 1;
-constexpr int kDotsMaxGrid = kNumSMs * 4;  // resident at 4 blocks per SM
+constexpr int kDotsMaxGrid = kMaxSMs * 4;  // resident at 4 blocks per SM
 constexpr int kDotsGroup = 32;  // blocks folded by one group's last block
 constexpr int kDotsMaxGroups = (kDotsMaxGrid + kDotsGroup - 1) / kDotsGroup;
 
@@ -763,13 +763,13 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
     constexpr int kEllRows = int(16 / sizeof(TA));
     const int ell_r = ell_rows_per_thread<TA>(ell_w);
     const int grid_ell = int(std::min<int64_t>(
-        std::max<int64_t>(1, ceildiv(ceildiv(n, ell_r), 256)), int64_t(kNumSMs) * 8));
+        std::max<int64_t>(1, ceildiv(ceildiv(n, ell_r), 256)), int64_t(num_sms()) * 8));
 
     const int grid_vec = int(std::min<int64_t>(
-        std::max<int64_t>(1, ceildiv(n, kSolverBlock)), kSolverGrid));
+        std::max<int64_t>(1, ceildiv(n, kSolverBlock)), solver_grid()));
     const int grid_dots = int(std::min<int64_t>(
         std::max<int64_t>(1, ceildiv(ceildiv(n, rows_per_group<TB>()), kSolverBlock)),
-        kDotsMaxGrid));
+        std::min(kDotsMaxGrid, num_sms() * 4)));
     // pipelined SpMV: persistent grid, as many blocks as fit at once
     const int lpr = async_lanes_per_row(max_row_nnz);
     const int64_t async_need = ceildiv(ceildiv(n, kWarp / lpr), kAsyncBlock / kWarp);

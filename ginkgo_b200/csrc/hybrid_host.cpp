@@ -2,6 +2,7 @@
 // lengths by the reference's strategy classes (include/ginkgo/core/matrix/
 // hybrid.hpp:103-360), which run on the host there too.  No CUDA.
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <new>
 #include <vector>
@@ -53,16 +54,29 @@ extern "C" int b2s_hybrid_config(int64_t num_rows, const int64_t* row_nnz, int s
     int64_t width;
     switch (strategy) {
     case B2S_HYBRID_COLUMN_LIMIT:
-        if (!(param1 >= 0)) {
-            b2s::set_error("b2s_hybrid_config: negative column limit");
+        // a column limit is a size_type in the reference: finite, >= 0 and
+        // representable
+        if (!(param1 >= 0 && param1 < 9.2e18)) {
+            b2s::set_error("b2s_hybrid_config: column limit must be finite and >= 0");
             return B2S_ERR_INVALID_ARG;
         }
         width = int64_t(param1);
         break;
     case B2S_HYBRID_IMBALANCE_LIMIT:
+        if (std::isnan(param1)) {
+            b2s::set_error("b2s_hybrid_config: imbalance percent is NaN");
+            return B2S_ERR_INVALID_ARG;
+        }
         width = imbalance_limit(sorted, param1);
         break;
     case B2S_HYBRID_IMBALANCE_BOUNDED:
+        // param2 is the ratio of the Ell width bound to the row count
+        if (std::isnan(param1) || !(param2 >= 0 && std::isfinite(param2)) ||
+            rows * param2 >= 9.2e18) {
+            b2s::set_error("b2s_hybrid_config: imbalance percent must not be NaN "
+                           "and the width ratio must be finite and >= 0");
+            return B2S_ERR_INVALID_ARG;
+        }
         width = std::min(imbalance_limit(sorted, param1), int64_t(rows * param2));
         break;
     case B2S_HYBRID_MINIMAL_STORAGE:

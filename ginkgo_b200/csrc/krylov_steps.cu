@@ -286,10 +286,10 @@ __global__ void residual_norm_k(int64_t k, const T* tau, const T* orig_tau,
 
 inline int grid_for(int64_t work)
 {
-    return int(std::max<int64_t>(1, std::min<int64_t>(ceildiv(work, kB), 16 * kNumSMs)));
+    return int(std::max<int64_t>(1, std::min<int64_t>(ceildiv(work, kB), 16 * num_sms())));
 }
 
-constexpr int kDotBlocks = 4 * kNumSMs;
+constexpr int kDotBlocks = 4 * kMaxSMs;  // grid-stride partials, any SM count
 
 }  // namespace
 }  // namespace b2s

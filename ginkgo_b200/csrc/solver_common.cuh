@@ -15,8 +15,11 @@ namespace b2s {
 
 constexpr int kSolverBlock = 256;
 constexpr int kMaxRhs = 16;
-// Grid of the fused kernels: a few blocks per SM, grid-stride over rows.
-constexpr int kSolverGrid = kNumSMs * 8;
+// Grid bound of the fused kernels (8 blocks per SM, grid-stride over rows);
+// it sizes their partial-sum buffers.  Launches use solver_grid(), the same
+// bound on the device's own SM count.
+constexpr int kSolverGrid = kMaxSMs * 8;
+inline int64_t solver_grid() { return std::min(kSolverGrid, num_sms() * 8); }
 
 // stopping_status bit layout of the reference
 // (include/ginkgo/core/stop/stopping_status.hpp:21-121): bit 7 converged,

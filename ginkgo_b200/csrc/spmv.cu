@@ -671,7 +671,7 @@ int ell_spmv(int64_t n, int64_t num_cols, int64_t width, int64_t stride,
         // (wide FP64 rows stay on the row-per-thread kernel below, which
         // measured faster there)
         const int64_t g = std::min<int64_t>(ceildiv(ceildiv(n, R), kBlock),
-                                            int64_t(kNumSMs) * 16);
+                                            int64_t(num_sms()) * 16);
         ell_rows_kernel_for<T, RV>()<<<g, kBlock, 0, st>>>(
             n, int(width), stride, ci, v, b, ldb, c, ldc, alpha, beta, nullptr);
         B2S_LAUNCH_CHECK();
@@ -738,7 +738,7 @@ int sellp_spmv(int64_t n, int64_t num_cols, int64_t slice_size,
         // measured faster on the 7-point matrix)
         const int64_t groups_blocks = ceildiv(ceildiv(n, R), kBlock);
         if constexpr (sizeof(T) == 8) {
-            const int64_t g = std::min<int64_t>(groups_blocks, int64_t(kNumSMs) * 16);
+            const int64_t g = std::min<int64_t>(groups_blocks, int64_t(num_sms()) * 16);
             if (alpha == nullptr && ldb == 1 && ldc == 1) {
                 sellp_rows_kernel<T, R, true, true><<<g, kBlock, 0, st>>>(
                     int(n), int(slice_size), shift, slice_sets, slice_lengths, ci, v, b, ldb,

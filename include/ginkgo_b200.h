@@ -155,6 +155,9 @@ int b2s_sellp_compute_slice_sets(int64_t num_rows, const int32_t* row_ptrs,
  * most 8,386,560 slices per call and rejects more with B2S_ERR_INVALID_ARG.
  * The first call on a device looks up the array's device address once (with
  * that device current); make that first call before any stream capture.
+ * The address is kept for the life of the process and is not looked up
+ * again after cudaDeviceReset or a reset of the primary context: do not
+ * call this entry point on a device after resetting it.
  * All calls share the array, so calls that overlap on the GPU race.  It
  * allocates nothing.  No counterpart in the reference: Ginkgo always takes
  * its scratch from the executor. */

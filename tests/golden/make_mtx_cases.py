@@ -9,7 +9,7 @@ write cases with their byte images.  Complex-valued cases are skipped (the
 path is real-valued) except where a real read of complex data must fail.
 Each case carries the file:line of its TEST.
 
-Run:  python tests/golden/make_mtx_cases.py [path to the reference tree]
+Run:  python tests/golden/make_mtx_cases.py <path to the reference tree>
 """
 import base64
 import json
@@ -18,7 +18,9 @@ import re
 import struct
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_mtx_cases.py <path to the reference tree>")
+REF = sys.argv[1]
 SRC = os.path.join(REF, "core", "test", "base", "mtx_io.cpp")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "mtx_cases.json")
 

@@ -121,3 +121,51 @@ def test_zero_rhs_and_absolute_tolerance(exe):
     s.apply(b, x)
     assert torch.count_nonzero(s.logger.iterations) == 0
     assert torch.count_nonzero(x) == 0
+
+
+@pytest.mark.parametrize("G,smem", [(64, 1), (128, 1), (256, 1), (256, 0)])
+def test_large_groups_with_half_step_exits(exe, G, smem):
+    """Groups of 64+ threads reduce through shared memory in two alternating
+    halves.  Systems that stop at the half step (||s|| small) leave the
+    alternation shifted for the group's next system, and with more systems
+    than resident groups every group solves several in a row: diagonal
+    systems (solved exactly by the first half step under scalar Jacobi) are
+    interleaved with convection-diffusion systems of the same size bucket,
+    and every system is checked against the oracle."""
+    A0, cd = convection_diffusion_batch(exe, 2400, lo=513, hi=1024, seed=11)
+    rng = np.random.default_rng(12)
+    systems = []
+    for i, s in enumerate(cd):
+        if i % 3 == 1:
+            n = len(s[0]) - 1
+            systems.append((np.arange(n + 1), np.arange(n),
+                            rng.uniform(0.5, 4.0, size=n)))
+        else:
+            systems.append(s)
+    A = BatchEll.from_csr(exe, systems, width=5)
+    b = rng.standard_normal(A.total_rows)
+    bd = torch.from_numpy(b).cuda()
+    x = torch.zeros_like(bd)
+    s = solver(exe, A, 500, 1e-8)
+    table = np.zeros(24, dtype=np.int32)
+    table[2 * 10], table[2 * 10 + 1] = G, smem  # the bucket of 513..1024 rows
+    s.tune_table = table
+    s.apply(bd, x)
+    it = s.logger.iterations.cpu().numpy()
+    xg = x.cpu().numpy()
+    offs = A.host_row_offsets
+    for i in range(A.num_systems):
+        o, e = offs[i], offs[i + 1]
+        rp, ci, v = systems[i]
+        bi = b[o:e]
+        if i % 3 == 1:
+            assert it[i] == 0, (i, it[i])
+            np.testing.assert_allclose(xg[o:e], bi / v, rtol=1e-14)
+            continue
+        w, st, eci, ev = orc.csr_to_ell(rp, ci, v)
+        _, it_o, _, conv_o = orc.batch_bicgstab_ell(e - o, w, st, eci, ev, bi,
+                                                    max_iters=500, tol=1e-8)
+        assert conv_o
+        assert abs(int(it[i]) - it_o) <= max(3, 0.3 * it_o), (i, it[i], it_o)
+        rel = np.linalg.norm(bi - orc.csr_spmv(rp, ci, v, xg[o:e])) / np.linalg.norm(bi)
+        assert rel <= 1.5e-8, (i, rel)

@@ -140,3 +140,39 @@ def test_hybrid_config_matches_the_oracle():
             assert hybrid_config(lens, strat, **kw) == (w, int(np.maximum(lens - w, 0).sum()))
     with pytest.raises(ValueError):
         hybrid_config([1, 2], "column_limit")
+
+
+def test_hybrid_config_rejects_bad_parameters():
+    from ginkgo_b200.matrix import hybrid_config
+    nan, inf = float("nan"), float("inf")
+    bad = [("imbalance_bounded_limit", {"percent": 0.8, "ratio": -0.5}),
+           ("imbalance_bounded_limit", {"percent": 0.8, "ratio": nan}),
+           ("imbalance_bounded_limit", {"percent": 0.8, "ratio": inf}),
+           ("imbalance_bounded_limit", {"percent": nan, "ratio": 0.1}),
+           ("imbalance_limit", {"percent": nan}),
+           ("column_limit", {"num_columns": nan}),
+           ("column_limit", {"num_columns": inf}),
+           ("column_limit", {"num_columns": -1}),
+           ("column_limit", {"num_columns": 1e30})]
+    for strat, kw in bad:
+        with pytest.raises(RuntimeError):
+            hybrid_config([3, 1, 4], strat, **kw)
+
+
+def test_slice_sets_reject_null_pointers_before_device_work():
+    import ctypes as C
+    from ginkgo_b200 import _lib
+    lib = _lib.lib()
+    fake = C.c_void_p(256)  # never dereferenced: validation fails first
+    # workspace form: null row_ptrs, then null slice_lengths
+    assert lib.b2s_sellp_compute_slice_sets(64, None, 32, 1, fake, fake, fake,
+                                            1 << 20, None) == -1
+    assert lib.b2s_sellp_compute_slice_sets(64, fake, 32, 1, fake, None, fake,
+                                            1 << 20, None) == -1
+    assert b"null" in lib.b2s_last_error()
+    # allocation-free form
+    assert lib.b2s_sellp_compute_slice_sets_noalloc(64, None, 32, 1, fake, fake,
+                                                    None) == -1
+    assert lib.b2s_sellp_compute_slice_sets_noalloc(64, fake, 32, 1, fake, None,
+                                                    None) == -1
+    assert b"null" in lib.b2s_last_error()
