@@ -79,14 +79,14 @@ __global__ void __launch_bounds__(kSolverBlock)
             for (int j = 0; j < K; ++j) {
                 uint8_t s = 0;
                 if (j >= k) stop_status(s, kIterationId, true);
-                sc->start[j] = sqrt(tot[j]);
+                sc->start[j] = start_norm(ctl, T(sqrt(tot[j])), T(sqrt(tot[2 * K + j])));
                 sc->rho[j] = tot[K + j];
                 sc->prev_rho[j] = T(1);
                 sc->alpha[j] = T(1);
                 sc->omega[j] = T(1);
                 sc->tau[j] = sqrt(tot[2 * K + j]);
                 if (ctl->max_iters <= 0) stop_status(s, kIterationId, true);
-                if (double(sc->tau[j]) <= ctl->reduction * double(sc->start[j])) {
+                if (residual_met(ctl, sc->tau[j], sc->rho[j], sc->start[j])) {
                     converge_status(s, kResidualId, true);
                 }
                 ctl->status[j] = s;
@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(kSolverBlock)
                 const T tau_s = sqrt(tot[2 * K + j]);
                 // check on s without finalising (core/solver/bicgstab.cpp
                 // second check): the update pass adds alpha y and finalises
-                if (double(tau_s) <= ctl->reduction * double(sc->start[j])) {
+                if (residual_met(ctl, tau_s, sc->rho[j], sc->start[j])) {
                     converge_status(st, kResidualId, false);
                     sc->tau[j] = tau_s;
                 }
@@ -322,7 +322,7 @@ __global__ void __launch_bounds__(kSolverBlock)
                     sc->prev_rho[j] = sc->rho[j];
                     sc->rho[j] = tot[j];
                     sc->tau[j] = sqrt(tot[K + j]);
-                    if (double(sc->tau[j]) <= ctl->reduction * double(sc->start[j])) {
+                    if (residual_met(ctl, sc->tau[j], sc->rho[j], sc->start[j])) {
                         converge_status(st, kResidualId, true);
                     }
                     if (iter >= ctl->max_iters) stop_status(st, kIterationId, true);
@@ -364,7 +364,8 @@ template <typename T>
 int bicgstab_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
                    int64_t max_row_nnz, const T* dinv, const T* b, int64_t ldb,
                    T* x, int64_t ldx, int64_t k, int64_t max_iters,
-                   double reduction, int64_t check_every, void* workspace,
+                   double reduction, int residual_mode, int64_t check_every,
+                   void* workspace,
                    int64_t workspace_bytes, int64_t* iterations,
                    double* residual_norms, uint8_t* status, void* stream)
 {
@@ -372,6 +373,8 @@ int bicgstab_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
     B2S_CHECK_ARG(ldb >= k && ldx >= k, "leading dimension < num_rhs");
     B2S_CHECK_ARG(max_iters >= 0 && max_iters < (int64_t(1) << 30),
                   "max_iters out of range");
+    B2S_CHECK_ARG(valid_residual_mode(residual_mode), "unknown residual mode %d",
+                  residual_mode);
     const int K = rhs_bucket(k);
     const BicgLayout lay = bicg_layout<T>(n, K);
     if (workspace_bytes < lay.bytes) {
@@ -395,6 +398,8 @@ int bicgstab_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
     SolveCtl h{};
     h.max_iters = int(max_iters);
     h.reduction = reduction;
+    h.baseline = residual_mode & ~B2S_STOP_IMPLICIT;
+    h.implicit = (residual_mode & B2S_STOP_IMPLICIT) != 0;
     B2S_CUDA_TRY(cudaMemcpyAsync(ctl, &h, sizeof(h), cudaMemcpyHostToDevice, st));
     const int sw = solver_subwarp(max_row_nnz);
     const int grid_spmv = int(std::min<int64_t>(
@@ -465,14 +470,16 @@ int64_t b2s_bicgstab_workspace_bytes(int64_t num_rows, int64_t num_rhs,
         int64_t num_rows, const int32_t* row_ptrs, const int32_t* col_idxs,   \
         const T* values, int64_t max_row_nnz, const T* inv_diag, const T* b,  \
         int64_t ldb, T* x, int64_t ldx, int64_t num_rhs, int64_t max_iters,   \
-        double reduction_factor, int64_t check_every, void* workspace,        \
+        double reduction_factor, int residual_mode, int64_t check_every,     \
+        void* workspace,                                                      \
         int64_t workspace_bytes, int64_t* iterations, double* residual_norms, \
         uint8_t* status, void* stream)                                        \
     {                                                                         \
         return bicgstab_solve<T>(num_rows, row_ptrs, col_idxs, values,        \
                                  max_row_nnz, inv_diag, b, ldb, x, ldx,       \
                                  num_rhs, max_iters, reduction_factor,        \
-                                 check_every, workspace, workspace_bytes,     \
+                                 residual_mode, check_every, workspace,       \
+                                 workspace_bytes,                             \
                                  iterations, residual_norms, status, stream); \
     }
 

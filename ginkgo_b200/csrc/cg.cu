@@ -82,13 +82,13 @@ __global__ void __launch_bounds__(kSolverBlock)
                 if (j >= k) {
                     stop_status(s, kIterationId, true);  // padding column
                 }
-                sc->start[j] = sqrt(tot[j]);
+                sc->start[j] = start_norm(ctl, T(sqrt(tot[j])), T(sqrt(tot[2 * K + j])));
                 sc->rho[j] = tot[K + j];
                 sc->prev_rho[j] = T(1);
                 sc->alpha[j] = T(0);
                 sc->tau[j] = sqrt(tot[2 * K + j]);
                 if (ctl->max_iters <= 0) stop_status(s, kIterationId, true);
-                if (double(sc->tau[j]) <= ctl->reduction * double(sc->start[j])) {
+                if (residual_met(ctl, sc->tau[j], sc->rho[j], sc->start[j])) {
                     converge_status(s, kResidualId, true);
                 }
                 ctl->status[j] = s;
@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(kSolverBlock)
                     sc->prev_rho[j] = sc->rho[j];
                     sc->rho[j] = tot[j];
                     sc->tau[j] = sqrt(tot[K + j]);
-                    if (double(sc->tau[j]) <= ctl->reduction * double(sc->start[j])) {
+                    if (residual_met(ctl, sc->tau[j], sc->rho[j], sc->start[j])) {
                         converge_status(s, kResidualId, true);
                     }
                     if (iter >= ctl->max_iters) stop_status(s, kIterationId, true);
@@ -435,7 +435,7 @@ __global__ void __launch_bounds__(kSolverBlock)
                     sc->prev_rho[j] = sc->rho[j];
                     sc->rho[j] = tot[j];
                     sc->tau[j] = sqrt(tot[K + j]);
-                    if (double(sc->tau[j]) <= ctl->reduction * double(sc->start[j])) {
+                    if (residual_met(ctl, sc->tau[j], sc->rho[j], sc->start[j])) {
                         converge_status(s, kResidualId, true);
                     }
                     if (iter >= ctl->max_iters) stop_status(s, kIterationId, true);
@@ -527,7 +527,8 @@ template <typename T>
 int cg_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
              int64_t max_row_nnz, const T* dinv, const T* b, int64_t ldb, T* x,
              int64_t ldx, int64_t k, int64_t max_iters, double reduction,
-             int64_t check_every, void* workspace, int64_t workspace_bytes,
+             int residual_mode, int64_t check_every, void* workspace,
+             int64_t workspace_bytes,
              int64_t* iterations, double* residual_norms, uint8_t* status,
              void* stream)
 {
@@ -535,6 +536,8 @@ int cg_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
     B2S_CHECK_ARG(ldb >= k && ldx >= k, "leading dimension < num_rhs");
     B2S_CHECK_ARG(max_iters >= 0 && max_iters < (int64_t(1) << 30),
                   "max_iters out of range");
+    B2S_CHECK_ARG(valid_residual_mode(residual_mode), "unknown residual mode %d",
+                  residual_mode);
     const int K = rhs_bucket(k);
     const CgLayout lay = cg_layout<T>(n, K);
     if (workspace_bytes < lay.bytes) {
@@ -556,6 +559,8 @@ int cg_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
     SolveCtl h{};
     h.max_iters = int(max_iters);
     h.reduction = reduction;
+    h.baseline = residual_mode & ~B2S_STOP_IMPLICIT;
+    h.implicit = (residual_mode & B2S_STOP_IMPLICIT) != 0;
     B2S_CUDA_TRY(cudaMemcpyAsync(ctl, &h, sizeof(h), cudaMemcpyHostToDevice, st));
     const int sw = solver_subwarp(max_row_nnz);
     const int64_t row_blocks = std::max<int64_t>(1, ceildiv(n * sw, kSolverBlock));
@@ -662,14 +667,16 @@ int64_t b2s_cg_workspace_bytes(int64_t num_rows, int64_t num_rhs,
                          int64_t max_row_nnz, const T* inv_diag, const T* b,  \
                          int64_t ldb, T* x, int64_t ldx, int64_t num_rhs,     \
                          int64_t max_iters, double reduction_factor,          \
-                         int64_t check_every, void* workspace,                \
+                         int residual_mode, int64_t check_every,              \
+                         void* workspace,                                     \
                          int64_t workspace_bytes, int64_t* iterations,        \
                          double* residual_norms, uint8_t* status,             \
                          void* stream)                                        \
     {                                                                         \
         return cg_solve<T>(num_rows, row_ptrs, col_idxs, values, max_row_nnz, \
                            inv_diag, b, ldb, x, ldx, num_rhs, max_iters,      \
-                           reduction_factor, check_every, workspace,          \
+                           reduction_factor, residual_mode, check_every,      \
+                           workspace,                                         \
                            workspace_bytes, iterations, residual_norms,       \
                            status, stream);                                   \
     }

@@ -54,27 +54,31 @@
 namespace b2s {
 namespace {
 
-constexpr int kMaxKrylov = 32;
+constexpr int kMaxKrylov = 128;
 constexpr int kLd = kMaxKrylov + 1;
 constexpr int kDotsMaxGrid = kMaxSMs * 4;  // resident at 4 blocks per SM
 constexpr int kDotsGroup = 32;  // blocks folded by one group's last block
 constexpr int kDotsMaxGroups = (kDotsMaxGrid + kDotsGroup - 1) / kDotsGroup;
 
+// The Hessenberg matrix (column j at H[j * ld], ld = krylov_dim + 1) and
+// the Gram matrix G of the stored basis (G(i, k) at G[i * ld + k]) live in
+// the workspace beside this state.
 struct GmresState {
     int done, cycle_done, j, final_iter;
     int total_iter, max_iters, outer_iter, converged;
-    int krylov_dim;
+    int krylov_dim, ld;
+    int ortho;     // B2S_ORTHO_*: CGS (h = h1) or CGS2 (h = (2I - G) h1)
+    int baseline;  // B2S_BASELINE_* of the residual goal
     int idle;  // done || cycle_done: the Arnoldi kernels have nothing to do
     unsigned ticket;
     int too_long;  // a row is longer than the Ell copy's width
     int too_far;   // a column offset does not fit 16 bits
     unsigned gticket[kDotsMaxGroups + 1];  // dots: per group of 32 blocks
     double bnorm, rnorm, reduction, inner_reduction, inner_thresh;
+    double base;  // ||b||, ||r_0|| or 1, by the baseline, set at the first restart
     double sigma[kLd];  // stored basis vector i is v_i / sigma[i] (unnormalised)
     double minus_one, one;       // alpha, beta of r = b - A x
     double h[kLd];               // combined projection coefficients of step j
-    double H[kMaxKrylov * kLd];  // column j at H[j * kLd]
-    double G[kLd * kLd];         // Gram matrix of the stored basis
     double g[kLd], cs[kMaxKrylov], sn[kMaxKrylov], y[kMaxKrylov];
 };
 
@@ -258,19 +262,22 @@ __device__ __forceinline__ void fold32(const double* src, int64_t ld, int base, 
                                        int nvec, double* dst, int64_t dst_ld, int dst_col)
 {
     const int lane = threadIdx.x % kWarp, wid = threadIdx.x / kWarp;
-    constexpr int K = (2 * kLd + 7) / 8;
-    double v[K];
+    constexpr int K = 4;  // values per warp and round: their loads in flight together
+    for (int c0 = 0; c0 < 2 * nvec; c0 += 8 * K) {
+        double v[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-        const int c = wid + 8 * k;
-        v[k] = c < 2 * nvec && lane < L ? __ldcg(src + dots_row(c, nvec) * ld + base + lane)
-                                        : 0.0;
-    }
+        for (int k = 0; k < K; ++k) {
+            const int c = c0 + wid + 8 * k;
+            v[k] = c < 2 * nvec && lane < L
+                       ? __ldcg(src + dots_row(c, nvec) * ld + base + lane)
+                       : 0.0;
+        }
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-        const int c = wid + 8 * k;
-        const double s = warp_sum(v[k]);
-        if (lane == 0 && c < 2 * nvec) dst[dots_row(c, nvec) * dst_ld + dst_col] = s;
+        for (int k = 0; k < K; ++k) {
+            const int c = c0 + wid + 8 * k;
+            const double s = warp_sum(v[k]);
+            if (lane == 0 && c < 2 * nvec) dst[dots_row(c, nvec) * dst_ld + dst_col] = s;
+        }
     }
 }
 
@@ -280,19 +287,20 @@ __device__ __forceinline__ void fold32(const double* src, int64_t ld, int base, 
 // one multi-value warp reduction and one block reduction into value-major
 // partials (partials[e * gridDim.x + block]).  The last block of every 32
 // blocks folds its group's partials; the last group to finish folds the
-// groups, completes G's row and column j and forms h = (2I - G) h1.  The
-// summation order is fixed: the result does not depend on scheduling.
+// groups, completes G's row and column j and forms h = (2I - G) h1 (CGS2),
+// or h = h1 (CGS).  The summation order is fixed: the result does not
+// depend on scheduling.
 template <typename TA, typename TB>
 __global__ void __launch_bounds__(kSolverBlock, 4)
     gmres_dots_kernel(int64_t n, int64_t ldv, const TB* __restrict__ V,
                       const TA* __restrict__ w, GmresState* st,
-                      double* __restrict__ partials, double* __restrict__ gpart)
+                      double* __restrict__ partials, double* __restrict__ gpart,
+                      double* __restrict__ Gm)
 {
     constexpr int CMAX = 4;
     constexpr int W = kSolverBlock / kWarp;
     __shared__ double redv[W][8];
     __shared__ double tot[2 * kLd];
-    __shared__ double Gs[kLd * kLd];
     __shared__ int last;
     if (st->idle) return;
     const int j = st->j;
@@ -343,24 +351,28 @@ __global__ void __launch_bounds__(kSolverBlock, 4)
         tot[kLd + threadIdx.x] *= sc;
     }
     __syncthreads();
-    // G(0..j-1, 0..j-1) from the earlier steps of this cycle
-    for (int e = threadIdx.x; e < j * kLd; e += kSolverBlock) Gs[e] = st->G[e];
-    __syncthreads();
+    if (st->ortho == B2S_ORTHO_CGS) {
+        // one projection: h = h1
+        if (threadIdx.x <= j) st->h[threadIdx.x] = tot[threadIdx.x];
+        return;
+    }
+    // row and column j of G; rows 0..j-1 hold the earlier steps of this
+    // cycle (G is symmetric, so row i of G(0..j, 0..j) is complete)
+    const int ld = st->ld;
     if (threadIdx.x <= j) {
         const int i = threadIdx.x;
         const double gij = tot[kLd + i];
-        Gs[i * kLd + j] = gij;
-        Gs[j * kLd + i] = gij;
-        st->G[i * kLd + j] = gij;
-        st->G[j * kLd + i] = gij;
+        Gm[int64_t(i) * ld + j] = gij;
+        Gm[int64_t(j) * ld + i] = gij;
     }
-    __syncthreads();
-    // h = (2I - G) h1: CGS2's second projection from G
-    if (threadIdx.x <= j) {
-        const int i = threadIdx.x;
+    __syncthreads();  // the block's own writes of G are visible to it
+    // h = (2I - G) h1: CGS2's second projection from G, one warp per row i
+    // (row i of G is contiguous, so the lanes' loads coalesce)
+    for (int i = wid; i <= j; i += W) {
         double gh = 0.0;
-        for (int k = 0; k <= j; ++k) gh += Gs[i * kLd + k] * tot[k];
-        st->h[i] = 2.0 * tot[i] - gh;
+        for (int k = lane; k <= j; k += kWarp) gh += __ldcg(Gm + int64_t(i) * ld + k) * tot[k];
+        gh = warp_sum(gh);
+        if (lane == 0) st->h[i] = 2.0 * tot[i] - gh;
     }
 }
 
@@ -369,12 +381,13 @@ __global__ void __launch_bounds__(kSolverBlock, 4)
 // and, when the cycle ends, the back substitution y = H \ g.  The small
 // arrays are staged in shared memory, so the serial chain runs at
 // shared-memory latency.
-__device__ void close_step(GmresState* st, double hnorm)
+__device__ void close_step(GmresState* st, double hnorm, double* __restrict__ Hm)
 {
     __shared__ double hc[kLd], gS[kLd], csS[kMaxKrylov], snS[kMaxKrylov];
-    __shared__ double Hs[kMaxKrylov * kLd], ts[kMaxKrylov];
+    __shared__ double ts[kMaxKrylov];
     __shared__ int fin;
     const int j = st->j;
+    const int ld = st->ld;
     for (int i = threadIdx.x; i <= j; i += kSolverBlock) {
         hc[i] = st->h[i];
         gS[i] = st->g[i];
@@ -426,23 +439,33 @@ __device__ void close_step(GmresState* st, double hnorm)
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i <= j + 1; i += kSolverBlock) st->H[j * kLd + i] = hc[i];
+    for (int i = threadIdx.x; i <= j + 1; i += kSolverBlock) Hm[int64_t(j) * ld + i] = hc[i];
     if (!fin) return;
     // y = H \ g over the m = j + 1 finished columns: one warp, column by
-    // column from the last (t -= H(:, k) y_k after each y_k)
+    // column from the last (t -= H(:, k) y_k after each y_k).  Column k is
+    // read from the workspace (this block wrote column j above); its loads
+    // do not depend on y_k, so they are issued before the division.
     const int m = j + 1;
-    for (int e = threadIdx.x; e < j * kLd; e += kSolverBlock) Hs[e] = st->H[e];
-    for (int i = threadIdx.x; i <= j; i += kSolverBlock) {
-        Hs[j * kLd + i] = hc[i];
-        ts[i] = gS[i];
-    }
+    for (int i = threadIdx.x; i <= j; i += kSolverBlock) ts[i] = gS[i];
     __syncthreads();
     if (threadIdx.x < kWarp) {
         const int lane = threadIdx.x;
+        constexpr int KC = (kMaxKrylov + kWarp - 1) / kWarp;
         for (int k = m - 1; k >= 0; --k) {
-            const double yk = ts[k] / Hs[k * kLd + k];
+            const double* col = Hm + int64_t(k) * ld;
+            double hcol[KC];
+#pragma unroll
+            for (int q = 0; q < KC; ++q) {
+                const int i = lane + q * kWarp;
+                hcol[q] = i < k ? __ldcg(col + i) : 0.0;
+            }
+            const double yk = ts[k] / __ldcg(col + k);
             if (lane == 0) st->y[k] = yk;
-            for (int i = lane; i < k; i += kWarp) ts[i] -= Hs[k * kLd + i] * yk;
+#pragma unroll
+            for (int q = 0; q < KC; ++q) {
+                const int i = lane + q * kWarp;
+                if (i < k) ts[i] -= hcol[q] * yk;
+            }
             __syncwarp();
         }
     }
@@ -459,7 +482,7 @@ __global__ void __launch_bounds__(kSolverBlock)
     gmres_update_kernel(int64_t n, int64_t ldv, TB* __restrict__ V,
                         const TA* __restrict__ w, const TA* __restrict__ dinv,
                         TA* __restrict__ y, GmresState* st,
-                        double* __restrict__ partials)
+                        double* __restrict__ partials, double* __restrict__ Hm)
 {
     constexpr int R = rows_per_group<TB>();
     __shared__ double red[kSolverBlock / kWarp];
@@ -510,7 +533,7 @@ __global__ void __launch_bounds__(kSolverBlock)
     block_partials<double, 1>(a, partials, red);
     if (last_block_done(&st->ticket, &last)) {
         sum_partials<double, 1>(partials, gridDim.x, tot, red);
-        close_step(st, sqrt(tot[0]));
+        close_step(st, sqrt(tot[0]), Hm);
     }
 }
 
@@ -597,7 +620,14 @@ __global__ void __launch_bounds__(kSolverBlock)
             st->rnorm = rn;
             st->bnorm = sqrt(tot[1]);
             st->final_iter = 0;
-            if (rn <= st->reduction * st->bnorm) {
+            if (st->outer_iter == 0) {
+                // the residual goal's baseline, fixed by the first residual
+                // (stop::ResidualNorm, core/stop/residual_norm.cpp:95-150)
+                st->base = st->baseline == B2S_BASELINE_INITIAL_RESNORM ? rn
+                           : st->baseline == B2S_BASELINE_ABSOLUTE      ? 1.0
+                                                                        : st->bnorm;
+            }
+            if (rn <= st->reduction * st->base) {
                 st->converged = 1;
                 st->done = 1;
                 st->idle = 1;
@@ -613,7 +643,7 @@ __global__ void __launch_bounds__(kSolverBlock)
                 for (int i = 1; i <= kMaxKrylov; ++i) st->g[i] = 0.0;
                 st->sigma[0] = 1.0 / rn;
                 st->inner_thresh = fmax(st->inner_reduction * rn,
-                                        st->reduction * st->bnorm);
+                                        st->reduction * st->base);
             }
         }
     }
@@ -641,16 +671,24 @@ inline int gmres_ell_width(int64_t n, int64_t nnz, int64_t max_row_nnz)
 
 struct GmresLayout {
     int64_t bytes, off_st, off_r, off_w, off_y, off_v, off_partials,
-        off_a32, off_d32, off_ell_c, off_ell_v, off_gpart;
+        off_a32, off_d32, off_ell_c, off_ell_v, off_gpart, off_H, off_G,
+        off_bcol, off_xcol;
     int ell_width;
 };
 
+// cols: contiguous FP64 copies of one column of b and x, for strided or
+// several right-hand sides (solved one column at a time)
 template <typename TA, typename TB>
-GmresLayout gmres_layout(int64_t n, int64_t nnz, int64_t max_row_nnz, int d, bool mixed)
+GmresLayout gmres_layout(int64_t n, int64_t nnz, int64_t max_row_nnz, int d, bool mixed,
+                         bool cols)
 {
     Carver c{nullptr};
     GmresLayout l;
     l.off_st = c.take<GmresState>(1);
+    l.off_H = c.take<double>(int64_t(d) * (d + 1));
+    l.off_G = c.take<double>(int64_t(d + 1) * (d + 1));
+    l.off_bcol = cols ? c.take<double>(n) : 0;
+    l.off_xcol = cols ? c.take<double>(n) : 0;
     l.off_r = c.take<double>(n);
     const int64_t ldv = gmres_ld(n);
     l.off_w = c.take<TA>(ldv);
@@ -667,41 +705,22 @@ GmresLayout gmres_layout(int64_t n, int64_t nnz, int64_t max_row_nnz, int d, boo
     return l;
 }
 
+// One right-hand side (b, x contiguous FP64 vectors); the layout was
+// checked against the workspace by the caller.
 template <typename TA, typename TB>
-int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
-                 const double* v64, int64_t max_row_nnz, const double* dinv64,
-                 const double* b, double* x, int krylov_dim,
-                 int64_t max_iters, double reduction, double inner_reduction,
-                 void* workspace, int64_t workspace_bytes,
-                 int64_t* iterations, int64_t* restarts, double* res_norm,
-                 int* converged, void* stream)
+int gmres_engine(const GmresLayout& lay, int64_t n, int64_t nnz, const int32_t* rp,
+                 const int32_t* ci, const double* v64, int64_t max_row_nnz,
+                 const double* dinv64, const double* b, double* x, int krylov_dim,
+                 int ortho, int64_t max_iters, double reduction, int baseline,
+                 double inner_reduction, void* workspace, int64_t* iterations,
+                 int64_t* restarts, double* res_norm, uint8_t* status, cudaStream_t st)
 {
     constexpr bool kMixed = !std::is_same<TA, double>::value;
-    B2S_CHECK_ARG(n >= 1, "GMRES needs at least one row");
-    B2S_CHECK_ARG(krylov_dim >= 1 && krylov_dim <= kMaxKrylov,
-                  "krylov_dim must be 1..%d", kMaxKrylov);
-    B2S_CHECK_ARG(max_iters >= 0 && max_iters < (int64_t(1) << 30),
-                  "max_iters out of range");
-    int64_t nnz = 0;
-    cudaStream_t st = as_stream(stream);
-    {
-        int32_t h_nnz = 0;
-        B2S_CUDA_TRY(cudaMemcpyAsync(&h_nnz, rp + n, sizeof(int32_t),
-                                     cudaMemcpyDeviceToHost, st));
-        B2S_CUDA_TRY(cudaStreamSynchronize(st));
-        nnz = h_nnz;
-    }
-    const GmresLayout lay = gmres_layout<TA, TB>(n, nnz, max_row_nnz, krylov_dim, kMixed);
-    if (workspace_bytes < lay.bytes) {
-        set_error("workspace of %lld bytes < %lld", (long long)workspace_bytes,
-                  (long long)lay.bytes);
-        return B2S_ERR_WORKSPACE;
-    }
-    B2S_CHECK_ARG(reinterpret_cast<uintptr_t>(workspace) % 256 == 0,
-                  "GMRES workspace must be 256-byte aligned");
     const int64_t ldv = gmres_ld(n);
     char* w = static_cast<char*>(workspace);
     auto* gs = reinterpret_cast<GmresState*>(w + lay.off_st);
+    double* Hm = reinterpret_cast<double*>(w + lay.off_H);
+    double* Gm = reinterpret_cast<double*>(w + lay.off_G);
     double* r = reinterpret_cast<double*>(w + lay.off_r);
     TA* wbuf = reinterpret_cast<TA*>(w + lay.off_w);
     TA* y = reinterpret_cast<TA*>(w + lay.off_y);
@@ -730,6 +749,11 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
     GmresState h{};
     h.max_iters = int(max_iters);
     h.krylov_dim = krylov_dim;
+    h.ld = krylov_dim + 1;
+    // modified Gram-Schmidt runs as CGS2: one pass over the basis per step
+    // instead of j + 1, with orthogonality at least as good
+    h.ortho = ortho == B2S_ORTHO_CGS ? B2S_ORTHO_CGS : B2S_ORTHO_CGS2;
+    h.baseline = baseline;
     h.reduction = reduction;
     h.inner_reduction = inner_reduction;
     h.cycle_done = 1;
@@ -819,9 +843,9 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
                 });
             }
             gmres_dots_kernel<TA, TB><<<grid_dots, kSolverBlock, 0, cs>>>(
-                n, ldv, V, dst, gs, partials, gpart);
+                n, ldv, V, dst, gs, partials, gpart, Gm);
             gmres_update_kernel<TA, TB><<<grid_vec, kSolverBlock, 0, cs>>>(
-                n, ldv, V, dst, da, y, gs, partials);
+                n, ldv, V, dst, da, y, gs, partials, Hm);
             B2S_LAUNCH_CHECK();
         }
         restart(cs);
@@ -866,7 +890,93 @@ int gmres_engine(int64_t n, const int32_t* rp, const int32_t* ci,
     if (iterations) *iterations = hs.total_iter;
     if (restarts) *restarts = hs.outer_iter;
     if (res_norm) *res_norm = hs.rnorm;
-    if (converged) *converged = hs.converged;
+    if (status) {
+        uint8_t s = 0;
+        if (hs.converged) {
+            converge_status(s, kResidualId, true);
+        } else {
+            stop_status(s, kIterationId, true);
+        }
+        *status = s;
+    }
+    return B2S_OK;
+}
+
+// Validates the arguments, then solves the right-hand sides one column at a
+// time (GMRES treats the columns independently: each has its own Krylov
+// basis, Hessenberg matrix and stop status).  A column that is not a
+// contiguous vector goes through FP64 copies in the workspace.
+template <typename TA, typename TB>
+int gmres_solve_columns(int64_t n, const int32_t* rp, const int32_t* ci,
+                        const double* v64, int64_t max_row_nnz, const double* dinv64,
+                        const double* b, int64_t ldb, double* x, int64_t ldx,
+                        int64_t k, int64_t krylov_dim, int ortho, int64_t max_iters,
+                        double reduction, int baseline, double inner_reduction,
+                        void* workspace, int64_t workspace_bytes, int64_t* iterations,
+                        int64_t* restarts, double* res_norms, uint8_t* status,
+                        void* stream)
+{
+    constexpr bool kMixed = !std::is_same<TA, double>::value;
+    B2S_CHECK_ARG(n >= 1, "GMRES needs at least one row");
+    B2S_CHECK_ARG(k >= 0, "negative number of right-hand sides");
+    B2S_CHECK_ARG(krylov_dim >= 1 && krylov_dim <= kMaxKrylov,
+                  "krylov_dim %lld is not supported: 1..%d", (long long)krylov_dim,
+                  kMaxKrylov);
+    B2S_CHECK_ARG(ortho == B2S_ORTHO_MGS || ortho == B2S_ORTHO_CGS || ortho == B2S_ORTHO_CGS2,
+                  "unknown orthogonalisation method %d", ortho);
+    B2S_CHECK_ARG(baseline == B2S_BASELINE_RHS_NORM ||
+                      baseline == B2S_BASELINE_INITIAL_RESNORM ||
+                      baseline == B2S_BASELINE_ABSOLUTE,
+                  "unknown residual baseline %d", baseline);
+    B2S_CHECK_ARG(max_iters >= 0 && max_iters < (int64_t(1) << 30),
+                  "max_iters out of range");
+    B2S_CHECK_ARG(k <= 1 || (ldb >= k && ldx >= k), "leading dimensions below num_rhs");
+    if (k == 0) return B2S_OK;
+    B2S_CHECK_ARG(b != nullptr && x != nullptr && rp != nullptr, "null pointer");
+    cudaStream_t st = as_stream(stream);
+    int64_t nnz = 0;
+    {
+        int32_t h_nnz = 0;
+        B2S_CUDA_TRY(cudaMemcpyAsync(&h_nnz, rp + n, sizeof(int32_t),
+                                     cudaMemcpyDeviceToHost, st));
+        B2S_CUDA_TRY(cudaStreamSynchronize(st));
+        nnz = h_nnz;
+    }
+    const bool cols = k > 1 || ldb != 1 || ldx != 1;
+    const GmresLayout lay =
+        gmres_layout<TA, TB>(n, nnz, max_row_nnz, int(krylov_dim), kMixed, cols);
+    if (workspace_bytes < lay.bytes) {
+        set_error("workspace of %lld bytes < %lld", (long long)workspace_bytes,
+                  (long long)lay.bytes);
+        return B2S_ERR_WORKSPACE;
+    }
+    B2S_CHECK_ARG(reinterpret_cast<uintptr_t>(workspace) % 256 == 0,
+                  "GMRES workspace must be 256-byte aligned");
+    char* w = static_cast<char*>(workspace);
+    double* bcol = cols ? reinterpret_cast<double*>(w + lay.off_bcol) : nullptr;
+    double* xcol = cols ? reinterpret_cast<double*>(w + lay.off_xcol) : nullptr;
+    for (int64_t c = 0; c < k; ++c) {
+        const double* bc = b + c;
+        double* xc = x + c;
+        if (cols) {
+            B2S_CUDA_TRY(cudaMemcpy2DAsync(bcol, sizeof(double), b + c, ldb * sizeof(double),
+                                           sizeof(double), n, cudaMemcpyDeviceToDevice, st));
+            B2S_CUDA_TRY(cudaMemcpy2DAsync(xcol, sizeof(double), x + c, ldx * sizeof(double),
+                                           sizeof(double), n, cudaMemcpyDeviceToDevice, st));
+            bc = bcol;
+            xc = xcol;
+        }
+        const int rc = gmres_engine<TA, TB>(
+            lay, n, nnz, rp, ci, v64, max_row_nnz, dinv64, bc, xc, int(krylov_dim), ortho,
+            max_iters, reduction, baseline, inner_reduction, workspace,
+            iterations ? iterations + c : nullptr, restarts ? restarts + c : nullptr,
+            res_norms ? res_norms + c : nullptr, status ? status + c : nullptr, st);
+        if (rc != B2S_OK) return rc;
+        if (cols) {
+            B2S_CUDA_TRY(cudaMemcpy2DAsync(x + c, ldx * sizeof(double), xcol, sizeof(double),
+                                           sizeof(double), n, cudaMemcpyDeviceToDevice, st));
+        }
+    }
     return B2S_OK;
 }
 
@@ -878,70 +988,63 @@ using namespace b2s;
 extern "C" {
 
 int64_t b2s_gmres_workspace_bytes(int64_t num_rows, int64_t nnz,
-                                  int64_t max_row_nnz, int64_t krylov_dim,
-                                  int variant)
+                                  int64_t max_row_nnz, int64_t num_rhs,
+                                  int64_t krylov_dim, int variant)
 {
-    if (num_rows < 1 || krylov_dim < 1 || krylov_dim > kMaxKrylov) return -1;
+    if (num_rows < 1 || num_rhs < 0 || krylov_dim < 1 || krylov_dim > kMaxKrylov) return -1;
+    // strided or several columns go through contiguous copies; the solve
+    // decides by the leading dimensions, so a single column reserves them too
+    const bool cols = true;
+    const int d = int(krylov_dim);
     switch (variant) {
     case B2S_GMRES_F64:
-        return gmres_layout<double, double>(num_rows, nnz, max_row_nnz, int(krylov_dim),
-                                            false).bytes;
+        return gmres_layout<double, double>(num_rows, nnz, max_row_nnz, d, false, cols).bytes;
     case B2S_GMRES_MIXED_F32:
-        return gmres_layout<float, float>(num_rows, nnz, max_row_nnz, int(krylov_dim),
-                                          true).bytes;
+        return gmres_layout<float, float>(num_rows, nnz, max_row_nnz, d, true, cols).bytes;
     case B2S_GMRES_MIXED_BF16:
-        return gmres_layout<float, __nv_bfloat16>(num_rows, nnz, max_row_nnz,
-                                                  int(krylov_dim), true).bytes;
+        return gmres_layout<float, __nv_bfloat16>(num_rows, nnz, max_row_nnz, d, true, cols)
+            .bytes;
     case B2S_GMRES_CB_F32:
-        return gmres_layout<double, float>(num_rows, nnz, max_row_nnz, int(krylov_dim),
-                                           false).bytes;
+        return gmres_layout<double, float>(num_rows, nnz, max_row_nnz, d, false, cols).bytes;
     default:
         return -1;
     }
 }
 
-int b2s_gmres_solve(int variant, int64_t num_rows, const int32_t* row_ptrs,
-                    const int32_t* col_idxs, const double* values,
-                    int64_t max_row_nnz, const double* inv_diag,
-                    const double* b, double* x, int64_t krylov_dim,
-                    int64_t max_iters, double reduction_factor,
+int b2s_gmres_solve(int variant, int ortho_method, int64_t num_rows,
+                    const int32_t* row_ptrs, const int32_t* col_idxs,
+                    const double* values, int64_t max_row_nnz,
+                    const double* inv_diag, const double* b, int64_t ldb,
+                    double* x, int64_t ldx, int64_t num_rhs,
+                    int64_t krylov_dim, int64_t max_iters,
+                    double reduction_factor, int baseline,
                     double inner_reduction, void* workspace,
                     int64_t workspace_bytes, int64_t* iterations,
-                    int64_t* restarts, double* residual_norm, int* converged,
-                    void* stream)
+                    int64_t* restarts, double* residual_norms,
+                    uint8_t* status, void* stream)
 {
+#define B2S_GMRES_ARGS(INNER)                                                      \
+    num_rows, row_ptrs, col_idxs, values, max_row_nnz, inv_diag, b, ldb, x, ldx,  \
+        num_rhs, krylov_dim, ortho_method, max_iters, reduction_factor, baseline, \
+        INNER, workspace, workspace_bytes, iterations, restarts, residual_norms,  \
+        status, stream
     switch (variant) {
     case B2S_GMRES_F64:
-        return gmres_engine<double, double>(
-            num_rows, row_ptrs, col_idxs, values, max_row_nnz, inv_diag, b, x,
-            int(krylov_dim), max_iters, reduction_factor, 0.0, workspace,
-            workspace_bytes, iterations, restarts, residual_norm, converged,
-            stream);
+        return gmres_solve_columns<double, double>(B2S_GMRES_ARGS(0.0));
     case B2S_GMRES_MIXED_F32:
-        return gmres_engine<float, float>(
-            num_rows, row_ptrs, col_idxs, values, max_row_nnz, inv_diag, b, x,
-            int(krylov_dim), max_iters, reduction_factor, inner_reduction,
-            workspace, workspace_bytes, iterations, restarts, residual_norm,
-            converged, stream);
+        return gmres_solve_columns<float, float>(B2S_GMRES_ARGS(inner_reduction));
     case B2S_GMRES_MIXED_BF16:
-        return gmres_engine<float, __nv_bfloat16>(
-            num_rows, row_ptrs, col_idxs, values, max_row_nnz, inv_diag, b, x,
-            int(krylov_dim), max_iters, reduction_factor, inner_reduction,
-            workspace, workspace_bytes, iterations, restarts, residual_norm,
-            converged, stream);
+        return gmres_solve_columns<float, __nv_bfloat16>(B2S_GMRES_ARGS(inner_reduction));
     case B2S_GMRES_CB_F32:
         // FP64 arithmetic over an FP32 basis: the plain (non-refinement)
         // engine; its row groups follow the basis type (4 rows, 16 bytes
         // of basis and 32 of FP64 vectors per load)
-        return gmres_engine<double, float>(
-            num_rows, row_ptrs, col_idxs, values, max_row_nnz, inv_diag, b, x,
-            int(krylov_dim), max_iters, reduction_factor, 0.0, workspace,
-            workspace_bytes, iterations, restarts, residual_norm, converged,
-            stream);
+        return gmres_solve_columns<double, float>(B2S_GMRES_ARGS(0.0));
     default:
         set_error("unknown GMRES variant %d", variant);
         return B2S_ERR_INVALID_ARG;
     }
+#undef B2S_GMRES_ARGS
 }
 
 }  // extern "C"

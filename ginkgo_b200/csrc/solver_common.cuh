@@ -57,9 +57,42 @@ struct SolveCtl {
     int all_stopped;   // every column stopped
     unsigned ticket;   // last-block ticket of the running reduction
     int max_iters;
-    double reduction;  // relative residual goal (rhs_norm baseline)
+    double reduction;  // residual goal relative to the baseline
+    int baseline;      // B2S_BASELINE_*: ||b||, ||r_0|| or 1
+    int implicit;      // stop::ImplicitResidualNorm: sqrt|rho| instead of ||r||
     uint8_t status[kMaxRhs];
 };
+
+// The residual criterion's baseline (stop::ResidualNorm's starting_tau,
+// core/stop/residual_norm.cpp:95-150): ||b|| (rhs_norm), the initial
+// residual norm (initial_resnorm) or 1 (absolute).
+template <typename T>
+__device__ __forceinline__ T start_norm(const SolveCtl* ctl, T bnorm, T rnorm)
+{
+    return ctl->baseline == B2S_BASELINE_INITIAL_RESNORM ? rnorm
+           : ctl->baseline == B2S_BASELINE_ABSOLUTE      ? T(1)
+                                                         : bnorm;
+}
+
+// Whether a column meets the residual goal: ||r|| (stop::ResidualNorm) or
+// sqrt|rho| of the solver's implicit squared residual norm
+// (stop::ImplicitResidualNorm, reference/stop/residual_norm_kernels.cpp:80)
+// against reduction * baseline.
+template <typename T>
+__device__ __forceinline__ bool residual_met(const SolveCtl* ctl, T tau, T rho, T start)
+{
+    const double m = ctl->implicit ? sqrt(fabs(double(rho))) : double(tau);
+    return m <= ctl->reduction * double(start);
+}
+
+// Host check of a residual_mode argument (B2S_BASELINE_* with
+// B2S_STOP_IMPLICIT or-ed in).
+inline bool valid_residual_mode(int mode)
+{
+    const int base = mode & ~B2S_STOP_IMPLICIT;
+    return base == B2S_BASELINE_RHS_NORM || base == B2S_BASELINE_INITIAL_RESNORM ||
+           base == B2S_BASELINE_ABSOLUTE;
+}
 
 // Rounding-exact helpers: the same expression evaluated in two kernels must
 // give the same bits, so no FMA contraction is allowed in them.

@@ -10,9 +10,10 @@ reference's ``gko::solver`` / ``gko::stop`` / ``gko::preconditioner`` API:
     solver.apply(b, x)                # x holds the initial guess
     solver.logger.num_iterations      # like gko::log::Convergence
 
-Only scalar Jacobi (max_block_size 1) or no preconditioner is supported on
-this path; stopping is Iteration + ResidualNorm with the rhs_norm baseline
-(the defaults of include/ginkgo/core/stop/residual_norm.hpp).
+Only scalar Jacobi (max_block_size 1) or no preconditioner is fused into
+the solvers; stopping is Iteration plus one residual criterion, ResidualNorm
+(baselines rhs_norm, initial_resnorm, absolute) or, for CG and BiCGStab,
+ImplicitResidualNorm (include/ginkgo/core/stop/residual_norm.hpp).
 """
 from __future__ import annotations
 
@@ -26,6 +27,9 @@ from ._lib import GinkgoError, call, lib
 from .matrix import Csr, _check_dense, _p, _stream
 
 _SFX = {torch.float64: "f64", torch.float32: "f32"}
+# gmres::ortho_method (include/ginkgo/core/solver/gmres.hpp:38-50) as the C
+# ABI's B2S_ORTHO_* values
+_ORTHO = {"mgs": 0, "cgs": 1, "cgs2": 2}
 
 
 # --------------------------------------------------------------- criteria --
@@ -64,34 +68,65 @@ class Iteration:
         self.max_iters = int(max_iters)
 
 
+# stop::mode (include/ginkgo/core/stop/residual_norm.hpp:37) as the C ABI's
+# B2S_BASELINE_* values; B2S_STOP_IMPLICIT marks ImplicitResidualNorm
+_BASELINES = {"rhs_norm": 0, "initial_resnorm": 1, "absolute": 2}
+_STOP_IMPLICIT = 4
+
+
 class ResidualNorm:
-    """stop::ResidualNorm with the rhs_norm baseline
-    (core/stop/residual_norm.cpp:95-230): ||r|| <= reduction_factor ||b||."""
+    """stop::ResidualNorm (core/stop/residual_norm.cpp:95-230):
+    ||r|| <= reduction_factor * baseline, baseline ||b|| (rhs_norm, the
+    default), ||b - A x_0|| (initial_resnorm) or 1 (absolute)."""
+    implicit = False
 
     @staticmethod
     def build():
         return _Builder(ResidualNorm, reduction_factor=1e-15, baseline="rhs_norm")
 
     def __init__(self, exec_=None, reduction_factor=1e-15, baseline="rhs_norm"):
-        if baseline != "rhs_norm":
-            raise NotImplementedError("only the rhs_norm baseline is on this path")
+        if baseline not in _BASELINES:
+            raise ValueError(f"unknown baseline {baseline!r}: one of {sorted(_BASELINES)}")
         self.reduction_factor = float(reduction_factor)
+        self.baseline = baseline
+
+    @property
+    def mode(self):
+        return _BASELINES[self.baseline] | (_STOP_IMPLICIT if self.implicit else 0)
+
+
+class ImplicitResidualNorm(ResidualNorm):
+    """stop::ImplicitResidualNorm (include/ginkgo/core/stop/residual_norm.hpp:175,
+    core/stop/residual_norm.cpp:205-225): sqrt|rho| <= reduction_factor *
+    baseline, rho the solver's implicit squared residual norm (r^T z in CG,
+    r_hat^T r in BiCGStab)."""
+    implicit = True
+
+    @staticmethod
+    def build():
+        return _Builder(ImplicitResidualNorm, reduction_factor=1e-15, baseline="rhs_norm")
 
 
 def _criteria(crits):
-    max_iters, red = None, None
+    """(max_iters, reduction_factor, residual_mode) of a criterion list: an
+    Iteration criterion and at most one residual criterion."""
+    max_iters, res = None, None
     for c in crits:
         if isinstance(c, _Builder):
             c = c.on(None)
         if isinstance(c, Iteration):
             max_iters = c.max_iters if max_iters is None else min(max_iters, c.max_iters)
         elif isinstance(c, ResidualNorm):
-            red = c.reduction_factor
+            if res is not None:
+                raise NotImplementedError("one residual criterion per solve on this path")
+            res = c
         else:
             raise TypeError(f"unsupported criterion {c!r}")
     if max_iters is None:
         raise ValueError("an Iteration criterion is required")
-    return max_iters, (0.0 if red is None else red)
+    if res is None:
+        return max_iters, 0.0, _BASELINES["rhs_norm"]
+    return max_iters, res.reduction_factor, res.mode
 
 
 # ---------------------------------------------------------- preconditioner --
@@ -244,13 +279,17 @@ class _SolverFactory:
     kind = ""
 
     def __init__(self, exec_, criteria=(), preconditioner=None, krylov_dim=100,
-                 check_every=8, storage_precision=None, inner_reduction=1e-6):
+                 check_every=8, storage_precision=None, inner_reduction=1e-6,
+                 ortho_method="mgs"):
         self.exec = exec_
         crit = criteria if isinstance(criteria, (list, tuple)) else (criteria,)
-        self.max_iters, self.reduction = _criteria(crit)
+        self.max_iters, self.reduction, self.residual_mode = _criteria(crit)
         self.preconditioner = preconditioner
-        # the device Hessenberg holds at most 32 columns
-        self.krylov_dim = min(int(krylov_dim), 32)
+        # 1..128: the device rejects anything else (no silent change)
+        self.krylov_dim = int(krylov_dim)
+        if ortho_method not in _ORTHO:
+            raise ValueError(f"unknown ortho_method {ortho_method!r}: one of {sorted(_ORTHO)}")
+        self.ortho_method = ortho_method
         self.check_every = int(check_every)
         self.storage_precision = storage_precision
         self.inner_reduction = float(inner_reduction)
@@ -306,7 +345,7 @@ class _Solver:
         call(f"b2s_{name}_solve_{_SFX[A.dtype]}", n, _p(A.row_ptrs), _p(A.col_idxs),
              _p(A.values), A.max_row_nnz, _p(self.inv_diag), _p(b2), b2.stride(0),
              _p(x2), x2.stride(0), k, self.f.max_iters, self.f.reduction,
-             self.f.check_every, _p(ws), ws.numel(), C.byref(it),
+             self.f.residual_mode, self.f.check_every, _p(ws), ws.numel(), C.byref(it),
              res.ctypes.data_as(C.c_void_p), st.ctypes.data_as(C.c_void_p),
              _stream(x2))
         self.logger = ConvergenceLog(int(it.value), res.tolist(),
@@ -318,11 +357,13 @@ class _Solver:
         if A.dtype != torch.float64:
             raise TypeError("GMRES on this path takes the FP64 matrix; the "
                             "low-precision inner solve converts it itself")
+        if self.f.residual_mode & _STOP_IMPLICIT:
+            raise NotImplementedError("GMRES provides no implicit squared residual norm "
+                                      "(the reference raises NotSupported too)")
         n = A.shape[0]
         b2 = _check_dense(b, n, A.dtype, "b")
         x2 = _check_dense(x, n, A.dtype, "x")
-        if b2.shape[1] != 1 or not x2.is_contiguous() or not b2.is_contiguous():
-            raise NotImplementedError("GMRES here takes one contiguous right-hand side")
+        k = b2.shape[1]
         if self.f.kind == "cb_gmres":
             sp = self.f.storage_precision or "reduce1"
             if sp not in ("keep", "reduce1"):
@@ -331,18 +372,26 @@ class _Solver:
             variant = 0 if sp == "keep" else 3
         else:
             variant = {None: 0, "f64": 0, "f32": 1, "bf16": 2}[self.f.storage_precision]
-        nbytes = lib().b2s_gmres_workspace_bytes(n, A.nnz, A.max_row_nnz,
+        nbytes = lib().b2s_gmres_workspace_bytes(n, A.nnz, A.max_row_nnz, k,
                                                  self.f.krylov_dim, variant)
+        if nbytes < 0:
+            raise GinkgoError("b2s_gmres_workspace_bytes", -1,
+                              f"krylov_dim {self.f.krylov_dim} is not supported: 1..128")
         ws = self._workspace(nbytes)
-        it, rs = C.c_int64(0), C.c_int64(0)
-        rn, conv = C.c_double(0), C.c_int(0)
-        call("b2s_gmres_solve", variant, n, _p(A.row_ptrs), _p(A.col_idxs),
-             _p(A.values), A.max_row_nnz, _p(self.inv_diag), _p(b2), _p(x2),
-             self.f.krylov_dim, self.f.max_iters, self.f.reduction,
-             self.f.inner_reduction, _p(ws), ws.numel(), C.byref(it),
-             C.byref(rs), C.byref(rn), C.byref(conv), _stream(x2))
-        self.logger = ConvergenceLog(int(it.value), [rn.value], bool(conv.value),
-                                     [0x82 if conv.value else 0x01], int(rs.value))
+        it = np.zeros(k, np.int64)
+        rs = np.zeros(k, np.int64)
+        rn = np.zeros(k, np.float64)
+        st = np.zeros(k, np.uint8)
+        call("b2s_gmres_solve", variant, _ORTHO[self.f.ortho_method], n, _p(A.row_ptrs),
+             _p(A.col_idxs), _p(A.values), A.max_row_nnz, _p(self.inv_diag), _p(b2),
+             b2.stride(0), _p(x2), x2.stride(0), k, self.f.krylov_dim, self.f.max_iters,
+             self.f.reduction, self.f.residual_mode, self.f.inner_reduction, _p(ws),
+             ws.numel(), it.ctypes.data_as(C.c_void_p), rs.ctypes.data_as(C.c_void_p),
+             rn.ctypes.data_as(C.c_void_p), st.ctypes.data_as(C.c_void_p), _stream(x2))
+        self.logger = ConvergenceLog(int(it.max()) if k else 0, rn.tolist(),
+                                     bool(np.all(st & 0x80)), st.tolist(),
+                                     int(rs.max()) if k else 0)
+        self.logger.iterations_per_column = it.tolist()
         return x
 
 
@@ -370,7 +419,8 @@ class _IrFactory(_SolverFactory):
         sp = inner.get("storage_precision", "f32")
         super().__init__(exec_, criteria=criteria,
                          preconditioner=inner.get("preconditioner", kw.pop("preconditioner", None)),
-                         krylov_dim=inner.get("krylov_dim", 30),
+                         krylov_dim=inner.get("krylov_dim", 100),
+                         ortho_method=inner.get("ortho_method", "mgs"),
                          storage_precision=sp if sp != "f64" else "f32",
                          inner_reduction=inner.get("inner_reduction", 1e-6), **kw)
 
@@ -392,25 +442,26 @@ class Bicgstab:
 
 
 class Gmres:
-    """solver::Gmres (core/solver/gmres.cpp); krylov_dim <= 32 here (the
-    reference default of 100 is capped).  with_storage_precision("f32" or
-    "bf16") selects the low-precision Arnoldi used inside Ir."""
+    """solver::Gmres (core/solver/gmres.cpp): krylov_dim 1..128 (default
+    100, as the reference), ortho_method "mgs" (default; run as CGS2 on the
+    device), "cgs" or "cgs2", any number of right-hand sides (independent
+    columns).  with_storage_precision("f32" or "bf16") selects the
+    low-precision Arnoldi used inside Ir."""
 
     @staticmethod
     def build():
-        return _Builder(_GmresFactory, krylov_dim=30)
+        return _Builder(_GmresFactory, krylov_dim=100)
 
 
 class CbGmres:
     """solver::CbGmres (core/solver/cb_gmres.cpp): restarted GMRES with FP64
     arithmetic and the Krylov basis stored in a reduced format;
     with_storage_precision("reduce1") (the default here, an FP32 basis) or
-    "keep" (FP64).  krylov_dim <= 32 (the reference default of 100 is
-    capped)."""
+    "keep" (FP64).  krylov_dim 1..128 (default 100, as the reference)."""
 
     @staticmethod
     def build():
-        return _Builder(_CbGmresFactory, krylov_dim=30, storage_precision="reduce1")
+        return _Builder(_CbGmresFactory, krylov_dim=100, storage_precision="reduce1")
 
 
 class Ir:

@@ -423,12 +423,26 @@ int b2s_residual_norm_check_f32(int64_t k, const float* tau,
  * iteration; the host checks the device stop flag once per replay of a
  * captured CUDA graph.  They synchronise `stream` before returning and
  * write the host outputs (iterations, residual norms, status).  Stopping:
- * Iteration(max_iters) + ResidualNorm(reduction_factor, rhs_norm baseline)
- * per right-hand-side column; status[j] uses the bit layout of
+ * Iteration(max_iters) + a residual criterion per right-hand-side column,
+ * ||r|| <= reduction_factor * baseline, chosen by residual_mode (below);
+ * status[j] uses the bit layout of
  * gko::stopping_status (include/ginkgo/core/stop/stopping_status.hpp):
  * bit 7 converged, bit 6 finalized, bits 0-5 criterion id (1 iteration
  * limit, 2 residual norm).  inv_diag: scalar Jacobi (from
  * b2s_jacobi_invert_diagonal_*) or NULL for no preconditioner. */
+
+/* residual_mode of the fused solvers: the baseline of the residual goal
+ * (stop::ResidualNorm's mode, include/ginkgo/core/stop/residual_norm.hpp:37:
+ * rhs_norm ||b||, initial_resnorm ||b - A x_0||, absolute 1), with
+ * B2S_STOP_IMPLICIT or-ed in for stop::ImplicitResidualNorm (:175), which
+ * compares sqrt|rho| of the solver's implicit squared residual norm instead
+ * of ||r|| (rho = r^T z for CG, r_hat^T r for BiCGStab: core/solver/cg.cpp:156,
+ * core/solver/bicgstab.cpp:173).  GMRES takes a baseline only (the
+ * reference's GMRES provides no implicit squared norm). */
+#define B2S_BASELINE_RHS_NORM 0
+#define B2S_BASELINE_INITIAL_RESNORM 1
+#define B2S_BASELINE_ABSOLUTE 2
+#define B2S_STOP_IMPLICIT 4
 
 /* Preconditioned CG, 1..16 right-hand sides (b, x row-major with leading
  * dimensions).  Replaces Cg<V>::apply_dense_impl (core/solver/cg.cpp:91-189)
@@ -442,7 +456,8 @@ int b2s_cg_solve_f64(int64_t num_rows, const int32_t* row_ptrs,
                      int64_t max_row_nnz, const double* inv_diag,
                      const double* b, int64_t ldb, double* x, int64_t ldx,
                      int64_t num_rhs, int64_t max_iters,
-                     double reduction_factor, int64_t check_every,
+                     double reduction_factor, int residual_mode,
+                     int64_t check_every,
                      void* workspace, int64_t workspace_bytes,
                      int64_t* iterations, double* residual_norms,
                      uint8_t* status, void* stream);
@@ -451,7 +466,8 @@ int b2s_cg_solve_f32(int64_t num_rows, const int32_t* row_ptrs,
                      int64_t max_row_nnz, const float* inv_diag,
                      const float* b, int64_t ldb, float* x, int64_t ldx,
                      int64_t num_rhs, int64_t max_iters,
-                     double reduction_factor, int64_t check_every,
+                     double reduction_factor, int residual_mode,
+                     int64_t check_every,
                      void* workspace, int64_t workspace_bytes,
                      int64_t* iterations, double* residual_norms,
                      uint8_t* status, void* stream);
@@ -467,7 +483,8 @@ int b2s_bicgstab_solve_f64(int64_t num_rows, const int32_t* row_ptrs,
                            int64_t max_row_nnz, const double* inv_diag,
                            const double* b, int64_t ldb, double* x,
                            int64_t ldx, int64_t num_rhs, int64_t max_iters,
-                           double reduction_factor, int64_t check_every,
+                           double reduction_factor, int residual_mode,
+                           int64_t check_every,
                            void* workspace, int64_t workspace_bytes,
                            int64_t* iterations, double* residual_norms,
                            uint8_t* status, void* stream);
@@ -476,7 +493,8 @@ int b2s_bicgstab_solve_f32(int64_t num_rows, const int32_t* row_ptrs,
                            int64_t max_row_nnz, const float* inv_diag,
                            const float* b, int64_t ldb, float* x, int64_t ldx,
                            int64_t num_rhs, int64_t max_iters,
-                           double reduction_factor, int64_t check_every,
+                           double reduction_factor, int residual_mode,
+                           int64_t check_every,
                            void* workspace, int64_t workspace_bytes,
                            int64_t* iterations, double* residual_norms,
                            uint8_t* status, void* stream);
@@ -486,37 +504,57 @@ int b2s_bicgstab_solve_f32(int64_t num_rows, const int32_t* row_ptrs,
 #define B2S_GMRES_MIXED_BF16 2
 #define B2S_GMRES_CB_F32 3
 
-/* Restarted GMRES(krylov_dim <= 32), right scalar-Jacobi preconditioning,
- * one right-hand side, FP64 matrix/b/x/inv_diag.  variant B2S_GMRES_F64 is
- * plain FP64 GMRES (Gmres<double>, core/solver/gmres.cpp:325-640);
- * B2S_GMRES_MIXED_F32 / _BF16 is iterative refinement (Ir<double>,
- * core/solver/ir.cpp:191-257) whose every outer step computes r = b - A x
- * and ||r|| in FP64 and runs one GMRES cycle on an FP32 copy of A with FP32
- * vectors and an FP32 or BF16 Krylov basis.  Hessenberg, Givens and the
- * triangular solve are FP64 in all variants.  B2S_GMRES_CB_F32 is
- * compressed-basis GMRES (CbGmres<double> with storage_precision reduce1,
- * core/solver/cb_gmres.cpp): FP64 matrix, vectors and arithmetic, the
- * Krylov basis stored in FP32 and read back for the orthogonalisation and
- * the solution update.  max_iters bounds the total
- * Arnoldi steps; reduction_factor is the goal on the explicit FP64 residual
- * relative to ||b||; inner_reduction ends an inner cycle early once its
- * estimate falls below inner_reduction * ||r||.  *restarts counts cycles.
- * max_row_nnz must be at least the longest row (the workspace holds a
- * column-major copy of A in the Arnoldi type when its padding stays within
- * a quarter of nnz; a longer row makes the solve return
- * B2S_ERR_INVALID_ARG). */
+/* Orthogonalisation of GMRES (solver::gmres::ortho_method,
+ * include/ginkgo/core/solver/gmres.hpp:38-50).  CGS projects once
+ * (h = V^T w); CGS2 projects twice, the second projection taken from the
+ * Gram matrix of the basis in the same pass over it.  MGS, the reference's
+ * default, runs as CGS2: one pass over the basis per Arnoldi step instead of
+ * j + 1, with orthogonality at least as good; results agree with MGS to
+ * rounding, iteration counts to within a few. */
+#define B2S_ORTHO_MGS 0
+#define B2S_ORTHO_CGS 1
+#define B2S_ORTHO_CGS2 2
+
+/* Restarted GMRES(krylov_dim), 1 <= krylov_dim <= 128 (larger values are
+ * rejected with B2S_ERR_INVALID_ARG), right scalar-Jacobi preconditioning,
+ * FP64 matrix/b/x/inv_diag; b and x are row-major num_rows x num_rhs with
+ * leading dimensions ldb, ldx.  The columns are independent GMRES solves
+ * (each with its own basis, Hessenberg matrix and stop status), run one
+ * after the other.  variant B2S_GMRES_F64 is plain FP64 GMRES (Gmres<double>,
+ * core/solver/gmres.cpp:325-640); B2S_GMRES_MIXED_F32 / _BF16 is iterative
+ * refinement (Ir<double>, core/solver/ir.cpp:191-257) whose every outer step
+ * computes r = b - A x and ||r|| in FP64 and runs one GMRES cycle on an FP32
+ * copy of A with FP32 vectors and an FP32 or BF16 Krylov basis.  Hessenberg,
+ * Givens and the triangular solve are FP64 in all variants.
+ * B2S_GMRES_CB_F32 is compressed-basis GMRES (CbGmres<double> with
+ * storage_precision reduce1, core/solver/cb_gmres.cpp): FP64 matrix, vectors
+ * and arithmetic, the Krylov basis stored in FP32 and read back for the
+ * orthogonalisation and the solution update.  max_iters bounds the total
+ * Arnoldi steps of a column; the goal is ||b - A x|| <= reduction_factor *
+ * baseline on the explicit FP64 residual, baseline one of B2S_BASELINE_*
+ * (||b||, the initial residual norm, or 1); inner_reduction ends an inner
+ * cycle early once its estimate falls below inner_reduction * ||r||.  Per
+ * column: iterations, restarts (cycles), residual_norms and status (the
+ * reference's stopping_status bits: 0x80 converged, 0x40 finalized, low six
+ * bits the criterion, 1 iteration limit, 2 residual norm); each output
+ * array may be NULL.  max_row_nnz must be at least the longest row (the
+ * workspace holds a column-major copy of A in the Arnoldi type when its
+ * padding stays within a quarter of nnz; a longer row makes the solve
+ * return B2S_ERR_INVALID_ARG). */
 int64_t b2s_gmres_workspace_bytes(int64_t num_rows, int64_t nnz,
-                                  int64_t max_row_nnz, int64_t krylov_dim,
-                                  int variant);
-int b2s_gmres_solve(int variant, int64_t num_rows, const int32_t* row_ptrs,
-                    const int32_t* col_idxs, const double* values,
-                    int64_t max_row_nnz, const double* inv_diag,
-                    const double* b, double* x, int64_t krylov_dim,
-                    int64_t max_iters, double reduction_factor,
+                                  int64_t max_row_nnz, int64_t num_rhs,
+                                  int64_t krylov_dim, int variant);
+int b2s_gmres_solve(int variant, int ortho_method, int64_t num_rows,
+                    const int32_t* row_ptrs, const int32_t* col_idxs,
+                    const double* values, int64_t max_row_nnz,
+                    const double* inv_diag, const double* b, int64_t ldb,
+                    double* x, int64_t ldx, int64_t num_rhs,
+                    int64_t krylov_dim, int64_t max_iters,
+                    double reduction_factor, int baseline,
                     double inner_reduction, void* workspace,
                     int64_t workspace_bytes, int64_t* iterations,
-                    int64_t* restarts, double* residual_norm, int* converged,
-                    void* stream);
+                    int64_t* restarts, double* residual_norms,
+                    uint8_t* status, void* stream);
 
 /* -------------------------------------------------------- gradients -- */
 

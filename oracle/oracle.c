@@ -97,8 +97,8 @@ int orc_ir_gmres_mixed(int64_t n, const int32_t* rp, const int32_t* ci,
         }
         int it = 0;
         double rn;
-        orc_gmres_f32(n, rp, ci, v32, inv32, r32, d32, krylov_dim, inner_iters,
-                      inner_reduction, &it, &rn);
+        orc_gmres_f32(n, rp, ci, v32, inv32, r32, d32, krylov_dim, 0, inner_iters,
+                      inner_reduction, 0, &it, &rn);
         inner_total += it;
         for (int64_t i = 0; i < n; ++i) x[i] += (double)d32[i];
     }

@@ -78,16 +78,17 @@ extern "C" {
                                     const char* finalized);                   \
     int orc_cg_##S(int64_t n, const int32_t* rp, const int32_t* ci,           \
                    const T* v, const T* inv_diag, const T* b, T* x,           \
-                   int64_t k, int max_iters, double reduction,                \
+                   int64_t k, int max_iters, double reduction, int mode,      \
                    int* iters_out, double* res_norm_out);                     \
     int orc_bicgstab_##S(int64_t n, const int32_t* rp, const int32_t* ci,     \
                          const T* v, const T* inv_diag, const T* b, T* x,     \
-                         int max_iters, double reduction, int* iters_out,     \
-                         double* res_norm_out);                               \
+                         int max_iters, double reduction, int mode,           \
+                         int* iters_out, double* res_norm_out);               \
     int orc_gmres_##S(int64_t n, const int32_t* rp, const int32_t* ci,        \
                       const T* v, const T* inv_diag, const T* b, T* x,        \
-                      int krylov_dim, int max_iters, double reduction,        \
-                      int* iters_out, double* res_norm_out);                  \
+                      int krylov_dim, int ortho, int max_iters,               \
+                      double reduction, int mode, int* iters_out,             \
+                      double* res_norm_out);                                  \
     int orc_batch_bicgstab_ell_##S(int64_t n, int64_t width, int64_t stride,  \
                                    const int32_t* ci, const T* v,             \
                                    const T* b, T* x, int max_iters,           \

@@ -58,13 +58,14 @@ def lib():
             getattr(_lib, f"orc_gmres_solve_krylov_{s}").argtypes = [
                 _i64, _p, _p, _i64, _p, _p, _p]
             f = getattr(_lib, f"orc_cg_{s}")
-            f.argtypes = [_i64, _p, _p, _p, _p, _p, _p, _i64, _i32, _f64, _p, _p]
+            f.argtypes = [_i64, _p, _p, _p, _p, _p, _p, _i64, _i32, _f64, _i32, _p, _p]
             f.restype = _i32
             f = getattr(_lib, f"orc_bicgstab_{s}")
-            f.argtypes = [_i64, _p, _p, _p, _p, _p, _p, _i32, _f64, _p, _p]
+            f.argtypes = [_i64, _p, _p, _p, _p, _p, _p, _i32, _f64, _i32, _p, _p]
             f.restype = _i32
             f = getattr(_lib, f"orc_gmres_{s}")
-            f.argtypes = [_i64, _p, _p, _p, _p, _p, _p, _i32, _i32, _f64, _p, _p]
+            f.argtypes = [_i64, _p, _p, _p, _p, _p, _p, _i32, _i32, _i32, _f64, _i32,
+                          _p, _p]
             f.restype = _i32
             f = getattr(_lib, f"orc_batch_bicgstab_ell_{s}")
             f.argtypes = [_i64, _i64, _i64, _p, _p, _p, _p, _i32, _f64, _i32,
@@ -210,7 +211,14 @@ def jacobi_invert_diagonal(rp, ci, v):
     return out
 
 
-def cg(rp, ci, v, b, x0=None, jacobi=True, max_iters=1000, reduction=1e-10):
+# residual criterion modes: baseline (0 rhs_norm, 1 initial_resnorm,
+# 2 absolute) plus 4 for the implicit residual norm
+MODES = {"rhs_norm": 0, "initial_resnorm": 1, "absolute": 2}
+IMPLICIT = 4
+ORTHO = {"mgs": 0, "cgs": 1, "cgs2": 2}
+
+
+def cg(rp, ci, v, b, x0=None, jacobi=True, max_iters=1000, reduction=1e-10, mode=0):
     """Returns (x, iterations, residual norms, converged columns)."""
     rp, ci, v = _c(rp, np.int32), _c(ci, np.int32), np.ascontiguousarray(v)
     dt = v.dtype
@@ -222,11 +230,12 @@ def cg(rp, ci, v, b, x0=None, jacobi=True, max_iters=1000, reduction=1e-10):
     res = np.zeros(k, np.float64)
     conv = getattr(lib(), f"orc_cg_{_sfx(dt)}")(
         n, _ptr(rp), _ptr(ci), _ptr(v), _ptr(inv), _ptr(b2), _ptr(x), k,
-        max_iters, reduction, C.byref(it), _ptr(res))
+        max_iters, reduction, int(mode), C.byref(it), _ptr(res))
     return x.reshape(np.shape(b)), it.value, res, conv
 
 
-def bicgstab(rp, ci, v, b, x0=None, jacobi=True, max_iters=1000, reduction=1e-10):
+def bicgstab(rp, ci, v, b, x0=None, jacobi=True, max_iters=1000, reduction=1e-10,
+             mode=0):
     rp, ci, v = _c(rp, np.int32), _c(ci, np.int32), np.ascontiguousarray(v)
     dt = v.dtype
     b = _c(b, dt)
@@ -236,12 +245,12 @@ def bicgstab(rp, ci, v, b, x0=None, jacobi=True, max_iters=1000, reduction=1e-10
     res = C.c_double(0)
     conv = getattr(lib(), f"orc_bicgstab_{_sfx(dt)}")(
         len(b), _ptr(rp), _ptr(ci), _ptr(v), _ptr(inv), _ptr(b), _ptr(x),
-        max_iters, reduction, C.byref(it), C.byref(res))
+        max_iters, reduction, int(mode), C.byref(it), C.byref(res))
     return x, it.value, res.value, conv
 
 
 def gmres(rp, ci, v, b, x0=None, jacobi=True, krylov_dim=30, max_iters=1000,
-          reduction=1e-10):
+          reduction=1e-10, ortho="mgs", mode=0):
     rp, ci, v = _c(rp, np.int32), _c(ci, np.int32), np.ascontiguousarray(v)
     dt = v.dtype
     b = _c(b, dt)
@@ -251,7 +260,8 @@ def gmres(rp, ci, v, b, x0=None, jacobi=True, krylov_dim=30, max_iters=1000,
     res = C.c_double(0)
     conv = getattr(lib(), f"orc_gmres_{_sfx(dt)}")(
         len(b), _ptr(rp), _ptr(ci), _ptr(v), _ptr(inv), _ptr(b), _ptr(x),
-        krylov_dim, max_iters, reduction, C.byref(it), C.byref(res))
+        krylov_dim, ORTHO[ortho], max_iters, reduction, int(mode), C.byref(it),
+        C.byref(res))
     return x, it.value, res.value, conv
 
 

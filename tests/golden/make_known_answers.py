@@ -142,7 +142,33 @@ cases = {
          "b": [72748.36, 297469.88, 347229.24, 36290.66, 82958.82, -80192.15],
          "expected": [52.7, 85.4, 134.2, -250.0, -16.8, 35.3],
          "krylov_dim": 100, "max_iters": 100, "tol_factor": 1e3},
+        {"name": "Gmres.SolvesBigDenseSystem2", "solver": "gmres",
+         "source": "reference/test/solver/gmres_kernels.cpp:54-67,648-665",
+         "dense": "Gmres.SolvesBigDenseSystem1",
+         "b": [175352.10, 313410.50, 131114.10, -134116.30, 179529.30, -43564.90],
+         "expected": [33.0, -56.0, 81.0, -30.0, 21.0, 40.0],
+         "krylov_dim": 100, "max_iters": 100, "tol_factor": 1e3},
+        # tolerance sqrt(r) * 1e2 (half_tol), written as tol_sqrt
+        {"name": "Gmres.SolvesBigDenseSystem1WithRestart", "solver": "gmres",
+         "source": "reference/test/solver/gmres_kernels.cpp:77-82,750-775",
+         "dense": [[-86.40, 153.30, -108.90, 8.60, -61.60],
+                   [7.70, -77.00, 3.30, -149.20, 74.80],
+                   [-121.40, 37.10, 55.30, -74.20, -19.20],
+                   [-111.40, -22.60, 110.10, -106.20, 88.90],
+                   [-0.70, 111.70, 154.40, 235.00, -76.50]],
+         "b": [-13945.16, 11205.66, 16132.96, 24342.18, -10910.98],
+         "expected": [-140.20, -142.20, 48.80, -17.70, -19.60],
+         "krylov_dim": 4, "max_iters": 200, "tol_factor": 1e2, "tol_sqrt": True},
     ],
+    # two right-hand sides solved together and one at a time: the combined
+    # solve is at least as accurate as the single ones and matches them
+    # within r (reference/test/solver/gmres_kernels.cpp:683-748)
+    "gmres_multi_rhs": {
+        "source": "reference/test/solver/gmres_kernels.cpp:54-67,683-748",
+        "dense": "Gmres.SolvesBigDenseSystem1",
+        "b1": [1300083.0, 1018120.5, 906410.0, -42679.5, 846779.5, 1176858.5],
+        "b2": [886630.5, -172578.0, 684522.0, -65310.5, 455487.5, 607436.0],
+        "krylov_dim": 100, "max_iters": 100},
     "gmres_kernels": {
         "source": "reference/test/solver/gmres_kernels.cpp:214-350",
         "hessenberg_qr_iter0": {

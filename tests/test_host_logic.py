@@ -77,17 +77,41 @@ def test_conductivity_assembly_matches_generator():
 def test_solver_factory_parameters():
     from ginkgo_b200.solver import (Cg, Gmres, Iteration, Jacobi, ResidualNorm,
                                     _criteria)
-    m, r = _criteria((Iteration.build().with_max_iters(50),
-                      ResidualNorm.build().with_reduction_factor(1e-8)))
-    assert (m, r) == (50, 1e-8)
+    m, r, mode = _criteria((Iteration.build().with_max_iters(50),
+                            ResidualNorm.build().with_reduction_factor(1e-8)))
+    assert (m, r, mode) == (50, 1e-8, 0)
     with pytest.raises(ValueError):
         _criteria((ResidualNorm.build().with_reduction_factor(1e-8),))
+    # baselines and the implicit norm map to the C ABI's residual modes
+    from ginkgo_b200.solver import ImplicitResidualNorm
+    it = Iteration.build().with_max_iters(5)
+    for base, code in (("rhs_norm", 0), ("initial_resnorm", 1), ("absolute", 2)):
+        assert _criteria((it, ResidualNorm.build().with_baseline(base)))[2] == code
+        assert _criteria((it, ImplicitResidualNorm.build().with_baseline(base)))[2] == code | 4
+    with pytest.raises(ValueError):
+        ResidualNorm.build().with_baseline("relative").on(None)
+    with pytest.raises(NotImplementedError):
+        _criteria((it, ResidualNorm.build(), ImplicitResidualNorm.build()))
     assert Jacobi.build().with_max_block_size(4).on(None).max_block_size == 4
-    f = (Gmres.build().with_krylov_dim(100)
-         .with_criteria(Iteration.build().with_max_iters(5)).on(None))
-    assert f.krylov_dim == 32  # capped by the device Hessenberg
+    # the reference's GMRES defaults: krylov_dim 100, modified Gram-Schmidt
+    f = Gmres.build().with_criteria(it).on(None)
+    assert f.krylov_dim == 100 and f.ortho_method == "mgs"
+    f = Gmres.build().with_krylov_dim(300).with_criteria(it).on(None)
+    assert f.krylov_dim == 300  # not changed here; the device rejects it
+    with pytest.raises(ValueError):
+        Gmres.build().with_ortho_method("householder").with_criteria(it).on(None)
     f = Cg.build().with_criteria(Iteration.build().with_max_iters(3)).on(None)
     assert f.kind == "cg" and f.max_iters == 3 and f.reduction == 0.0
+
+
+def test_gmres_workspace_query_rejects_unsupported_krylov_dims():
+    from ginkgo_b200._lib import lib
+    q = lib().b2s_gmres_workspace_bytes
+    assert q(1000, 5000, 7, 1, 128, 0) > 0
+    assert q(1000, 5000, 7, 4, 100, 3) > 0
+    assert q(1000, 5000, 7, 1, 129, 0) == -1
+    assert q(1000, 5000, 7, 1, 0, 0) == -1
+    assert q(1000, 5000, 7, 1, 30, 9) == -1
 
 
 def test_block_detection_matches_the_oracle():

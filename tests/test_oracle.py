@@ -155,7 +155,8 @@ def test_solver_known_answers(known, dt):
                               max_iters=c["max_iters"], reduction=r)
         exp = np.array(c["expected"])
         err = np.linalg.norm(x - exp) / max(np.linalg.norm(x), np.linalg.norm(exp))
-        assert err <= r * c["tol_factor"], (c["name"], err)
+        tol = (np.sqrt(r) if c.get("tol_sqrt") else r) * c["tol_factor"]
+        assert err <= tol, (c["name"], err)
 
 
 @pytest.mark.parametrize("dt", DTYPES)
@@ -208,3 +209,51 @@ def test_ell_sellp_match_csr_random():
     dense[np.repeat(np.arange(3000), np.diff(rp)), ci] = v
     np.testing.assert_allclose(orc.csr_spmv(trp, tci, tv, x), dense.T @ x,
                                rtol=1e-10, atol=1e-10)
+
+
+@pytest.mark.parametrize("ortho", ["cgs", "cgs2"])
+def test_gmres_orthogonalisations_meet_known_answers(known, ortho):
+    # reference/test/solver/gmres_kernels.cpp:777-812 solves with every
+    # ortho_method; the oracle's CGS and CGS2 meet the GMRES known answers
+    dense = {c["name"]: c["dense"] for c in known["solves"]
+             if not isinstance(c["dense"], str)}
+    r = np.finfo(np.float64).eps * 10
+    for c in known["solves"]:
+        if c["solver"] != "gmres":
+            continue
+        d = c["dense"] if not isinstance(c["dense"], str) else dense[c["dense"]]
+        rp, ci, v = dense_to_csr(d)
+        x, *_ = orc.gmres(rp, ci, v, np.array(c["b"]), jacobi=False,
+                          krylov_dim=c["krylov_dim"], max_iters=c["max_iters"],
+                          reduction=r, ortho=ortho)
+        exp = np.array(c["expected"])
+        err = np.linalg.norm(x - exp) / max(np.linalg.norm(x), np.linalg.norm(exp))
+        tol = (np.sqrt(r) if c.get("tol_sqrt") else r) * c["tol_factor"]
+        assert err <= tol, (c["name"], ortho, err)
+
+
+def test_residual_modes_of_the_oracle():
+    # the three baselines and the implicit norm change when CG stops:
+    # ||r_k|| <= red * baseline with baseline ||b||, ||r_0|| or 1
+    from ginkgo_b200 import stencils
+    rp, ci, v = stencils.poisson_2d_5pt(24)
+    n = len(rp) - 1
+    rng = np.random.default_rng(3)
+    b = rng.standard_normal(n)
+    x0 = 5 * rng.standard_normal(n)
+    r0 = np.linalg.norm(b - orc.csr_spmv(rp, ci, v, x0))
+    for mode, base in ((0, np.linalg.norm(b)), (1, r0), (2, 1.0)):
+        red = 1e-8 if mode != 2 else 1e-6
+        x, it, res, conv = orc.cg(rp, ci, v, b, x0=x0, max_iters=2000, reduction=red,
+                                  mode=mode)
+        assert conv == 1
+        assert res[0] <= red * base
+        # one iteration fewer does not meet the goal
+        _, it2, res2, conv2 = orc.cg(rp, ci, v, b, x0=x0, max_iters=it - 1,
+                                     reduction=red, mode=mode)
+        assert conv2 == 0 and res2[0] > red * base
+    # ImplicitResidualNorm stops on sqrt(r^T z), not on ||r||
+    _, it_i, _, conv_i = orc.cg(rp, ci, v, b, x0=x0, max_iters=2000, reduction=1e-8,
+                                mode=orc.IMPLICIT)
+    _, it_e, _, _ = orc.cg(rp, ci, v, b, x0=x0, max_iters=2000, reduction=1e-8, mode=0)
+    assert conv_i == 1 and it_i != it_e
