@@ -18,6 +18,8 @@ import torch
 from ._lib import call, lib
 
 _SFX = {torch.float64: "f64", torch.float32: "f32"}
+# B2S_VALUE_* codes of the mixed-type entry points
+_VT = {torch.float64: 0, torch.float32: 1}
 
 
 class CudaExecutor:
@@ -52,9 +54,13 @@ def _as2d(t: torch.Tensor):
 
 
 def _check_dense(t: torch.Tensor, rows: int, dtype, what: str):
+    """dtype None accepts FP64 and FP32 (mixed-precision operands)."""
     if not t.is_cuda:
         raise ValueError(f"{what} must be a CUDA tensor")
-    if t.dtype != dtype:
+    if dtype is None:
+        if t.dtype not in _SFX:
+            raise TypeError(f"{what} has dtype {t.dtype}, expected float64 or float32")
+    elif t.dtype != dtype:
         raise TypeError(f"{what} has dtype {t.dtype}, expected {dtype}")
     t2 = _as2d(t)
     if t2.shape[0] != rows:
@@ -77,7 +83,10 @@ class _SparseBase:
     dtype: torch.dtype
     shape: tuple
 
-    def _apply_args(self, args):
+    def _apply_args(self, args, mixed=False):
+        """(b, x, alpha, beta) as 2-D views; with mixed, b and x may each be
+        FP64 or FP32 (alpha then has the matrix type, beta the type of x, as
+        core/matrix/csr.cpp:301-311 converts them)."""
         if len(args) == 2:
             b, x = args
             alpha = beta = None
@@ -86,13 +95,16 @@ class _SparseBase:
         else:
             raise TypeError("apply(b, x) or apply(alpha, b, beta, x)")
         n, m = self.shape
-        b2 = _check_dense(b, m, self.dtype, "b")
-        x2 = _check_dense(x, n, self.dtype, "x")
+        b2 = _check_dense(b, m, None if mixed else self.dtype, "b")
+        x2 = _check_dense(x, n, None if mixed else self.dtype, "x")
         if b2.shape[1] != x2.shape[1]:
             raise ValueError("b and x have different numbers of columns")
         dev = x2.device
         return (b2, x2, _scalar(alpha, self.dtype, dev),
-                _scalar(beta, self.dtype, dev))
+                _scalar(beta, x2.dtype, dev))
+
+    def _uniform(self, b2, x2):
+        return b2.dtype == self.dtype and x2.dtype == self.dtype
 
 
 class Csr(_SparseBase):
@@ -154,7 +166,15 @@ class Csr(_SparseBase):
         return self._max_row_nnz
 
     def apply(self, *args):
-        b2, x2, alpha, beta = self._apply_args(args)
+        """x = A b or x = alpha A b + beta x; b and x may each be FP64 or
+        FP32 (mixed types run in the most precise of the three)."""
+        b2, x2, alpha, beta = self._apply_args(args, mixed=True)
+        if not self._uniform(b2, x2):
+            call("b2s_csr_spmv_mixed", _VT[self.dtype], _VT[b2.dtype], _VT[x2.dtype],
+                 self.shape[0], self.shape[1], _p(self.row_ptrs), _p(self.col_idxs),
+                 _p(self.values), self.max_row_nnz, _p(b2), b2.stride(0), _p(x2),
+                 x2.stride(0), x2.shape[1], _p(alpha), _p(beta), _stream(x2))
+            return args[-1]
         strat = 1 if self.strategy == "load_balance" else 0
         nt = 0 if self._tiles is None else self._tiles.numel() - 1
         call(f"b2s_csr_spmv_{_SFX[self.dtype]}", strat, self.shape[0],
@@ -228,7 +248,14 @@ class Ell(_SparseBase):
         self.dtype = values.dtype
 
     def apply(self, *args):
-        b2, x2, alpha, beta = self._apply_args(args)
+        """As Csr.apply: b and x may each be FP64 or FP32."""
+        b2, x2, alpha, beta = self._apply_args(args, mixed=True)
+        if not self._uniform(b2, x2):
+            call("b2s_ell_spmv_mixed", _VT[self.dtype], _VT[b2.dtype], _VT[x2.dtype],
+                 self.shape[0], self.shape[1], self.width, self.stride,
+                 _p(self.col_idxs), _p(self.values), _p(b2), b2.stride(0), _p(x2),
+                 x2.stride(0), x2.shape[1], _p(alpha), _p(beta), _stream(x2))
+            return args[-1]
         call(f"b2s_ell_spmv_{_SFX[self.dtype]}", self.shape[0], self.shape[1],
              self.width, self.stride, _p(self.col_idxs), _p(self.values),
              _p(b2), b2.stride(0), _p(x2), x2.stride(0), x2.shape[1],
@@ -254,12 +281,32 @@ class Sellp(_SparseBase):
         return int(self.values.numel())
 
     def apply(self, *args):
-        b2, x2, alpha, beta = self._apply_args(args)
+        """Operands of another type are converted to the matrix type and the
+        result back (precision_dispatch, core/matrix/sellp.cpp:150-180)."""
+        b2, x2, alpha, beta = self._apply_args(args, mixed=True)
+        bt, xt = b2, x2
+        if b2.dtype != self.dtype:
+            bt = _convert(b2, self.dtype)
+        if x2.dtype != self.dtype:
+            xt = _convert(x2, self.dtype) if beta is not None else \
+                torch.empty(x2.shape, dtype=self.dtype, device=x2.device)
+            beta = None if beta is None else beta.to(self.dtype)
         call(f"b2s_sellp_spmv_{_SFX[self.dtype]}", self.shape[0], self.shape[1],
              self.slice_size, _p(self.slice_sets), _p(self.slice_lengths),
-             _p(self.col_idxs), _p(self.values), _p(b2), b2.stride(0), _p(x2),
-             x2.stride(0), x2.shape[1], _p(alpha), _p(beta), _stream(x2))
+             _p(self.col_idxs), _p(self.values), _p(bt), bt.stride(0), _p(xt),
+             xt.stride(0), xt.shape[1], _p(alpha), _p(beta), _stream(xt))
+        if xt is not x2:
+            call("b2s_dense_convert", _VT[xt.dtype], _VT[x2.dtype], x2.shape[0], x2.shape[1],
+                 _p(xt), xt.stride(0), _p(x2), x2.stride(0), _stream(x2))
         return args[-1]
+
+
+def _convert(t, dtype):
+    """A contiguous copy of the 2-D block t in dtype, by the library."""
+    out = torch.empty(t.shape, dtype=dtype, device=t.device)
+    call("b2s_dense_convert", _VT[t.dtype], _VT[dtype], t.shape[0], t.shape[1],
+         _p(t), t.stride(0), _p(out), out.stride(0), _stream(t))
+    return out
 
 
 _HYBRID = {"column_limit": 0, "imbalance_limit": 1, "imbalance_bounded_limit": 2,

@@ -113,6 +113,42 @@ int b2s_sellp_spmv_f32(int64_t num_rows, int64_t num_cols, int64_t slice_size,
                        float* c, int64_t ldc, int64_t num_rhs,
                        const float* alpha, const float* beta, void* stream);
 
+/* Value type codes of the mixed-type entry points. */
+#define B2S_VALUE_F64 0
+#define B2S_VALUE_F32 1
+
+/* Csr and Ell SpMV with the matrix, b and c each FP64 or FP32 (type codes
+ * B2S_VALUE_*), computed in the most precise of the three; replaces the
+ * mixed instantiations of csr::spmv / csr::advanced_spmv and ell::spmv /
+ * ell::advanced_spmv (GKO_INSTANTIATE_FOR_EACH_MIXED_VALUE_AND_INDEX_TYPE,
+ * core/matrix/csr_kernels.hpp:29-42, core/matrix/ell_kernels.hpp:21-26;
+ * highest_precision arithmetic as in common/cuda_hip/matrix/
+ * csr_kernels.template.cpp:2109-2110).  alpha has the matrix type and beta
+ * the output type (core/matrix/csr.cpp:301-311); both or neither.  Csr rows
+ * are summed by a subwarp sized from max_row_nnz (any strategy); uniform
+ * types are accepted, but b2s_csr_spmv_f64/_f32 and b2s_ell_spmv_* are
+ * their tuned path. */
+int b2s_csr_spmv_mixed(int matrix_type, int input_type, int output_type,
+                       int64_t num_rows, int64_t num_cols, const int32_t* row_ptrs,
+                       const int32_t* col_idxs, const void* values,
+                       int64_t max_row_nnz, const void* b, int64_t ldb, void* c,
+                       int64_t ldc, int64_t num_rhs, const void* alpha,
+                       const void* beta, void* stream);
+int b2s_ell_spmv_mixed(int matrix_type, int input_type, int output_type,
+                       int64_t num_rows, int64_t num_cols, int64_t width, int64_t stride,
+                       const int32_t* col_idxs, const void* values, const void* b,
+                       int64_t ldb, void* c, int64_t ldc, int64_t num_rhs,
+                       const void* alpha, const void* beta, void* stream);
+
+/* dst = src converted between FP64 and FP32 (num_rows x num_cols,
+ * row-major with leading dimensions): the temporary conversions of
+ * make_temporary_conversion (include/ginkgo/core/base/
+ * precision_dispatch.hpp:43-83) for operands whose type differs from the
+ * operator's, e.g. Sellp, which computes in its own type only
+ * (core/matrix/sellp.cpp:150-180). */
+int b2s_dense_convert(int src_type, int dst_type, int64_t num_rows, int64_t num_cols,
+                      const void* src, int64_t lds, void* dst, int64_t ldd, void* stream);
+
 /* ------------------------------------------------------- conversions -- */
 
 /* Longest row; synchronises the stream and writes *result on the host.

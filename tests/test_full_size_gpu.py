@@ -1,0 +1,194 @@
+"""Parity at the benchmark sizes, against the oracle.
+
+- SpMV on the 4M-row power-law matrix (row lengths round(lognormal(2.5, 1))
+  clipped to [1, 4096], seed 0; about 80M entries, rows up to ~1.8k) in Csr
+  classical, Csr load_balance and Sellp (slices of 32), FP64 and FP32, with
+  1, 4 and 16 right-hand sides.  Ell is not applicable to this matrix: its
+  padded storage is n x (longest row) slots, tens of GB.
+- SpMV on the 7-point 128^3 matrix in FP32, every format, 1/4/16 columns.
+- The batched BiCGStab workload: 8192 ragged convection-diffusion systems
+  (n ~ U[32, 1024]), FP64 and FP32, relative tolerance 1e-8.
+- Mixed-precision IR-GMRES on the 27-point anisotropic 96^3 operator to a
+  relative residual of 1e-10, checked on the explicit FP64 residual.
+
+Tolerances: FP64 SpMV within 1e-14 of the FP64 oracle relative to the row's
+|A||x|, FP32 within 1e-5 of the FP64 oracle on the FP32-rounded inputs (the
+same scale); solvers by the residual their criterion promises.
+"""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from ginkgo_b200 import stencils
+from ginkgo_b200.matrix import Csr, CudaExecutor
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+TOL = {torch.float64: 1e-14, torch.float32: 1e-5}
+NP = {torch.float64: np.float64, torch.float32: np.float32}
+THREADS = os.cpu_count() or 8
+
+
+@pytest.fixture(scope="module")
+def exe():
+    return CudaExecutor.create(0)
+
+
+def par_spmv(rp, ci, v, x):
+    """FP64 y = A x with the oracle's threaded row loop."""
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.empty((len(rp) - 1,) + x.shape[1:], dtype=np.float64)
+    orc.csr_spmv_par(rp, ci, v, x, y, THREADS)
+    return y
+
+
+def check_rows(got, ref, scale, tol, what):
+    err = np.abs(got.astype(np.float64) - ref) / np.maximum(scale, np.finfo(np.float64).tiny)
+    worst = float(err.max())
+    assert worst <= tol, (what, worst)
+
+
+@pytest.fixture(scope="module")
+def matrix_b():
+    return stencils.power_law(4_000_000, seed=0, mu=2.5, sigma=1.0, max_len=4096)
+
+
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+@pytest.mark.parametrize("k", [1, 4, 16])
+def test_power_law_4m_all_formats(exe, matrix_b, dt, k):
+    rp, ci, v = matrix_b
+    n = len(rp) - 1
+    assert n == 4_000_000 and len(ci) > 75_000_000
+    vd = v.astype(NP[dt])
+    x = np.random.default_rng(100 + k).standard_normal((n, k)).astype(NP[dt])
+    ref = par_spmv(rp, ci, vd, x)
+    scale = par_spmv(rp, ci, np.abs(vd), np.abs(x))
+    A = Csr.read(exe, rp, ci, vd, dtype=dt)
+    xd = torch.from_numpy(x).cuda()
+    for fmt in ("classical", "load_balance", "sellp"):
+        op = A.convert_to_sellp(32, 1) if fmt == "sellp" else A.set_strategy(fmt)
+        y = torch.full((n, k), float("nan"), dtype=dt, device="cuda")
+        op.apply(xd, y)
+        check_rows(y.cpu().numpy(), ref, scale, TOL[dt], fmt)
+        del op, y
+    # Ell: n x (longest row) padded slots, not applicable to this matrix
+    width = orc.max_row_nnz(rp)
+    assert n * width * (vd.itemsize + 4) > 40e9
+
+
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+@pytest.mark.parametrize("k", [1, 4, 16])
+def test_poisson_128_all_formats(exe, dt, k):
+    rp, ci, v = stencils.poisson_3d_7pt(128)
+    n = len(rp) - 1
+    vd = v.astype(NP[dt])
+    x = np.random.default_rng(k).standard_normal((n, k)).astype(NP[dt])
+    ref = par_spmv(rp, ci, vd, x)
+    scale = par_spmv(rp, ci, np.abs(vd), np.abs(x))
+    A = Csr.read(exe, rp, ci, vd, dtype=dt)
+    xd = torch.from_numpy(x).cuda()
+    for fmt in ("classical", "load_balance", "ell", "sellp"):
+        if fmt == "ell":
+            op = A.convert_to_ell()
+        elif fmt == "sellp":
+            op = A.convert_to_sellp(32, 1)
+        else:
+            op = A.set_strategy(fmt)
+        y = torch.full((n, k), float("nan"), dtype=dt, device="cuda")
+        op.apply(xd, y)
+        check_rows(y.cpu().numpy(), ref, scale, TOL[dt], fmt)
+
+
+def _block_diagonal(systems):
+    """One Csr of all systems on the diagonal (for checking residuals)."""
+    rps, cis, vs = [], [], []
+    row0, nnz0 = 0, 0
+    for rp, ci, v in systems:
+        rp = np.asarray(rp, np.int64)
+        rps.append(rp[:-1] + nnz0)
+        cis.append(np.asarray(ci, np.int64) + row0)
+        vs.append(np.asarray(v, np.float64))
+        row0 += len(rp) - 1
+        nnz0 += int(rp[-1])
+    rp = np.concatenate(rps + [np.array([nnz0])]).astype(np.int32)
+    return rp, np.concatenate(cis).astype(np.int32), np.concatenate(vs)
+
+
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+def test_batch_8192_systems(exe, dt):
+    from ginkgo_b200.batch import BatchBicgstab, convection_diffusion_batch
+    A, systems = convection_diffusion_batch(exe, 8192, lo=32, hi=1024, seed=3, dtype=dt)
+    b = np.random.default_rng(3).standard_normal(A.total_rows)
+    bd = torch.from_numpy(b).to(dt).cuda()
+    s = (BatchBicgstab.build().with_max_iterations(500).with_tolerance(1e-8)
+         .with_tolerance_type("relative").with_preconditioner("jacobi").on(exe).generate(A))
+    x = torch.zeros_like(bd)
+    s.tune(bd, x)        # autotunes (and solves); the next solve reuses the table
+    x.zero_()
+    s.apply(bd, x)
+    it = s.logger.iterations.cpu().numpy()
+    res = s.logger.residual_norms.cpu().numpy()
+    offs = A.host_row_offsets
+    bq = b.astype(NP[dt]).astype(np.float64)
+    bnorm = np.sqrt(np.add.reduceat(bq ** 2, offs[:-1]))
+    # every system stopped by the residual criterion on its logged residual
+    assert np.all(it < 500), int(it.max())
+    assert np.all(res <= 1e-8 * bnorm * (1 + 1e-6)), float((res / bnorm).max())
+    # the explicit FP64 residual of every system
+    rp, ci, v = _block_diagonal([(r, c, w.astype(NP[dt])) for r, c, w in systems])
+    xg = x.cpu().numpy().astype(np.float64)
+    r = bq - par_spmv(rp, ci, v, xg)
+    rel = np.sqrt(np.add.reduceat(r ** 2, offs[:-1])) / bnorm
+    assert rel.max() <= (1.5e-8 if dt == torch.float64 else 2e-5), float(rel.max())
+    # the oracle's reference algorithm on a seeded sample of 256 systems
+    sample = np.random.default_rng(8).choice(A.num_systems, 256, replace=False)
+    npdt = NP[dt]
+    for i in sample:
+        o, e = offs[i], offs[i + 1]
+        srp, sci, sv = systems[i]
+        w, st, eci, ev = orc.csr_to_ell(srp, sci, sv.astype(npdt))
+        _, it_o, _, conv_o = orc.batch_bicgstab_ell(e - o, w, st, eci, ev,
+                                                    b[o:e].astype(npdt),
+                                                    max_iters=500, tol=1e-8)
+        assert conv_o
+        assert abs(int(it[i]) - it_o) <= max(3, 0.3 * it_o), (i, it[i], it_o)
+
+
+def test_ir_gmres_96_cubed_reaches_fp64_accuracy(exe):
+    from ginkgo_b200.solver import Gmres, Ir, Iteration, Jacobi, ResidualNorm
+    rp, ci, v = stencils.anisotropic_27pt(96)
+    n = len(rp) - 1
+    assert n == 884_736
+    b = np.random.default_rng(3).standard_normal(n)
+    A = Csr.read(exe, rp, ci, v)
+    crit = (Iteration.build().with_max_iters(20000),
+            ResidualNorm.build().with_reduction_factor(1e-10))
+    jac = Jacobi.build().with_max_block_size(1)
+    variants = {
+        "f64": Gmres.build().with_krylov_dim(30).with_criteria(*crit).with_preconditioner(jac),
+        "ir_f32": Ir.build().with_criteria(*crit).with_solver(
+            Gmres.build().with_krylov_dim(30).with_storage_precision("f32")
+            .with_preconditioner(jac)),
+        "ir_bf16": Ir.build().with_criteria(*crit).with_solver(
+            Gmres.build().with_krylov_dim(30).with_storage_precision("bf16")
+            .with_preconditioner(jac)),
+    }
+    xs = {}
+    bn = np.linalg.norm(b)
+    for name, f in variants.items():
+        s = f.on(exe).generate(A)
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        s.apply(torch.from_numpy(b).cuda(), x)
+        assert s.logger.has_converged, name
+        xs[name] = x.cpu().numpy()
+        rel = np.linalg.norm(b - par_spmv(rp, ci, v, xs[name])) / bn
+        assert rel <= 1e-10, (name, rel)
+    # the low-precision variants against the FP64 GPU solution (both within
+    # the 1e-10 residual; the error is bounded by the conditioning)
+    for name in ("ir_f32", "ir_bf16"):
+        err = np.linalg.norm(xs[name] - xs["f64"]) / np.linalg.norm(xs["f64"])
+        assert err <= 1e-7, (name, err)

@@ -233,3 +233,55 @@ def test_poisson_128_full_size_fp64(exe):
             y = torch.empty((n, k), dtype=torch.float64, device="cuda")
             op.apply(xd, y)
             assert_spmv_close(rp, ci, v, x, y.cpu().numpy(), ref, 1e-14)
+
+
+MIXED = [(m, i, o) for m in (torch.float64, torch.float32)
+         for i in (torch.float64, torch.float32) for o in (torch.float64, torch.float32)]
+
+
+def _mixed_tol(m, i, o):
+    # arithmetic in the most precise type; one rounding to the output type
+    if o == torch.float64:
+        return 1e-14  # FP64 arithmetic, FP64 result
+    return 1e-6 if torch.float64 in (m, i) else 1e-5
+
+
+@pytest.mark.parametrize("fmt", FORMATS)
+@pytest.mark.parametrize("m,i,o", MIXED, ids=lambda t: str(t).split(".")[-1])
+@pytest.mark.parametrize("k", [1, 3, 20])
+def test_mixed_value_types_match_oracle(exe, fmt, m, i, o, k):
+    """Matrix, b and x each FP64 or FP32 (Csr and Ell compute in the most
+    precise type; Sellp converts the operands to its own type)."""
+    rng = np.random.default_rng(31 + k)
+    rp, ci, v = stencils.power_law(6000, seed=13, mu=2.0, sigma=1.0, max_len=600)
+    n = len(rp) - 1
+    vm = v.astype(NP[m])
+    x = rng.standard_normal((n, k)).astype(NP[i])
+    y0 = rng.standard_normal((n, k)).astype(NP[o])
+    A = Csr.read(exe, rp, ci, vm, dtype=m)
+    op = formats(A, fmt)
+    # what the operator computes from: Sellp rounds b and x to its own type
+    xs = x.astype(NP[m]) if fmt == "sellp" else x
+    ref = orc.csr_spmv(rp, ci, vm.astype(np.float64), xs.astype(np.float64))
+    tol = _mixed_tol(m, i, o)
+    if fmt == "sellp":
+        tol = TOL[m] if o == torch.float64 or m == torch.float32 else 1e-6
+    y = torch.full((n, k), float("nan"), dtype=o, device="cuda")
+    op.apply(torch.from_numpy(x).cuda(), y)
+    assert_spmv_close(rp, ci, vm, xs, y.cpu().numpy(), ref, max(tol, 1e-14))
+    # advanced: alpha in the matrix type, beta in the output type
+    y0s = y0.astype(NP[m]) if fmt == "sellp" else y0
+    ref2 = 0.75 * ref - 1.25 * y0s.astype(np.float64)
+    y2 = torch.from_numpy(y0.copy()).cuda()
+    op.apply(0.75, torch.from_numpy(x).cuda(), -1.25, y2)
+    assert_spmv_close(rp, ci, vm, xs, y2.cpu().numpy(), ref2, max(tol, 1e-14) * 4,
+                      alpha=0.75, beta_y=1.25 * y0s.astype(np.float64))
+
+
+def test_dense_convert_round_trip(exe):
+    from ginkgo_b200.matrix import _convert
+    x = torch.randn(1000, 5, dtype=torch.float64, device="cuda")[:, :3]
+    f = _convert(x, torch.float32)
+    assert f.dtype == torch.float32 and torch.equal(f, x.float())
+    d = _convert(f, torch.float64)
+    assert torch.equal(d, x.float().double())
