@@ -167,7 +167,13 @@ class Csr(_SparseBase):
 
     def apply(self, *args):
         """x = A b or x = alpha A b + beta x; b and x may each be FP64 or
-        FP32 (mixed types run in the most precise of the three)."""
+        FP32 (mixed types run in the most precise of the three).  As in the
+        reference (core/matrix/csr.cpp:257-314): with b a Csr matrix and x a
+        Csr, x = A b (SpGEMM) or x = alpha A b + beta x; with b an Identity,
+        x = alpha A + beta x (SpGEAM).  x's arrays are replaced."""
+        b = args[1] if len(args) == 4 else args[0]
+        if isinstance(b, (Csr, Identity)):
+            return self._apply_sparse(args)
         b2, x2, alpha, beta = self._apply_args(args, mixed=True)
         if not self._uniform(b2, x2):
             call("b2s_csr_spmv_mixed", _VT[self.dtype], _VT[b2.dtype], _VT[x2.dtype],
@@ -183,6 +189,51 @@ class Csr(_SparseBase):
              _p(self._tiles), nt, _p(b2), b2.stride(0), _p(x2), x2.stride(0),
              x2.shape[1], _p(alpha), _p(beta), _stream(x2))
         return args[-1]
+
+    def _apply_sparse(self, args):
+        if len(args) == 2:
+            b, x = args
+            if isinstance(b, Identity):
+                raise TypeError("A.apply(Identity, x): use apply(alpha, Identity, beta, x)")
+            x._replace(spgemm(self, b))
+        else:
+            alpha, b, beta, x = args
+            if not isinstance(x, Csr):
+                raise TypeError("the result of a sparse product is a Csr matrix")
+            if isinstance(b, Identity):
+                x._replace(spgeam(alpha, self, beta, x))
+            else:
+                x._replace(spgemm(self, b, alpha=alpha, beta=beta, d=x))
+        return args[-1]
+
+    def _replace(self, other):
+        """Takes other's arrays (the result of a sparse product)."""
+        self.shape, self.row_ptrs, self.col_idxs = other.shape, other.row_ptrs, other.col_idxs
+        self.values, self.dtype, self.nnz = other.values, other.dtype, other.nnz
+        self._max_row_nnz, self._tiles = None, None
+        self.set_strategy(self.strategy)
+
+    def convert_to_hybrid(self, strategy="automatic", **params):
+        """Csr -> Hybrid with one of the reference's width strategies
+        (hybrid_config): the Ell width and Coo size are set up on the host,
+        the scatter runs on the device (b2s_csr_convert_to_hybrid_*)."""
+        rp = self.row_ptrs.cpu().numpy().astype(np.int64)
+        width, coo = hybrid_config(np.diff(rp), strategy,
+                                   value_bytes=self.values.element_size(), **params)
+        n = self.shape[0]
+        dev = self.values.device
+        ell_ci = torch.empty(max(width * n, 1), dtype=torch.int32, device=dev)
+        ell_v = torch.empty(max(width * n, 1), dtype=self.dtype, device=dev)
+        coo_r = torch.empty(max(coo, 1), dtype=torch.int32, device=dev)
+        coo_c = torch.empty(max(coo, 1), dtype=torch.int32, device=dev)
+        coo_v = torch.empty(max(coo, 1), dtype=self.dtype, device=dev)
+        wsb = lib().b2s_hybrid_convert_workspace_bytes(n)
+        ws = torch.empty(max(wsb, 8), dtype=torch.uint8, device=dev)
+        call(f"b2s_csr_convert_to_hybrid_{_SFX[self.dtype]}", n, _p(self.row_ptrs),
+             _p(self.col_idxs), _p(self.values), width, n, _p(ell_ci), _p(ell_v), coo,
+             _p(coo_r), _p(coo_c), _p(coo_v), _p(ws), wsb, _stream(ell_v))
+        return Hybrid(self.exec, self.shape, width, n, ell_ci[:width * n], ell_v[:width * n],
+                      coo_r[:coo], coo_c[:coo], coo_v[:coo])
 
     def convert_to_precision(self, dtype):
         return Csr(self.exec, self.shape, self.row_ptrs, self.col_idxs,
@@ -299,6 +350,128 @@ class Sellp(_SparseBase):
             call("b2s_dense_convert", _VT[xt.dtype], _VT[x2.dtype], x2.shape[0], x2.shape[1],
                  _p(xt), xt.stride(0), _p(x2), x2.stride(0), _stream(x2))
         return args[-1]
+
+
+class Identity:
+    """matrix::Identity of size n: A.apply(alpha, Identity(n), beta, C)
+    computes C = alpha A + beta C (SpGEAM), as the reference does."""
+
+    def __init__(self, n):
+        self.shape = (int(n), int(n))
+
+
+def _dev_scalar(v, dtype, device):
+    if v is None:
+        return None
+    return _scalar(v, dtype, device)
+
+
+def spgemm(a: Csr, b: Csr, alpha=None, beta=None, d: Csr = None) -> Csr:
+    """C = A B, or C = alpha A B + beta D (csr::spgemm / advanced_spgemm):
+    bit-exact with the reference executor, columns ascending."""
+    if a.shape[1] != b.shape[0]:
+        raise ValueError("A's columns and B's rows differ (DimensionMismatch)")
+    if a.dtype != b.dtype or (d is not None and d.dtype != a.dtype):
+        raise TypeError("SpGEMM operands must share one value type")
+    if (d is None) != (beta is None):
+        raise ValueError("D and beta go together")
+    if d is not None and d.shape != (a.shape[0], b.shape[1]):
+        raise ValueError("D has the wrong shape (DimensionMismatch)")
+    n, m = a.shape[0], b.shape[1]
+    dev = a.values.device
+    wsb = lib().b2s_csr_spgemm_workspace_bytes(n, m)
+    ws = torch.empty(max(wsb, 8), dtype=torch.uint8, device=dev)
+    rp = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    nnz = C.c_int64(0)
+    st = _stream(a.values)
+    call("b2s_csr_spgemm_symbolic", n, m, _p(a.row_ptrs), _p(a.col_idxs), _p(b.row_ptrs),
+         _p(b.col_idxs), _p(d.row_ptrs) if d is not None else None,
+         _p(d.col_idxs) if d is not None else None, _p(rp), C.byref(nnz), _p(ws), wsb, st)
+    k = int(nnz.value)
+    ci = torch.empty(max(k, 1), dtype=torch.int32, device=dev)
+    v = torch.empty(max(k, 1), dtype=a.dtype, device=dev)
+    al = _dev_scalar(alpha, a.dtype, dev)
+    be = _dev_scalar(beta, a.dtype, dev)
+    call(f"b2s_csr_spgemm_numeric_{_SFX[a.dtype]}", n, m, _p(al), _p(a.row_ptrs),
+         _p(a.col_idxs), _p(a.values), _p(b.row_ptrs), _p(b.col_idxs), _p(b.values), _p(be),
+         _p(d.row_ptrs) if d is not None else None, _p(d.col_idxs) if d is not None else None,
+         _p(d.values) if d is not None else None, _p(rp), _p(ci), _p(v), _p(ws), wsb, st)
+    return Csr(a.exec, (n, m), rp, ci[:k], v[:k], a.strategy)
+
+
+def spgeam(alpha, a: Csr, beta, b: Csr) -> Csr:
+    """C = alpha A + beta B (csr::spgeam) for matrices with ascending
+    columns: bit-exact with the reference executor."""
+    if a.shape != b.shape:
+        raise ValueError("A and B differ in shape (DimensionMismatch)")
+    if a.dtype != b.dtype:
+        raise TypeError("SpGEAM operands must share one value type")
+    n = a.shape[0]
+    dev = a.values.device
+    wsb = lib().b2s_csr_spgeam_workspace_bytes(n)
+    ws = torch.empty(max(wsb, 8), dtype=torch.uint8, device=dev)
+    rp = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    nnz = C.c_int64(0)
+    st = _stream(a.values)
+    call("b2s_csr_spgeam_symbolic", n, _p(a.row_ptrs), _p(a.col_idxs), _p(b.row_ptrs),
+         _p(b.col_idxs), _p(rp), C.byref(nnz), _p(ws), wsb, st)
+    k = int(nnz.value)
+    ci = torch.empty(max(k, 1), dtype=torch.int32, device=dev)
+    v = torch.empty(max(k, 1), dtype=a.dtype, device=dev)
+    al = _dev_scalar(alpha, a.dtype, dev)
+    be = _dev_scalar(beta, a.dtype, dev)
+    call(f"b2s_csr_spgeam_numeric_{_SFX[a.dtype]}", n, _p(al), _p(a.row_ptrs),
+         _p(a.col_idxs), _p(a.values), _p(be), _p(b.row_ptrs), _p(b.col_idxs),
+         _p(b.values), _p(rp), _p(ci), _p(v), st)
+    return Csr(a.exec, a.shape, rp, ci[:k], v[:k], a.strategy)
+
+
+class Hybrid(_SparseBase):
+    """matrix::Hybrid (include/ginkgo/core/matrix/hybrid.hpp): an Ell part
+    of `width` entries per row (column-major, stride >= rows, padding column
+    -1) and a Coo part, sorted by row, with the rest of every longer row."""
+
+    def __init__(self, exec_, shape, width, stride, ell_col_idxs, ell_values,
+                 coo_row_idxs, coo_col_idxs, coo_values):
+        self.exec = exec_
+        self.shape = tuple(shape)
+        self.width, self.stride = int(width), int(stride)
+        self.ell_col_idxs, self.ell_values = ell_col_idxs, ell_values
+        self.coo_row_idxs, self.coo_col_idxs = coo_row_idxs, coo_col_idxs
+        self.coo_values = coo_values
+        self.dtype = ell_values.dtype
+
+    @property
+    def coo_nnz(self):
+        return int(self.coo_values.numel())
+
+    def apply(self, *args):
+        b2, x2, alpha, beta = self._apply_args(args)
+        call(f"b2s_hybrid_spmv_{_SFX[self.dtype]}", self.shape[0], self.shape[1],
+             self.width, self.stride, _p(self.ell_col_idxs), _p(self.ell_values),
+             self.coo_nnz, _p(self.coo_row_idxs), _p(self.coo_col_idxs),
+             _p(self.coo_values), _p(b2), b2.stride(0), _p(x2), x2.stride(0), x2.shape[1],
+             _p(alpha), _p(beta), _stream(x2))
+        return args[-1]
+
+    def convert_to_csr(self) -> Csr:
+        n = self.shape[0]
+        dev = self.ell_values.device
+        wsb = lib().b2s_hybrid_convert_workspace_bytes(n)
+        ws = torch.empty(max(wsb, 8), dtype=torch.uint8, device=dev)
+        rp = torch.empty(n + 1, dtype=torch.int32, device=dev)
+        nnz = C.c_int64(0)
+        st = _stream(self.ell_values)
+        call("b2s_hybrid_csr_row_ptrs", n, self.width, self.stride, _p(self.ell_col_idxs),
+             self.coo_nnz, _p(self.coo_row_idxs), _p(rp), C.byref(nnz), _p(ws), wsb, st)
+        k = int(nnz.value)
+        ci = torch.empty(max(k, 1), dtype=torch.int32, device=dev)
+        v = torch.empty(max(k, 1), dtype=self.dtype, device=dev)
+        call(f"b2s_hybrid_convert_to_csr_{_SFX[self.dtype]}", n, self.width, self.stride,
+             _p(self.ell_col_idxs), _p(self.ell_values), self.coo_nnz,
+             _p(self.coo_row_idxs), _p(self.coo_col_idxs), _p(self.coo_values), _p(rp),
+             _p(ci), _p(v), st)
+        return Csr(self.exec, self.shape, rp, ci[:k], v[:k])
 
 
 def _convert(t, dtype):

@@ -665,6 +665,132 @@ int b2s_batch_ell_bicgstab_tune_f32(
     void* workspace, int64_t workspace_bytes, int32_t* iterations,
     double* residual_norms, int32_t* tune_table_out, void* stream);
 
+/* ------------------------------------------ sparse products and sums -- */
+
+/* C = A B (csr::spgemm, core/matrix/csr_kernels.hpp:72-76) and
+ * C = alpha A B + beta D (csr::advanced_spgemm, :78-86), A num_rows x k,
+ * B k x num_cols, int32 indices, in two calls because the caller owns C:
+ * the symbolic call writes C's row pointers (num_rows + 1 entries) and its
+ * entry count to *c_nnz (host); the caller allocates c_nnz columns and
+ * values; the numeric call fills them.  D (and beta) are null for the plain
+ * product; d_row_ptrs/d_col_idxs must then be null in the symbolic call too.
+ * alpha and beta are device scalars (alpha may be null: 1).  Results are
+ * bit-exact with the reference executor (reference/matrix/csr_kernels.cpp:
+ * 199-300): columns ascending, each entry accumulated as beta d, then
+ * + (alpha a_ik) b_kj over A's row in storage order, without fused
+ * multiply-adds.  B's rows must not repeat a column.  Workspace:
+ * b2s_csr_spgemm_workspace_bytes, the same for both calls. */
+int64_t b2s_csr_spgemm_workspace_bytes(int64_t num_rows, int64_t num_cols);
+int b2s_csr_spgemm_symbolic(int64_t num_rows, int64_t num_cols, const int32_t* a_row_ptrs,
+                            const int32_t* a_col_idxs, const int32_t* b_row_ptrs,
+                            const int32_t* b_col_idxs, const int32_t* d_row_ptrs,
+                            const int32_t* d_col_idxs, int32_t* c_row_ptrs, int64_t* c_nnz,
+                            void* workspace, int64_t workspace_bytes, void* stream);
+int b2s_csr_spgemm_numeric_f64(int64_t num_rows, int64_t num_cols, const double* alpha,
+                               const int32_t* a_row_ptrs, const int32_t* a_col_idxs,
+                               const double* a_values, const int32_t* b_row_ptrs,
+                               const int32_t* b_col_idxs, const double* b_values,
+                               const double* beta, const int32_t* d_row_ptrs,
+                               const int32_t* d_col_idxs, const double* d_values,
+                               const int32_t* c_row_ptrs, int32_t* c_col_idxs,
+                               double* c_values, void* workspace, int64_t workspace_bytes,
+                               void* stream);
+int b2s_csr_spgemm_numeric_f32(int64_t num_rows, int64_t num_cols, const float* alpha,
+                               const int32_t* a_row_ptrs, const int32_t* a_col_idxs,
+                               const float* a_values, const int32_t* b_row_ptrs,
+                               const int32_t* b_col_idxs, const float* b_values,
+                               const float* beta, const int32_t* d_row_ptrs,
+                               const int32_t* d_col_idxs, const float* d_values,
+                               const int32_t* c_row_ptrs, int32_t* c_col_idxs,
+                               float* c_values, void* workspace, int64_t workspace_bytes,
+                               void* stream);
+
+/* C = alpha A + beta B for matrices with ascending columns in every row
+ * (csr::spgeam, core/matrix/csr_kernels.hpp:88-93; reference/matrix/
+ * csr_kernels.cpp:424-470): symbolic (C's row pointers, *c_nnz on the host)
+ * then numeric; every column of either operand is stored, entries
+ * alpha * a + beta * b with a missing side read as zero, bit-exact.
+ * alpha, beta: device scalars. */
+int64_t b2s_csr_spgeam_workspace_bytes(int64_t num_rows);
+int b2s_csr_spgeam_symbolic(int64_t num_rows, const int32_t* a_row_ptrs,
+                            const int32_t* a_col_idxs, const int32_t* b_row_ptrs,
+                            const int32_t* b_col_idxs, int32_t* c_row_ptrs, int64_t* c_nnz,
+                            void* workspace, int64_t workspace_bytes, void* stream);
+int b2s_csr_spgeam_numeric_f64(int64_t num_rows, const double* alpha,
+                               const int32_t* a_row_ptrs, const int32_t* a_col_idxs,
+                               const double* a_values, const double* beta,
+                               const int32_t* b_row_ptrs, const int32_t* b_col_idxs,
+                               const double* b_values, const int32_t* c_row_ptrs,
+                               int32_t* c_col_idxs, double* c_values, void* stream);
+int b2s_csr_spgeam_numeric_f32(int64_t num_rows, const float* alpha,
+                               const int32_t* a_row_ptrs, const int32_t* a_col_idxs,
+                               const float* a_values, const float* beta,
+                               const int32_t* b_row_ptrs, const int32_t* b_col_idxs,
+                               const float* b_values, const int32_t* c_row_ptrs,
+                               int32_t* c_col_idxs, float* c_values, void* stream);
+
+/* ------------------------------------------------------------- Hybrid -- */
+
+/* Csr -> Hybrid (csr::convert_to_hybrid, core/matrix/csr_kernels.hpp:
+ * 106-110): the first ell_width entries of every row into the Ell part
+ * (column-major, ell_stride >= num_rows, padding column -1 and value 0),
+ * the rest into the Coo part in row order (coo_nnz entries, from
+ * b2s_hybrid_config; a mismatch is B2S_ERR_INVALID_ARG).  Bit-exact. */
+int64_t b2s_hybrid_convert_workspace_bytes(int64_t num_rows);
+int b2s_csr_convert_to_hybrid_f64(int64_t num_rows, const int32_t* row_ptrs,
+                                  const int32_t* col_idxs, const double* values,
+                                  int64_t ell_width, int64_t ell_stride,
+                                  int32_t* ell_col_idxs, double* ell_values, int64_t coo_nnz,
+                                  int32_t* coo_row_idxs, int32_t* coo_col_idxs,
+                                  double* coo_values, void* workspace,
+                                  int64_t workspace_bytes, void* stream);
+int b2s_csr_convert_to_hybrid_f32(int64_t num_rows, const int32_t* row_ptrs,
+                                  const int32_t* col_idxs, const float* values,
+                                  int64_t ell_width, int64_t ell_stride,
+                                  int32_t* ell_col_idxs, float* ell_values, int64_t coo_nnz,
+                                  int32_t* coo_row_idxs, int32_t* coo_col_idxs,
+                                  float* coo_values, void* workspace,
+                                  int64_t workspace_bytes, void* stream);
+
+/* Hybrid SpMV (hybrid::spmv / advanced_spmv, core/matrix/hybrid_kernels.hpp:
+ * the Ell part then the Coo part): per row, the Ell slots in order, then the
+ * row's Coo entries in order (the Coo part sorted by row), c = A b or
+ * alpha A b + beta c (beta == 0 ignores c). */
+int b2s_hybrid_spmv_f64(int64_t num_rows, int64_t num_cols, int64_t ell_width,
+                        int64_t ell_stride, const int32_t* ell_col_idxs,
+                        const double* ell_values, int64_t coo_nnz,
+                        const int32_t* coo_row_idxs, const int32_t* coo_col_idxs,
+                        const double* coo_values, const double* b, int64_t ldb, double* c,
+                        int64_t ldc, int64_t num_rhs, const double* alpha, const double* beta,
+                        void* stream);
+int b2s_hybrid_spmv_f32(int64_t num_rows, int64_t num_cols, int64_t ell_width,
+                        int64_t ell_stride, const int32_t* ell_col_idxs,
+                        const float* ell_values, int64_t coo_nnz,
+                        const int32_t* coo_row_idxs, const int32_t* coo_col_idxs,
+                        const float* coo_values, const float* b, int64_t ldb, float* c,
+                        int64_t ldc, int64_t num_rhs, const float* alpha, const float* beta,
+                        void* stream);
+
+/* Hybrid -> Csr (Hybrid::convert_to(Csr), core/matrix/hybrid.cpp): row
+ * pointers and the entry count (host) first, then the row's Ell entries
+ * and Coo entries, columns sorted (stable). */
+int b2s_hybrid_csr_row_ptrs(int64_t num_rows, int64_t ell_width, int64_t ell_stride,
+                            const int32_t* ell_col_idxs, int64_t coo_nnz,
+                            const int32_t* coo_row_idxs, int32_t* row_ptrs, int64_t* nnz,
+                            void* workspace, int64_t workspace_bytes, void* stream);
+int b2s_hybrid_convert_to_csr_f64(int64_t num_rows, int64_t ell_width, int64_t ell_stride,
+                                  const int32_t* ell_col_idxs, const double* ell_values,
+                                  int64_t coo_nnz, const int32_t* coo_row_idxs,
+                                  const int32_t* coo_col_idxs, const double* coo_values,
+                                  const int32_t* row_ptrs, int32_t* col_idxs, double* values,
+                                  void* stream);
+int b2s_hybrid_convert_to_csr_f32(int64_t num_rows, int64_t ell_width, int64_t ell_stride,
+                                  const int32_t* ell_col_idxs, const float* ell_values,
+                                  int64_t coo_nnz, const int32_t* coo_row_idxs,
+                                  const int32_t* coo_col_idxs, const float* coo_values,
+                                  const int32_t* row_ptrs, int32_t* col_idxs, float* values,
+                                  void* stream);
+
 /* ------------------------------------------------------- Hybrid set-up -- */
 /* Ell width and Coo entry count of a Hybrid matrix (Ell + Coo) from its row
  * lengths, a HOST array, as the strategy classes compute them on the host
