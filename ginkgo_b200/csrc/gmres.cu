@@ -46,6 +46,7 @@
 // The serial parts (Givens chain, back substitution, (2I - G) h1) run in
 // the last block on shared-memory copies of the small arrays.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include "csr_async.cuh"
 #include "ell_rows.cuh"
@@ -76,16 +77,86 @@ struct GmresState {
     unsigned gticket[kDotsMaxGroups + 1];  // dots: per group of 32 blocks
     double bnorm, rnorm, reduction, inner_reduction, inner_thresh;
     double base;  // ||b||, ||r_0|| or 1, by the baseline, set at the first restart
+    double qscale;  // scaled bases: factor from the formed vector to its storage
     double sigma[kLd];  // stored basis vector i is v_i / sigma[i] (unnormalised)
     double minus_one, one;       // alpha, beta of r = b - A x
     double h[kLd];               // combined projection coefficients of step j
     double g[kLd], cs[kMaxKrylov], sn[kMaxKrylov], y[kMaxKrylov];
 };
 
+// Bases stored scaled (CB-GMRES reduce2 and the scaled-integer formats of
+// core/solver/cb_gmres.cpp:100-157): the next vector is formed in the
+// arithmetic type first and written by a second pass once its norm and
+// largest entry are known.  Half stores the normalised vector; an integer
+// type stores trunc(v / s) with s = (max|v| / ||v||) * 2 / INT_MAX, one
+// scale per vector (core/solver/cb_gmres_accessor.hpp), so that the stored
+// vector read as a number times sigma is the normalised one.
+template <typename TB>
+struct BasisKind {
+    static constexpr bool kScaled = false;
+    static constexpr double kIntMax = 0.0;
+};
+template <>
+struct BasisKind<__half> {
+    static constexpr bool kScaled = true;
+    static constexpr double kIntMax = 0.0;
+};
+template <>
+struct BasisKind<int64_t> {
+    static constexpr bool kScaled = true;
+    static constexpr double kIntMax = 9223372036854775807.0;
+};
+template <>
+struct BasisKind<int32_t> {
+    static constexpr bool kScaled = true;
+    static constexpr double kIntMax = 2147483647.0;
+};
+template <>
+struct BasisKind<int16_t> {
+    static constexpr bool kScaled = true;
+    static constexpr double kIntMax = 32767.0;
+};
+
+// Storage scale and sigma of a scaled basis vector of norm nrm and largest
+// entry mx: stored = formed * qscale, normalised = stored * sigma.
+template <typename TB>
+__device__ __forceinline__ void basis_scales(double nrm, double mx, double* qscale,
+                                             double* sigma)
+{
+    constexpr double kMax = BasisKind<TB>::kIntMax;
+    if constexpr (kMax == 0.0) {
+        *qscale = nrm > 0.0 ? 1.0 / nrm : 0.0;
+        *sigma = 1.0;
+    } else {
+        *qscale = mx > 0.0 ? kMax / (2.0 * mx) : 0.0;
+        *sigma = nrm > 0.0 ? 2.0 * mx / (nrm * kMax) : 0.0;
+    }
+}
+
 template <typename TB, typename TA>
 __device__ __forceinline__ TB to_basis(TA v)
 {
     return TB(v);
+}
+template <>
+__device__ __forceinline__ __half to_basis<__half, double>(double v)
+{
+    return __double2half(v);
+}
+template <>
+__device__ __forceinline__ int64_t to_basis<int64_t, double>(double v)
+{
+    return __double2ll_rz(v);
+}
+template <>
+__device__ __forceinline__ int32_t to_basis<int32_t, double>(double v)
+{
+    return __double2int_rz(v);
+}
+template <>
+__device__ __forceinline__ int16_t to_basis<int16_t, double>(double v)
+{
+    return int16_t(__double2int_rz(v));
 }
 template <>
 __device__ __forceinline__ __nv_bfloat16 to_basis<__nv_bfloat16, float>(float v)
@@ -96,6 +167,11 @@ template <typename TA, typename TB>
 __device__ __forceinline__ TA from_basis(TB v)
 {
     return TA(v);
+}
+template <>
+__device__ __forceinline__ double from_basis<double, __half>(__half v)
+{
+    return double(__half2float(v));
 }
 template <>
 __device__ __forceinline__ float from_basis<float, __nv_bfloat16>(__nv_bfloat16 v)
@@ -482,9 +558,11 @@ __global__ void __launch_bounds__(kSolverBlock)
     gmres_update_kernel(int64_t n, int64_t ldv, TB* __restrict__ V,
                         const TA* __restrict__ w, const TA* __restrict__ dinv,
                         TA* __restrict__ y, GmresState* st,
-                        double* __restrict__ partials, double* __restrict__ Hm)
+                        double* __restrict__ partials, double* __restrict__ Hm,
+                        TA* __restrict__ wq)
 {
     constexpr int R = rows_per_group<TB>();
+    constexpr bool kQ = BasisKind<TB>::kScaled;
     __shared__ double red[kSolverBlock / kWarp];
     __shared__ double tot[1];
     __shared__ TA hs[kLd];
@@ -495,7 +573,7 @@ __global__ void __launch_bounds__(kSolverBlock)
     const TA sj = TA(st->sigma[j]);
     __syncthreads();
     TB* vnext = V + int64_t(j + 1) * ldv;
-    double nrm = 0.0;
+    double nrm = 0.0, mx = 0.0;
     auto group = [&](int64_t r0, int valid) {
         TA wr[R];
         load_rows<TA, R>(w + r0, wr, valid);
@@ -510,30 +588,84 @@ __global__ void __launch_bounds__(kSolverBlock)
 #pragma unroll
             for (int r = 0; r < R; ++r) wr[r] -= hi * x[r];
         }
-        TB vb[R];
-        TA yv[R];
-        TA d[R];
-        if (dinv) load_rows<TA, R>(dinv + r0, d, valid);
+        if constexpr (kQ) {
+            // formed here, stored scaled by gmres_quantize_kernel
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            vb[r] = to_basis<TB>(wr[r]);
-            const TA va = from_basis<TA>(vb[r]);
-            yv[r] = dinv ? d[r] * va : va;
-            nrm += double(wr[r]) * double(wr[r]);
+            for (int r = 0; r < R; ++r) {
+                nrm += double(wr[r]) * double(wr[r]);
+                mx = fmax(mx, fabs(double(wr[r])));
+            }
+            store_rows<TA, R>(wq + r0, wr, valid);
+        } else {
+            TB vb[R];
+            TA yv[R];
+            TA d[R];
+            if (dinv) load_rows<TA, R>(dinv + r0, d, valid);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                vb[r] = to_basis<TB>(wr[r]);
+                const TA va = from_basis<TA>(vb[r]);
+                yv[r] = dinv ? d[r] * va : va;
+                nrm += double(wr[r]) * double(wr[r]);
+            }
+            store_rows<TB, R>(vnext + r0, vb, valid);
+            store_rows<TA, R>(y + r0, yv, valid);
         }
-        store_rows<TB, R>(vnext + r0, vb, valid);
-        store_rows<TA, R>(y + r0, yv, valid);
     };
     // full row groups on the vector path; the partial one by its thread
     const int64_t full = n / R;
     int64_t grp = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x;
     for (; grp < full; grp += int64_t(gridDim.x) * kSolverBlock) group(grp * R, R);
     if (grp == full && n % R != 0) group(full * R, int(n % R));
+    if constexpr (kQ) {
+        // the block's largest entry beside its partial sum
+        double m = mx;
+#pragma unroll
+        for (int off = 16; off > 0; off /= 2) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+        __shared__ double mred[kSolverBlock / kWarp];
+        if (threadIdx.x % kWarp == 0) mred[threadIdx.x / kWarp] = m;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int k = 1; k < kSolverBlock / kWarp; ++k) m = fmax(m, mred[k]);
+            partials[kSolverGrid + blockIdx.x] = m;
+        }
+    }
     double a[1] = {nrm};
     block_partials<double, 1>(a, partials, red);
     if (last_block_done(&st->ticket, &last)) {
         sum_partials<double, 1>(partials, gridDim.x, tot, red);
-        close_step(st, sqrt(tot[0]), Hm);
+        const double hnorm = sqrt(tot[0]);
+        close_step(st, hnorm, Hm);
+        if constexpr (kQ) {
+            if (threadIdx.x == 0) {
+                double m = 0.0;
+                for (int b = 0; b < int(gridDim.x); ++b)
+                    m = fmax(m, __ldcg(partials + kSolverGrid + b));
+                basis_scales<TB>(hnorm, m, &st->qscale, &st->sigma[j + 1]);
+            }
+        }
+    }
+}
+
+// Scaled bases: stored = round_basis(formed * qscale) and the SpMV input
+// y = D^-1 stored, for the vector that the previous kernel formed (the next
+// Arnoldi vector, index st->j, after gmres_update_kernel; V_0 after the
+// restart).  Skipped when the cycle (restart: the solve) is over.
+template <typename TA, typename TB, typename TS>
+__global__ void __launch_bounds__(kSolverBlock)
+    gmres_quantize_kernel(int64_t n, int64_t ldv, const TS* __restrict__ src,
+                          TB* __restrict__ V, const TA* __restrict__ dinv,
+                          TA* __restrict__ y, const GmresState* st, int after_restart)
+{
+    if (after_restart ? st->done : st->idle) return;
+    TB* dst = V + (after_restart ? 0 : int64_t(st->j) * ldv);
+    const TA c = TA(st->qscale);
+    for (int64_t row = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; row < n;
+         row += int64_t(gridDim.x) * kSolverBlock) {
+        const TB vb = to_basis<TB>(TA(src[row]) * c);
+        dst[row] = vb;
+        const TA va = from_basis<TA>(vb);
+        y[row] = dinv ? dinv[row] * va : va;
     }
 }
 
@@ -594,22 +726,39 @@ __global__ void __launch_bounds__(kSolverBlock)
                          const TA* __restrict__ dinv, TA* __restrict__ y,
                          GmresState* st, double* __restrict__ partials)
 {
+    constexpr bool kQ = BasisKind<TB>::kScaled;
     __shared__ double red[kSolverBlock / kWarp * 2];
     __shared__ double tot[2];
     __shared__ int last;
     if (st->done) return;
     double acc2[2] = {0.0, 0.0};
+    double mx = 0.0;
     for (int64_t row = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; row < n;
          row += int64_t(gridDim.x) * kSolverBlock) {
         const double rr = r[row], bb = b[row];
         acc2[0] += rr * rr;
         acc2[1] += bb * bb;
-        // the first basis vector of the next cycle, unnormalised
-        // (sigma_0 = 1 / ||r||), and the first SpMV input
-        const TB vb = to_basis<TB>(TA(rr));
-        V0[row] = vb;
-        const TA va = from_basis<TA>(vb);
-        y[row] = dinv ? dinv[row] * va : va;
+        if constexpr (kQ) {
+            mx = fmax(mx, fabs(rr));  // V_0 is written by gmres_quantize_kernel
+        } else {
+            // the first basis vector of the next cycle, unnormalised
+            // (sigma_0 = 1 / ||r||), and the first SpMV input
+            const TB vb = to_basis<TB>(TA(rr));
+            V0[row] = vb;
+            const TA va = from_basis<TA>(vb);
+            y[row] = dinv ? dinv[row] * va : va;
+        }
+    }
+    if constexpr (kQ) {
+#pragma unroll
+        for (int off = 16; off > 0; off /= 2) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+        __shared__ double mred[kSolverBlock / kWarp];
+        if (threadIdx.x % kWarp == 0) mred[threadIdx.x / kWarp] = mx;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int k = 1; k < kSolverBlock / kWarp; ++k) mx = fmax(mx, mred[k]);
+            partials[2 * kSolverGrid + blockIdx.x] = mx;
+        }
     }
     block_partials<double, 2>(acc2, partials, red);
     if (last_block_done(&st->ticket, &last)) {
@@ -642,6 +791,12 @@ __global__ void __launch_bounds__(kSolverBlock)
                 st->g[0] = rn;
                 for (int i = 1; i <= kMaxKrylov; ++i) st->g[i] = 0.0;
                 st->sigma[0] = 1.0 / rn;
+                if constexpr (kQ) {
+                    double m = 0.0;
+                    for (int b = 0; b < int(gridDim.x); ++b)
+                        m = fmax(m, __ldcg(partials + 2 * kSolverGrid + b));
+                    basis_scales<TB>(rn, m, &st->qscale, &st->sigma[0]);
+                }
                 st->inner_thresh = fmax(st->inner_reduction * rn,
                                         st->reduction * st->base);
             }
@@ -672,7 +827,7 @@ inline int gmres_ell_width(int64_t n, int64_t nnz, int64_t max_row_nnz)
 struct GmresLayout {
     int64_t bytes, off_st, off_r, off_w, off_y, off_v, off_partials,
         off_a32, off_d32, off_ell_c, off_ell_v, off_gpart, off_H, off_G,
-        off_bcol, off_xcol;
+        off_bcol, off_xcol, off_wq;
     int ell_width;
 };
 
@@ -693,6 +848,7 @@ GmresLayout gmres_layout(int64_t n, int64_t nnz, int64_t max_row_nnz, int d, boo
     const int64_t ldv = gmres_ld(n);
     l.off_w = c.take<TA>(ldv);
     l.off_y = c.take<TA>(ldv);
+    l.off_wq = BasisKind<TB>::kScaled ? c.take<TA>(ldv) : 0;
     l.off_v = c.take<TB>((int64_t(d) + 1) * ldv);
     l.off_partials = c.take<double>(int64_t(kSolverGrid) * 2 * kLd);
     l.off_gpart = c.take<double>(int64_t(kDotsMaxGroups) * 2 * kLd);
@@ -725,6 +881,8 @@ int gmres_engine(const GmresLayout& lay, int64_t n, int64_t nnz, const int32_t* 
     TA* wbuf = reinterpret_cast<TA*>(w + lay.off_w);
     TA* y = reinterpret_cast<TA*>(w + lay.off_y);
     TB* V = reinterpret_cast<TB*>(w + lay.off_v);
+    constexpr bool kScaled = BasisKind<TB>::kScaled;
+    TA* wq = kScaled ? reinterpret_cast<TA*>(w + lay.off_wq) : nullptr;
     double* partials = reinterpret_cast<double*>(w + lay.off_partials);
     double* gpart = reinterpret_cast<double*>(w + lay.off_gpart);
     const TA* va;
@@ -808,6 +966,10 @@ int gmres_engine(const GmresLayout& lay, int64_t n, int64_t nnz, const int32_t* 
         });
         gmres_restart_kernel<TA, TB><<<grid_vec, kSolverBlock, 0, cs>>>(n, r, b, V, da, y,
                                                                         gs, partials);
+        if constexpr (kScaled) {
+            gmres_quantize_kernel<TA, TB, double><<<grid_vec, kSolverBlock, 0, cs>>>(
+                n, ldv, r, V, da, y, gs, 1);
+        }
     };
     // first residual outside the graph (final_iter = 0: x is not touched)
     restart(st);
@@ -845,7 +1007,11 @@ int gmres_engine(const GmresLayout& lay, int64_t n, int64_t nnz, const int32_t* 
             gmres_dots_kernel<TA, TB><<<grid_dots, kSolverBlock, 0, cs>>>(
                 n, ldv, V, dst, gs, partials, gpart, Gm);
             gmres_update_kernel<TA, TB><<<grid_vec, kSolverBlock, 0, cs>>>(
-                n, ldv, V, dst, da, y, gs, partials, Hm);
+                n, ldv, V, dst, da, y, gs, partials, Hm, wq);
+            if constexpr (kScaled) {
+                gmres_quantize_kernel<TA, TB, TA><<<grid_vec, kSolverBlock, 0, cs>>>(
+                    n, ldv, wq, V, da, y, gs, 0);
+            }
             B2S_LAUNCH_CHECK();
         }
         restart(cs);
@@ -1006,6 +1172,14 @@ int64_t b2s_gmres_workspace_bytes(int64_t num_rows, int64_t nnz,
             .bytes;
     case B2S_GMRES_CB_F32:
         return gmres_layout<double, float>(num_rows, nnz, max_row_nnz, d, false, cols).bytes;
+    case B2S_GMRES_CB_F16:
+        return gmres_layout<double, __half>(num_rows, nnz, max_row_nnz, d, false, cols).bytes;
+    case B2S_GMRES_CB_I64:
+        return gmres_layout<double, int64_t>(num_rows, nnz, max_row_nnz, d, false, cols).bytes;
+    case B2S_GMRES_CB_I32:
+        return gmres_layout<double, int32_t>(num_rows, nnz, max_row_nnz, d, false, cols).bytes;
+    case B2S_GMRES_CB_I16:
+        return gmres_layout<double, int16_t>(num_rows, nnz, max_row_nnz, d, false, cols).bytes;
     default:
         return -1;
     }
@@ -1040,6 +1214,16 @@ int b2s_gmres_solve(int variant, int ortho_method, int64_t num_rows,
         // engine; its row groups follow the basis type (4 rows, 16 bytes
         // of basis and 32 of FP64 vectors per load)
         return gmres_solve_columns<double, float>(B2S_GMRES_ARGS(0.0));
+    // the other CB-GMRES storage formats: FP64 arithmetic over a basis
+    // stored scaled (half: normalised; integers: per-vector scale)
+    case B2S_GMRES_CB_F16:
+        return gmres_solve_columns<double, __half>(B2S_GMRES_ARGS(0.0));
+    case B2S_GMRES_CB_I64:
+        return gmres_solve_columns<double, int64_t>(B2S_GMRES_ARGS(0.0));
+    case B2S_GMRES_CB_I32:
+        return gmres_solve_columns<double, int32_t>(B2S_GMRES_ARGS(0.0));
+    case B2S_GMRES_CB_I16:
+        return gmres_solve_columns<double, int16_t>(B2S_GMRES_ARGS(0.0));
     default:
         set_error("unknown GMRES variant %d", variant);
         return B2S_ERR_INVALID_ARG;

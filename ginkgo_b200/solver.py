@@ -30,6 +30,10 @@ _SFX = {torch.float64: "f64", torch.float32: "f32"}
 # gmres::ortho_method (include/ginkgo/core/solver/gmres.hpp:38-50) as the C
 # ABI's B2S_ORTHO_* values
 _ORTHO = {"mgs": 0, "cgs": 1, "cgs2": 2}
+# cb_gmres::storage_precision (include/ginkgo/core/solver/cb_gmres.hpp:38-67)
+# of CbGmres<double> as the C ABI's GMRES variants (keep is plain FP64 GMRES)
+_CB_STORAGE = {"keep": 0, "reduce1": 3, "reduce2": 4, "integer": 5, "ireduce1": 6,
+               "ireduce2": 7}
 
 
 # --------------------------------------------------------------- criteria --
@@ -366,10 +370,10 @@ class _Solver:
         k = b2.shape[1]
         if self.f.kind == "cb_gmres":
             sp = self.f.storage_precision or "reduce1"
-            if sp not in ("keep", "reduce1"):
-                raise NotImplementedError(
-                    f"CbGmres storage_precision {sp!r}: keep and reduce1 are on this path")
-            variant = 0 if sp == "keep" else 3
+            if sp not in _CB_STORAGE:
+                raise ValueError(f"unknown CbGmres storage_precision {sp!r}: one of "
+                                 f"{sorted(_CB_STORAGE)}")
+            variant = _CB_STORAGE[sp]
         else:
             variant = {None: 0, "f64": 0, "f32": 1, "bf16": 2}[self.f.storage_precision]
         nbytes = lib().b2s_gmres_workspace_bytes(n, A.nnz, A.max_row_nnz, k,
@@ -455,9 +459,11 @@ class Gmres:
 
 class CbGmres:
     """solver::CbGmres (core/solver/cb_gmres.cpp): restarted GMRES with FP64
-    arithmetic and the Krylov basis stored in a reduced format;
-    with_storage_precision("reduce1") (the default here, an FP32 basis) or
-    "keep" (FP64).  krylov_dim 1..128 (default 100, as the reference)."""
+    arithmetic and the Krylov basis stored in a reduced format,
+    with_storage_precision: "keep" (FP64), "reduce1" (FP32, the default),
+    "reduce2" (half), "integer" (int64), "ireduce1" (int32), "ireduce2"
+    (int16), the integers with one scale per vector.  krylov_dim 1..128
+    (default 100, as the reference)."""
 
     @staticmethod
     def build():

@@ -539,6 +539,10 @@ int b2s_bicgstab_solve_f32(int64_t num_rows, const int32_t* row_ptrs,
 #define B2S_GMRES_MIXED_F32 1
 #define B2S_GMRES_MIXED_BF16 2
 #define B2S_GMRES_CB_F32 3
+#define B2S_GMRES_CB_F16 4
+#define B2S_GMRES_CB_I64 5
+#define B2S_GMRES_CB_I32 6
+#define B2S_GMRES_CB_I16 7
 
 /* Orthogonalisation of GMRES (solver::gmres::ortho_method,
  * include/ginkgo/core/solver/gmres.hpp:38-50).  CGS projects once
@@ -565,7 +569,16 @@ int b2s_bicgstab_solve_f32(int64_t num_rows, const int32_t* row_ptrs,
  * B2S_GMRES_CB_F32 is compressed-basis GMRES (CbGmres<double> with
  * storage_precision reduce1, core/solver/cb_gmres.cpp): FP64 matrix, vectors
  * and arithmetic, the Krylov basis stored in FP32 and read back for the
- * orthogonalisation and the solution update.  max_iters bounds the total
+ * orthogonalisation and the solution update.  B2S_GMRES_CB_F16, _I64,
+ * _I32 and _I16 are CbGmres<double> with storage_precision reduce2, integer,
+ * ireduce1 and ireduce2: the basis stored as the normalised vector in half,
+ * or as trunc(v / s) in a 64-, 32- or 16-bit integer with one scale
+ * s = (max|v| / ||v||) * 2 / INT_MAX per vector (core/solver/
+ * cb_gmres_accessor.hpp); each new vector is formed in FP64 and then written
+ * by a second pass once its norm and largest entry are known.  The
+ * orthogonalisation of every CB-GMRES variant is the engine's CGS2 (the
+ * reference re-orthogonalises CGS only while the norm drops below
+ * 1/sqrt(2) of the previous one).  max_iters bounds the total
  * Arnoldi steps of a column; the goal is ||b - A x|| <= reduction_factor *
  * baseline on the explicit FP64 residual, baseline one of B2S_BASELINE_*
  * (||b||, the initial residual norm, or 1); inner_reduction ends an inner
