@@ -1,15 +1,45 @@
 // Block Jacobi: inversion of the diagonal blocks (at most 32 rows) and their
-// application, one warp per block.  Lane r owns row r of its block in shared
-// memory; Gauss-Jordan with partial pivoting follows the reference's
-// invert_block (reference/preconditioner/jacobi_kernels.cpp:128-240) step
-// for step, with the pivot search as a warp arg-max.
+// application.  Generation runs one warp per block: lane r owns row r of its
+// block in shared memory; Gauss-Jordan with partial pivoting follows the
+// reference's invert_block (reference/preconditioner/jacobi_kernels.cpp:
+// 128-240) step for step, with the pivot search as a warp arg-max.
+//
+// The inverses are stored in the reference's block-interleaved layout
+// (block_interleaved_storage_scheme, include/ginkgo/core/preconditioner/
+// jacobi.hpp:37-140, with the CUDA executor's block stride of 32,
+// jacobi.hpp:589-621): blocks form groups of gs = 32 / pow2ceil(max_bs);
+// element (row, col) of block b sits at
+//   (b / gs) * group_offset + (b % gs) * max_bs + row + col * stride,
+// stride = gs * max_bs, group_offset = max_bs * stride.  Column col of the
+// gs blocks of a group is one contiguous run of gs * max_bs values, so the
+// apply reads it with one coalesced warp load.
 #include "common.cuh"
 
 namespace b2s {
 namespace {
 
-constexpr int kJacobiWarps = 4;  // warps (blocks of the matrix) per CTA
+constexpr int kJacobiWarps = 4;  // warps per CTA
 constexpr int kMaxBs = 32;
+
+struct BlockScheme {
+    int gs;          // blocks per group (a power of two)
+    int power;       // log2(gs)
+    int64_t stride;  // between the columns of a block
+    int64_t group;   // between groups
+};
+
+inline __host__ __device__ BlockScheme block_scheme(int max_bs)
+{
+    int p2 = 1;
+    while (p2 < max_bs) p2 *= 2;
+    BlockScheme sc;
+    sc.gs = kMaxBs / p2;
+    sc.power = 0;
+    while ((1 << sc.power) < sc.gs) ++sc.power;
+    sc.stride = int64_t(sc.gs) * max_bs;
+    sc.group = int64_t(max_bs) * sc.stride;
+    return sc;
+}
 
 // Valid extent of block `blk`: 0 <= s <= e <= n and e - s <= max_bs.
 __device__ __forceinline__ bool block_extent(const int32_t* ptrs, int64_t blk, int64_t n,
@@ -103,19 +133,24 @@ __global__ void __launch_bounds__(kJacobiWarps * kWarp)
         if (lane == 0) A[k][k] = T(1) / d;
         __syncwarp();
     }
-    // permute_and_transpose_block: inverse(i, perm[j]) = A(i, j), stored
-    // column-major with stride max_bs
-    T* out = blocks + blk * int64_t(max_bs) * max_bs;
+    // permute_and_transpose_block: inverse(i, perm[j]) = A(i, j), in the
+    // interleaved layout
+    const BlockScheme sc = block_scheme(max_bs);
+    T* out = blocks + (blk >> sc.power) * sc.group + (blk & (sc.gs - 1)) * max_bs;
     if (lane < bs) {
-        for (int j = 0; j < bs; ++j) out[lane + int64_t(perm[j]) * max_bs] = A[lane][j];
+        for (int j = 0; j < bs; ++j) out[lane + int64_t(perm[j]) * sc.stride] = A[lane][j];
     }
 }
 
-// Apply: floor(32 / max_bs) blocks per warp, lane = (block in warp, row),
-// so small blocks keep the whole warp busy.  Every lane runs the same
-// max_bs broadcast steps (full-mask shuffles); lanes outside a valid row
-// only pass values along.
-template <typename T>
+// Apply: one warp per group of gs blocks, lane = (block in the group, row),
+// so column `inner` of the whole group is one coalesced load; all max_bs
+// columns of the lane's row are loaded before the sums (MB2 = pow2ceil of
+// max_bs, a compile-time bound).  Every lane runs the same broadcast steps
+// (full-mask shuffles); lanes outside a valid row only pass values along.
+// x(row) = beta x(row) (or 0), then += (alpha inv(row, inner)) b(inner) for
+// inner in order, as apply_block (jacobi_kernels.cpp:419-445); KC columns of
+// b at a time reuse the loaded block.
+template <typename T, int MB2, int KC>
 __global__ void __launch_bounds__(kJacobiWarps * kWarp)
     jacobi_block_apply_kernel(int64_t n, int64_t num_blocks, const int32_t* __restrict__ ptrs,
                               int max_bs, const T* __restrict__ blocks,
@@ -123,30 +158,53 @@ __global__ void __launch_bounds__(kJacobiWarps * kWarp)
                               int64_t ldx, int64_t k, const T* __restrict__ alpha,
                               const T* __restrict__ beta)
 {
+    const BlockScheme sc = block_scheme(max_bs);
     const int lane = threadIdx.x % kWarp, w = threadIdx.x / kWarp;
-    const int per_warp = kWarp / max_bs;
     const int sub = lane / max_bs, r = lane % max_bs;
-    const int64_t warp = int64_t(blockIdx.x) * kJacobiWarps + w;
-    const int64_t blk = warp * per_warp + sub;
-    if (warp * per_warp >= num_blocks) return;  // the whole warp: uniform
+    const int64_t grp = int64_t(blockIdx.x) * kJacobiWarps + w;
+    if (grp * sc.gs >= num_blocks) return;  // the whole warp: uniform
+    const int64_t blk = grp * sc.gs + sub;
     int s = 0, bs = 0;
-    const bool in_block = sub < per_warp && blk < num_blocks &&
+    const bool in_block = sub < sc.gs && blk < num_blocks &&
                           block_extent(ptrs, blk, n, max_bs, s, bs);
     const bool active = in_block && r < bs;
-    const T* inv = blocks + (in_block ? blk : 0) * int64_t(max_bs) * max_bs;
+    // the lane's row of the inverse, one coalesced load per column
+    const T* g = blocks + grp * sc.group + lane;
+    const bool in_group = lane < sc.gs * max_bs;
+    T inv[MB2];
+#pragma unroll
+    for (int inner = 0; inner < MB2; ++inner) {
+        inv[inner] = in_group && inner < max_bs ? __ldg(g + inner * sc.stride) : T(0);
+    }
     const T a = alpha ? *alpha : T(1);
     const T be = beta ? *beta : T(0);
     const int base = sub * max_bs;  // first lane of this lane's block
-    for (int64_t col = 0; col < k; ++col) {
-        const T bv = active ? b[(s + r) * ldb + col] : T(0);
-        T acc = T(0);
-        if (active && be != T(0)) acc = x[(s + r) * ldx + col] * be;
-        // apply_block: x(row) += alpha * inv(row, inner) * b(inner), inner in order
-        for (int inner = 0; inner < max_bs; ++inner) {
-            const T bi = __shfl_sync(0xffffffffu, bv, (base + inner) % kWarp);
-            if (active && inner < bs) acc += a * inv[r + int64_t(inner) * max_bs] * bi;
+    for (int64_t c0 = 0; c0 < k; c0 += KC) {
+        T bv[KC], acc[KC];
+#pragma unroll
+        for (int c = 0; c < KC; ++c) {
+            const bool col_ok = c0 + c < k;
+            bv[c] = active && col_ok ? b[(s + r) * ldb + c0 + c] : T(0);
+            acc[c] = active && col_ok && be != T(0) ? x[(s + r) * ldx + c0 + c] * be : T(0);
         }
-        if (active) x[(s + r) * ldx + col] = acc;
+#pragma unroll
+        for (int inner = 0; inner < MB2; ++inner) {
+            if (inner < max_bs) {
+                const T ai = a * inv[inner];
+                const bool use = active && inner < bs;
+#pragma unroll
+                for (int c = 0; c < KC; ++c) {
+                    const T bi = __shfl_sync(0xffffffffu, bv[c], (base + inner) % kWarp);
+                    if (use) acc[c] += ai * bi;
+                }
+            }
+        }
+        if (active) {
+#pragma unroll
+            for (int c = 0; c < KC; ++c) {
+                if (c0 + c < k) x[(s + r) * ldx + c0 + c] = acc[c];
+            }
+        }
     }
 }
 
@@ -176,11 +234,27 @@ int block_apply(int64_t n, int64_t num_blocks, const int32_t* ptrs, int max_bs,
                   "alpha and beta must both be given or both be null");
     B2S_CHECK_ARG(k == 0 || (ldb >= k && ldx >= k), "leading dimension < num_rhs");
     if (num_blocks == 0 || k == 0) return B2S_OK;
-    const int64_t warps = ceildiv(num_blocks, kWarp / max_bs);
-    jacobi_block_apply_kernel<T><<<ceildiv(warps, kJacobiWarps), kJacobiWarps * kWarp,
-                                   0, as_stream(stream)>>>(n, num_blocks, ptrs, max_bs,
-                                                           blocks, b, ldb, x, ldx, k,
-                                                           alpha, beta);
+    const BlockScheme sc = block_scheme(max_bs);
+    const int64_t grid = ceildiv(ceildiv(num_blocks, sc.gs), kJacobiWarps);
+    cudaStream_t st = as_stream(stream);
+    auto launch = [&](auto kernel) {
+        kernel<<<grid, kJacobiWarps * kWarp, 0, st>>>(n, num_blocks, ptrs, max_bs, blocks, b,
+                                                      ldb, x, ldx, k, alpha, beta);
+    };
+    const int mb2 = kMaxBs / sc.gs;
+#define B2S_JAC_APPLY(MB)                                                    \
+    if (mb2 == MB) {                                                         \
+        if (k == 1) launch(jacobi_block_apply_kernel<T, MB, 1>);             \
+        else if (k == 2) launch(jacobi_block_apply_kernel<T, MB, 2>);        \
+        else launch(jacobi_block_apply_kernel<T, MB, 4>);                    \
+    }
+    B2S_JAC_APPLY(1)
+    B2S_JAC_APPLY(2)
+    B2S_JAC_APPLY(4)
+    B2S_JAC_APPLY(8)
+    B2S_JAC_APPLY(16)
+    B2S_JAC_APPLY(32)
+#undef B2S_JAC_APPLY
     B2S_LAUNCH_CHECK();
     return B2S_OK;
 }
@@ -191,6 +265,21 @@ int block_apply(int64_t n, int64_t num_blocks, const int32_t* ptrs, int max_bs,
 using namespace b2s;
 
 extern "C" {
+
+int b2s_jacobi_storage_scheme(int max_block_size, int64_t num_blocks, int64_t* block_offset,
+                              int64_t* group_offset, int32_t* group_power,
+                              int64_t* storage_space)
+{
+    B2S_CHECK_ARG(max_block_size >= 1 && max_block_size <= kMaxBs,
+                  "max_block_size must be 1..32");
+    B2S_CHECK_ARG(num_blocks >= 0, "negative number of blocks");
+    const BlockScheme sc = block_scheme(max_block_size);
+    if (block_offset) *block_offset = max_block_size;
+    if (group_offset) *group_offset = sc.group;
+    if (group_power) *group_power = sc.power;
+    if (storage_space) *storage_space = ceildiv(num_blocks, sc.gs) * sc.group;
+    return B2S_OK;
+}
 
 int b2s_jacobi_block_generate_f64(int64_t num_rows, const int32_t* row_ptrs,
                                   const int32_t* col_idxs, const double* values,

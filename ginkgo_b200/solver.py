@@ -209,7 +209,12 @@ class BlockJacobi:
         self.num_blocks = len(bp) - 1
         self._ptrs = torch.from_numpy(bp).to(dev)
         m = self.max_block_size
-        self.blocks = torch.zeros(max(self.num_blocks, 1) * m * m, dtype=A.dtype, device=dev)
+        bo, go, gp, space = C.c_int64(0), C.c_int64(0), C.c_int32(0), C.c_int64(0)
+        call("b2s_jacobi_storage_scheme", m, self.num_blocks, C.byref(bo), C.byref(go),
+             C.byref(gp), C.byref(space))
+        # block_interleaved_storage_scheme: (block_offset, group_offset, group_power)
+        self.storage_scheme = (int(bo.value), int(go.value), int(gp.value))
+        self.blocks = torch.zeros(max(int(space.value), 1), dtype=A.dtype, device=dev)
         call(f"b2s_jacobi_block_generate_{_SFX[A.dtype]}", A.shape[0], _p(A.row_ptrs),
              _p(A.col_idxs), _p(A.values), self.num_blocks, _p(self._ptrs), m,
              _p(self.blocks), _stream(self.blocks))
@@ -236,23 +241,45 @@ class BlockJacobi:
              _p(x2), x2.stride(0), b2.shape[1], _p(alpha), _p(beta), _stream(x2))
         return x
 
+    def _positions(self):
+        """Index of entry (i, j) of block b in the interleaved storage, as an
+        array [num_blocks, m, m] (get_global_block_offset(b) + i + j * stride,
+        include/ginkgo/core/preconditioner/jacobi.hpp:100-140)."""
+        bo, go, gp = self.storage_scheme
+        gs = 1 << gp
+        stride = bo << gp
+        m = self.max_block_size
+        b = np.arange(self.num_blocks)[:, None, None]
+        i = np.arange(m)[None, :, None]
+        j = np.arange(m)[None, None, :]
+        return (b >> gp) * go + (b & (gs - 1)) * bo + i + j * stride
+
+    def block(self, b):
+        """The max_block_size x max_block_size slot of block b (host)."""
+        return self.blocks.cpu().numpy()[self._positions()[b]]
+
     def to_dense(self):
         """The block-diagonal inverse as a dense host array."""
-        n, m = self.A.shape[0], self.max_block_size
+        n = self.A.shape[0]
         blk = self.blocks.cpu().numpy()
+        pos = self._positions()
         out = np.zeros((n, n), dtype=blk.dtype)
         for i, (s, e) in enumerate(zip(self.block_pointers[:-1], self.block_pointers[1:])):
             bs = e - s
-            slot = blk[i * m * m:(i + 1) * m * m].reshape(m, m)  # [col][row]
-            out[s:e, s:e] = slot[:bs, :bs].T
+            out[s:e, s:e] = blk[pos[i]][:bs, :bs]
         return out
 
     def transpose(self):
-        """Jacobi::transpose: the same blocks, each transposed."""
+        """Jacobi::transpose: the same blocks, each transposed in place in
+        the interleaved layout."""
         t = BlockJacobi.__new__(BlockJacobi)
         t.__dict__.update(self.__dict__)
-        m = self.max_block_size
-        t.blocks = (self.blocks.reshape(-1, m, m).transpose(1, 2).contiguous().reshape(-1))
+        pos = self._positions()
+        src = torch.from_numpy(pos.transpose(0, 2, 1).reshape(-1)).to(self.blocks.device)
+        dst = torch.from_numpy(pos.reshape(-1)).to(self.blocks.device)
+        t.blocks = self.blocks.clone()
+        if len(dst):
+            t.blocks[dst] = self.blocks[src]
         return t
 
 

@@ -267,10 +267,16 @@ int b2s_jacobi_apply_f32(int64_t num_rows, int64_t num_rhs,
 
 /* Block Jacobi with full-precision blocks of at most max_block_size <= 32
  * rows.  block_ptrs (device, num_blocks + 1 entries, from 0 to num_rows)
- * delimit the diagonal blocks; a block with a bad extent is skipped.  Block
- * b's inverse is stored at blocks + b * max_block_size^2, entry (i, j) at
- * i + j * max_block_size (column-major), as the reference's storage with a
- * stride of max_block_size.  Generate: Gauss-Jordan with partial pivoting
+ * delimit the diagonal blocks; a block with a bad extent is skipped.  The
+ * inverses use the reference's block-interleaved layout
+ * (block_interleaved_storage_scheme, include/ginkgo/core/preconditioner/
+ * jacobi.hpp:37-140, with the CUDA block stride of 32): with
+ * gs = 32 / pow2ceil(max_block_size) blocks per group, entry (i, j) of
+ * block b is at (b >> group_power) * group_offset + (b % gs) * block_offset
+ * + i + j * stride, stride = gs * max_block_size; b2s_jacobi_storage_scheme
+ * gives block_offset, group_offset, group_power and the storage space (in
+ * values) for num_blocks blocks, the values Jacobi::get_storage_scheme()
+ * and the blocks array of the reference hold.  Generate: Gauss-Jordan with partial pivoting
  * in place (the first row of largest magnitude is the pivot; a zero pivot
  * ends the elimination of that block, as the reference's invert_block
  * does); replaces jacobi::generate (core/preconditioner/jacobi_kernels.hpp,
@@ -287,6 +293,9 @@ int b2s_jacobi_apply_f32(int64_t num_rows, int64_t num_rhs,
 int64_t b2s_jacobi_find_blocks(int64_t num_rows, const int32_t* row_ptrs,
                                const int32_t* col_idxs, int max_block_size,
                                int32_t* block_ptrs_out);
+int b2s_jacobi_storage_scheme(int max_block_size, int64_t num_blocks, int64_t* block_offset,
+                              int64_t* group_offset, int32_t* group_power,
+                              int64_t* storage_space);
 int b2s_jacobi_block_generate_f64(int64_t num_rows, const int32_t* row_ptrs,
                                   const int32_t* col_idxs, const double* values,
                                   int64_t num_blocks, const int32_t* block_ptrs,

@@ -129,3 +129,33 @@ def test_random_blocks_match_oracle(exe, dt, npdt, mbs, kind):
     bj.apply(-0.5, bd, 2.0, xd)
     np.testing.assert_allclose(xd.cpu().numpy(), J.apply(ref, b, x0, -0.5, 2.0), rtol=0,
                                atol=tol * scale * np.abs(b).max() * 40 + tol * 4)
+
+
+@pytest.mark.parametrize("mbs,scheme", [(3, (3, 72, 3)), (8, (8, 256, 2)), (13, (13, 338, 1)),
+                                        (32, (32, 1024, 0))])
+def test_blocks_use_the_reference_interleaved_layout(exe, mbs, scheme):
+    """The raw blocks array is the reference's block_interleaved_storage_scheme
+    (jacobi.hpp:589-621 with the CUDA block stride of 32): group size
+    32 / pow2ceil(max_block_size), block_offset = max_block_size,
+    stride = group size * block_offset, group_offset = max_block_size * stride;
+    entry (i, j) of block b at get_global_block_offset(b) + i + j * stride."""
+    rp, ci, v = _random_blocks(mbs + 100)
+    n = len(rp) - 1
+    A = Csr.read(exe, rp, ci, v)
+    bj = BlockJacobi(A, mbs)
+    assert bj.storage_scheme == scheme
+    bo, go, gp = scheme
+    gs = 1 << gp
+    stride = bo << gp
+    nb = bj.num_blocks
+    assert bj.blocks.numel() == -(-nb // gs) * go  # compute_storage_space
+    raw = bj.blocks.cpu().numpy()
+    ref = J.to_dense(J.generate(rp, ci, v, mbs), n)
+    ptrs = bj.block_pointers
+    for b in range(nb):
+        s, e = ptrs[b], ptrs[b + 1]
+        off = go * (b >> gp) + bo * (b & (gs - 1))
+        for i in range(e - s):
+            for j in range(e - s):
+                assert abs(raw[off + i + j * stride] - ref[s + i, s + j]) <= \
+                    1e-11 * max(1.0, abs(ref[s + i, s + j])), (b, i, j)
