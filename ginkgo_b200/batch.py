@@ -28,7 +28,11 @@ _SFX = {torch.float64: "f64", torch.float32: "f32"}
 
 class BatchEll:
     """Ragged batch Ell: system s owns rows [row_offsets[s], row_offsets[s+1])
-    and its entries at values[width * row_offsets[s] + j * n_s + r]."""
+    and its entries at values[width * row_offsets[s] + j * n_s + r].
+    BatchEll.uniform builds the reference's own uniform batch::matrix::Ell
+    (one size, one column-index array shared by all systems)."""
+
+    uniform_rows = None  # rows per system when the column indices are shared
 
     def __init__(self, exec_, row_offsets, width, col_idxs, values):
         dev = exec_.device
@@ -45,6 +49,21 @@ class BatchEll:
     @property
     def sizes(self):
         return np.diff(self.host_row_offsets)
+
+    @classmethod
+    def uniform(cls, exec_, num_systems, num_rows, width, col_idxs, values):
+        """batch::matrix::Ell (include/ginkgo/core/matrix/batch_ell.hpp):
+        num_systems systems of num_rows rows, col_idxs (num_rows * width,
+        column-major, -1 = padding) shared by all systems, values
+        (num_systems * num_rows * width) per system."""
+        offs = np.arange(num_systems + 1, dtype=np.int64) * num_rows
+        A = cls(exec_, offs, width, col_idxs, values)
+        if A.col_idxs.numel() != num_rows * width:
+            raise ValueError("shared col_idxs must hold num_rows * width entries")
+        if A.values.numel() != num_systems * num_rows * width:
+            raise ValueError("values must hold num_systems * num_rows * width entries")
+        A.uniform_rows = int(num_rows)
+        return A
 
     @classmethod
     def from_csr(cls, exec_, systems, width=None, dtype=torch.float64):
@@ -72,6 +91,8 @@ class BatchEll:
     def to_csr_list(self):
         """Host CSR per system (for checking)."""
         ci = self.col_idxs.cpu().numpy()
+        if self.uniform_rows is not None:
+            ci = np.tile(ci, self.num_systems)
         v = self.values.cpu().numpy()
         out = []
         for s in range(self.num_systems):
@@ -182,12 +203,23 @@ class _BatchSolver:
                 _p(A.col_idxs), _p(A.values), _p(b), _p(x),
                 int(p["max_iterations"]), float(p["tolerance"]), tol_abs, jac)
 
+    def _uniform_call(self, b, x, tt, table_out):
+        A = self.A
+        args = self._args(b, x)  # validates b and x
+        call(f"b2s_batch_ell_uniform_bicgstab_solve_{_SFX[A.dtype]}", A.num_systems,
+             A.uniform_rows, A.width, _p(A.col_idxs), _p(A.values), _p(b), _p(x),
+             *args[8:], tt, _p(self.ws), self.ws.numel(), _p(self.iters), _p(self.res),
+             _stream(x), table_out)
+
     def apply(self, b, x):
         tt = None if self.tune_table is None else \
             self.tune_table.ctypes.data_as(C.c_void_p)
-        call(f"b2s_batch_ell_bicgstab_solve_{_SFX[self.A.dtype]}",
-             *self._args(b, x), tt, _p(self.ws), self.ws.numel(),
-             _p(self.iters), _p(self.res), _stream(x))
+        if self.A.uniform_rows is not None:
+            self._uniform_call(b, x, tt, None)
+        else:
+            call(f"b2s_batch_ell_bicgstab_solve_{_SFX[self.A.dtype]}",
+                 *self._args(b, x), tt, _p(self.ws), self.ws.numel(),
+                 _p(self.iters), _p(self.res), _stream(x))
         self.logger = BatchLog(self.iters, self.res)
         return x
 
@@ -195,9 +227,12 @@ class _BatchSolver:
         """Autotunes threads-per-system and vector placement per size bucket
         (and solves); later applies reuse the table."""
         table = np.zeros(24, dtype=np.int32)
-        call(f"b2s_batch_ell_bicgstab_tune_{_SFX[self.A.dtype]}",
-             *self._args(b, x), _p(self.ws), self.ws.numel(), _p(self.iters),
-             _p(self.res), table.ctypes.data_as(C.c_void_p), _stream(x))
+        if self.A.uniform_rows is not None:
+            self._uniform_call(b, x, None, table.ctypes.data_as(C.c_void_p))
+        else:
+            call(f"b2s_batch_ell_bicgstab_tune_{_SFX[self.A.dtype]}",
+                 *self._args(b, x), _p(self.ws), self.ws.numel(), _p(self.iters),
+                 _p(self.res), table.ctypes.data_as(C.c_void_p), _stream(x))
         self.tune_table = table
         self.logger = BatchLog(self.iters, self.res)
         return table
@@ -231,6 +266,9 @@ def slice_systems(A: BatchEll, s0: int, s1: int, exec_) -> BatchEll:
     contiguous slice: system s owns entries from width * row_offsets[s])."""
     o0, o1 = int(A.host_row_offsets[s0]), int(A.host_row_offsets[s1])
     w = A.width
+    if A.uniform_rows is not None:
+        return BatchEll.uniform(exec_, s1 - s0, A.uniform_rows, w, A.col_idxs,
+                                A.values[w * o0:w * o1])
     return BatchEll(exec_, A.host_row_offsets[s0:s1 + 1] - o0, w,
                     A.col_idxs[w * o0:w * o1], A.values[w * o0:w * o1])
 

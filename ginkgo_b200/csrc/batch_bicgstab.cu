@@ -20,7 +20,9 @@
 // column-major inside the system with local column indices (-1 = padding);
 // for equal sizes this is the reference's batch::matrix::Ell value layout
 // (include/ginkgo/core/matrix/batch_ell.hpp:149-221) with the column indices
-// stored per system.
+// stored per system.  The uniform entry points take the reference's own
+// batch::matrix::Ell: every system n rows, one col_idxs array of n * width
+// entries shared by all systems (core/matrix/batch_struct.hpp:268-280).
 #include <algorithm>
 #include <map>
 #include <vector>
@@ -81,7 +83,9 @@ __device__ __forceinline__ void group_sum(T (&v)[M], T* red, int& parity,
 }
 
 struct BatchArgs {
-    const int32_t* row_offsets;
+    const int32_t* row_offsets;  // ragged batch; unused when uniform_n > 0
+    int uniform_n;               // > 0: every system has this many rows and
+                                 // the column indices are shared
     const int32_t* sys_list;  // systems of this bucket
     int num_sys;
     int width;
@@ -118,10 +122,10 @@ __global__ void __launch_bounds__(kBatchBlock, 1)
     const int total_groups = gridDim.x * GPB;
     for (int q = blockIdx.x * GPB + group; q < a.num_sys; q += total_groups) {
         const int sys = a.sys_list[q];
-        const int off = a.row_offsets[sys];
-        const int n = a.row_offsets[sys + 1] - off;
+        const int off = a.uniform_n ? sys * a.uniform_n : a.row_offsets[sys];
+        const int n = a.uniform_n ? a.uniform_n : a.row_offsets[sys + 1] - off;
         const int64_t vbase = int64_t(a.width) * off;
-        const int32_t* cs = ci + vbase;
+        const int32_t* cs = a.uniform_n ? ci : ci + vbase;
         const T* vs = val + vbase;
         T r[RPT], rh[RPT], p[RPT], v[RPT], s[RPT], tt[RPT], xx[RPT], pr[RPT];
         T bb2 = T(0);
@@ -396,7 +400,7 @@ int batch_solve(int64_t num_sys, const int32_t* row_offsets,
                 int64_t max_iters, double tol, int tol_absolute,
                 int use_jacobi, const int32_t* tune_table, void* workspace,
                 int64_t workspace_bytes, int32_t* iters_out, double* res_out,
-                void* stream, int32_t* tune_out)
+                void* stream, int32_t* tune_out, int uniform_n = 0)
 {
     B2S_CHECK_ARG(num_sys >= 0 && width >= 1 && width <= 64, "bad batch shape");
     B2S_CHECK_ARG(host_row_offsets != nullptr, "host row offsets required");
@@ -434,6 +438,7 @@ int batch_solve(int64_t num_sys, const int32_t* row_offsets,
     auto args_for = [&](const BucketPlan& pl) {
         BatchArgs a;
         a.row_offsets = row_offsets;
+        a.uniform_n = uniform_n;
         a.sys_list = dev_list + pl.first;
         a.num_sys = pl.count;
         a.width = int(width);
@@ -602,5 +607,37 @@ int64_t b2s_batch_bicgstab_workspace_bytes(int64_t num_systems,
 
 B2S_BATCH_ENTRY(double, f64)
 B2S_BATCH_ENTRY(float, f32)
+
+// The reference's uniform batch::matrix::Ell: num_systems systems of
+// num_rows rows each, column indices shared (num_rows * width entries).
+#define B2S_BATCH_UNIFORM_ENTRY(T, S)                                          \
+    int b2s_batch_ell_uniform_bicgstab_solve_##S(                              \
+        int64_t num_systems, int64_t num_rows, int64_t width,                  \
+        const int32_t* col_idxs, const T* values, const T* b, T* x,            \
+        int64_t max_iters, double tolerance, int tolerance_absolute,           \
+        int use_jacobi, const int32_t* tune_table, void* workspace,            \
+        int64_t workspace_bytes, int32_t* iterations, double* residual_norms, \
+        void* stream, int32_t* tune_table_out)                                 \
+    {                                                                          \
+        B2S_CHECK_ARG(num_systems >= 0 && num_rows >= 1 &&                     \
+                          num_rows <= (1 << (kBuckets - 1)),                   \
+                      "uniform batch: num_rows must be 1..%d",                 \
+                      1 << (kBuckets - 1));                                    \
+        B2S_CHECK_ARG(num_systems * num_rows < (int64_t(1) << 31),             \
+                      "uniform batch too large for int32 row offsets");        \
+        std::vector<int32_t> offs(size_t(num_systems) + 1);                    \
+        for (int64_t s = 0; s <= num_systems; ++s)                             \
+            offs[size_t(s)] = int32_t(s * num_rows);                           \
+        return batch_solve<T>(num_systems, nullptr, offs.data(), width,        \
+                              col_idxs, values, b, x, max_iters, tolerance,    \
+                              tolerance_absolute, use_jacobi,                  \
+                              tune_table_out ? nullptr : tune_table,           \
+                              workspace, workspace_bytes, iterations,          \
+                              residual_norms, stream, tune_table_out,          \
+                              int(num_rows));                                  \
+    }
+
+B2S_BATCH_UNIFORM_ENTRY(double, f64)
+B2S_BATCH_UNIFORM_ENTRY(float, f32)
 
 }  // extern "C"

@@ -687,6 +687,28 @@ int b2s_batch_ell_bicgstab_tune_f32(
     void* workspace, int64_t workspace_bytes, int32_t* iterations,
     double* residual_norms, int32_t* tune_table_out, void* stream);
 
+/* The same solve on the reference's uniform batch::matrix::Ell
+ * (include/ginkgo/core/matrix/batch_ell.hpp:149-221, core/matrix/
+ * batch_struct.hpp:268-280): num_systems systems of num_rows rows
+ * (1..2048), one col_idxs array of num_rows * width entries shared by all
+ * systems, values[s * num_rows * width + j * num_rows + r].  With
+ * tune_table_out non-NULL the call autotunes (and solves) as
+ * b2s_batch_ell_bicgstab_tune_*; otherwise tune_table (or NULL) selects the
+ * configuration.  Workspace as b2s_batch_bicgstab_workspace_bytes with
+ * total_rows = num_systems * num_rows. */
+int b2s_batch_ell_uniform_bicgstab_solve_f64(
+    int64_t num_systems, int64_t num_rows, int64_t width, const int32_t* col_idxs,
+    const double* values, const double* b, double* x, int64_t max_iters,
+    double tolerance, int tolerance_absolute, int use_jacobi,
+    const int32_t* tune_table, void* workspace, int64_t workspace_bytes,
+    int32_t* iterations, double* residual_norms, void* stream, int32_t* tune_table_out);
+int b2s_batch_ell_uniform_bicgstab_solve_f32(
+    int64_t num_systems, int64_t num_rows, int64_t width, const int32_t* col_idxs,
+    const float* values, const float* b, float* x, int64_t max_iters,
+    double tolerance, int tolerance_absolute, int use_jacobi,
+    const int32_t* tune_table, void* workspace, int64_t workspace_bytes,
+    int32_t* iterations, double* residual_norms, void* stream, int32_t* tune_table_out);
+
 /* ------------------------------------------ sparse products and sums -- */
 
 /* C = A B (csr::spgemm, core/matrix/csr_kernels.hpp:72-76) and

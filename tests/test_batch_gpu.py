@@ -169,3 +169,44 @@ def test_large_groups_with_half_step_exits(exe, G, smem):
         assert abs(int(it[i]) - it_o) <= max(3, 0.3 * it_o), (i, it[i], it_o)
         rel = np.linalg.norm(bi - orc.csr_spmv(rp, ci, v, xg[o:e])) / np.linalg.norm(bi)
         assert rel <= 1.5e-8, (i, rel)
+
+
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+def test_uniform_batch_shares_column_indices(exe, dt):
+    """The reference's uniform batch::matrix::Ell: one pattern for all
+    systems.  Same systems as a ragged batch with the pattern copied per
+    system: the solutions and iteration counts are identical."""
+    from ginkgo_b200 import stencils
+    nx, ny, nsys = 20, 16, 700
+    rp, ci, _ = stencils.convection_diffusion_2d(nx, ny, 1.0, 0.0, 0.0)
+    n = nx * ny
+    rng = np.random.default_rng(4)
+    systems = []
+    for s in range(nsys):
+        _, _, v = stencils.convection_diffusion_2d(nx, ny, rng.uniform(0.5, 2),
+                                                   rng.uniform(-1, 1), rng.uniform(-1, 1))
+        systems.append((rp, ci, v))
+    R = BatchEll.from_csr(exe, systems, width=5, dtype=dt)
+    U = BatchEll.uniform(exe, nsys, n, 5, R.col_idxs[:5 * n], R.values)
+    assert U.col_idxs.numel() == 5 * n
+    b = torch.from_numpy(rng.standard_normal(nsys * n)).to(dt).cuda()
+    tol = 1e-8 if dt == torch.float64 else 1e-5
+    out = {}
+    for name, A in (("ragged", R), ("uniform", U)):
+        s = solver(exe, A, 500, tol)
+        x = torch.zeros_like(b)
+        s.apply(b, x)
+        out[name] = (x.clone(), s.logger.iterations.clone())
+    assert torch.equal(out["ragged"][0], out["uniform"][0])
+    assert torch.equal(out["ragged"][1], out["uniform"][1])
+    # and systems against the oracle's FP64 residual
+    xg = out["uniform"][0].cpu().numpy().astype(np.float64)
+    bh = b.cpu().numpy().astype(np.float64)
+    for i in range(0, nsys, 37):
+        r = bh[i * n:(i + 1) * n] - orc.csr_spmv(*systems[i], xg[i * n:(i + 1) * n])
+        assert np.linalg.norm(r) <= tol * 10 * np.linalg.norm(bh[i * n:(i + 1) * n])
+    # autotuning the uniform batch
+    s = solver(exe, U, 500, tol)
+    x = torch.zeros_like(b)
+    table = s.tune(b, x)
+    assert table[2 * 9] in (32, 64, 128, 256)  # 320 rows: the 2^9 bucket

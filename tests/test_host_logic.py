@@ -200,3 +200,25 @@ def test_slice_sets_reject_null_pointers_before_device_work():
     assert lib.b2s_sellp_compute_slice_sets_noalloc(64, fake, 32, 1, fake, None,
                                                     None) == -1
     assert b"null" in lib.b2s_last_error()
+
+
+def test_uniform_batch_ell_layout():
+    from ginkgo_b200.batch import BatchEll
+
+    class FakeExec:
+        device = torch.device("cpu")
+
+    rp, ci, v = stencils.convection_diffusion_2d(4, 3, 1.0, 0.2, -0.1)
+    n = len(rp) - 1
+    w, st, eci, ev = orc.csr_to_ell(rp, ci, v, width=5)
+    vals = np.concatenate([ev, 2 * ev, 3 * ev])
+    U = BatchEll.uniform(FakeExec(), 3, n, 5, torch.from_numpy(eci),
+                         torch.from_numpy(vals))
+    assert U.uniform_rows == n and U.total_rows == 3 * n
+    back = U.to_csr_list()
+    for s, (rp2, c2, v2) in enumerate(back):
+        assert np.array_equal(rp2, rp) and np.array_equal(c2, ci)
+        assert np.allclose(v2, (s + 1) * v)
+    with pytest.raises(ValueError):
+        BatchEll.uniform(FakeExec(), 3, n, 5, torch.from_numpy(eci[:-1]),
+                         torch.from_numpy(vals))
