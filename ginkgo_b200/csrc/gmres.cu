@@ -59,6 +59,7 @@ constexpr int kMaxKrylov = 128;
 constexpr int kLd = kMaxKrylov + 1;
 constexpr int kDotsMaxGrid = kMaxSMs * 4;  // resident at 4 blocks per SM
 constexpr int kDotsGroup = 32;  // blocks folded by one group's last block
+constexpr int kSmallGram = 32;  // steps j < 32: the Gram matrix staged in shared memory
 constexpr int kDotsMaxGroups = (kDotsMaxGrid + kDotsGroup - 1) / kDotsGroup;
 
 // The Hessenberg matrix (column j at H[j * ld], ld = krylov_dim + 1) and
@@ -334,11 +335,13 @@ __device__ __forceinline__ bool last_of(unsigned* ticket, unsigned count, int* f
 // In one block: for the 2 nvec values c, the sum over the L partials
 // src[dots_row(c) * ld + base + k], k < L <= 32, one warp load per value
 // (warp w takes c = w, w + 8, ...; all loads issued before the sums).
-__device__ __forceinline__ void fold32(const double* src, int64_t ld, int base, int L,
+__device__ __noinline__ void fold32(const double* src, int64_t ld, int base, int L,
                                        int nvec, double* dst, int64_t dst_ld, int dst_col)
 {
     const int lane = threadIdx.x % kWarp, wid = threadIdx.x / kWarp;
-    constexpr int K = 4;  // values per warp and round: their loads in flight together
+    // values per warp and round, their loads in flight together: one round
+    // covers 2 nvec <= 64 (Krylov dimensions up to 32)
+    constexpr int K = 8;
     for (int c0 = 0; c0 < 2 * nvec; c0 += 8 * K) {
         double v[K];
 #pragma unroll
@@ -377,6 +380,7 @@ __global__ void __launch_bounds__(kSolverBlock, 4)
     constexpr int W = kSolverBlock / kWarp;
     __shared__ double redv[W][8];
     __shared__ double tot[2 * kLd];
+    __shared__ double Gs[kSmallGram * kSmallGram];
     __shared__ int last;
     if (st->idle) return;
     const int j = st->j;
@@ -435,6 +439,30 @@ __global__ void __launch_bounds__(kSolverBlock, 4)
     // row and column j of G; rows 0..j-1 hold the earlier steps of this
     // cycle (G is symmetric, so row i of G(0..j, 0..j) is complete)
     const int ld = st->ld;
+    if (j < kSmallGram) {
+        // the whole G(0..j, 0..j) in shared memory (one parallel pass of
+        // loads), then one thread per row: the short serial tail of every
+        // Arnoldi step of the usual Krylov dimensions
+        for (int e = threadIdx.x; e < j * (j + 1); e += kSolverBlock) {
+            const int i = e / j, k = e - i * j;  // G(i, k), k < j, from earlier steps
+            Gs[i * kSmallGram + k] = __ldcg(Gm + int64_t(i) * ld + k);
+        }
+        if (threadIdx.x <= j) {
+            const int i = threadIdx.x;
+            const double gij = tot[kLd + i];
+            Gs[i * kSmallGram + j] = gij;
+            Gm[int64_t(i) * ld + j] = gij;
+            Gm[int64_t(j) * ld + i] = gij;
+        }
+        __syncthreads();
+        if (threadIdx.x <= j) {
+            const int i = threadIdx.x;
+            double gh = 0.0;
+            for (int k = 0; k <= j; ++k) gh += Gs[i * kSmallGram + k] * tot[k];
+            st->h[i] = 2.0 * tot[i] - gh;
+        }
+        return;
+    }
     if (threadIdx.x <= j) {
         const int i = threadIdx.x;
         const double gij = tot[kLd + i];
