@@ -333,7 +333,8 @@ def main():
         result["ir_gmres"] = solve
         result["gpu_launches"] += solve.pop("gpu_launches")
     if not args.no_extra:
-        for key, fn in (("cg", cg_section), ("batch_bicgstab", batch_section),
+        for key, fn in (("cg", cg_section), ("krylov_iteration", krylov_iteration_section),
+                        ("batch_bicgstab", batch_section),
                         ("autograd", autograd_section),
                         ("block_jacobi", block_jacobi_section)):
             try:
@@ -623,6 +624,30 @@ def cg_section(exe, stream, grid=256):
             "iterations": s.logger.num_iterations,
             "explicit_rel_residual": float(r.norm() / b.norm()),
             "reference_iterations": 710}
+
+
+def krylov_iteration_section(exe, stream, iters=40):
+    """Time per iteration of the fused CG and BiCGStab (scalar Jacobi, one
+    right-hand side) on the 3D 7-point 128^3 matrix: `iters` iterations with
+    the residual goal out of reach (reduction 1e-30), median of 3 solves,
+    set-up included, divided by the iteration count."""
+    import torch
+    from ginkgo_b200.matrix import Csr
+    from ginkgo_b200.solver import Bicgstab, Cg, Iteration, Jacobi, ResidualNorm
+    rp, ci, v = build_matrix()
+    n = len(rp) - 1
+    A = Csr.read(exe, rp, ci, v)
+    b = torch.from_numpy(np.random.default_rng(SEED).standard_normal(n)).cuda()
+    out = {"workload": "poisson3d_7pt_128", "n": n, "iterations": iters}
+    for name, f in (("cg", Cg), ("bicgstab", Bicgstab)):
+        s = (f.build().with_criteria(Iteration.build().with_max_iters(iters),
+                                     ResidualNorm.build().with_reduction_factor(1e-30))
+             .with_preconditioner(Jacobi.build().with_max_block_size(1)).on(exe).generate(A))
+        x = torch.zeros_like(b)
+        ms = _event_ms(lambda: (x.zero_(), s.apply(b, x)), stream)
+        out[name] = {"ms": round(ms, 3), "us_per_iteration": round(ms * 1e3 / iters, 1),
+                     "iterations": s.logger.num_iterations}
+    return out
 
 
 def batch_section(exe, stream, num_systems=8192, seed=3):

@@ -19,6 +19,18 @@
 //           (step_3 / finalize + next dot + check)
 //
 // p and v are double-buffered so every row reads the previous iterate.
+//
+// One right-hand side on a large system runs the two SpMV passes split, so
+// the matrix streams through the pipelined Csr kernel with one gather per
+// stored entry (forming p' and s at every gathered column triples the
+// gathers once the vectors no longer sit in L2):
+//   bicg_pupdate  p' and y = D^-1 p'      csr_async  v = A y
+//   bicg_dot1     dot(rr, v) -> alpha      bicg_supdate  s, z = D^-1 s
+//   csr_async     t = A z                  bicg_dot2  dot(s, t), dot(t, t),
+//                                          ||s|| -> the check on s, omega
+// then the update pass as above.  Every vector entry is rounded as in the
+// fused passes.
+#include "csr_async.cuh"
 #include "solver_common.cuh"
 
 namespace b2s {
@@ -335,9 +347,108 @@ __global__ void __launch_bounds__(kSolverBlock)
     }
 }
 
+constexpr int64_t kBicgSplitRows = int64_t(1) << 19;
+
+template <typename T>
+__global__ void __launch_bounds__(kSolverBlock)
+    bicg_pupdate_kernel(int64_t n, const T* __restrict__ dinv, const T* __restrict__ r,
+                        const T* __restrict__ p_old, const T* __restrict__ v_old,
+                        T* __restrict__ p_new, T* __restrict__ y, SolveCtl* ctl,
+                        BicgScalars<T>* sc)
+{
+    if (ctl->all_stopped) return;
+    const T om = sc->omega[0];
+    const bool from_r = sc->prev_rho[0] * om == T(0);
+    const T tmp = from_r ? T(0) : sc->rho[0] / sc->prev_rho[0] * sc->alpha[0] / om;
+    for (int64_t i = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * kSolverBlock) {
+        const T pc = bicg_p(r[i], p_old[i], v_old[i], tmp, om, from_r);
+        p_new[i] = pc;
+        y[i] = dinv ? mul_rn(dinv[i], pc) : pc;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSolverBlock)
+    bicg_dot1_kernel(int64_t n, const T* __restrict__ rr, const T* __restrict__ v,
+                     SolveCtl* ctl, BicgScalars<T>* sc, T* __restrict__ partials)
+{
+    __shared__ T red[kSolverBlock / kWarp];
+    __shared__ T tot[1];
+    __shared__ int last;
+    if (ctl->all_stopped) return;
+    T acc[1] = {T(0)};
+    for (int64_t i = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * kSolverBlock) {
+        acc[0] += rr[i] * v[i];
+    }
+    block_partials<T, 1>(acc, partials, red);
+    if (last_block_done(&ctl->ticket, &last)) {
+        sum_partials<T, 1>(partials, gridDim.x, tot, red);
+        if (threadIdx.x == 0) {
+            const T bv = tot[0];
+            sc->alpha[0] = bv != T(0) ? sc->rho[0] / bv : T(0);
+            ctl->ticket = 0;
+        }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSolverBlock)
+    bicg_supdate_kernel(int64_t n, const T* __restrict__ dinv, const T* __restrict__ r,
+                        const T* __restrict__ v, T* __restrict__ s, T* __restrict__ z,
+                        SolveCtl* ctl, BicgScalars<T>* sc)
+{
+    if (ctl->all_stopped) return;
+    const T alpha = sc->alpha[0];
+    for (int64_t i = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * kSolverBlock) {
+        const T sr = bicg_s(r[i], v[i], alpha);
+        s[i] = sr;
+        z[i] = dinv ? mul_rn(dinv[i], sr) : sr;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSolverBlock)
+    bicg_dot2_kernel(int64_t n, const T* __restrict__ s, const T* __restrict__ t,
+                     SolveCtl* ctl, BicgScalars<T>* sc, T* __restrict__ partials)
+{
+    __shared__ T red[kSolverBlock / kWarp * 3];
+    __shared__ T tot[3];
+    __shared__ int last;
+    if (ctl->all_stopped) return;
+    T acc[3] = {T(0), T(0), T(0)};
+    for (int64_t i = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * kSolverBlock) {
+        const T si = s[i], ti = t[i];
+        acc[0] += si * ti;
+        acc[1] += ti * ti;
+        acc[2] += si * si;
+    }
+    block_partials<T, 3>(acc, partials, red);
+    if (last_block_done(&ctl->ticket, &last)) {
+        sum_partials<T, 3>(partials, gridDim.x, tot, red);
+        if (threadIdx.x == 0) {
+            ctl->ticket = 0;
+            uint8_t st = ctl->status[0];
+            if (!has_stopped(st)) {
+                const T tau_s = sqrt(tot[2]);
+                // the check on s without finalising, as in bicg_spmv2_kernel
+                if (residual_met(ctl, tau_s, sc->rho[0], sc->start[0])) {
+                    converge_status(st, kResidualId, false);
+                    sc->tau[0] = tau_s;
+                }
+                ctl->status[0] = st;
+                sc->omega[0] = tot[1] != T(0) ? tot[0] / tot[1] : T(0);
+            }
+        }
+    }
+}
+
 struct BicgLayout {
     int64_t bytes, off_ctl, off_sc, off_r, off_rr, off_p0, off_p1, off_v0,
-        off_v1, off_s, off_t, off_partials;
+        off_v1, off_s, off_t, off_partials, off_y, off_z;
 };
 
 template <typename T>
@@ -356,6 +467,9 @@ BicgLayout bicg_layout(int64_t n, int K)
     l.off_s = c.take<T>(n * K);
     l.off_t = c.take<T>(n * K);
     l.off_partials = c.take<T>(int64_t(kSolverGrid) * 3 * K);
+    // the SpMV inputs of the split single-column pass
+    l.off_y = K == 1 ? c.take<T>(n) : 0;
+    l.off_z = K == 1 ? c.take<T>(n) : 0;
     l.bytes = c.used;
     return l;
 }
@@ -394,6 +508,8 @@ int bicgstab_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
     T* s = reinterpret_cast<T*>(w + lay.off_s);
     T* t = reinterpret_cast<T*>(w + lay.off_t);
     T* partials = reinterpret_cast<T*>(w + lay.off_partials);
+    T* yv = K == 1 ? reinterpret_cast<T*>(w + lay.off_y) : nullptr;
+    T* zv = K == 1 ? reinterpret_cast<T*>(w + lay.off_z) : nullptr;
 
     SolveCtl h{};
     h.max_iters = int(max_iters);
@@ -417,9 +533,36 @@ int bicgstab_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
             n, b, ldb, int(k), r, rr, p[0], vv[0], ctl, sc, partials);
         B2S_LAUNCH_CHECK();
     });
+    // the split single-RHS passes (large systems)
+    const int lpr = async_lanes_per_row(max_row_nnz);
+    const int64_t async_need = ceildiv(ceildiv(n, kWarp / lpr), kAsyncBlock / kWarp);
+    auto async_spmv = [&](cudaStream_t cs, const T* in, T* out) {
+        with_async_kernel<T, 1, false>(lpr, [&](auto kernel) {
+            const int64_t grid = std::min<int64_t>(async_need, async_resident_blocks(kernel));
+            kernel<<<grid, kAsyncBlock, 0, cs>>>(n, rp, ci, v, in, 1, out, 1, nullptr,
+                                                 nullptr, &ctl->all_stopped);
+        });
+    };
+    const bool split = K == 1 && n >= kBicgSplitRows;
     auto capture = [&](cudaStream_t cs) -> int {
         for (int it = 0; it < chunk; ++it) {
             const int o = it % 2, nw = (it + 1) % 2;
+            if (split) {
+                bicg_pupdate_kernel<T><<<grid_vec, kSolverBlock, 0, cs>>>(
+                    n, dinv, r, p[o], vv[o], p[nw], yv, ctl, sc);
+                async_spmv(cs, yv, vv[nw]);
+                bicg_dot1_kernel<T><<<grid_vec, kSolverBlock, 0, cs>>>(n, rr, vv[nw], ctl, sc,
+                                                                      partials);
+                bicg_supdate_kernel<T><<<grid_vec, kSolverBlock, 0, cs>>>(
+                    n, dinv, r, vv[nw], s, zv, ctl, sc);
+                async_spmv(cs, zv, t);
+                bicg_dot2_kernel<T><<<grid_vec, kSolverBlock, 0, cs>>>(n, s, t, ctl, sc,
+                                                                      partials);
+                bicg_update_kernel<T, 1><<<grid_vec, kSolverBlock, 0, cs>>>(
+                    n, dinv, x, ldx, r, rr, p[nw], s, t, ctl, sc, partials);
+                B2S_LAUNCH_CHECK();
+                continue;
+            }
             B2S_DISPATCH_RHS(K, {
                 B2S_DISPATCH_SW(sw, {
                     bicg_spmv1_kernel<T, SW, K><<<grid_spmv, kSolverBlock, 0, cs>>>(

@@ -618,3 +618,32 @@ def test_gmres_residual_baselines(exe, baseline):
           .on(exe).generate(A))
     with pytest.raises(NotImplementedError):
         s2.apply(torch.from_numpy(b).cuda(), torch.zeros(n, dtype=torch.float64, device="cuda"))
+
+
+def test_bicgstab_large_single_rhs_split_pass_matches_oracle(exe):
+    # 800 x 700 = 560,000 rows: one right-hand side on a system this large
+    # runs the split passes (p update, pipelined Csr SpMV, dots, s update,
+    # SpMV, dots); 30 iterations against 30 of the oracle's BiCGStab
+    from ginkgo_b200.solver import Bicgstab
+    rp, ci, v = stencils.convection_diffusion_2d(800, 700, 1.0, 0.6, -0.3)
+    n = len(rp) - 1
+    assert n >= 1 << 19
+    b = np.random.default_rng(12).standard_normal(n)
+    A = Csr.read(exe, rp, ci, v)
+    s = (Bicgstab.build().with_criteria(*crit(30, 1e-14))
+         .with_preconditioner(Jacobi.build().with_max_block_size(1))
+         .on(exe).generate(A))
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    s.apply(torch.from_numpy(b).cuda(), x)
+    xo, it_o, res_o, conv_o = orc.bicgstab(rp, ci, v, b, max_iters=30, reduction=1e-14)
+    assert s.logger.num_iterations == 30 == it_o
+    assert not s.logger.has_converged
+    np.testing.assert_allclose(x.cpu().numpy(), xo, rtol=1e-8, atol=1e-10 * np.abs(xo).max())
+    # and to convergence: the explicit residual meets the goal
+    s2 = (Bicgstab.build().with_criteria(*crit(3000, 1e-10))
+          .with_preconditioner(Jacobi.build().with_max_block_size(1))
+          .on(exe).generate(A))
+    x2 = torch.zeros(n, dtype=torch.float64, device="cuda")
+    s2.apply(torch.from_numpy(b).cuda(), x2)
+    assert s2.logger.has_converged
+    assert explicit_rel_res(rp, ci, v, x2.cpu().numpy(), b)[0] <= 2e-10
