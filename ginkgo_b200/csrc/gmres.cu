@@ -443,14 +443,15 @@ __global__ void __launch_bounds__(kSolverBlock, 4)
         // the whole G(0..j, 0..j) in shared memory (one parallel pass of
         // loads), then one thread per row: the short serial tail of every
         // Arnoldi step of the usual Krylov dimensions
-        for (int e = threadIdx.x; e < j * (j + 1); e += kSolverBlock) {
-            const int i = e / j, k = e - i * j;  // G(i, k), k < j, from earlier steps
+        for (int e = threadIdx.x; e < j * j; e += kSolverBlock) {
+            const int i = e / j, k = e - i * j;  // G(i, k), i, k < j: earlier steps
             Gs[i * kSmallGram + k] = __ldcg(Gm + int64_t(i) * ld + k);
         }
-        if (threadIdx.x <= j) {
+        if (threadIdx.x <= j) {  // row and column j: this step
             const int i = threadIdx.x;
             const double gij = tot[kLd + i];
             Gs[i * kSmallGram + j] = gij;
+            Gs[j * kSmallGram + i] = gij;
             Gm[int64_t(i) * ld + j] = gij;
             Gm[int64_t(j) * ld + i] = gij;
         }
