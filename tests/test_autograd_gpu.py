@@ -88,3 +88,34 @@ def test_gpu_transpose_used_by_adjoint_matches_oracle():
     np.testing.assert_array_equal(T.row_ptrs.cpu().numpy(), trp)
     np.testing.assert_array_equal(T.col_idxs.cpu().numpy(), tci)
     np.testing.assert_array_equal(T.values.cpu().numpy(), tv)
+
+
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+@pytest.mark.parametrize("k", [1, 3, 4, 8, 16])
+def test_sddmm_matches_dense_sampling(dt, k):
+    """out[e] = alpha u(row_e, :) . w(col_e, :) on a Csr pattern: the
+    subwarp kernel (narrow blocks) and the 16-byte lane kernel (k * value
+    size a multiple of 32 bytes) against numpy in FP64."""
+    from ginkgo_b200 import stencils
+    from ginkgo_b200._lib import call
+    from ginkgo_b200.matrix import _p, _stream
+    rp, ci, _ = stencils.power_law(3000, seed=4, mu=2.0, max_len=200)
+    n = len(rp) - 1
+    rng = np.random.default_rng(k)
+    u = rng.standard_normal((n, k))
+    w = rng.standard_normal((n, k))
+    npdt = np.float64 if dt == torch.float64 else np.float32
+    ud = torch.from_numpy(u.astype(npdt)).cuda()
+    wd = torch.from_numpy(w.astype(npdt)).cuda()
+    out = torch.empty(len(ci), dtype=dt, device="cuda")
+    rpd = torch.from_numpy(rp).cuda()
+    cid = torch.from_numpy(ci).cuda()
+    sfx = "f64" if dt == torch.float64 else "f32"
+    call(f"b2s_csr_sddmm_{sfx}", n, _p(rpd), _p(cid), int(np.diff(rp).max()), _p(ud), k,
+         _p(wd), k, k, -0.5, _p(out), _stream(out))
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    uq, wq = u.astype(npdt).astype(np.float64), w.astype(npdt).astype(np.float64)
+    ref = -0.5 * np.einsum("ij,ij->i", uq[rows], wq[ci])
+    scale = 0.5 * np.einsum("ij,ij->i", np.abs(uq[rows]), np.abs(wq[ci]))
+    tol = 1e-14 if dt == torch.float64 else 1e-6
+    assert (np.abs(out.cpu().numpy() - ref) / scale).max() <= tol
