@@ -78,12 +78,6 @@ __device__ __forceinline__ void cp_async_elem(E* smem, const E* gmem)
         asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
     }
 }
-// One 16-byte copy that bypasses L1 (both addresses 16-byte aligned).
-__device__ __forceinline__ void cp_async_16(void* smem, const void* gmem)
-{
-    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
-}
 __device__ __forceinline__ void cp_async_commit()
 {
     asm volatile("cp.async.commit_group;\n" ::);
@@ -100,13 +94,7 @@ struct __align__(16) AsyncStage {
     int32_t cols[kAsyncCap];
 };
 
-// WIDE: the stage is filled with 16-byte copies from the aligned-down group
-// start (v and ci must then be 16-byte aligned; a unit that would reach past
-// the last stored entry is copied element by element), so a group of 224
-// FP64 entries takes about 6 copy instructions per lane instead of 14.  The
-// copied range starts up to 3 entries early, so a staged group holds at
-// most kAsyncCap - 4 entries.
-template <typename T, int K, bool VEC, int LPR = 1, bool WIDE = false>
+template <typename T, int K, bool VEC, int LPR = 1>
 __global__ void __launch_bounds__(kAsyncBlock)
     csr_async_kernel(int64_t n, const int32_t* __restrict__ rp,
                      const int32_t* __restrict__ ci, const T* __restrict__ v,
@@ -118,7 +106,7 @@ __global__ void __launch_bounds__(kAsyncBlock)
     static_assert(LPR >= 1 && LPR <= 32 && (32 % LPR) == 0, "LPR divides 32");
     constexpr unsigned kFull = 0xffffffffu;
     constexpr int R = kWarp / LPR;  // rows per group
-    constexpr int kCap = WIDE ? kAsyncCap - 4 : kAsyncCap;  // staged entries
+    constexpr int kCap = kAsyncCap;  // staged entries
     __shared__ AsyncStage<T> stages[kAsyncBlock / kWarp][2];
     const int lane = threadIdx.x % kWarp, wid = threadIdx.x / kWarp;
     const int myrow = lane / LPR, sub = lane % LPR;
@@ -141,40 +129,10 @@ __global__ void __launch_bounds__(kAsyncBlock)
         start = __shfl_sync(kFull, p, 0);
         cnt = pe - start;
     };
-    constexpr int VPU = int(16 / sizeof(T));  // values per 16-byte unit
-    constexpr int CPU = 4;                     // column indices per unit
-    // offsets of the group's first entry inside its stage arrays
-    auto vmis = [&](int start) { return WIDE ? start & (VPU - 1) : 0; };
-    auto cmis = [&](int start) { return WIDE ? start & (CPU - 1) : 0; };
-    int nnz = 0;  // stored entries (bounds the 16-byte units)
-    if constexpr (WIDE) nnz = __ldg(rp + n);
     auto issue = [&](int s, int start, int cnt) {
-        if constexpr (WIDE) {
-            const int va = start - vmis(start), vu = (vmis(start) + cnt + VPU - 1) / VPU;
-            for (int u = lane; u < vu; u += kWarp) {
-                const int e = va + u * VPU;
-                if (e + VPU <= nnz) {
-                    cp_async_16(&st[s].vals[u * VPU], v + e);
-                } else {
-                    for (int q = 0; q < VPU && e + q < nnz; ++q)
-                        cp_async_elem(&st[s].vals[u * VPU + q], v + e + q);
-                }
-            }
-            const int ca = start - cmis(start), cu = (cmis(start) + cnt + CPU - 1) / CPU;
-            for (int u = lane; u < cu; u += kWarp) {
-                const int e = ca + u * CPU;
-                if (e + CPU <= nnz) {
-                    cp_async_16(&st[s].cols[u * CPU], ci + e);
-                } else {
-                    for (int q = 0; q < CPU && e + q < nnz; ++q)
-                        cp_async_elem(&st[s].cols[u * CPU + q], ci + e + q);
-                }
-            }
-        } else {
-            for (int i = lane; i < cnt; i += kWarp) {
-                cp_async_elem(&st[s].vals[i], v + start + i);
-                cp_async_elem(&st[s].cols[i], ci + start + i);
-            }
+        for (int i = lane; i < cnt; i += kWarp) {
+            cp_async_elem(&st[s].vals[i], v + start + i);
+            cp_async_elem(&st[s].cols[i], ci + start + i);
         }
     };
     if (skip != nullptr && *skip) return;  // whole grid (solver idle)
@@ -206,8 +164,8 @@ __global__ void __launch_bounds__(kAsyncBlock)
         const int64_t row = g * R + myrow;
         if (cnt <= kCap) {
             const AsyncStage<T>& cur = st[s];
-            const T* cv = cur.vals + vmis(start);
-            const int32_t* cc = cur.cols + cmis(start);
+            const T* cv = cur.vals;
+            const int32_t* cc = cur.cols;
 #pragma unroll 4
             for (int i = rs - start + sub; i < re - start; i += LPR) {
                 T xr[K];

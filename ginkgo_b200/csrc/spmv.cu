@@ -62,229 +62,199 @@ __global__ void __launch_bounds__(kBlock)
 }
 
 // ---------------------------------------------------------------------------
-// Csr load_balance: the rows are binned into tiles of kTileItems merge-path
-// items (one item per row plus one per stored entry; row r goes to tile
-// floor((r + rp[r]) / kTileItems)), built once on the GPU by
-// csr_tile_rows_kernel.  A block stages its tile's products val * b(col, :)
-// through shared memory with coalesced loads, in chunks of kChunk entries,
-// and a block-wide segmented scan (heads at row starts) sums every row.  A
-// row longer than a chunk is carried from chunk to chunk inside the block,
-// so no row is split across blocks: no atomics, no fix-up pass, and the
-// result does not depend on scheduling.
+// Csr load_balance: the stored entries are cut into chunks of kLbChunk
+// consecutive entries (nnz-balanced, whatever the row lengths), one warp per
+// chunk, persistent over the chunks.  A warp stages its chunk's values and
+// column indices in shared memory with coalesced loads and sums the rows it
+// owns, the rows whose last entry lies in the chunk (an empty row belongs to
+// the chunk holding its position): a lane per row for short segments, the
+// whole warp for a segment of more than 32 entries.  The part of a row that
+// lies in earlier chunks arrives through those chunks' tail partials: a
+// chunk whose last entry's row continues past it sums that row's entries in
+// the chunk into its partial slot, and a fix-up pass adds every run of
+// partials to its row (alpha times their sum, in chunk order).  No atomics;
+// the result does not depend on scheduling.
+//
+// The partition buffer (built once per matrix on the GPU, the role of
+// srow): own_first[nc + 1] (the first row each chunk owns), tail_row[nc],
+// and nc slots of 16 partial sums (the scratch of the fix-up, rewritten by
+// every SpMV: SpMVs of one matrix that overlap on the GPU race on it).
 // ---------------------------------------------------------------------------
-constexpr int kTileItems = 2048;
+constexpr int kLbChunk = 256;  // entries per chunk
+constexpr int kLbSlot = 16;    // partial sums per chunk (right-hand sides)
 
-__global__ void csr_tile_rows_kernel(int64_t n, const int32_t* __restrict__ rp,
-                                     int64_t num_tiles,
-                                     int32_t* __restrict__ tile_rows)
+inline int64_t lb_chunks(int64_t nnz) { return std::max<int64_t>(1, ceildiv(nnz, kLbChunk)); }
+// int32 words of the partition buffer of nc chunks: own_first, tail_row, an
+// 8-byte aligned block of nc * 16 doubles
+inline int64_t lb_words(int64_t nc) { return 34 * nc + 4; }
+inline int64_t lb_chunks_of_words(int64_t words) { return (words - 4) / 34; }
+inline int64_t lb_partials_offset(int64_t nc) { return (2 * nc + 1 + 1) / 2 * 2; }
+
+// The chunk that owns row r: that of its last entry, or (empty row) that of
+// its position, clamped to the last chunk.
+__device__ __forceinline__ int64_t lb_owner(const int32_t* __restrict__ rp, int64_t r,
+                                            int64_t nc)
 {
-    const int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-    if (t > num_tiles) return;
-    // first row r with r + rp[r] >= t * kTileItems (n when none)
-    const int64_t target = t * kTileItems;
+    const int64_t s = __ldg(rp + r), e = __ldg(rp + r + 1);
+    const int64_t q = e > s ? e - 1 : min(s, nc * kLbChunk - 1);
+    return q / kLbChunk;
+}
+
+// own_first[c]: the first row whose owner is c or later (n for c = nc).
+__global__ void csr_lb_setup_kernel(int64_t n, const int32_t* __restrict__ rp, int64_t nc,
+                                    int32_t* __restrict__ own_first)
+{
+    const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+    if (c > nc) return;
     int64_t lo = 0, hi = n;
     while (lo < hi) {
         const int64_t mid = (lo + hi) / 2;
-        if (mid + int64_t(__ldg(rp + mid)) >= target) {
+        if (lb_owner(rp, mid, nc) >= c) {
             hi = mid;
         } else {
             lo = mid + 1;
         }
     }
-    tile_rows[t] = int32_t(t == num_tiles ? n : lo);
+    own_first[c] = int32_t(c == nc ? n : lo);
 }
 
-// One pad word per 16: thread t scans the 8-byte words [8t, 8t + 8), which
-// would otherwise fall into the same banks every other thread.
-__device__ __forceinline__ int lb_pad(int w) { return w + (w >> 4); }
+// K sums of the staged chunk entries [s, e) (offsets into the chunk's stage
+// sv/sc), taking every step-th entry from s + first.
+template <typename T, int K, bool VEC>
+__device__ __forceinline__ void lb_row_sum(const T* sv, const int32_t* sc, int s, int e,
+                                           int step, int first, const T* __restrict__ b,
+                                           int64_t ldb, T (&acc)[K])
+{
+#pragma unroll
+    for (int j = 0; j < K; ++j) acc[j] = T(0);
+    // unrolled so that several gathers of b are in flight per lane
+#pragma unroll 4
+    for (int i = s + first; i < e; i += step) {
+        const T val = sv[i];
+        T xr[K];
+        RowLoad<T, K, VEC>::load(b + int64_t(sc[i]) * ldb, xr);
+#pragma unroll
+        for (int j = 0; j < K; ++j) acc[j] += val * xr[j];
+    }
+}
 
+// lane j < K receives the warp total of acc[j]
 template <typename T, int K>
-struct LbSmem {
-    static constexpr int kIpt = K >= 8 ? 1 : 8 / K;  // entries per thread
-    static constexpr int kChunk = kBlock * kIpt;
-    T prod[kChunk * K + kChunk * K / 16 + 1];
-    unsigned char head[kChunk];
-    int32_t rows[kTileItems + 1];  // rp[r0 .. r1]
-    T carry[K];
-    T warp_sum[kBlock / kWarp][K];
-    int warp_flag[kBlock / kWarp];
-};
+__device__ __forceinline__ T lb_warp_totals(T (&acc)[K], int lane)
+{
+    T a = T(0);
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        const T t = warp_sum(acc[j]);
+        if (lane == j) a = t;
+    }
+    return a;
+}
+
+// A row of more than 32 entries in the chunk, summed by the whole warp.  Kept
+// out of line: rows this long are rare, and inlined the loop costs the
+// lane-per-row path registers.
+template <typename T, int K, bool VEC>
+__device__ __noinline__ void lb_long_row(const T* sv, const int32_t* sc, int s, int e, int lane,
+                                         const T* __restrict__ b, int64_t ldb, T* dst,
+                                         const T* __restrict__ alpha, const T* __restrict__ beta)
+{
+    T acc[K];
+    lb_row_sum<T, K, VEC>(sv, sc, s, e, kWarp, lane, b, ldb, acc);
+    const T a = lb_warp_totals<T, K>(acc, lane);
+    if (lane < K) dst[lane] = combine(a, alpha, beta, dst + lane);
+}
 
 template <typename T, int K, bool VEC>
 __global__ void __launch_bounds__(kBlock)
-    csr_lb_kernel(const int32_t* __restrict__ tile_rows,
-                  const int32_t* __restrict__ rp,
-                  const int32_t* __restrict__ ci, const T* __restrict__ v,
-                  const T* __restrict__ b, int64_t ldb, T* __restrict__ c,
-                  int64_t ldc, const T* __restrict__ alpha,
+    csr_lb_kernel(int64_t n, int64_t nc, const int32_t* __restrict__ own_first,
+                  int32_t* __restrict__ tail_row, T* __restrict__ partials,
+                  const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                  const T* __restrict__ v, const T* __restrict__ b, int64_t ldb,
+                  T* __restrict__ c, int64_t ldc, const T* __restrict__ alpha,
                   const T* __restrict__ beta)
 {
-    using Smem = LbSmem<T, K>;
-    constexpr int kIpt = Smem::kIpt;
-    constexpr int kChunk = Smem::kChunk;
-    __shared__ Smem sm;
-    const int tid = threadIdx.x;
-    const int32_t r0 = tile_rows[blockIdx.x];
-    const int32_t r1 = tile_rows[blockIdx.x + 1];
-    if (r0 >= r1) return;
-    const int nrows = r1 - r0;  // <= kTileItems by construction
-    for (int i = tid; i <= nrows; i += kBlock) sm.rows[i] = __ldg(rp + r0 + i);
-    if (tid < K) sm.carry[tid] = T(0);
-    __syncthreads();
-    const int e_begin = sm.rows[0];
-    const int e_end = sm.rows[nrows];
-    // empty rows produce 0 (alpha A b is 0 there)
-    for (int i = tid; i < nrows; i += kBlock) {
-        if (sm.rows[i] == sm.rows[i + 1]) {
-            T* dst = c + int64_t(r0 + i) * ldc;
-#pragma unroll
-            for (int j = 0; j < K; ++j) dst[j] = combine(T(0), alpha, beta, dst + j);
+    constexpr unsigned kFull = 0xffffffffu;
+    __shared__ T sv_all[kBlock / kWarp][kLbChunk];
+    __shared__ int32_t sc_all[kBlock / kWarp][kLbChunk];
+    const int lane = threadIdx.x % kWarp, wid = threadIdx.x / kWarp;
+    T* sv = sv_all[wid];
+    int32_t* sc = sc_all[wid];
+    const int64_t nwarps = int64_t(gridDim.x) * (kBlock / kWarp);
+    const int64_t nnz = __ldg(rp + n);
+    for (int64_t ch = blockIdx.x * int64_t(kBlock / kWarp) + wid; ch < nc; ch += nwarps) {
+        const int64_t e0 = ch * kLbChunk;
+        const int len = int(min(int64_t(kLbChunk), nnz - e0));  // entries in the chunk
+        for (int i = lane; i < len; i += kWarp) {
+            sv[i] = ld_stream(v + e0 + i);
+            sc[i] = ld_stream(ci + e0 + i);
         }
+        __syncwarp();
+        const int r0 = own_first[ch], r1 = own_first[ch + 1];
+        // owned rows, 32 at a time (warp-uniform trip count); entry offsets
+        // are relative to the chunk: an owned row ends inside it and may
+        // start before it
+        for (int rb = r0; rb < r1; rb += kWarp) {
+            const int r = rb + lane;
+            const bool valid = r < r1;
+            const int s = valid ? int(max(int64_t(__ldg(rp + r)) - e0, int64_t(0))) : 0;
+            const int e = valid ? int(int64_t(__ldg(rp + r + 1)) - e0) : 0;
+            const bool longseg = e - s > kWarp;
+            if (valid && !longseg) {
+                T acc[K];
+                lb_row_sum<T, K, VEC>(sv, sc, s, e, 1, 0, b, ldb, acc);
+                T* dst = c + int64_t(r) * ldc;
+#pragma unroll
+                for (int j = 0; j < K; ++j) dst[j] = combine(acc[j], alpha, beta, dst + j);
+            }
+            unsigned mask = __ballot_sync(kFull, longseg);
+            while (mask) {
+                const int bit = __ffs(mask) - 1;
+                mask &= mask - 1;
+                const int rl = __shfl_sync(kFull, r, bit);
+                const int sl = __shfl_sync(kFull, s, bit);
+                const int el = __shfl_sync(kFull, e, bit);
+                lb_long_row<T, K, VEC>(sv, sc, sl, el, lane, b, ldb, c + int64_t(rl) * ldc,
+                                       alpha, beta);
+            }
+        }
+        // the row that continues past the chunk: its part here, as a partial
+        const int rt = r1;
+        const int64_t st = rt < n ? int64_t(__ldg(rp + rt)) : nnz;
+        const bool tail = st < e0 + len;
+        if (tail) {
+            T acc[K];
+            lb_row_sum<T, K, VEC>(sv, sc, int(max(st - e0, int64_t(0))), len, kWarp, lane, b,
+                                  ldb, acc);
+            const T a = lb_warp_totals<T, K>(acc, lane);
+            if (lane < K) partials[ch * kLbSlot + lane] = a;
+        }
+        if (lane == 0) tail_row[ch] = tail ? rt : -1;
+        __syncwarp();  // the stage is refilled for the next chunk
     }
-    for (int cs = e_begin; cs < e_end; cs += kChunk) {
-        const int ce = min(cs + kChunk, e_end);
-        const int cnt = ce - cs;
-        // 1. stage products and clear head flags
-        for (int i = tid; i < kChunk; i += kBlock) {
-            sm.head[i] = 0;
-            if (i < cnt) {
-                const T val = ld_stream(v + cs + i);
-                const int64_t col = ld_stream(ci + cs + i);
-                T xr[K];
-                RowLoad<T, K, VEC>::load(b + col * ldb, xr);
+}
+
+// Adds each run of tail partials to its row: c(r, :) += alpha * sum.
+template <typename T, int K>
+__global__ void csr_lb_fixup_kernel(int64_t nc, const int32_t* __restrict__ tail_row,
+                                    const T* __restrict__ partials, T* __restrict__ c,
+                                    int64_t ldc, const T* __restrict__ alpha)
+{
+    const int64_t ch = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+    if (ch >= nc) return;
+    const int32_t r = tail_row[ch];
+    if (r < 0 || (ch > 0 && tail_row[ch - 1] == r)) return;  // not a run start
+    T acc[K];
 #pragma unroll
-                for (int j = 0; j < K; ++j) sm.prod[lb_pad(i * K + j)] = val * xr[j];
-            }
-        }
-        __syncthreads();
-        // 2. mark row starts inside the chunk (rows sorted by start)
-        for (int i = tid; i < nrows; i += kBlock) {
-            const int s = sm.rows[i];
-            if (s > cs && s < ce && sm.rows[i + 1] > s) sm.head[s - cs] = 1;
-        }
-        if (tid == 0) sm.head[0] = 1;  // chunk start: carry added below
-        __syncthreads();
-        // 3. segmented inclusive scan: per-thread run, then warp/block
-        T run[K];
-        int any_head = 0;
-        const int base = tid * kIpt;
+    for (int j = 0; j < K; ++j) acc[j] = T(0);
+    for (int64_t q = ch; q < nc && tail_row[q] == r; ++q) {
 #pragma unroll
-        for (int j = 0; j < K; ++j) run[j] = T(0);
-#pragma unroll
-        for (int q = 0; q < kIpt; ++q) {
-            const int i = base + q;
-            if (i < cnt) {
-                if (sm.head[i]) {
-                    any_head = 1;
-#pragma unroll
-                    for (int j = 0; j < K; ++j) run[j] = T(0);
-                }
-#pragma unroll
-                for (int j = 0; j < K; ++j) {
-                    run[j] += sm.prod[lb_pad(i * K + j)];
-                    sm.prod[lb_pad(i * K + j)] = run[j];
-                }
-            }
-        }
-        // exclusive segmented prefix of thread aggregates (flag, run)
-        const int lane = tid % kWarp, wid = tid / kWarp;
-        T pre[K];
-        int pflag = any_head;
-#pragma unroll
-        for (int j = 0; j < K; ++j) pre[j] = run[j];
-#pragma unroll
-        for (int off = 1; off < kWarp; off *= 2) {
-            const int of = __shfl_up_sync(0xffffffffu, pflag, off);
-            T ov[K];
-#pragma unroll
-            for (int j = 0; j < K; ++j) ov[j] = __shfl_up_sync(0xffffffffu, pre[j], off);
-            if (lane >= off) {
-                if (!pflag) {
-#pragma unroll
-                    for (int j = 0; j < K; ++j) pre[j] += ov[j];
-                }
-                pflag |= of;
-            }
-        }
-        // pre/pflag: inclusive over lanes 0..lane
-        if (lane == kWarp - 1) {
-            sm.warp_flag[wid] = pflag;
-#pragma unroll
-            for (int j = 0; j < K; ++j) sm.warp_sum[wid][j] = pre[j];
-        }
-        __syncthreads();
-        // exclusive prefix for this thread = inclusive of lane-1 combined
-        // with the preceding warps' aggregates
-        T ex[K];
-        {
-            int f = __shfl_up_sync(0xffffffffu, pflag, 1);
-            T t[K];
-#pragma unroll
-            for (int j = 0; j < K; ++j) t[j] = __shfl_up_sync(0xffffffffu, pre[j], 1);
-            if (lane == 0) {
-                f = 0;
-#pragma unroll
-                for (int j = 0; j < K; ++j) t[j] = T(0);
-            }
-            if (!f) {
-                // walk back over previous warps until one has a head
-                for (int w = wid - 1; w >= 0; --w) {
-#pragma unroll
-                    for (int j = 0; j < K; ++j) t[j] += sm.warp_sum[w][j];
-                    if (sm.warp_flag[w]) {
-                        f = 1;
-                        break;
-                    }
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < K; ++j) ex[j] = t[j];
-        }
-        // add the exclusive prefix to this thread's entries up to its first
-        // head (those continue the previous segment)
-#pragma unroll
-        for (int q = 0; q < kIpt; ++q) {
-            const int i = base + q;
-            if (i < cnt) {
-                if (sm.head[i]) break;
-#pragma unroll
-                for (int j = 0; j < K; ++j) sm.prod[lb_pad(i * K + j)] += ex[j];
-            }
-        }
-        __syncthreads();
-        // 4. rows ending in this chunk write their sums; the first of them
-        //    adds the carry when it started in an earlier chunk
-        for (int i = tid; i < nrows; i += kBlock) {
-            const int s = sm.rows[i], e = sm.rows[i + 1];
-            if (e > s && e > cs && e <= ce) {
-                T* dst = c + int64_t(r0 + i) * ldc;
-#pragma unroll
-                for (int j = 0; j < K; ++j) {
-                    T val = sm.prod[lb_pad((e - 1 - cs) * K + j)];
-                    if (s < cs) val += sm.carry[j];
-                    dst[j] = combine(val, alpha, beta, dst + j);
-                }
-            }
-        }
-        __syncthreads();
-        // 5. carry of the row still open at the chunk end: the row holding
-        //    entry ce - 1 is the last i with rows[i] <= ce - 1; its partial
-        //    is prod[cnt - 1], plus the old carry if it began before cs
-        if (tid < K && ce < e_end) {
-            int lo = 0, hi = nrows;  // rows[lo] <= ce - 1 < rows[hi]
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) / 2;
-                if (sm.rows[mid] <= ce - 1) {
-                    lo = mid;
-                } else {
-                    hi = mid;
-                }
-            }
-            const T part = sm.prod[lb_pad((cnt - 1) * K + tid)];
-            sm.carry[tid] = sm.rows[lo] < cs ? sm.carry[tid] + part : part;
-        }
-        __syncthreads();
+        for (int j = 0; j < K; ++j) acc[j] += partials[q * kLbSlot + j];
     }
+    const T a = alpha ? *alpha : T(1);
+    T* dst = c + int64_t(r) * ldc;
+#pragma unroll
+    for (int j = 0; j < K; ++j) dst[j] += a * acc[j];
 }
 
 // ---------------------------------------------------------------------------
@@ -490,6 +460,123 @@ __global__ void __launch_bounds__(kBlock)
 }
 
 // ---------------------------------------------------------------------------
+// Csr load_balance with K >= 4 right-hand sides in 16-byte aligned rows: the
+// chunk partition and partial sums of csr_lb_kernel, with KL = K / VW lanes
+// per row each owning one 16-byte column slice (as rhs_lanes_kernel), so
+// 32 / KL rows of a chunk run at a time.  A row with more than 2 * 32 / KL
+// entries in the chunk, and the row that continues past it, are summed by
+// all 32 / KL row slots together (entries strided by the slot count, then
+// a shuffle reduction over the slots).
+// ---------------------------------------------------------------------------
+template <typename T, int K>
+__device__ __forceinline__ void lb_slice_sum(const T* sv, const int32_t* sc, int s, int e,
+                                             int step, int first, const T* __restrict__ bc,
+                                             int64_t ldb, typename Vec16<T>::type& acc)
+{
+#pragma unroll 4
+    for (int i = s + first; i < e; i += step) fma_vec<T>(acc, sv[i], bc + int64_t(sc[i]) * ldb);
+}
+
+template <typename T, int KL>
+__device__ __forceinline__ void lb_slot_reduce(typename Vec16<T>::type& acc)
+{
+    T* a = reinterpret_cast<T*>(&acc);
+#pragma unroll
+    for (int off = KL; off < kWarp; off *= 2) {
+#pragma unroll
+        for (int u = 0; u < Vec16<T>::width; ++u) {
+            a[u] += __shfl_xor_sync(0xffffffffu, a[u], off);
+        }
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void vec_zero(typename Vec16<T>::type& acc)
+{
+    T* a = reinterpret_cast<T*>(&acc);
+#pragma unroll
+    for (int u = 0; u < Vec16<T>::width; ++u) a[u] = T(0);
+}
+
+template <typename T, int K>
+__global__ void __launch_bounds__(kBlock)
+    csr_lb_lanes_kernel(int64_t n, int64_t nc, const int32_t* __restrict__ own_first,
+                        int32_t* __restrict__ tail_row, T* __restrict__ partials,
+                        const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                        const T* __restrict__ v, const T* __restrict__ b, int64_t ldb,
+                        T* __restrict__ c, int64_t ldc, const T* __restrict__ alpha,
+                        const T* __restrict__ beta)
+{
+    using V = typename Vec16<T>::type;
+    constexpr int VW = Vec16<T>::width;
+    constexpr int KL = K / VW;     // lanes per row
+    constexpr int R = kWarp / KL;  // rows at a time
+    constexpr unsigned kFull = 0xffffffffu;
+    __shared__ T sv_all[kBlock / kWarp][kLbChunk];
+    __shared__ int32_t sc_all[kBlock / kWarp][kLbChunk];
+    const int lane = threadIdx.x % kWarp, wid = threadIdx.x / kWarp;
+    const int part = lane % KL, slot = lane / KL;
+    T* sv = sv_all[wid];
+    int32_t* sc = sc_all[wid];
+    const T* bc = b + part * VW;
+    const int64_t nwarps = int64_t(gridDim.x) * (kBlock / kWarp);
+    const int64_t nnz = __ldg(rp + n);
+    for (int64_t ch = blockIdx.x * int64_t(kBlock / kWarp) + wid; ch < nc; ch += nwarps) {
+        const int64_t e0 = ch * kLbChunk;
+        const int len = int(min(int64_t(kLbChunk), nnz - e0));
+        for (int i = lane; i < len; i += kWarp) {
+            sv[i] = ld_stream(v + e0 + i);
+            sc[i] = ld_stream(ci + e0 + i);
+        }
+        __syncwarp();
+        const int r0 = own_first[ch], r1 = own_first[ch + 1];
+        for (int rb = r0; rb < r1; rb += R) {  // warp-uniform trip count
+            const int r = rb + slot;
+            const bool valid = r < r1;
+            const int s = valid ? int(max(int64_t(__ldg(rp + r)) - e0, int64_t(0))) : 0;
+            const int e = valid ? int(int64_t(__ldg(rp + r + 1)) - e0) : 0;
+            const bool longseg = e - s > 2 * R;
+            if (valid && !longseg) {
+                V acc;
+                vec_zero<T>(acc);
+                lb_slice_sum<T, K>(sv, sc, s, e, 1, 0, bc, ldb, acc);
+                store_vec<T>(c + int64_t(r) * ldc + part * VW, acc, alpha, beta);
+            }
+            unsigned mask = __ballot_sync(kFull, longseg && part == 0);
+            while (mask) {
+                const int bit = __ffs(mask) - 1;
+                mask &= mask - 1;
+                const int rl = __shfl_sync(kFull, r, bit);
+                const int sl = __shfl_sync(kFull, s, bit);
+                const int el = __shfl_sync(kFull, e, bit);
+                V acc;
+                vec_zero<T>(acc);
+                lb_slice_sum<T, K>(sv, sc, sl, el, R, slot, bc, ldb, acc);
+                lb_slot_reduce<T, KL>(acc);
+                if (slot == 0) store_vec<T>(c + int64_t(rl) * ldc + part * VW, acc, alpha, beta);
+            }
+        }
+        // the row that continues past the chunk: its part here, as a partial
+        const int rt = r1;
+        const int64_t st = rt < n ? int64_t(__ldg(rp + rt)) : nnz;
+        const bool tail = st < e0 + len;
+        if (tail) {
+            V acc;
+            vec_zero<T>(acc);
+            lb_slice_sum<T, K>(sv, sc, int(max(st - e0, int64_t(0))), len, R, slot, bc, ldb, acc);
+            lb_slot_reduce<T, KL>(acc);
+            if (slot == 0) {
+                const T* a = reinterpret_cast<const T*>(&acc);
+#pragma unroll
+                for (int u = 0; u < VW; ++u) partials[ch * kLbSlot + part * VW + u] = a[u];
+            }
+        }
+        if (lane == 0) tail_row[ch] = tail ? rt : -1;
+        __syncwarp();  // the stage is refilled for the next chunk
+    }
+}
+
+// ---------------------------------------------------------------------------
 // host-side dispatch
 // ---------------------------------------------------------------------------
 
@@ -587,8 +674,8 @@ int csr_spmv(int strategy, int64_t n, int64_t num_cols, const int32_t* rp,
     B2S_CHECK_ARG(rp && b && c, "null pointer");
     cudaStream_t st = as_stream(stream);
     if (strategy == B2S_CSR_LOAD_BALANCE) {
-        B2S_CHECK_ARG(tile_rows != nullptr && num_tiles >= 1,
-                      "load_balance needs the tile partition");
+        B2S_CHECK_ARG(tile_rows != nullptr && num_tiles >= 37 && (num_tiles - 3) % 34 == 0,
+                      "load_balance needs the partition from b2s_csr_load_balance_setup");
     } else {
         B2S_CHECK_ARG(strategy == B2S_CSR_CLASSICAL, "unknown strategy %d",
                       strategy);
@@ -600,14 +687,38 @@ int csr_spmv(int strategy, int64_t n, int64_t num_cols, const int32_t* rp,
         const T* bb = b + col0;
         T* cc = c + col0;
         if (strategy == B2S_CSR_LOAD_BALANCE) {
+            const int64_t nc = lb_chunks_of_words(num_tiles + 1);
+            int32_t* own_first = const_cast<int32_t*>(tile_rows);
+            int32_t* tail_row = own_first + nc + 1;
+            T* partials = reinterpret_cast<T*>(own_first + lb_partials_offset(nc));
+            const int64_t grid = std::min<int64_t>(ceildiv(nc, kBlock / kWarp),
+                                                   int64_t(num_sms()) * 8);
+            const bool lanes = lanes_ok(b, ldb, c, ldc, col0, kk);
+            // lanes_ok implies K >= 4 and K a multiple of the vector width
             B2S_DISPATCH_K(kk, VEC, {
-                if (vec) {
-                    csr_lb_kernel<T, K, true><<<num_tiles, kBlock, 0, st>>>(
-                        tile_rows, rp, ci, v, bb, ldb, cc, ldc, alpha, beta);
-                } else {
-                    csr_lb_kernel<T, K, false><<<num_tiles, kBlock, 0, st>>>(
-                        tile_rows, rp, ci, v, bb, ldb, cc, ldc, alpha, beta);
+                bool launched = false;
+                if constexpr (K >= 4 && K % Vec16<T>::width == 0) {
+                    if (lanes) {
+                        csr_lb_lanes_kernel<T, K><<<grid, kBlock, 0, st>>>(
+                            n, nc, own_first, tail_row, partials, rp, ci, v, bb, ldb, cc, ldc,
+                            alpha, beta);
+                        launched = true;
+                    }
                 }
+                if (launched) {
+                    // the column-slice form above
+                } else if (vec) {
+                    csr_lb_kernel<T, K, true><<<grid, kBlock, 0, st>>>(
+                        n, nc, own_first, tail_row, partials, rp, ci, v, bb, ldb, cc, ldc,
+                        alpha, beta);
+                } else {
+                    csr_lb_kernel<T, K, false><<<grid, kBlock, 0, st>>>(
+                        n, nc, own_first, tail_row, partials, rp, ci, v, bb, ldb, cc, ldc,
+                        alpha, beta);
+                }
+                B2S_LAUNCH_CHECK();
+                csr_lb_fixup_kernel<T, K><<<ceildiv(nc, 256), 256, 0, st>>>(
+                    nc, tail_row, partials, cc, ldc, alpha);
             });
         } else if (lanes_ok(b, ldb, c, ldc, col0, kk)) {
             B2S_DISPATCH_K(kk, VEC, {
@@ -795,25 +906,22 @@ extern "C" {
 
 int64_t b2s_csr_load_balance_num_tiles(int64_t num_rows, int64_t nnz)
 {
-    if (num_rows <= 0) return 1;
-    return ceildiv(num_rows + nnz, kTileItems);
+    if (num_rows < 0 || nnz < 0) return -1;
+    return lb_words(lb_chunks(nnz)) - 1;
 }
 
 int b2s_csr_load_balance_setup(int64_t num_rows, int64_t nnz,
                                const int32_t* row_ptrs, int64_t num_tiles,
                                int32_t* tile_rows, void* stream)
 {
+    B2S_CHECK_ARG(num_rows >= 0 && nnz >= 0, "negative size");
     B2S_CHECK_ARG(num_tiles == b2s_csr_load_balance_num_tiles(num_rows, nnz),
                   "num_tiles must come from b2s_csr_load_balance_num_tiles");
-    B2S_CHECK_ARG(tile_rows != nullptr, "null tile_rows");
-    if (num_rows <= 0) {
-        B2S_CUDA_TRY(cudaMemsetAsync(tile_rows, 0, 2 * sizeof(int32_t),
-                                     as_stream(stream)));
-        return B2S_OK;
-    }
-    const int64_t threads = num_tiles + 1;
-    csr_tile_rows_kernel<<<ceildiv(threads, 256), 256, 0, as_stream(stream)>>>(
-        num_rows, row_ptrs, num_tiles, tile_rows);
+    B2S_CHECK_ARG(tile_rows != nullptr && (num_rows == 0 || row_ptrs != nullptr),
+                  "null pointer");
+    const int64_t nc = lb_chunks(nnz);
+    csr_lb_setup_kernel<<<ceildiv(nc + 1, 256), 256, 0, as_stream(stream)>>>(
+        num_rows, row_ptrs, nc, tile_rows);
     B2S_LAUNCH_CHECK();
     return B2S_OK;
 }

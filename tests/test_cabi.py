@@ -18,10 +18,13 @@ def test_library_exports_every_declared_symbol():
 
 def test_load_balance_tile_count():
     lib = _lib.lib()
-    assert lib.b2s_csr_load_balance_num_tiles(0, 0) == 1
-    assert lib.b2s_csr_load_balance_num_tiles(2048, 0) == 1
+    # 34 words per 256-entry chunk (at least one chunk) + 4, minus one
+    assert lib.b2s_csr_load_balance_num_tiles(0, 0) == 37
+    assert lib.b2s_csr_load_balance_num_tiles(2048, 0) == 37
+    assert lib.b2s_csr_load_balance_num_tiles(10, 257) == 34 * 2 + 3
     assert lib.b2s_csr_load_balance_num_tiles(2097152, 14581760) == \
-        (2097152 + 14581760 + 2047) // 2048
+        34 * ((14581760 + 255) // 256) + 3
+    assert lib.b2s_csr_load_balance_num_tiles(-1, 0) == -1
 
 
 def _spmv(**kw):
@@ -41,6 +44,9 @@ def test_spmv_rejects_bad_arguments_without_device_work():
     assert b"alpha and beta" in lib.b2s_last_error()
     assert _spmv(k=3, ldb=2, ldc=3, rp=fake, b=fake, c=fake) == -1
     assert _spmv(strategy=1, rp=fake, b=fake, c=fake) == -1
+    assert b"partition" in lib.b2s_last_error()
+    # a partition size that b2s_csr_load_balance_num_tiles cannot return
+    assert _spmv(strategy=1, rp=fake, b=fake, c=fake, tiles=fake, nt=40) == -1
     assert b"partition" in lib.b2s_last_error()
     # empty work is a no-op that needs no device
     assert _spmv(n=0) == 0

@@ -138,6 +138,41 @@ def test_empty_rows_and_single_long_row(exe, fmt):
     assert_spmv_close(rp, ci, v, x, y.cpu().numpy(), ref, 1e-14)
 
 
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+@pytest.mark.parametrize("k", [1, 5, 20])
+def test_load_balance_chunk_boundaries(exe, dt, k):
+    # load_balance cuts the entries into 256-entry chunks: rows that end
+    # exactly on a boundary, rows of 250..260 entries that straddle one or
+    # two, runs of empty rows at boundaries and at the end, rows longer than a
+    # warp inside a chunk, and nnz a multiple of 256.  k = 20 runs two column
+    # passes (16 + 4) over the same partial-sum scratch; plain and advanced.
+    rng = np.random.default_rng(31 + k)
+    n = 6000
+    lens = rng.choice([0, 0, 0, 1, 3, 40, 250, 256, 260, 600], n)
+    lens[-50:] = 0
+    lens[0] = 256
+    total = int(lens.sum())
+    lens[1] += (-total) % 256  # nnz a multiple of 256
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    ci = np.concatenate([rng.choice(n, l, replace=False) for l in lens]).astype(np.int32)
+    v = rng.standard_normal(int(rp[-1])).astype(NP[dt])
+    x = rng.standard_normal((n, k)).astype(NP[dt])
+    y0 = rng.standard_normal((n, k)).astype(NP[dt])
+    A = Csr.read(exe, rp, ci, v, dtype=dt).set_strategy("load_balance")
+    xd = torch.from_numpy(x).cuda()
+    y = torch.full((n, k), float("nan"), dtype=dt, device="cuda")
+    A.apply(xd, y)
+    assert_spmv_close(rp, ci, v, x, y.cpu().numpy(), orc.csr_spmv(rp, ci, v, x), TOL[dt])
+    y2 = torch.from_numpy(y0).cuda()
+    A.apply(0.75, xd, -2.0, y2)
+    assert_spmv_close(rp, ci, v, x, y2.cpu().numpy(), orc.csr_spmv(rp, ci, v, x, y0, 0.75, -2.0),
+                      TOL[dt] * 4, alpha=0.75, beta_y=2.0 * y0.astype(np.float64))
+    # run to run identical: no atomics in the partial sums
+    y3 = torch.full((n, k), float("nan"), dtype=dt, device="cuda")
+    A.apply(xd, y3)
+    assert torch.equal(y, y3)
+
+
 @pytest.mark.parametrize("fmt", FORMATS)
 def test_empty_matrix(exe, fmt):
     A = Csr(exe, (0, 0), torch.zeros(1, dtype=torch.int32), torch.zeros(0, dtype=torch.int32),
