@@ -1,4 +1,4 @@
-// Fused preconditioned CG (scalar Jacobi or identity), the loop of
+// Fused preconditioned CG (scalar Jacobi, block Jacobi or identity), the loop of
 // core/solver/cg.cpp:91-189 with the kernels of
 // common/unified/solver/cg_kernels.cpp:23-107 regrouped into two passes per
 // iteration and no host synchronisation inside the loop:
@@ -19,13 +19,17 @@
 // one right-hand side on a system of 2^19 rows or more the SpMV pass is
 // split so that the matrix streams through the pipelined Csr kernel.
 //
-// z is never stored.  Per-column stopping status uses the reference's bit
+// With scalar Jacobi z is never stored.  A block Jacobi preconditioner
+// stores z = M^-1 r, formed in the update pass (see cg_block_kernel), and
+// the SpMV passes read it in place of D^-1 r.  Per-column stopping status
+// uses the reference's bit
 // layout; stopped columns are frozen as in the reference.  The host replays
 // a CUDA graph of `check_every` iterations and reads the stop flag once per
 // replay.
 #include <cstring>
 
 #include "csr_async.cuh"
+#include "jacobi_scheme.cuh"
 #include "solver_common.cuh"
 
 namespace b2s {
@@ -42,6 +46,62 @@ __device__ __forceinline__ T cg_p(T d, T r, T beta, T p, bool from_z)
 {
     const T z = mul_rn(d, r);
     return from_z ? z : add_rn(z, mul_rn(beta, p));
+}
+
+// The last block's part of the initial pass (thread 0): tot holds ||b||^2,
+// rho = dot(r, z) and ||r||^2 of every column (K each); sets the starting
+// norms, rho and the initial stopping status.
+template <typename T, int K>
+__device__ void cg_init_finish(const T* tot, int k, SolveCtl* ctl, CgScalars<T>* sc)
+{
+    ctl->ticket = 0;
+    ctl->iter = 0;
+    int all = 1;
+    for (int j = 0; j < K; ++j) {
+        uint8_t s = 0;
+        if (j >= k) {
+            stop_status(s, kIterationId, true);  // padding column
+        }
+        sc->start[j] = start_norm(ctl, T(sqrt(tot[j])), T(sqrt(tot[2 * K + j])));
+        sc->rho[j] = tot[K + j];
+        sc->prev_rho[j] = T(1);
+        sc->alpha[j] = T(0);
+        sc->tau[j] = sqrt(tot[2 * K + j]);
+        if (ctl->max_iters <= 0) stop_status(s, kIterationId, true);
+        if (residual_met(ctl, sc->tau[j], sc->rho[j], sc->start[j])) {
+            converge_status(s, kResidualId, true);
+        }
+        ctl->status[j] = s;
+        all &= has_stopped(s);
+    }
+    ctl->all_stopped = all;
+}
+
+// The last block's part of the update pass (thread 0): tot holds the new
+// rho = dot(r, z) and ||r||^2 per column; advances the iteration, swaps rho
+// and applies the Iteration and residual checks.
+template <typename T, int K>
+__device__ void cg_update_finish(const T* tot, SolveCtl* ctl, CgScalars<T>* sc)
+{
+    ctl->ticket = 0;
+    const int iter = ctl->iter + 1;
+    ctl->iter = iter;
+    int all = 1;
+    for (int j = 0; j < K; ++j) {
+        uint8_t s = ctl->status[j];
+        if (!has_stopped(s)) {
+            sc->prev_rho[j] = sc->rho[j];
+            sc->rho[j] = tot[j];
+            sc->tau[j] = sqrt(tot[K + j]);
+            if (residual_met(ctl, sc->tau[j], sc->rho[j], sc->start[j])) {
+                converge_status(s, kResidualId, true);
+            }
+            if (iter >= ctl->max_iters) stop_status(s, kIterationId, true);
+            ctl->status[j] = s;
+        }
+        all &= has_stopped(s);
+    }
+    ctl->all_stopped = all;
 }
 
 template <typename T, int K>
@@ -73,29 +133,7 @@ __global__ void __launch_bounds__(kSolverBlock)
     block_partials<T, 3 * K>(acc, partials, red);
     if (last_block_done(&ctl->ticket, &last)) {
         sum_partials<T, 3 * K>(partials, gridDim.x, tot, red);
-        if (threadIdx.x == 0) {
-            ctl->ticket = 0;
-            ctl->iter = 0;
-            int all = 1;
-            for (int j = 0; j < K; ++j) {
-                uint8_t s = 0;
-                if (j >= k) {
-                    stop_status(s, kIterationId, true);  // padding column
-                }
-                sc->start[j] = start_norm(ctl, T(sqrt(tot[j])), T(sqrt(tot[2 * K + j])));
-                sc->rho[j] = tot[K + j];
-                sc->prev_rho[j] = T(1);
-                sc->alpha[j] = T(0);
-                sc->tau[j] = sqrt(tot[2 * K + j]);
-                if (ctl->max_iters <= 0) stop_status(s, kIterationId, true);
-                if (residual_met(ctl, sc->tau[j], sc->rho[j], sc->start[j])) {
-                    converge_status(s, kResidualId, true);
-                }
-                ctl->status[j] = s;
-                all &= has_stopped(s);
-            }
-            ctl->all_stopped = all;
-        }
+        if (threadIdx.x == 0) cg_init_finish<T, K>(tot, k, ctl, sc);
     }
 }
 
@@ -215,27 +253,7 @@ __global__ void __launch_bounds__(kSolverBlock)
     block_partials<T, 2 * K>(acc, partials, red);
     if (last_block_done(&ctl->ticket, &last)) {
         sum_partials<T, 2 * K>(partials, gridDim.x, tot, red);
-        if (threadIdx.x == 0) {
-            ctl->ticket = 0;
-            const int iter = ctl->iter + 1;
-            ctl->iter = iter;
-            int all = 1;
-            for (int j = 0; j < K; ++j) {
-                uint8_t s = ctl->status[j];
-                if (!has_stopped(s)) {
-                    sc->prev_rho[j] = sc->rho[j];
-                    sc->rho[j] = tot[j];
-                    sc->tau[j] = sqrt(tot[K + j]);
-                    if (residual_met(ctl, sc->tau[j], sc->rho[j], sc->start[j])) {
-                        converge_status(s, kResidualId, true);
-                    }
-                    if (iter >= ctl->max_iters) stop_status(s, kIterationId, true);
-                    ctl->status[j] = s;
-                }
-                all &= has_stopped(s);
-            }
-            ctl->all_stopped = all;
-        }
+        if (threadIdx.x == 0) cg_update_finish<T, K>(tot, ctl, sc);
     }
 }
 
@@ -424,27 +442,7 @@ __global__ void __launch_bounds__(kSolverBlock)
         sum_partials<T, K>(partials, gridDim.x, tot, reinterpret_cast<T*>(red));
         sum_partials<T, K>(partials + int64_t(gridDim.x) * K, gridDim.x, tot + K,
                            reinterpret_cast<T*>(red));
-        if (threadIdx.x == 0) {
-            ctl->ticket = 0;
-            const int iter = ctl->iter + 1;
-            ctl->iter = iter;
-            int all = 1;
-            for (int j = 0; j < K; ++j) {
-                uint8_t s = ctl->status[j];
-                if (!has_stopped(s)) {
-                    sc->prev_rho[j] = sc->rho[j];
-                    sc->rho[j] = tot[j];
-                    sc->tau[j] = sqrt(tot[K + j]);
-                    if (residual_met(ctl, sc->tau[j], sc->rho[j], sc->start[j])) {
-                        converge_status(s, kResidualId, true);
-                    }
-                    if (iter >= ctl->max_iters) stop_status(s, kIterationId, true);
-                    ctl->status[j] = s;
-                }
-                all &= has_stopped(s);
-            }
-            ctl->all_stopped = all;
-        }
+        if (threadIdx.x == 0) cg_update_finish<T, K>(tot, ctl, sc);
     }
 }
 
@@ -502,13 +500,142 @@ __global__ void __launch_bounds__(kSolverBlock)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Block Jacobi: z = M^-1 r is no longer a row-wise scale, so it is stored.
+// The SpMV passes above run with z in place of r and no diagonal
+// (p' = z + beta p); the update pass below (and the initial one, INIT)
+// runs one warp per group of the block-interleaved storage, lane (sub, i)
+// owning row i of block sub of the group: r -= alpha q and x += alpha p'
+// for the lane's row, then z of the row from the block's new residual,
+// which the block's lanes pass along by shuffles (inverse columns in the
+// order of apply_block, reference/preconditioner/jacobi_kernels.cpp:
+// 419-445), and dot(r, z), ||r||^2.  INIT additionally zeroes p and sums
+// ||b||^2 (cg::initialize and the first z = M r, core/solver/cg.cpp:
+// 122-149).
+// ---------------------------------------------------------------------------
+template <typename T, int MB2, int K, bool INIT>
+__global__ void __launch_bounds__(kSolverBlock)
+    cg_block_kernel(int64_t n, BlockPrec<T> bp, const T* __restrict__ b, int64_t ldb, int k,
+                    T* __restrict__ x, int64_t ldx, T* __restrict__ r, T* __restrict__ z,
+                    T* __restrict__ p, const T* __restrict__ q, SolveCtl* ctl,
+                    CgScalars<T>* sc, T* __restrict__ partials)
+{
+    constexpr int NS = INIT ? 3 : 2;  // sums per column
+    constexpr unsigned kFull = 0xffffffffu;
+    __shared__ T red[kSolverBlock / kWarp * NS * K];
+    __shared__ T tot[NS * K];
+    __shared__ int last;
+    if (!INIT && ctl->all_stopped) return;
+    bool active[K];
+    T alpha[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        active[j] = INIT || !has_stopped(ctl->status[j]);
+        alpha[j] = INIT ? T(0) : sc->alpha[j];
+    }
+    T acc[NS * K];
+#pragma unroll
+    for (int j = 0; j < NS * K; ++j) acc[j] = T(0);
+    const BlockScheme bsc = block_scheme(bp.max_bs);
+    const int lane = threadIdx.x % kWarp;
+    const int sub = lane / bp.max_bs, i = lane % bp.max_bs;
+    const bool in_group = lane < bsc.gs * bp.max_bs;
+    const int base = sub * bp.max_bs;  // first lane of this lane's block
+    const int64_t ngroups = (bp.num_blocks + bsc.gs - 1) / bsc.gs;
+    const int64_t nwarps = int64_t(gridDim.x) * (kSolverBlock / kWarp);
+    for (int64_t grp = blockIdx.x * int64_t(kSolverBlock / kWarp) + threadIdx.x / kWarp;
+         grp < ngroups; grp += nwarps) {
+        const int64_t blk = grp * bsc.gs + sub;
+        int s = 0, bs = 0;
+        const bool in_block = in_group && blk < bp.num_blocks &&
+                              block_extent(bp.ptrs, blk, n, bp.max_bs, s, bs);
+        const bool act = in_block && i < bs;
+        const int64_t row = s + i;
+        T inv[MB2];
+        const T* g = bp.blocks + grp * bsc.group + lane;
+#pragma unroll
+        for (int c = 0; c < MB2; ++c) {
+            inv[c] = in_group && c < bp.max_bs ? __ldg(g + c * bsc.stride) : T(0);
+        }
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            T rn = T(0);
+            if (act) {
+                if (INIT) {
+                    rn = r[row * K + j];
+                    p[row * K + j] = T(0);
+                    const T bb = j < k ? b[row * ldb + j] : T(0);
+                    acc[j] += bb * bb;
+                } else if (active[j]) {
+                    x[row * ldx + j] += alpha[j] * p[row * K + j];
+                    rn = r[row * K + j] - alpha[j] * q[row * K + j];
+                    r[row * K + j] = rn;
+                }
+            }
+            if (!active[j]) continue;  // uniform: a frozen column keeps its z
+            T zz = T(0);
+#pragma unroll
+            for (int c = 0; c < MB2; ++c) {
+                if (c < bp.max_bs) {
+                    const T rc = __shfl_sync(kFull, rn, (base + c) % kWarp);
+                    if (act && c < bs) zz += inv[c] * rc;
+                }
+            }
+            if (act) {
+                z[row * K + j] = zz;
+                acc[(NS - 2) * K + j] += rn * zz;
+                acc[(NS - 1) * K + j] += rn * rn;
+            }
+        }
+    }
+    block_partials<T, NS * K>(acc, partials, red);
+    if (last_block_done(&ctl->ticket, &last)) {
+        sum_partials<T, NS * K>(partials, gridDim.x, tot, red);
+        if (threadIdx.x == 0) {
+            if constexpr (INIT) {
+                cg_init_finish<T, K>(tot, k, ctl, sc);
+            } else {
+                cg_update_finish<T, K>(tot, ctl, sc);
+            }
+        }
+    }
+}
+
+// Launches cg_block_kernel for the block size class of bp.
+template <typename T, int K, bool INIT>
+void launch_cg_block(int64_t n, const BlockPrec<T>& bp, const T* b, int64_t ldb, int k, T* x,
+                     int64_t ldx, T* r, T* z, T* p, const T* q, SolveCtl* ctl,
+                     CgScalars<T>* sc, T* partials, cudaStream_t st)
+{
+    const BlockScheme bsc = block_scheme(bp.max_bs);
+    const int64_t ngroups = ceildiv(bp.num_blocks, bsc.gs);
+    const int grid = int(std::min<int64_t>(
+        std::max<int64_t>(1, ceildiv(ngroups, kSolverBlock / kWarp)), solver_grid()));
+    const int mb2 = kMaxBs / bsc.gs;
+#define B2S_CG_BLOCK(MB)                                                           \
+    case MB:                                                                       \
+        cg_block_kernel<T, MB, K, INIT><<<grid, kSolverBlock, 0, st>>>(            \
+            n, bp, b, ldb, k, x, ldx, r, z, p, q, ctl, sc, partials);              \
+        break;
+    switch (mb2) {
+        B2S_CG_BLOCK(2)
+        B2S_CG_BLOCK(4)
+        B2S_CG_BLOCK(8)
+        B2S_CG_BLOCK(16)
+        B2S_CG_BLOCK(32)
+    default: B2S_CG_BLOCK(1)
+    }
+#undef B2S_CG_BLOCK
+}
+
 struct CgLayout {
     int64_t bytes;
-    int64_t off_ctl, off_sc, off_r, off_p0, off_p1, off_q, off_partials;
+    int64_t off_ctl, off_sc, off_r, off_p0, off_p1, off_q, off_partials, off_z;
 };
 
+// with_z: the stored z = M^-1 r of a block preconditioner
 template <typename T>
-CgLayout cg_layout(int64_t n, int K)
+CgLayout cg_layout(int64_t n, int K, bool with_z = false)
 {
     Carver c{nullptr};
     CgLayout l;
@@ -519,14 +646,16 @@ CgLayout cg_layout(int64_t n, int K)
     l.off_p1 = c.take<T>(n * K);
     l.off_q = c.take<T>(n * K);
     l.off_partials = c.take<T>(int64_t(kSolverGrid) * 3 * K);
+    l.off_z = with_z ? c.take<T>(n * K) : 0;
     l.bytes = c.used;
     return l;
 }
 
+// bp: a block Jacobi preconditioner (dinv then null), or null
 template <typename T>
 int cg_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
-             int64_t max_row_nnz, const T* dinv, const T* b, int64_t ldb, T* x,
-             int64_t ldx, int64_t k, int64_t max_iters, double reduction,
+             int64_t max_row_nnz, const T* dinv, const BlockPrec<T>* bp, const T* b,
+             int64_t ldb, T* x, int64_t ldx, int64_t k, int64_t max_iters, double reduction,
              int residual_mode, int64_t check_every, void* workspace,
              int64_t workspace_bytes,
              int64_t* iterations, double* residual_norms, uint8_t* status,
@@ -538,8 +667,14 @@ int cg_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
                   "max_iters out of range");
     B2S_CHECK_ARG(valid_residual_mode(residual_mode), "unknown residual mode %d",
                   residual_mode);
+    if (bp) {
+        B2S_CHECK_ARG(bp->max_bs >= 1 && bp->max_bs <= kMaxBs,
+                      "max_block_size must be 1..32");
+        B2S_CHECK_ARG(bp->num_blocks >= 1 && bp->ptrs && bp->blocks,
+                      "block preconditioner without blocks");
+    }
     const int K = rhs_bucket(k);
-    const CgLayout lay = cg_layout<T>(n, K);
+    const CgLayout lay = cg_layout<T>(n, K, bp != nullptr);
     if (workspace_bytes < lay.bytes) {
         set_error("workspace of %lld bytes < %lld", (long long)workspace_bytes,
                   (long long)lay.bytes);
@@ -555,6 +690,9 @@ int cg_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
                reinterpret_cast<T*>(w + lay.off_p1)};
     T* q = reinterpret_cast<T*>(w + lay.off_q);
     T* partials = reinterpret_cast<T*>(w + lay.off_partials);
+    // block preconditioner: the SpMV passes read the stored z in place of r
+    T* z = bp ? reinterpret_cast<T*>(w + lay.off_z) : nullptr;
+    T* zr = bp ? z : r;
 
     SolveCtl h{};
     h.max_iters = int(max_iters);
@@ -575,23 +713,33 @@ int cg_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
                 n, rp, ci, v, x, ldx, b, ldb, int(k), r);
         });
         B2S_LAUNCH_CHECK();
-        cg_init_kernel<T, K><<<grid_vec, kSolverBlock, 0, st>>>(
-            n, dinv, b, ldb, int(k), r, p[0], ctl, sc, partials);
+        if (bp) {
+            launch_cg_block<T, K, true>(n, *bp, b, ldb, int(k), x, ldx, r, z, p[0], nullptr,
+                                        ctl, sc, partials, st);
+        } else {
+            cg_init_kernel<T, K><<<grid_vec, kSolverBlock, 0, st>>>(
+                n, dinv, b, ldb, int(k), r, p[0], ctl, sc, partials);
+        }
         B2S_LAUNCH_CHECK();
     });
     // the split single-RHS pass (large systems)
     const int lpr = async_lanes_per_row(max_row_nnz);
     const int64_t async_need = ceildiv(ceildiv(n, kWarp / lpr), kAsyncBlock / kWarp);
     auto launch_split = [&](cudaStream_t cs, T* po, T* pn) {
-        cg_pupdate_kernel<T><<<grid_vec, kSolverBlock, 0, cs>>>(n, dinv, r, po, pn, ctl, sc);
+        cg_pupdate_kernel<T><<<grid_vec, kSolverBlock, 0, cs>>>(n, dinv, zr, po, pn, ctl, sc);
         with_async_kernel<T, 1, false>(lpr, [&](auto kernel) {
             const int64_t grid = std::min<int64_t>(async_need, async_resident_blocks(kernel));
             kernel<<<grid, kAsyncBlock, 0, cs>>>(n, rp, ci, v, pn, 1, q, 1, nullptr, nullptr,
                                                  &ctl->all_stopped);
         });
         cg_pq_kernel<T><<<grid_vec, kSolverBlock, 0, cs>>>(n, pn, q, ctl, sc, partials);
-        cg_update_kernel<T, 1><<<grid_vec, kSolverBlock, 0, cs>>>(n, dinv, x, ldx, r, pn, q,
-                                                                  ctl, sc, partials);
+        if (bp) {
+            launch_cg_block<T, 1, false>(n, *bp, nullptr, 0, 1, x, ldx, r, z, pn, q, ctl, sc,
+                                         partials, cs);
+        } else {
+            cg_update_kernel<T, 1><<<grid_vec, kSolverBlock, 0, cs>>>(n, dinv, x, ldx, r, pn,
+                                                                      q, ctl, sc, partials);
+        }
     };
     auto capture = [&](cudaStream_t cs) -> int {
         for (int it = 0; it < chunk; ++it) {
@@ -613,16 +761,26 @@ int cg_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
                     const int gu = int(std::min<int64_t>(
                         std::max<int64_t>(1, ceildiv(n * K / VW, kSolverBlock)), solver_grid()));
                     cg_spmv_lanes_kernel<T, K><<<gs, kSolverBlock, 0, cs>>>(
-                        n, rp, ci, v, dinv, r, po, pn, q, ctl, sc, partials);
-                    cg_update_lanes_kernel<T, K><<<gu, kSolverBlock, 0, cs>>>(
-                        n, dinv, x, ldx, r, pn, q, ctl, sc, partials);
+                        n, rp, ci, v, dinv, zr, po, pn, q, ctl, sc, partials);
+                    if (bp) {
+                        launch_cg_block<T, K, false>(n, *bp, nullptr, 0, int(k), x, ldx, r, z,
+                                                     pn, q, ctl, sc, partials, cs);
+                    } else {
+                        cg_update_lanes_kernel<T, K><<<gu, kSolverBlock, 0, cs>>>(
+                            n, dinv, x, ldx, r, pn, q, ctl, sc, partials);
+                    }
                 } else {
                     B2S_DISPATCH_SW(sw, {
                         cg_spmv_kernel<T, SW, K><<<grid_spmv, kSolverBlock, 0, cs>>>(
-                            n, rp, ci, v, dinv, r, po, pn, q, ctl, sc, partials);
+                            n, rp, ci, v, dinv, zr, po, pn, q, ctl, sc, partials);
                     });
-                    cg_update_kernel<T, K><<<grid_vec, kSolverBlock, 0, cs>>>(
-                        n, dinv, x, ldx, r, pn, q, ctl, sc, partials);
+                    if (bp) {
+                        launch_cg_block<T, K, false>(n, *bp, nullptr, 0, int(k), x, ldx, r, z,
+                                                     pn, q, ctl, sc, partials, cs);
+                    } else {
+                        cg_update_kernel<T, K><<<grid_vec, kSolverBlock, 0, cs>>>(
+                            n, dinv, x, ldx, r, pn, q, ctl, sc, partials);
+                    }
                 }
             });
             B2S_LAUNCH_CHECK();
@@ -661,6 +819,15 @@ int64_t b2s_cg_workspace_bytes(int64_t num_rows, int64_t num_rhs,
                             : cg_layout<float>(num_rows, K).bytes;
 }
 
+int64_t b2s_cg_block_workspace_bytes(int64_t num_rows, int64_t num_rhs,
+                                     int value_bytes)
+{
+    const int K = rhs_bucket(num_rhs);
+    if (K < 0 || num_rows < 0) return -1;
+    return value_bytes == 8 ? cg_layout<double>(num_rows, K, true).bytes
+                            : cg_layout<float>(num_rows, K, true).bytes;
+}
+
 #define B2S_CG_ENTRY(T, S)                                                    \
     int b2s_cg_solve_##S(int64_t num_rows, const int32_t* row_ptrs,           \
                          const int32_t* col_idxs, const T* values,            \
@@ -674,11 +841,32 @@ int64_t b2s_cg_workspace_bytes(int64_t num_rows, int64_t num_rhs,
                          void* stream)                                        \
     {                                                                         \
         return cg_solve<T>(num_rows, row_ptrs, col_idxs, values, max_row_nnz, \
-                           inv_diag, b, ldb, x, ldx, num_rhs, max_iters,      \
-                           reduction_factor, residual_mode, check_every,      \
-                           workspace,                                         \
+                           inv_diag, nullptr, b, ldb, x, ldx, num_rhs,        \
+                           max_iters, reduction_factor, residual_mode,        \
+                           check_every, workspace,                            \
                            workspace_bytes, iterations, residual_norms,       \
                            status, stream);                                   \
+    }                                                                         \
+    int b2s_cg_block_solve_##S(                                               \
+        int64_t num_rows, const int32_t* row_ptrs, const int32_t* col_idxs,  \
+        const T* values, int64_t max_row_nnz, int64_t num_blocks,            \
+        const int32_t* block_ptrs, int max_block_size, const T* blocks,       \
+        const T* b, int64_t ldb, T* x, int64_t ldx, int64_t num_rhs,          \
+        int64_t max_iters, double reduction_factor, int residual_mode,        \
+        int64_t check_every, void* workspace, int64_t workspace_bytes,        \
+        int64_t* iterations, double* residual_norms, uint8_t* status,         \
+        void* stream)                                                         \
+    {                                                                         \
+        BlockPrec<T> bp;                                                      \
+        bp.num_blocks = num_blocks;                                           \
+        bp.ptrs = block_ptrs;                                                 \
+        bp.max_bs = max_block_size;                                           \
+        bp.blocks = blocks;                                                   \
+        return cg_solve<T>(num_rows, row_ptrs, col_idxs, values, max_row_nnz, \
+                           nullptr, &bp, b, ldb, x, ldx, num_rhs, max_iters,  \
+                           reduction_factor, residual_mode, check_every,      \
+                           workspace, workspace_bytes, iterations,            \
+                           residual_norms, status, stream);                   \
     }
 
 B2S_CG_ENTRY(double, f64)

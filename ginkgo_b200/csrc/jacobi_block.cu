@@ -13,44 +13,12 @@
 // stride = gs * max_bs, group_offset = max_bs * stride.  Column col of the
 // gs blocks of a group is one contiguous run of gs * max_bs values, so the
 // apply reads it with one coalesced warp load.
-#include "common.cuh"
+#include "jacobi_scheme.cuh"
 
 namespace b2s {
 namespace {
 
 constexpr int kJacobiWarps = 4;  // warps per CTA
-constexpr int kMaxBs = 32;
-
-struct BlockScheme {
-    int gs;          // blocks per group (a power of two)
-    int power;       // log2(gs)
-    int64_t stride;  // between the columns of a block
-    int64_t group;   // between groups
-};
-
-inline __host__ __device__ BlockScheme block_scheme(int max_bs)
-{
-    int p2 = 1;
-    while (p2 < max_bs) p2 *= 2;
-    BlockScheme sc;
-    sc.gs = kMaxBs / p2;
-    sc.power = 0;
-    while ((1 << sc.power) < sc.gs) ++sc.power;
-    sc.stride = int64_t(sc.gs) * max_bs;
-    sc.group = int64_t(max_bs) * sc.stride;
-    return sc;
-}
-
-// Valid extent of block `blk`: 0 <= s <= e <= n and e - s <= max_bs.
-__device__ __forceinline__ bool block_extent(const int32_t* ptrs, int64_t blk, int64_t n,
-                                             int max_bs, int& s, int& bs)
-{
-    const int64_t s64 = ptrs[blk], e64 = ptrs[blk + 1];
-    if (s64 < 0 || e64 > n || e64 < s64 || e64 - s64 > max_bs) return false;
-    s = int(s64);
-    bs = int(e64 - s64);
-    return true;
-}
 
 template <typename T>
 __device__ __forceinline__ T magnitude(T v)

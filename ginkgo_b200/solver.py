@@ -10,8 +10,8 @@ reference's ``gko::solver`` / ``gko::stop`` / ``gko::preconditioner`` API:
     solver.apply(b, x)                # x holds the initial guess
     solver.logger.num_iterations      # like gko::log::Convergence
 
-Only scalar Jacobi (max_block_size 1) or no preconditioner is fused into
-the solvers; stopping is Iteration plus one residual criterion, ResidualNorm
+Scalar Jacobi (max_block_size 1) is fused into every solver, block Jacobi
+into CG; stopping is Iteration plus one residual criterion, ResidualNorm
 (baselines rhs_norm, initial_resnorm, absolute) or, for CG and BiCGStab,
 ImplicitResidualNorm (include/ginkgo/core/stop/residual_norm.hpp).
 """
@@ -187,8 +187,9 @@ class BlockJacobi:
     """preconditioner::Jacobi with max_block_size 2..32 and full-precision
     blocks (core/preconditioner/jacobi.cpp:370-420): the diagonal blocks
     inverted on the device (b2s_jacobi_block_generate_*), applied as
-    x = D^-1 b or alpha D^-1 b + beta x.  Not fused into the solvers here
-    (they take scalar Jacobi)."""
+    x = D^-1 b or alpha D^-1 b + beta x.  CG applies the blocks inside its
+    update pass (b2s_cg_block_solve_*); BiCGStab and GMRES take scalar
+    Jacobi only."""
 
     def __init__(self, A: Csr, max_block_size: int, block_pointers=None):
         self.A = A
@@ -221,8 +222,8 @@ class BlockJacobi:
 
     @property
     def inv_diag(self):
-        raise NotImplementedError("the solvers here fuse scalar Jacobi only "
-                                  "(with_max_block_size(1))")
+        raise NotImplementedError("BiCGStab and GMRES here fuse scalar Jacobi only "
+                                  "(with_max_block_size(1)); CG takes block Jacobi")
 
     def apply(self, *args):
         """apply(b, x) or apply(alpha, b, beta, x)."""
@@ -367,18 +368,27 @@ class _Solver:
         x2 = _check_dense(x, n, A.dtype, "x")
         k = b2.shape[1]
         name = self.f.kind
-        nbytes = getattr(lib(), f"b2s_{name}_workspace_bytes")(
-            n, k, A.values.element_size())
-        ws = self._workspace(nbytes)
         it = C.c_int64(0)
         res = np.zeros(k, np.float64)
         st = np.zeros(k, np.uint8)
-        call(f"b2s_{name}_solve_{_SFX[A.dtype]}", n, _p(A.row_ptrs), _p(A.col_idxs),
-             _p(A.values), A.max_row_nnz, _p(self.inv_diag), _p(b2), b2.stride(0),
-             _p(x2), x2.stride(0), k, self.f.max_iters, self.f.reduction,
-             self.f.residual_mode, self.f.check_every, _p(ws), ws.numel(), C.byref(it),
-             res.ctypes.data_as(C.c_void_p), st.ctypes.data_as(C.c_void_p),
-             _stream(x2))
+        tail = (_p(b2), b2.stride(0), _p(x2), x2.stride(0), k, self.f.max_iters,
+                self.f.reduction, self.f.residual_mode, self.f.check_every)
+        outs = (C.byref(it), res.ctypes.data_as(C.c_void_p),
+                st.ctypes.data_as(C.c_void_p), _stream(x2))
+        M = self.precond
+        if name == "cg" and isinstance(M, BlockJacobi):
+            nbytes = lib().b2s_cg_block_workspace_bytes(n, k, A.values.element_size())
+            ws = self._workspace(nbytes)
+            call(f"b2s_cg_block_solve_{_SFX[A.dtype]}", n, _p(A.row_ptrs), _p(A.col_idxs),
+                 _p(A.values), A.max_row_nnz, M.num_blocks, _p(M._ptrs), M.max_block_size,
+                 _p(M.blocks), *tail, _p(ws), ws.numel(), *outs)
+        else:
+            nbytes = getattr(lib(), f"b2s_{name}_workspace_bytes")(
+                n, k, A.values.element_size())
+            ws = self._workspace(nbytes)
+            call(f"b2s_{name}_solve_{_SFX[A.dtype]}", n, _p(A.row_ptrs), _p(A.col_idxs),
+                 _p(A.values), A.max_row_nnz, _p(self.inv_diag), *tail, _p(ws), ws.numel(),
+                 *outs)
         self.logger = ConvergenceLog(int(it.value), res.tolist(),
                                      bool(np.all(st & 0x80)), st.tolist())
         return x

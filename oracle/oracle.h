@@ -80,6 +80,11 @@ extern "C" {
                    const T* v, const T* inv_diag, const T* b, T* x,           \
                    int64_t k, int max_iters, double reduction, int mode,      \
                    int* iters_out, double* res_norm_out);                     \
+    int orc_cg_block_##S(int64_t n, const int32_t* rp, const int32_t* ci,     \
+                         const T* v, int64_t nblocks, const int32_t* bptrs,   \
+                         int max_bs, const T* binv, const T* b, T* x,         \
+                         int64_t k, int max_iters, double reduction,          \
+                         int mode, int* iters_out, double* res_norm_out);                     \
     int orc_bicgstab_##S(int64_t n, const int32_t* rp, const int32_t* ci,     \
                          const T* v, const T* inv_diag, const T* b, T* x,     \
                          int max_iters, double reduction, int mode,           \

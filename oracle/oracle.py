@@ -60,6 +60,10 @@ def lib():
             f = getattr(_lib, f"orc_cg_{s}")
             f.argtypes = [_i64, _p, _p, _p, _p, _p, _p, _i64, _i32, _f64, _i32, _p, _p]
             f.restype = _i32
+            f = getattr(_lib, f"orc_cg_block_{s}")
+            f.argtypes = [_i64, _p, _p, _p, _i64, _p, _i32, _p, _p, _p, _i64, _i32, _f64,
+                          _i32, _p, _p]
+            f.restype = _i32
             f = getattr(_lib, f"orc_bicgstab_{s}")
             f.argtypes = [_i64, _p, _p, _p, _p, _p, _p, _i32, _f64, _i32, _p, _p]
             f.restype = _i32
@@ -231,6 +235,30 @@ def cg(rp, ci, v, b, x0=None, jacobi=True, max_iters=1000, reduction=1e-10, mode
     conv = getattr(lib(), f"orc_cg_{_sfx(dt)}")(
         n, _ptr(rp), _ptr(ci), _ptr(v), _ptr(inv), _ptr(b2), _ptr(x), k,
         max_iters, reduction, int(mode), C.byref(it), _ptr(res))
+    return x.reshape(np.shape(b)), it.value, res, conv
+
+
+def cg_block(rp, ci, v, b, block_ptrs, blocks, max_block_size, x0=None, max_iters=1000,
+             reduction=1e-10, mode=0):
+    """CG with a block Jacobi preconditioner: block_ptrs delimit the blocks,
+    blocks[i] is block i's inverse (square, its block's size), as
+    oracle.jacobi.generate returns them.  Returns as cg."""
+    rp, ci, v = _c(rp, np.int32), _c(ci, np.int32), np.ascontiguousarray(v)
+    dt = v.dtype
+    b2 = _as2d(_c(b, dt))
+    n, k = b2.shape
+    x = np.zeros((n, k), dt) if x0 is None else _as2d(_c(x0, dt)).copy()
+    m = int(max_block_size)
+    ptrs = _c(block_ptrs, np.int32)
+    binv = np.zeros((len(ptrs) - 1, m, m), dt)
+    for i, blk in enumerate(blocks):
+        s = np.asarray(blk).shape[0]
+        binv[i, :s, :s] = blk
+    it = C.c_int(0)
+    res = np.zeros(k, np.float64)
+    conv = getattr(lib(), f"orc_cg_block_{_sfx(dt)}")(
+        n, _ptr(rp), _ptr(ci), _ptr(v), len(ptrs) - 1, _ptr(ptrs), m, _ptr(binv), _ptr(b2),
+        _ptr(x), k, max_iters, reduction, int(mode), C.byref(it), _ptr(res))
     return x.reshape(np.shape(b)), it.value, res, conv
 
 

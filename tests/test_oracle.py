@@ -257,3 +257,22 @@ def test_residual_modes_of_the_oracle():
                                 mode=orc.IMPLICIT)
     _, it_e, _, _ = orc.cg(rp, ci, v, b, x0=x0, max_iters=2000, reduction=1e-8, mode=0)
     assert conv_i == 1 and it_i != it_e
+
+
+def test_cg_block_oracle():
+    # unit blocks reproduce the scalar-Jacobi CG bit for bit; blocks of 4
+    # consecutive rows converge to the explicit residual goal
+    from oracle import jacobi as J
+    rp, ci, v = stencils.poisson_3d_7pt(8)
+    n = len(rp) - 1
+    b = np.random.default_rng(1).standard_normal(n)
+    _, inv = J.generate(rp, ci, v, 1)
+    x1, i1, _, _ = orc.cg(rp, ci, v, b, max_iters=500, reduction=1e-10)
+    x2, i2, _, c2 = orc.cg_block(rp, ci, v, b, np.arange(n + 1), [np.array([[d]]) for d in inv],
+                                 1, max_iters=500, reduction=1e-10)
+    assert i1 == i2 and c2 == 1 and np.array_equal(x1, x2)
+    ptrs = list(range(0, n + 1, 4))
+    _, bp, blocks = J.generate(rp, ci, v, 4, block_ptrs=ptrs)
+    x3, i3, _, c3 = orc.cg_block(rp, ci, v, b, bp, blocks, 4, max_iters=500, reduction=1e-10)
+    r = b - orc.csr_spmv(rp, ci, v, x3)
+    assert c3 == 1 and i3 <= i1 and np.linalg.norm(r) <= 1e-10 * np.linalg.norm(b)
