@@ -453,11 +453,13 @@ def mtx_section(steps):
 
 def profile_tour():
     """One capped invocation of every kernel family on inputs larger than
-    L2, for an ncu launch list with DRAM byte counters: SpMV in every
-    format (FP64, one and four right-hand sides) on the 7-point 128^3
-    matrix, the Ell and Sellp conversions, 20 CG and 20 BiCGStab iterations
-    (one and sixteen right-hand sides), the batched BiCGStab on 1024
-    systems, and the transpose + SDDMM of the differentiable solve."""
+    L2, for the ncu launch list: SpMV in every format (FP64, one and four
+    right-hand sides) on the 7-point 128^3 matrix, the Ell and Sellp
+    conversions, 20 CG and 20 BiCGStab iterations (one and sixteen
+    right-hand sides), the batched BiCGStab on 1024 systems, the transpose +
+    SDDMM of the differentiable solve, mixed-type Csr/Ell SpMV, block Jacobi
+    (blocks of 8), 10 Arnoldi steps of GMRES and of every CB-GMRES basis
+    format, SpGEMM (A^2), SpGEAM and the Hybrid conversions and SpMV."""
     import torch
     from ginkgo_b200 import stencils
     from ginkgo_b200._lib import call
@@ -497,6 +499,30 @@ def profile_tour():
     g = torch.empty_like(A.values)
     call("b2s_csr_sddmm_f64", n, _p(At.row_ptrs), _p(At.col_idxs), At.max_row_nnz, _p(lam),
          lam.stride(0), _p(xx), xx.stride(0), 16, -1.0, _p(g), _stream(g))
+    # mixed value types: FP32 matrix with FP64 vectors (Csr and Ell)
+    A32 = A.convert_to_precision(torch.float32)
+    x1 = torch.from_numpy(rng.standard_normal((n, 1))).cuda()
+    y1 = torch.empty_like(x1)
+    A32.apply(x1, y1)
+    A32.convert_to_ell().apply(x1, y1)
+    # block Jacobi (blocks of 8), generate and apply
+    from ginkgo_b200.solver import BlockJacobi, CbGmres, Gmres
+    bj = BlockJacobi(A, 8)
+    bj.apply(x1, y1)
+    # 10 Arnoldi steps of GMRES and of each CB-GMRES basis format
+    crit10 = (Iteration.build().with_max_iters(10), ResidualNorm.build().with_reduction_factor(1e-14))
+    for fac in [Gmres.build().with_krylov_dim(30)] + [
+            CbGmres.build().with_krylov_dim(30).with_storage_precision(sp)
+            for sp in ("reduce1", "reduce2", "integer", "ireduce1", "ireduce2")]:
+        s = fac.with_criteria(*crit10).with_preconditioner(jac).on(exe).generate(A)
+        s.apply(x1[:, 0].contiguous(), torch.zeros(n, dtype=torch.float64, device="cuda"))
+    # sparse products: A^2 (SpGEMM), A + A (SpGEAM), Csr -> Hybrid -> SpMV, Csr
+    from ginkgo_b200.matrix import spgeam, spgemm
+    spgemm(A, A)
+    spgeam(1.0, A, -0.5, A)
+    H = A.convert_to_hybrid("imbalance_limit", percent=0.5)
+    H.apply(x1, y1)
+    H.convert_to_csr()
     torch.cuda.synchronize()
     print(json.dumps({"profile_tour": "done", "n": n}))
 

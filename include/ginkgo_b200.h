@@ -52,14 +52,18 @@ int b2s_version(void);
 
 /* ---------------------------------------------------------------- SpMV -- */
 
-/* Number of tiles of the load_balance partition (rows binned by their
- * merge-path start row + row_ptrs[row] into tiles of 2048 items).  The
- * partition array has num_tiles + 1 int32 entries.  Stands in for the host
- * computed srow of Csr::load_balance (include/ginkgo/core/matrix/csr.hpp:
- * 417-468, make_srow :1651-1655). */
+/* Size of the load_balance partition: the stored entries are cut into
+ * nc = ceil(nnz / 256) chunks of consecutive entries (at least one), each
+ * SpMV warp sums the rows whose last entry lies in its chunk and leaves a
+ * partial sum for a row that continues past it.  The partition array has
+ * num_tiles + 1 = 34 nc + 4 int32 entries (8-byte aligned): the first row of
+ * every chunk, the continuing row of every chunk and the partial-sum
+ * scratch every SpMV rewrites (SpMVs of one matrix must not overlap on the
+ * GPU).  Stands in for the host computed srow of Csr::load_balance
+ * (include/ginkgo/core/matrix/csr.hpp:417-468, make_srow :1651-1655). */
 int64_t b2s_csr_load_balance_num_tiles(int64_t num_rows, int64_t nnz);
 /* Builds the load_balance partition on the GPU (one binary search per
- * tile); called once per matrix like Csr::make_srow. */
+ * chunk); called once per matrix like Csr::make_srow. */
 int b2s_csr_load_balance_setup(int64_t num_rows, int64_t nnz,
                                const int32_t* row_ptrs, int64_t num_tiles,
                                int32_t* tile_rows, void* stream);
@@ -516,6 +520,39 @@ int b2s_cg_solve_f32(int64_t num_rows, const int32_t* row_ptrs,
                      void* workspace, int64_t workspace_bytes,
                      int64_t* iterations, double* residual_norms,
                      uint8_t* status, void* stream);
+/* CG preconditioned by block Jacobi: num_blocks blocks delimited by
+ * block_ptrs (num_blocks + 1 entries covering 0..num_rows, each block at
+ * most max_block_size rows), inverses in the interleaved storage that
+ * b2s_jacobi_block_generate_* writes.  z = M^-1 r is formed inside the
+ * update pass, one warp per group of blocks, and stored; otherwise as
+ * b2s_cg_solve_*.  The workspace query adds the stored z.  Replaces
+ * Cg<V>::apply_dense_impl with a Jacobi<V> preconditioner of block size
+ * > 1 (z = M r at core/solver/cg.cpp:146-149; Jacobi::apply_impl,
+ * core/preconditioner/jacobi.cpp:150-168, simple_apply). */
+int64_t b2s_cg_block_workspace_bytes(int64_t num_rows, int64_t num_rhs,
+                                     int value_bytes);
+int b2s_cg_block_solve_f64(int64_t num_rows, const int32_t* row_ptrs,
+                           const int32_t* col_idxs, const double* values,
+                           int64_t max_row_nnz, int64_t num_blocks,
+                           const int32_t* block_ptrs, int max_block_size,
+                           const double* blocks, const double* b, int64_t ldb,
+                           double* x, int64_t ldx, int64_t num_rhs,
+                           int64_t max_iters, double reduction_factor,
+                           int residual_mode, int64_t check_every,
+                           void* workspace, int64_t workspace_bytes,
+                           int64_t* iterations, double* residual_norms,
+                           uint8_t* status, void* stream);
+int b2s_cg_block_solve_f32(int64_t num_rows, const int32_t* row_ptrs,
+                           const int32_t* col_idxs, const float* values,
+                           int64_t max_row_nnz, int64_t num_blocks,
+                           const int32_t* block_ptrs, int max_block_size,
+                           const float* blocks, const float* b, int64_t ldb,
+                           float* x, int64_t ldx, int64_t num_rhs,
+                           int64_t max_iters, double reduction_factor,
+                           int residual_mode, int64_t check_every,
+                           void* workspace, int64_t workspace_bytes,
+                           int64_t* iterations, double* residual_norms,
+                           uint8_t* status, void* stream);
 
 /* Preconditioned BiCGStab, 1..16 right-hand sides.  Replaces
  * Bicgstab<V>::apply_dense_impl (core/solver/bicgstab.cpp:95-250) with
