@@ -1,5 +1,5 @@
-// Fused preconditioned BiCGStab (scalar Jacobi or identity), the loop of
-// core/solver/bicgstab.cpp:95-250 with the kernels of
+// Fused preconditioned BiCGStab (scalar Jacobi, block Jacobi or identity),
+// the loop of core/solver/bicgstab.cpp:95-250 with the kernels of
 // common/unified/solver/bicgstab_kernels.cpp:23-195 regrouped into three
 // passes per iteration, no host synchronisation inside the loop:
 //
@@ -31,6 +31,7 @@
 // then the update pass as above.  Every vector entry is rounded as in the
 // fused passes.
 #include "csr_async.cuh"
+#include "jacobi_scheme.cuh"
 #include "solver_common.cuh"
 
 namespace b2s {
@@ -273,6 +274,8 @@ __global__ void __launch_bounds__(kSolverBlock)
     }
 }
 
+// zs: block Jacobi, x += alpha p + omega zs with p = M p' and zs = M s
+// already formed (dinv then null); null: x += alpha D^-1 p + omega D^-1 s.
 template <typename T, int K>
 __global__ void __launch_bounds__(kSolverBlock)
     bicg_update_kernel(int64_t n, const T* __restrict__ dinv,
@@ -280,7 +283,7 @@ __global__ void __launch_bounds__(kSolverBlock)
                        const T* __restrict__ rr, const T* __restrict__ p,
                        const T* __restrict__ s, const T* __restrict__ t,
                        SolveCtl* ctl, BicgScalars<T>* sc,
-                       T* __restrict__ partials)
+                       T* __restrict__ partials, const T* __restrict__ zs = nullptr)
 {
     __shared__ T red[kSolverBlock / kWarp * 2 * K];
     __shared__ T tot[2 * K];
@@ -307,8 +310,8 @@ __global__ void __launch_bounds__(kSolverBlock)
                 x[i * ldx + j] += alpha[j] * mul_rn(d, p[i * K + j]);
             } else if (mode[j] == 2) {
                 const T si = s[i * K + j];
-                x[i * ldx + j] += alpha[j] * mul_rn(d, p[i * K + j]) +
-                                  omega[j] * mul_rn(d, si);
+                const T zi = zs ? zs[i * K + j] : mul_rn(d, si);
+                x[i * ldx + j] += alpha[j] * mul_rn(d, p[i * K + j]) + omega[j] * zi;
                 const T ri = si - omega[j] * t[i * K + j];
                 r[i * K + j] = ri;
                 acc[j] += rr[i * K + j] * ri;
@@ -446,13 +449,205 @@ __global__ void __launch_bounds__(kSolverBlock)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Block Jacobi (right preconditioning by the block-diagonal inverse M): the
+// preconditioned vectors M p' and M s are no longer row-wise scales, so the
+// iteration runs split for any number of right-hand sides:
+//   bicg_block_vec  p' = r + tmp (p - omega v) and y = M p'   (STEP 1)
+//   csr_async       v = A y
+//   bicg_dot1k      dot(rr, v) -> alpha
+//   bicg_block_vec  s = r - alpha v and z = M s             (STEP 2)
+//   csr_async       t = A z
+//   bicg_dot2k      dot(s, t), dot(t, t), ||s|| -> check on s, omega
+//   bicg_update     x += alpha y + omega z, r = s - omega t (zs = z)
+// bicg_block_vec runs one warp per group of the block-interleaved storage,
+// lane (sub, i) owning row i of block sub: the block's lanes form their
+// rows' entries, then M times them by shuffles (apply_block's column order,
+// reference/preconditioner/jacobi_kernels.cpp:419-445).  The sequence is
+// core/solver/bicgstab.cpp:190-250 with the preconditioner applies at
+// :194 and :229.
+// ---------------------------------------------------------------------------
+template <typename T, int MB2, int K, int STEP>
+__global__ void __launch_bounds__(kSolverBlock)
+    bicg_block_vec_kernel(int64_t n, BlockPrec<T> bp, const T* __restrict__ r,
+                          const T* __restrict__ a_old, const T* __restrict__ v_old,
+                          T* __restrict__ out, T* __restrict__ prec, SolveCtl* ctl,
+                          BicgScalars<T>* sc)
+{
+    constexpr unsigned kFull = 0xffffffffu;
+    if (ctl->all_stopped) return;
+    bool active[K], from_r[K];
+    T c1[K], c2[K];  // STEP 1: tmp, omega; STEP 2: alpha
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        active[j] = !has_stopped(ctl->status[j]);
+        if (STEP == 1) {
+            c2[j] = sc->omega[j];
+            from_r[j] = sc->prev_rho[j] * c2[j] == T(0);
+            c1[j] = from_r[j] ? T(0) : sc->rho[j] / sc->prev_rho[j] * sc->alpha[j] / c2[j];
+        } else {
+            from_r[j] = false;
+            c1[j] = sc->alpha[j];
+            c2[j] = T(0);
+        }
+    }
+    const BlockScheme bsc = block_scheme(bp.max_bs);
+    const int lane = threadIdx.x % kWarp;
+    const int sub = lane / bp.max_bs, i = lane % bp.max_bs;
+    const bool in_group = lane < bsc.gs * bp.max_bs;
+    const int base = sub * bp.max_bs;
+    const int64_t ngroups = (bp.num_blocks + bsc.gs - 1) / bsc.gs;
+    const int64_t nwarps = int64_t(gridDim.x) * (kSolverBlock / kWarp);
+    for (int64_t grp = blockIdx.x * int64_t(kSolverBlock / kWarp) + threadIdx.x / kWarp;
+         grp < ngroups; grp += nwarps) {
+        const int64_t blk = grp * bsc.gs + sub;
+        int s0 = 0, bs = 0;
+        const bool in_block = in_group && blk < bp.num_blocks &&
+                              block_extent(bp.ptrs, blk, n, bp.max_bs, s0, bs);
+        const bool act = in_block && i < bs;
+        const int64_t row = s0 + i;
+        T inv[MB2];
+        const T* g = bp.blocks + grp * bsc.group + lane;
+#pragma unroll
+        for (int c = 0; c < MB2; ++c) {
+            inv[c] = in_group && c < bp.max_bs ? __ldg(g + c * bsc.stride) : T(0);
+        }
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            if (!active[j]) continue;  // uniform
+            T val = T(0);
+            if (act) {
+                const int64_t e = row * K + j;
+                val = STEP == 1 ? bicg_p(r[e], a_old[e], v_old[e], c1[j], c2[j], from_r[j])
+                                : bicg_s(r[e], a_old[e], c1[j]);
+                out[e] = val;
+            }
+            T mz = T(0);
+#pragma unroll
+            for (int c = 0; c < MB2; ++c) {
+                if (c < bp.max_bs) {
+                    const T vc = __shfl_sync(kFull, val, (base + c) % kWarp);
+                    if (act && c < bs) mz += inv[c] * vc;
+                }
+            }
+            if (act) prec[row * K + j] = mz;
+        }
+    }
+}
+
+// dot(rr, v) per column; the last block sets alpha (as bicg_spmv1_kernel)
+template <typename T, int K>
+__global__ void __launch_bounds__(kSolverBlock)
+    bicg_dot1k_kernel(int64_t n, const T* __restrict__ rr, const T* __restrict__ v,
+                      SolveCtl* ctl, BicgScalars<T>* sc, T* __restrict__ partials)
+{
+    __shared__ T red[kSolverBlock / kWarp * K];
+    __shared__ T tot[K];
+    __shared__ int last;
+    if (ctl->all_stopped) return;
+    T acc[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) acc[j] = T(0);
+    for (int64_t i = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * kSolverBlock) {
+#pragma unroll
+        for (int j = 0; j < K; ++j) acc[j] += rr[i * K + j] * v[i * K + j];
+    }
+    block_partials<T, K>(acc, partials, red);
+    if (last_block_done(&ctl->ticket, &last)) {
+        sum_partials<T, K>(partials, gridDim.x, tot, red);
+        if (threadIdx.x < K && !has_stopped(ctl->status[threadIdx.x])) {
+            const T bv = tot[threadIdx.x];
+            sc->alpha[threadIdx.x] = bv != T(0) ? sc->rho[threadIdx.x] / bv : T(0);
+        }
+        if (threadIdx.x == 0) ctl->ticket = 0;
+    }
+}
+
+// dot(s, t), dot(t, t), ||s||^2 per column; the last block checks s and
+// sets omega (as bicg_spmv2_kernel)
+template <typename T, int K>
+__global__ void __launch_bounds__(kSolverBlock)
+    bicg_dot2k_kernel(int64_t n, const T* __restrict__ s, const T* __restrict__ t,
+                      SolveCtl* ctl, BicgScalars<T>* sc, T* __restrict__ partials)
+{
+    __shared__ T red[kSolverBlock / kWarp * 3 * K];
+    __shared__ T tot[3 * K];
+    __shared__ int last;
+    if (ctl->all_stopped) return;
+    T acc[3 * K];
+#pragma unroll
+    for (int j = 0; j < 3 * K; ++j) acc[j] = T(0);
+    for (int64_t i = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * kSolverBlock) {
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            const T si = s[i * K + j], ti = t[i * K + j];
+            acc[j] += si * ti;
+            acc[K + j] += ti * ti;
+            acc[2 * K + j] += si * si;
+        }
+    }
+    block_partials<T, 3 * K>(acc, partials, red);
+    if (last_block_done(&ctl->ticket, &last)) {
+        sum_partials<T, 3 * K>(partials, gridDim.x, tot, red);
+        if (threadIdx.x == 0) {
+            ctl->ticket = 0;
+            for (int j = 0; j < K; ++j) {
+                uint8_t st = ctl->status[j];
+                if (has_stopped(st)) continue;
+                const T tau_s = sqrt(tot[2 * K + j]);
+                if (residual_met(ctl, tau_s, sc->rho[j], sc->start[j])) {
+                    converge_status(st, kResidualId, false);
+                    sc->tau[j] = tau_s;
+                }
+                ctl->status[j] = st;
+                const T tt = tot[K + j];
+                sc->omega[j] = tt != T(0) ? tot[j] / tt : T(0);
+            }
+        }
+    }
+}
+
+// grid of the warp-per-group block kernels
+template <typename T>
+int bicg_block_grid(const BlockPrec<T>& bp)
+{
+    const BlockScheme bsc = block_scheme(bp.max_bs);
+    const int64_t ngroups = ceildiv(bp.num_blocks, bsc.gs);
+    return int(std::min<int64_t>(std::max<int64_t>(1, ceildiv(ngroups, kSolverBlock / kWarp)),
+                                 solver_grid()));
+}
+
+template <typename T, int K, int STEP>
+void launch_bicg_block_vec(int64_t n, const BlockPrec<T>& bp, const T* r, const T* a_old,
+                           const T* v_old, T* out, T* prec, SolveCtl* ctl,
+                           BicgScalars<T>* sc, cudaStream_t st)
+{
+    const int grid = bicg_block_grid(bp);
+#define B2S_BICG_BLOCK(MB)                                                        \
+    case MB:                                                                      \
+        bicg_block_vec_kernel<T, MB, K, STEP><<<grid, kSolverBlock, 0, st>>>(     \
+            n, bp, r, a_old, v_old, out, prec, ctl, sc);                          \
+        break;
+    switch (kMaxBs / block_scheme(bp.max_bs).gs) {
+        B2S_BICG_BLOCK(2)
+        B2S_BICG_BLOCK(4)
+        B2S_BICG_BLOCK(8)
+        B2S_BICG_BLOCK(16)
+        B2S_BICG_BLOCK(32)
+    default: B2S_BICG_BLOCK(1)
+    }
+#undef B2S_BICG_BLOCK
+}
+
 struct BicgLayout {
     int64_t bytes, off_ctl, off_sc, off_r, off_rr, off_p0, off_p1, off_v0,
         off_v1, off_s, off_t, off_partials, off_y, off_z;
 };
 
 template <typename T>
-BicgLayout bicg_layout(int64_t n, int K)
+BicgLayout bicg_layout(int64_t n, int K, bool with_yz = false)
 {
     Carver c{nullptr};
     BicgLayout l;
@@ -467,16 +662,18 @@ BicgLayout bicg_layout(int64_t n, int K)
     l.off_s = c.take<T>(n * K);
     l.off_t = c.take<T>(n * K);
     l.off_partials = c.take<T>(int64_t(kSolverGrid) * 3 * K);
-    // the SpMV inputs of the split single-column pass
-    l.off_y = K == 1 ? c.take<T>(n) : 0;
-    l.off_z = K == 1 ? c.take<T>(n) : 0;
+    // the SpMV inputs of the split passes (single column, or block Jacobi)
+    l.off_y = K == 1 || with_yz ? c.take<T>(n * K) : 0;
+    l.off_z = K == 1 || with_yz ? c.take<T>(n * K) : 0;
     l.bytes = c.used;
     return l;
 }
 
+// bp: a block Jacobi preconditioner (dinv then null), or null
 template <typename T>
 int bicgstab_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
-                   int64_t max_row_nnz, const T* dinv, const T* b, int64_t ldb,
+                   int64_t max_row_nnz, const T* dinv, const BlockPrec<T>* bp,
+                   const T* b, int64_t ldb,
                    T* x, int64_t ldx, int64_t k, int64_t max_iters,
                    double reduction, int residual_mode, int64_t check_every,
                    void* workspace,
@@ -489,8 +686,14 @@ int bicgstab_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
                   "max_iters out of range");
     B2S_CHECK_ARG(valid_residual_mode(residual_mode), "unknown residual mode %d",
                   residual_mode);
+    if (bp) {
+        B2S_CHECK_ARG(bp->max_bs >= 1 && bp->max_bs <= kMaxBs,
+                      "max_block_size must be 1..32");
+        B2S_CHECK_ARG(bp->num_blocks >= 1 && bp->ptrs && bp->blocks,
+                      "block preconditioner without blocks");
+    }
     const int K = rhs_bucket(k);
-    const BicgLayout lay = bicg_layout<T>(n, K);
+    const BicgLayout lay = bicg_layout<T>(n, K, bp != nullptr);
     if (workspace_bytes < lay.bytes) {
         set_error("workspace of %lld bytes < %lld", (long long)workspace_bytes,
                   (long long)lay.bytes);
@@ -508,8 +711,8 @@ int bicgstab_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
     T* s = reinterpret_cast<T*>(w + lay.off_s);
     T* t = reinterpret_cast<T*>(w + lay.off_t);
     T* partials = reinterpret_cast<T*>(w + lay.off_partials);
-    T* yv = K == 1 ? reinterpret_cast<T*>(w + lay.off_y) : nullptr;
-    T* zv = K == 1 ? reinterpret_cast<T*>(w + lay.off_z) : nullptr;
+    T* yv = K == 1 || bp ? reinterpret_cast<T*>(w + lay.off_y) : nullptr;
+    T* zv = K == 1 || bp ? reinterpret_cast<T*>(w + lay.off_z) : nullptr;
 
     SolveCtl h{};
     h.max_iters = int(max_iters);
@@ -544,9 +747,37 @@ int bicgstab_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
         });
     };
     const bool split = K == 1 && n >= kBicgSplitRows;
+    // block Jacobi: the split passes with K columns
+    auto block_iteration = [&](cudaStream_t cs, int o, int nw) {
+        B2S_DISPATCH_RHS(K, {
+            auto spmv_k = [&](const T* in, T* out) {
+                with_async_kernel<T, K, (K >= 2)>(lpr, [&](auto kernel) {
+                    const int64_t grid = std::min<int64_t>(async_need,
+                                                           async_resident_blocks(kernel));
+                    kernel<<<grid, kAsyncBlock, 0, cs>>>(n, rp, ci, v, in, K, out, K, nullptr,
+                                                         nullptr, &ctl->all_stopped);
+                });
+            };
+            launch_bicg_block_vec<T, K, 1>(n, *bp, r, p[o], vv[o], p[nw], yv, ctl, sc, cs);
+            spmv_k(yv, vv[nw]);
+            bicg_dot1k_kernel<T, K><<<grid_vec, kSolverBlock, 0, cs>>>(n, rr, vv[nw], ctl, sc,
+                                                                      partials);
+            launch_bicg_block_vec<T, K, 2>(n, *bp, r, vv[nw], nullptr, s, zv, ctl, sc, cs);
+            spmv_k(zv, t);
+            bicg_dot2k_kernel<T, K><<<grid_vec, kSolverBlock, 0, cs>>>(n, s, t, ctl, sc,
+                                                                      partials);
+            bicg_update_kernel<T, K><<<grid_vec, kSolverBlock, 0, cs>>>(
+                n, nullptr, x, ldx, r, rr, yv, s, t, ctl, sc, partials, zv);
+        });
+    };
     auto capture = [&](cudaStream_t cs) -> int {
         for (int it = 0; it < chunk; ++it) {
             const int o = it % 2, nw = (it + 1) % 2;
+            if (bp) {
+                block_iteration(cs, o, nw);
+                B2S_LAUNCH_CHECK();
+                continue;
+            }
             if (split) {
                 bicg_pupdate_kernel<T><<<grid_vec, kSolverBlock, 0, cs>>>(
                     n, dinv, r, p[o], vv[o], p[nw], yv, ctl, sc);
@@ -608,6 +839,15 @@ int64_t b2s_bicgstab_workspace_bytes(int64_t num_rows, int64_t num_rhs,
                             : bicg_layout<float>(num_rows, K).bytes;
 }
 
+int64_t b2s_bicgstab_block_workspace_bytes(int64_t num_rows, int64_t num_rhs,
+                                           int value_bytes)
+{
+    const int K = rhs_bucket(num_rhs);
+    if (K < 0 || num_rows < 0) return -1;
+    return value_bytes == 8 ? bicg_layout<double>(num_rows, K, true).bytes
+                            : bicg_layout<float>(num_rows, K, true).bytes;
+}
+
 #define B2S_BICG_ENTRY(T, S)                                                  \
     int b2s_bicgstab_solve_##S(                                               \
         int64_t num_rows, const int32_t* row_ptrs, const int32_t* col_idxs,   \
@@ -619,11 +859,33 @@ int64_t b2s_bicgstab_workspace_bytes(int64_t num_rows, int64_t num_rhs,
         uint8_t* status, void* stream)                                        \
     {                                                                         \
         return bicgstab_solve<T>(num_rows, row_ptrs, col_idxs, values,        \
-                                 max_row_nnz, inv_diag, b, ldb, x, ldx,       \
-                                 num_rhs, max_iters, reduction_factor,        \
+                                 max_row_nnz, inv_diag, nullptr, b, ldb, x,   \
+                                 ldx, num_rhs, max_iters, reduction_factor,   \
                                  residual_mode, check_every, workspace,       \
                                  workspace_bytes,                             \
                                  iterations, residual_norms, status, stream); \
+    }                                                                         \
+    int b2s_bicgstab_block_solve_##S(                                         \
+        int64_t num_rows, const int32_t* row_ptrs, const int32_t* col_idxs,   \
+        const T* values, int64_t max_row_nnz, int64_t num_blocks,             \
+        const int32_t* block_ptrs, int max_block_size, const T* blocks,       \
+        const T* b, int64_t ldb, T* x, int64_t ldx, int64_t num_rhs,          \
+        int64_t max_iters, double reduction_factor, int residual_mode,        \
+        int64_t check_every, void* workspace, int64_t workspace_bytes,        \
+        int64_t* iterations, double* residual_norms, uint8_t* status,         \
+        void* stream)                                                         \
+    {                                                                         \
+        BlockPrec<T> bp;                                                      \
+        bp.num_blocks = num_blocks;                                           \
+        bp.ptrs = block_ptrs;                                                 \
+        bp.max_bs = max_block_size;                                           \
+        bp.blocks = blocks;                                                   \
+        return bicgstab_solve<T>(num_rows, row_ptrs, col_idxs, values,        \
+                                 max_row_nnz, nullptr, &bp, b, ldb, x, ldx,   \
+                                 num_rhs, max_iters, reduction_factor,        \
+                                 residual_mode, check_every, workspace,       \
+                                 workspace_bytes, iterations, residual_norms, \
+                                 status, stream);                             \
     }
 
 B2S_BICG_ENTRY(double, f64)

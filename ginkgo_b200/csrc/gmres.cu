@@ -50,6 +50,7 @@
 
 #include "csr_async.cuh"
 #include "ell_rows.cuh"
+#include "jacobi_scheme.cuh"
 #include "solver_common.cuh"
 
 namespace b2s {
@@ -486,7 +487,7 @@ __global__ void __launch_bounds__(kSolverBlock, 4)
 // and, when the cycle ends, the back substitution y = H \ g.  The small
 // arrays are staged in shared memory, so the serial chain runs at
 // shared-memory latency.
-__device__ void close_step(GmresState* st, double hnorm, double* __restrict__ Hm)
+__device__ __noinline__ void close_step(GmresState* st, double hnorm, double* __restrict__ Hm)
 {
     __shared__ double hc[kLd], gS[kLd], csS[kMaxKrylov], snS[kMaxKrylov];
     __shared__ double ts[kMaxKrylov];
@@ -582,8 +583,18 @@ __device__ void close_step(GmresState* st, double hnorm, double* __restrict__ Hm
 // next basis vector V_{j+1} = round_basis(w'') and the next SpMV input
 // y = D^-1 V_{j+1}; its scale sigma_{j+1} = 1 / ||w''|| is set by the last
 // block, which closes the Arnoldi step.
+// Blocks per SM the update pass is held to: its registers decide how many
+// row groups are in flight (measured: FP64 at 40 registers, six blocks per
+// SM, runs 30 us per step on the 27-point 96^3 operator, 39 us at 48
+// registers); the scaled bases, with up to eight rows per group, four.
 template <typename TA, typename TB>
-__global__ void __launch_bounds__(kSolverBlock)
+constexpr int update_min_blocks()
+{
+    return BasisKind<TB>::kScaled ? 4 : (sizeof(TA) == 8 && sizeof(TB) == 8 ? 6 : 5);
+}
+
+template <typename TA, typename TB>
+__global__ void __launch_bounds__(kSolverBlock, (update_min_blocks<TA, TB>()))
     gmres_update_kernel(int64_t n, int64_t ldv, TB* __restrict__ V,
                         const TA* __restrict__ w, const TA* __restrict__ dinv,
                         TA* __restrict__ y, GmresState* st,
@@ -892,10 +903,133 @@ GmresLayout gmres_layout(int64_t n, int64_t nnz, int64_t max_row_nnz, int d, boo
 
 // One right-hand side (b, x contiguous FP64 vectors); the layout was
 // checked against the workspace by the caller.
+// ---------------------------------------------------------------------------
+// Block Jacobi (right preconditioning by the block-diagonal inverse M): the
+// SpMV input y = M V_{j+1} is no longer a row-wise scale, so the update,
+// restart and quantize passes write y = V_{j+1} unscaled and
+// gmres_block_apply_kernel applies M to it in place, one warp per group of
+// the block-interleaved storage (every lane loads its row before the
+// block's shuffles, so the in-place write is safe).  The cycle's solution
+// update x += M V (sigma y) runs as gmres_xupdate_block_kernel, warp per
+// group: the lanes form u = V (sigma y) for the group's rows, then M u by
+// shuffles.  The blocks are FP64 in every variant; an FP32 Arnoldi cycle
+// rounds M y to FP32.
+// ---------------------------------------------------------------------------
+template <typename TA, int MB2>
+__global__ void __launch_bounds__(kSolverBlock)
+    gmres_block_apply_kernel(int64_t n, BlockPrec<double> bp, TA* __restrict__ y,
+                             const int* __restrict__ skip)
+{
+    constexpr unsigned kFull = 0xffffffffu;
+    if (*skip) return;
+    const BlockScheme bsc = block_scheme(bp.max_bs);
+    const int lane = threadIdx.x % kWarp;
+    const int sub = lane / bp.max_bs, i = lane % bp.max_bs;
+    const bool in_group = lane < bsc.gs * bp.max_bs;
+    const int base = sub * bp.max_bs;
+    const int64_t ngroups = (bp.num_blocks + bsc.gs - 1) / bsc.gs;
+    const int64_t nwarps = int64_t(gridDim.x) * (kSolverBlock / kWarp);
+    for (int64_t grp = blockIdx.x * int64_t(kSolverBlock / kWarp) + threadIdx.x / kWarp;
+         grp < ngroups; grp += nwarps) {
+        const int64_t blk = grp * bsc.gs + sub;
+        int s = 0, bs = 0;
+        const bool in_block = in_group && blk < bp.num_blocks &&
+                              block_extent(bp.ptrs, blk, n, bp.max_bs, s, bs);
+        const bool act = in_block && i < bs;
+        const double yv = act ? double(y[s + i]) : 0.0;
+        const double* g = bp.blocks + grp * bsc.group + lane;
+        double z = 0.0;
+#pragma unroll
+        for (int c = 0; c < MB2; ++c) {
+            if (c < bp.max_bs) {
+                const double inv = in_group ? __ldg(g + c * bsc.stride) : 0.0;
+                const double yc = __shfl_sync(kFull, yv, (base + c) % kWarp);
+                if (act && c < bs) z += inv * yc;
+            }
+        }
+        if (act) y[s + i] = TA(z);
+    }
+}
+
+template <typename TA, typename TB, int MB2>
+__global__ void __launch_bounds__(kSolverBlock)
+    gmres_xupdate_block_kernel(int64_t n, int64_t ldv, const TB* __restrict__ V,
+                               BlockPrec<double> bp, double* __restrict__ x,
+                               const double* __restrict__ b, double* __restrict__ r,
+                               GmresState* st)
+{
+    constexpr unsigned kFull = 0xffffffffu;
+    __shared__ TA ys[kMaxKrylov];
+    if (st->done) return;
+    const int m = st->final_iter;
+    for (int q = threadIdx.x; q < m; q += kSolverBlock) ys[q] = TA(st->y[q] * st->sigma[q]);
+    __syncthreads();
+    const BlockScheme bsc = block_scheme(bp.max_bs);
+    const int lane = threadIdx.x % kWarp;
+    const int sub = lane / bp.max_bs, i = lane % bp.max_bs;
+    const bool in_group = lane < bsc.gs * bp.max_bs;
+    const int base = sub * bp.max_bs;
+    const int64_t ngroups = (bp.num_blocks + bsc.gs - 1) / bsc.gs;
+    const int64_t nwarps = int64_t(gridDim.x) * (kSolverBlock / kWarp);
+    for (int64_t grp = blockIdx.x * int64_t(kSolverBlock / kWarp) + threadIdx.x / kWarp;
+         grp < ngroups; grp += nwarps) {
+        const int64_t blk = grp * bsc.gs + sub;
+        int s = 0, bs = 0;
+        const bool in_block = in_group && blk < bp.num_blocks &&
+                              block_extent(bp.ptrs, blk, n, bp.max_bs, s, bs);
+        const bool act = in_block && i < bs;
+        const int64_t row = s + i;
+        TA u = TA(0);
+        if (act) {
+#pragma unroll 4
+            for (int q = 0; q < m; ++q) u += ys[q] * from_basis<TA>(V[int64_t(q) * ldv + row]);
+        }
+        const double uv = double(u);
+        const double* g = bp.blocks + grp * bsc.group + lane;
+        double z = 0.0;
+#pragma unroll
+        for (int c = 0; c < MB2; ++c) {
+            if (c < bp.max_bs) {
+                const double inv = in_group ? __ldg(g + c * bsc.stride) : 0.0;
+                const double uc = __shfl_sync(kFull, uv, (base + c) % kWarp);
+                if (act && c < bs) z += inv * uc;
+            }
+        }
+        if (act) {
+            if (m > 0) x[row] += z;
+            r[row] = b[row];
+        }
+    }
+}
+
+// grid of the warp-per-group block kernels
+inline int block_grid(const BlockPrec<double>& bp)
+{
+    const BlockScheme bsc = block_scheme(bp.max_bs);
+    const int64_t ngroups = ceildiv(bp.num_blocks, bsc.gs);
+    return int(std::min<int64_t>(std::max<int64_t>(1, ceildiv(ngroups, kSolverBlock / kWarp)),
+                                 solver_grid()));
+}
+
+// Calls f(std::integral_constant<int, MB2>) for the block size class of bp.
+template <typename F>
+void with_block_class(const BlockPrec<double>& bp, F&& f)
+{
+    switch (kMaxBs / block_scheme(bp.max_bs).gs) {
+    case 1: f(std::integral_constant<int, 1>{}); break;
+    case 2: f(std::integral_constant<int, 2>{}); break;
+    case 4: f(std::integral_constant<int, 4>{}); break;
+    case 8: f(std::integral_constant<int, 8>{}); break;
+    case 16: f(std::integral_constant<int, 16>{}); break;
+    default: f(std::integral_constant<int, 32>{}); break;
+    }
+}
+
 template <typename TA, typename TB>
 int gmres_engine(const GmresLayout& lay, int64_t n, int64_t nnz, const int32_t* rp,
                  const int32_t* ci, const double* v64, int64_t max_row_nnz,
-                 const double* dinv64, const double* b, double* x, int krylov_dim,
+                 const double* dinv64, const BlockPrec<double>* bp, const double* b,
+                 double* x, int krylov_dim,
                  int ortho, int64_t max_iters, double reduction, int baseline,
                  double inner_reduction, void* workspace, int64_t* iterations,
                  int64_t* restarts, double* res_norm, uint8_t* status, cudaStream_t st)
@@ -985,9 +1119,25 @@ int gmres_engine(const GmresLayout& lay, int64_t n, int64_t nnz, const int32_t* 
     const int lpr = async_lanes_per_row(max_row_nnz);
     const int64_t async_need = ceildiv(ceildiv(n, kWarp / lpr), kAsyncBlock / kWarp);
     // x += D^-1 V y and r = b; r -= A x (FP64); ||r||, ||b|| and the check
+    // block Jacobi: M applied to the SpMV input in place (skipped when the
+    // cycle is over)
+    auto block_apply = [&](cudaStream_t cs) {
+        if (!bp) return;
+        with_block_class(*bp, [&](auto mb) {
+            gmres_block_apply_kernel<TA, decltype(mb)::value>
+                <<<block_grid(*bp), kSolverBlock, 0, cs>>>(n, *bp, y, &gs->idle);
+        });
+    };
     auto restart = [&](cudaStream_t cs) {
-        gmres_xupdate_kernel<TA, TB><<<grid_vec, kSolverBlock, 0, cs>>>(n, ldv, V, da, x,
-                                                                        b, r, gs);
+        if (bp) {
+            with_block_class(*bp, [&](auto mb) {
+                gmres_xupdate_block_kernel<TA, TB, decltype(mb)::value>
+                    <<<block_grid(*bp), kSolverBlock, 0, cs>>>(n, ldv, V, *bp, x, b, r, gs);
+            });
+        } else {
+            gmres_xupdate_kernel<TA, TB><<<grid_vec, kSolverBlock, 0, cs>>>(n, ldv, V, da, x,
+                                                                            b, r, gs);
+        }
         with_async_kernel<double, 1, false>(lpr, [&](auto kernel) {
             const int64_t grid = std::min<int64_t>(async_need, async_resident_blocks(kernel));
             kernel<<<grid, kAsyncBlock, 0, cs>>>(n, rp, ci, v64, x, 1, r, 1,
@@ -999,6 +1149,7 @@ int gmres_engine(const GmresLayout& lay, int64_t n, int64_t nnz, const int32_t* 
             gmres_quantize_kernel<TA, TB, double><<<grid_vec, kSolverBlock, 0, cs>>>(
                 n, ldv, r, V, da, y, gs, 1);
         }
+        block_apply(cs);
     };
     // first residual outside the graph (final_iter = 0: x is not touched)
     restart(st);
@@ -1041,6 +1192,7 @@ int gmres_engine(const GmresLayout& lay, int64_t n, int64_t nnz, const int32_t* 
                 gmres_quantize_kernel<TA, TB, TA><<<grid_vec, kSolverBlock, 0, cs>>>(
                     n, ldv, wq, V, da, y, gs, 0);
             }
+            block_apply(cs);
             B2S_LAUNCH_CHECK();
         }
         restart(cs);
@@ -1104,6 +1256,7 @@ int gmres_engine(const GmresLayout& lay, int64_t n, int64_t nnz, const int32_t* 
 template <typename TA, typename TB>
 int gmres_solve_columns(int64_t n, const int32_t* rp, const int32_t* ci,
                         const double* v64, int64_t max_row_nnz, const double* dinv64,
+                        const BlockPrec<double>* bp,
                         const double* b, int64_t ldb, double* x, int64_t ldx,
                         int64_t k, int64_t krylov_dim, int ortho, int64_t max_iters,
                         double reduction, int baseline, double inner_reduction,
@@ -1126,6 +1279,13 @@ int gmres_solve_columns(int64_t n, const int32_t* rp, const int32_t* ci,
     B2S_CHECK_ARG(max_iters >= 0 && max_iters < (int64_t(1) << 30),
                   "max_iters out of range");
     B2S_CHECK_ARG(k <= 1 || (ldb >= k && ldx >= k), "leading dimensions below num_rhs");
+    if (bp) {
+        B2S_CHECK_ARG(bp->max_bs >= 1 && bp->max_bs <= kMaxBs,
+                      "max_block_size must be 1..32");
+        B2S_CHECK_ARG(bp->num_blocks >= 1 && bp->ptrs && bp->blocks,
+                      "block preconditioner without blocks");
+        B2S_CHECK_ARG(dinv64 == nullptr, "scalar and block Jacobi together");
+    }
     if (k == 0) return B2S_OK;
     B2S_CHECK_ARG(b != nullptr && x != nullptr && rp != nullptr, "null pointer");
     cudaStream_t st = as_stream(stream);
@@ -1162,7 +1322,7 @@ int gmres_solve_columns(int64_t n, const int32_t* rp, const int32_t* ci,
             xc = xcol;
         }
         const int rc = gmres_engine<TA, TB>(
-            lay, n, nnz, rp, ci, v64, max_row_nnz, dinv64, bc, xc, int(krylov_dim), ortho,
+            lay, n, nnz, rp, ci, v64, max_row_nnz, dinv64, bp, bc, xc, int(krylov_dim), ortho,
             max_iters, reduction, baseline, inner_reduction, workspace,
             iterations ? iterations + c : nullptr, restarts ? restarts + c : nullptr,
             res_norms ? res_norms + c : nullptr, status ? status + c : nullptr, st);
@@ -1214,22 +1374,24 @@ int64_t b2s_gmres_workspace_bytes(int64_t num_rows, int64_t nnz,
     }
 }
 
-int b2s_gmres_solve(int variant, int ortho_method, int64_t num_rows,
-                    const int32_t* row_ptrs, const int32_t* col_idxs,
-                    const double* values, int64_t max_row_nnz,
-                    const double* inv_diag, const double* b, int64_t ldb,
-                    double* x, int64_t ldx, int64_t num_rhs,
-                    int64_t krylov_dim, int64_t max_iters,
-                    double reduction_factor, int baseline,
-                    double inner_reduction, void* workspace,
-                    int64_t workspace_bytes, int64_t* iterations,
-                    int64_t* restarts, double* residual_norms,
-                    uint8_t* status, void* stream)
+}  // extern "C"
+
+namespace b2s {
+namespace {
+
+int gmres_dispatch(int variant, int ortho_method, int64_t num_rows, const int32_t* row_ptrs,
+                   const int32_t* col_idxs, const double* values, int64_t max_row_nnz,
+                   const double* inv_diag, const BlockPrec<double>* bp, const double* b,
+                   int64_t ldb, double* x, int64_t ldx, int64_t num_rhs, int64_t krylov_dim,
+                   int64_t max_iters, double reduction_factor, int baseline,
+                   double inner_reduction, void* workspace, int64_t workspace_bytes,
+                   int64_t* iterations, int64_t* restarts, double* residual_norms,
+                   uint8_t* status, void* stream)
 {
-#define B2S_GMRES_ARGS(INNER)                                                      \
-    num_rows, row_ptrs, col_idxs, values, max_row_nnz, inv_diag, b, ldb, x, ldx,  \
-        num_rhs, krylov_dim, ortho_method, max_iters, reduction_factor, baseline, \
-        INNER, workspace, workspace_bytes, iterations, restarts, residual_norms,  \
+#define B2S_GMRES_ARGS(INNER)                                                          \
+    num_rows, row_ptrs, col_idxs, values, max_row_nnz, inv_diag, bp, b, ldb, x, ldx,  \
+        num_rhs, krylov_dim, ortho_method, max_iters, reduction_factor, baseline,     \
+        INNER, workspace, workspace_bytes, iterations, restarts, residual_norms,      \
         status, stream
     switch (variant) {
     case B2S_GMRES_F64:
@@ -1258,6 +1420,54 @@ int b2s_gmres_solve(int variant, int ortho_method, int64_t num_rows,
         return B2S_ERR_INVALID_ARG;
     }
 #undef B2S_GMRES_ARGS
+}
+
+}  // namespace
+}  // namespace b2s
+
+extern "C" {
+
+int b2s_gmres_solve(int variant, int ortho_method, int64_t num_rows,
+                    const int32_t* row_ptrs, const int32_t* col_idxs,
+                    const double* values, int64_t max_row_nnz,
+                    const double* inv_diag, const double* b, int64_t ldb,
+                    double* x, int64_t ldx, int64_t num_rhs,
+                    int64_t krylov_dim, int64_t max_iters,
+                    double reduction_factor, int baseline,
+                    double inner_reduction, void* workspace,
+                    int64_t workspace_bytes, int64_t* iterations,
+                    int64_t* restarts, double* residual_norms,
+                    uint8_t* status, void* stream)
+{
+    return gmres_dispatch(variant, ortho_method, num_rows, row_ptrs, col_idxs, values,
+                          max_row_nnz, inv_diag, nullptr, b, ldb, x, ldx, num_rhs,
+                          krylov_dim, max_iters, reduction_factor, baseline, inner_reduction,
+                          workspace, workspace_bytes, iterations, restarts, residual_norms,
+                          status, stream);
+}
+
+int b2s_gmres_block_solve(int variant, int ortho_method, int64_t num_rows,
+                          const int32_t* row_ptrs, const int32_t* col_idxs,
+                          const double* values, int64_t max_row_nnz, int64_t num_blocks,
+                          const int32_t* block_ptrs, int max_block_size,
+                          const double* blocks, const double* b, int64_t ldb, double* x,
+                          int64_t ldx, int64_t num_rhs, int64_t krylov_dim,
+                          int64_t max_iters, double reduction_factor, int baseline,
+                          double inner_reduction, void* workspace,
+                          int64_t workspace_bytes, int64_t* iterations,
+                          int64_t* restarts, double* residual_norms, uint8_t* status,
+                          void* stream)
+{
+    BlockPrec<double> bp;
+    bp.num_blocks = num_blocks;
+    bp.ptrs = block_ptrs;
+    bp.max_bs = max_block_size;
+    bp.blocks = blocks;
+    return gmres_dispatch(variant, ortho_method, num_rows, row_ptrs, col_idxs, values,
+                          max_row_nnz, nullptr, &bp, b, ldb, x, ldx, num_rhs, krylov_dim,
+                          max_iters, reduction_factor, baseline, inner_reduction, workspace,
+                          workspace_bytes, iterations, restarts, residual_norms, status,
+                          stream);
 }
 
 }  // extern "C"

@@ -10,8 +10,8 @@ reference's ``gko::solver`` / ``gko::stop`` / ``gko::preconditioner`` API:
     solver.apply(b, x)                # x holds the initial guess
     solver.logger.num_iterations      # like gko::log::Convergence
 
-Scalar Jacobi (max_block_size 1) is fused into every solver, block Jacobi
-into CG; stopping is Iteration plus one residual criterion, ResidualNorm
+Scalar Jacobi (max_block_size 1) and block Jacobi (2..32) are fused into
+every solver; stopping is Iteration plus one residual criterion, ResidualNorm
 (baselines rhs_norm, initial_resnorm, absolute) or, for CG and BiCGStab,
 ImplicitResidualNorm (include/ginkgo/core/stop/residual_norm.hpp).
 """
@@ -187,9 +187,10 @@ class BlockJacobi:
     """preconditioner::Jacobi with max_block_size 2..32 and full-precision
     blocks (core/preconditioner/jacobi.cpp:370-420): the diagonal blocks
     inverted on the device (b2s_jacobi_block_generate_*), applied as
-    x = D^-1 b or alpha D^-1 b + beta x.  CG applies the blocks inside its
-    update pass (b2s_cg_block_solve_*); BiCGStab and GMRES take scalar
-    Jacobi only."""
+    x = D^-1 b or alpha D^-1 b + beta x.  The solvers apply the blocks
+    inside their passes: CG in its update pass (b2s_cg_block_solve_*),
+    BiCGStab to p' and s (b2s_bicgstab_block_solve_*), GMRES and IR over
+    GMRES to each Krylov vector (b2s_gmres_block_solve)."""
 
     def __init__(self, A: Csr, max_block_size: int, block_pointers=None):
         self.A = A
@@ -222,8 +223,8 @@ class BlockJacobi:
 
     @property
     def inv_diag(self):
-        raise NotImplementedError("BiCGStab and GMRES here fuse scalar Jacobi only "
-                                  "(with_max_block_size(1)); CG takes block Jacobi")
+        raise NotImplementedError("a block Jacobi preconditioner has no inverse "
+                                  "diagonal; the solvers take its blocks")
 
     def apply(self, *args):
         """apply(b, x) or apply(alpha, b, beta, x)."""
@@ -376,12 +377,13 @@ class _Solver:
         outs = (C.byref(it), res.ctypes.data_as(C.c_void_p),
                 st.ctypes.data_as(C.c_void_p), _stream(x2))
         M = self.precond
-        if name == "cg" and isinstance(M, BlockJacobi):
-            nbytes = lib().b2s_cg_block_workspace_bytes(n, k, A.values.element_size())
+        if isinstance(M, BlockJacobi):
+            nbytes = getattr(lib(), f"b2s_{name}_block_workspace_bytes")(
+                n, k, A.values.element_size())
             ws = self._workspace(nbytes)
-            call(f"b2s_cg_block_solve_{_SFX[A.dtype]}", n, _p(A.row_ptrs), _p(A.col_idxs),
-                 _p(A.values), A.max_row_nnz, M.num_blocks, _p(M._ptrs), M.max_block_size,
-                 _p(M.blocks), *tail, _p(ws), ws.numel(), *outs)
+            call(f"b2s_{name}_block_solve_{_SFX[A.dtype]}", n, _p(A.row_ptrs),
+                 _p(A.col_idxs), _p(A.values), A.max_row_nnz, M.num_blocks, _p(M._ptrs),
+                 M.max_block_size, _p(M.blocks), *tail, _p(ws), ws.numel(), *outs)
         else:
             nbytes = getattr(lib(), f"b2s_{name}_workspace_bytes")(
                 n, k, A.values.element_size())
@@ -423,12 +425,20 @@ class _Solver:
         rs = np.zeros(k, np.int64)
         rn = np.zeros(k, np.float64)
         st = np.zeros(k, np.uint8)
-        call("b2s_gmres_solve", variant, _ORTHO[self.f.ortho_method], n, _p(A.row_ptrs),
-             _p(A.col_idxs), _p(A.values), A.max_row_nnz, _p(self.inv_diag), _p(b2),
-             b2.stride(0), _p(x2), x2.stride(0), k, self.f.krylov_dim, self.f.max_iters,
-             self.f.reduction, self.f.residual_mode, self.f.inner_reduction, _p(ws),
-             ws.numel(), it.ctypes.data_as(C.c_void_p), rs.ctypes.data_as(C.c_void_p),
-             rn.ctypes.data_as(C.c_void_p), st.ctypes.data_as(C.c_void_p), _stream(x2))
+        tail = (_p(b2), b2.stride(0), _p(x2), x2.stride(0), k, self.f.krylov_dim,
+                self.f.max_iters, self.f.reduction, self.f.residual_mode,
+                self.f.inner_reduction, _p(ws), ws.numel(), it.ctypes.data_as(C.c_void_p),
+                rs.ctypes.data_as(C.c_void_p), rn.ctypes.data_as(C.c_void_p),
+                st.ctypes.data_as(C.c_void_p), _stream(x2))
+        M = self.precond
+        if isinstance(M, BlockJacobi):
+            call("b2s_gmres_block_solve", variant, _ORTHO[self.f.ortho_method], n,
+                 _p(A.row_ptrs), _p(A.col_idxs), _p(A.values), A.max_row_nnz, M.num_blocks,
+                 _p(M._ptrs), M.max_block_size, _p(M.blocks), *tail)
+        else:
+            call("b2s_gmres_solve", variant, _ORTHO[self.f.ortho_method], n,
+                 _p(A.row_ptrs), _p(A.col_idxs), _p(A.values), A.max_row_nnz,
+                 _p(self.inv_diag), *tail)
         self.logger = ConvergenceLog(int(it.max()) if k else 0, rn.tolist(),
                                      bool(np.all(st & 0x80)), st.tolist(),
                                      int(rs.max()) if k else 0)

@@ -580,6 +580,37 @@ int b2s_bicgstab_solve_f32(int64_t num_rows, const int32_t* row_ptrs,
                            void* workspace, int64_t workspace_bytes,
                            int64_t* iterations, double* residual_norms,
                            uint8_t* status, void* stream);
+/* BiCGStab preconditioned by block Jacobi (blocks as for
+ * b2s_cg_block_solve_*): every iteration runs split, M p' and M s formed
+ * one warp per block group right after p' and s and stored for the SpMVs
+ * and the solution update; otherwise as b2s_bicgstab_solve_*.  The
+ * workspace query adds the two stored vectors.  Replaces
+ * Bicgstab<V>::apply_dense_impl with a Jacobi<V> of block size > 1
+ * (preconditioner applies at core/solver/bicgstab.cpp:194 and :229). */
+int64_t b2s_bicgstab_block_workspace_bytes(int64_t num_rows, int64_t num_rhs,
+                                           int value_bytes);
+int b2s_bicgstab_block_solve_f64(int64_t num_rows, const int32_t* row_ptrs,
+                                 const int32_t* col_idxs, const double* values,
+                                 int64_t max_row_nnz, int64_t num_blocks,
+                                 const int32_t* block_ptrs, int max_block_size,
+                                 const double* blocks, const double* b, int64_t ldb,
+                                 double* x, int64_t ldx, int64_t num_rhs,
+                                 int64_t max_iters, double reduction_factor,
+                                 int residual_mode, int64_t check_every,
+                                 void* workspace, int64_t workspace_bytes,
+                                 int64_t* iterations, double* residual_norms,
+                                 uint8_t* status, void* stream);
+int b2s_bicgstab_block_solve_f32(int64_t num_rows, const int32_t* row_ptrs,
+                                 const int32_t* col_idxs, const float* values,
+                                 int64_t max_row_nnz, int64_t num_blocks,
+                                 const int32_t* block_ptrs, int max_block_size,
+                                 const float* blocks, const float* b, int64_t ldb,
+                                 float* x, int64_t ldx, int64_t num_rhs,
+                                 int64_t max_iters, double reduction_factor,
+                                 int residual_mode, int64_t check_every,
+                                 void* workspace, int64_t workspace_bytes,
+                                 int64_t* iterations, double* residual_norms,
+                                 uint8_t* status, void* stream);
 
 #define B2S_GMRES_F64 0
 #define B2S_GMRES_MIXED_F32 1
@@ -650,6 +681,28 @@ int b2s_gmres_solve(int variant, int ortho_method, int64_t num_rows,
                     int64_t workspace_bytes, int64_t* iterations,
                     int64_t* restarts, double* residual_norms,
                     uint8_t* status, void* stream);
+/* GMRES (every variant above) right-preconditioned by block Jacobi:
+ * num_blocks FP64 blocks delimited by block_ptrs (covering 0..num_rows, at
+ * most max_block_size rows each), inverses in the interleaved storage of
+ * b2s_jacobi_block_generate_f64.  Each SpMV input y = M V_j is formed in
+ * place after the pass that writes V_j, one warp per block group, and the
+ * cycle's update x += M V y likewise; an FP32 Arnoldi cycle rounds M y to
+ * FP32.  Workspace as b2s_gmres_workspace_bytes.  Replaces the
+ * preconditioner applies of Gmres<V>::apply_dense_impl with a Jacobi<V> of
+ * block size > 1 (core/solver/gmres.cpp:530-531 on each Krylov vector,
+ * :642-643 before the solution update). */
+int b2s_gmres_block_solve(int variant, int ortho_method, int64_t num_rows,
+                          const int32_t* row_ptrs, const int32_t* col_idxs,
+                          const double* values, int64_t max_row_nnz,
+                          int64_t num_blocks, const int32_t* block_ptrs,
+                          int max_block_size, const double* blocks,
+                          const double* b, int64_t ldb, double* x, int64_t ldx,
+                          int64_t num_rhs, int64_t krylov_dim, int64_t max_iters,
+                          double reduction_factor, int baseline,
+                          double inner_reduction, void* workspace,
+                          int64_t workspace_bytes, int64_t* iterations,
+                          int64_t* restarts, double* residual_norms,
+                          uint8_t* status, void* stream);
 
 /* -------------------------------------------------------- gradients -- */
 

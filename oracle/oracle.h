@@ -89,11 +89,23 @@ extern "C" {
                          const T* v, const T* inv_diag, const T* b, T* x,     \
                          int max_iters, double reduction, int mode,           \
                          int* iters_out, double* res_norm_out);               \
+    int orc_bicgstab_block_##S(int64_t n, const int32_t* rp,                  \
+                               const int32_t* ci, const T* v, int64_t nblocks,\
+                               const int32_t* bptrs, int max_bs,              \
+                               const T* binv, const T* b, T* x,               \
+                               int max_iters, double reduction, int mode,     \
+                               int* iters_out, double* res_norm_out);               \
     int orc_gmres_##S(int64_t n, const int32_t* rp, const int32_t* ci,        \
                       const T* v, const T* inv_diag, const T* b, T* x,        \
                       int krylov_dim, int ortho, int max_iters,               \
                       double reduction, int mode, int* iters_out,             \
                       double* res_norm_out);                                  \
+    int orc_gmres_block_##S(int64_t n, const int32_t* rp, const int32_t* ci,  \
+                            const T* v, int64_t nblocks, const int32_t* bptrs,\
+                            int max_bs, const T* binv, const T* b, T* x,      \
+                            int krylov_dim, int ortho, int max_iters,         \
+                            double reduction, int mode, int* iters_out,       \
+                            double* res_norm_out);                                  \
     int orc_batch_bicgstab_ell_##S(int64_t n, int64_t width, int64_t stride,  \
                                    const int32_t* ci, const T* v,             \
                                    const T* b, T* x, int max_iters,           \

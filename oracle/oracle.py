@@ -67,9 +67,17 @@ def lib():
             f = getattr(_lib, f"orc_bicgstab_{s}")
             f.argtypes = [_i64, _p, _p, _p, _p, _p, _p, _i32, _f64, _i32, _p, _p]
             f.restype = _i32
+            f = getattr(_lib, f"orc_bicgstab_block_{s}")
+            f.argtypes = [_i64, _p, _p, _p, _i64, _p, _i32, _p, _p, _p, _i32, _f64, _i32,
+                          _p, _p]
+            f.restype = _i32
             f = getattr(_lib, f"orc_gmres_{s}")
             f.argtypes = [_i64, _p, _p, _p, _p, _p, _p, _i32, _i32, _i32, _f64, _i32,
                           _p, _p]
+            f.restype = _i32
+            f = getattr(_lib, f"orc_gmres_block_{s}")
+            f.argtypes = [_i64, _p, _p, _p, _i64, _p, _i32, _p, _p, _p, _i32, _i32, _i32,
+                          _f64, _i32, _p, _p]
             f.restype = _i32
             f = getattr(_lib, f"orc_batch_bicgstab_ell_{s}")
             f.argtypes = [_i64, _i64, _i64, _p, _p, _p, _p, _i32, _f64, _i32,
@@ -238,6 +246,36 @@ def cg(rp, ci, v, b, x0=None, jacobi=True, max_iters=1000, reduction=1e-10, mode
     return x.reshape(np.shape(b)), it.value, res, conv
 
 
+def _block_inverses(block_ptrs, blocks, max_block_size, dt):
+    """The inverses as one [num_blocks, m, m] array (block i in the top-left
+    corner of slot i), the layout of the oracle's block preconditioners."""
+    m = int(max_block_size)
+    ptrs = _c(block_ptrs, np.int32)
+    binv = np.zeros((len(ptrs) - 1, m, m), dt)
+    for i, blk in enumerate(blocks):
+        s = np.asarray(blk).shape[0]
+        binv[i, :s, :s] = blk
+    return ptrs, binv
+
+
+def bicgstab_block(rp, ci, v, b, block_ptrs, blocks, max_block_size, x0=None,
+                   max_iters=1000, reduction=1e-10, mode=0):
+    """BiCGStab (one right-hand side) with a block Jacobi preconditioner;
+    block arguments as cg_block, returns as bicgstab."""
+    rp, ci, v = _c(rp, np.int32), _c(ci, np.int32), np.ascontiguousarray(v)
+    dt = v.dtype
+    b = _c(b, dt)
+    x = np.zeros_like(b) if x0 is None else _c(x0, dt).copy()
+    ptrs, binv = _block_inverses(block_ptrs, blocks, max_block_size, dt)
+    it = C.c_int(0)
+    res = C.c_double(0)
+    conv = getattr(lib(), f"orc_bicgstab_block_{_sfx(dt)}")(
+        len(b), _ptr(rp), _ptr(ci), _ptr(v), len(ptrs) - 1, _ptr(ptrs), int(max_block_size),
+        _ptr(binv), _ptr(b), _ptr(x), max_iters, reduction, int(mode), C.byref(it),
+        C.byref(res))
+    return x, it.value, res.value, conv
+
+
 def cg_block(rp, ci, v, b, block_ptrs, blocks, max_block_size, x0=None, max_iters=1000,
              reduction=1e-10, mode=0):
     """CG with a block Jacobi preconditioner: block_ptrs delimit the blocks,
@@ -249,11 +287,7 @@ def cg_block(rp, ci, v, b, block_ptrs, blocks, max_block_size, x0=None, max_iter
     n, k = b2.shape
     x = np.zeros((n, k), dt) if x0 is None else _as2d(_c(x0, dt)).copy()
     m = int(max_block_size)
-    ptrs = _c(block_ptrs, np.int32)
-    binv = np.zeros((len(ptrs) - 1, m, m), dt)
-    for i, blk in enumerate(blocks):
-        s = np.asarray(blk).shape[0]
-        binv[i, :s, :s] = blk
+    ptrs, binv = _block_inverses(block_ptrs, blocks, m, dt)
     it = C.c_int(0)
     res = np.zeros(k, np.float64)
     conv = getattr(lib(), f"orc_cg_block_{_sfx(dt)}")(
@@ -290,6 +324,24 @@ def gmres(rp, ci, v, b, x0=None, jacobi=True, krylov_dim=30, max_iters=1000,
         len(b), _ptr(rp), _ptr(ci), _ptr(v), _ptr(inv), _ptr(b), _ptr(x),
         krylov_dim, ORTHO[ortho], max_iters, reduction, int(mode), C.byref(it),
         C.byref(res))
+    return x, it.value, res.value, conv
+
+
+def gmres_block(rp, ci, v, b, block_ptrs, blocks, max_block_size, x0=None, krylov_dim=30,
+                max_iters=1000, reduction=1e-10, ortho="mgs", mode=0):
+    """GMRES with a block Jacobi preconditioner; block arguments as
+    cg_block, returns as gmres."""
+    rp, ci, v = _c(rp, np.int32), _c(ci, np.int32), np.ascontiguousarray(v)
+    dt = v.dtype
+    b = _c(b, dt)
+    x = np.zeros_like(b) if x0 is None else _c(x0, dt).copy()
+    ptrs, binv = _block_inverses(block_ptrs, blocks, max_block_size, dt)
+    it = C.c_int(0)
+    res = C.c_double(0)
+    conv = getattr(lib(), f"orc_gmres_block_{_sfx(dt)}")(
+        len(b), _ptr(rp), _ptr(ci), _ptr(v), len(ptrs) - 1, _ptr(ptrs), int(max_block_size),
+        _ptr(binv), _ptr(b), _ptr(x), krylov_dim, ORTHO[ortho], max_iters, reduction,
+        int(mode), C.byref(it), C.byref(res))
     return x, it.value, res.value, conv
 
 

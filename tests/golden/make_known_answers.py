@@ -148,6 +148,15 @@ cases = {
          "b": [175352.10, 313410.50, 131114.10, -134116.30, 179529.30, -43564.90],
          "expected": [33.0, -56.0, 81.0, -30.0, 21.0, 40.0],
          "krylov_dim": 100, "max_iters": 100, "tol_factor": 1e3},
+        # with a block Jacobi preconditioner of max_block_size 3, solved
+        # with every ortho_method
+        {"name": "Gmres.SolvesWithPreconditioner", "solver": "gmres",
+         "source": "reference/test/solver/gmres_kernels.cpp:54-67,777-810",
+         "dense": "Gmres.SolvesBigDenseSystem1",
+         "b": [175352.10, 313410.50, 131114.10, -134116.30, 179529.30, -43564.90],
+         "expected": [33.0, -56.0, 81.0, -30.0, 21.0, 40.0],
+         "krylov_dim": 100, "max_iters": 100, "tol_factor": 1e3,
+         "jacobi_block_size": 3},
         # tolerance sqrt(r) * 1e2 (half_tol), written as tol_sqrt
         {"name": "Gmres.SolvesBigDenseSystem1WithRestart", "solver": "gmres",
          "source": "reference/test/solver/gmres_kernels.cpp:77-82,750-775",

@@ -276,3 +276,28 @@ def test_cg_block_oracle():
     x3, i3, _, c3 = orc.cg_block(rp, ci, v, b, bp, blocks, 4, max_iters=500, reduction=1e-10)
     r = b - orc.csr_spmv(rp, ci, v, x3)
     assert c3 == 1 and i3 <= i1 and np.linalg.norm(r) <= 1e-10 * np.linalg.norm(b)
+
+
+def test_bicgstab_and_gmres_block_oracles():
+    # unit blocks reproduce the scalar-Jacobi solvers bit for bit; blocks of
+    # four rows converge to the explicit residual goal
+    from oracle import jacobi as J
+    rp, ci, v = stencils.convection_diffusion_2d(30, 30, 1.0, 0.6, -0.3)
+    n = len(rp) - 1
+    b = np.random.default_rng(1).standard_normal(n)
+    _, inv = J.generate(rp, ci, v, 1)
+    unit = [np.array([[d]]) for d in inv]
+    x1, i1, _, _ = orc.bicgstab(rp, ci, v, b, max_iters=500, reduction=1e-10)
+    x2, i2, _, c2 = orc.bicgstab_block(rp, ci, v, b, np.arange(n + 1), unit, 1,
+                                       max_iters=500, reduction=1e-10)
+    assert i1 == i2 and c2 == 1 and np.array_equal(x1, x2)
+    g1, j1, _, _ = orc.gmres(rp, ci, v, b, krylov_dim=20, max_iters=500, reduction=1e-10)
+    g2, j2, _, c3 = orc.gmres_block(rp, ci, v, b, np.arange(n + 1), unit, 1, krylov_dim=20,
+                                    max_iters=500, reduction=1e-10)
+    assert j1 == j2 and c3 == 1 and np.array_equal(g1, g2)
+    ptrs = list(range(0, n + 1, 4))
+    _, bp, blocks = J.generate(rp, ci, v, 4, block_ptrs=ptrs)
+    for solve in (orc.bicgstab_block, orc.gmres_block):
+        x, _, _, conv = solve(rp, ci, v, b, bp, blocks, 4, max_iters=500, reduction=1e-10)
+        r = b - orc.csr_spmv(rp, ci, v, x)
+        assert conv == 1 and np.linalg.norm(r) <= 1e-10 * np.linalg.norm(b)
