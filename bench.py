@@ -220,6 +220,10 @@ def main():
                     help="profiling aid: one capped invocation of every kernel "
                     "family (SpMV formats, conversions, CG, BiCGStab, batch, "
                     "transpose + SDDMM) and exit")
+    ap.add_argument("--profile-op", choices=sorted(PROFILE_OPS),
+                    help="profiling aid: three launches of one operation on the "
+                    "7-point 128^3 matrix (inputs larger than L2) and exit, the "
+                    "small case for a single-kernel ncu capture")
     ap.add_argument("--mtx", action="store_true",
                     help="host-side matrix I/O: MatrixMarket text and binary "
                     "read/write of the 128^3 matrix (no GPU needed) and exit")
@@ -233,6 +237,8 @@ def main():
         return solve_case(args.solve_case, args.solve_iters)
     if args.profile_tour:
         return profile_tour()
+    if args.profile_op:
+        return profile_op(args.profile_op)
 
     import torch
     world, rank, local = dist_env()
@@ -459,7 +465,8 @@ def profile_tour():
     right-hand sides), the batched BiCGStab on 1024 systems, the transpose +
     SDDMM of the differentiable solve, mixed-type Csr/Ell SpMV, block Jacobi
     (blocks of 8), 10 Arnoldi steps of GMRES and of every CB-GMRES basis
-    format, SpGEMM (A^2), SpGEAM and the Hybrid conversions and SpMV."""
+    format, CG / BiCGStab / GMRES with block Jacobi inside (blocks of 8),
+    SpGEMM (A^2), SpGEAM and the Hybrid conversions and SpMV."""
     import torch
     from ginkgo_b200 import stencils
     from ginkgo_b200._lib import call
@@ -516,6 +523,13 @@ def profile_tour():
             for sp in ("reduce1", "reduce2", "integer", "ireduce1", "ireduce2")]:
         s = fac.with_criteria(*crit10).with_preconditioner(jac).on(exe).generate(A)
         s.apply(x1[:, 0].contiguous(), torch.zeros(n, dtype=torch.float64, device="cuda"))
+    # block Jacobi inside CG, BiCGStab and GMRES (blocks of 8 consecutive rows)
+    jb = Jacobi.build().with_max_block_size(8).with_block_pointers(np.arange(0, n + 1, 8))
+    b1 = x1[:, 0].contiguous()
+    for fac in (Cg.build().with_criteria(*crit), Bicgstab.build().with_criteria(*crit),
+                Gmres.build().with_krylov_dim(30).with_criteria(*crit10)):
+        s = fac.with_preconditioner(jb).on(exe).generate(A)
+        s.apply(b1, torch.zeros(n, dtype=torch.float64, device="cuda"))
     # sparse products: A^2 (SpGEMM), A + A (SpGEAM), Csr -> Hybrid -> SpMV, Csr
     from ginkgo_b200.matrix import spgeam, spgemm
     spgemm(A, A)
@@ -525,6 +539,58 @@ def profile_tour():
     H.convert_to_csr()
     torch.cuda.synchronize()
     print(json.dumps({"profile_tour": "done", "n": n}))
+
+
+# operations of --profile-op: the kernel each one runs three times
+PROFILE_OPS = {
+    "lb1": "csr_lb_kernel (load_balance, one right-hand side)",
+    "lb16": "csr_lb_lanes_kernel (load_balance, 16 right-hand sides)",
+    "cg_block": "cg_block_kernel (CG update pass with 8-row block Jacobi)",
+    "bicg_block": "bicg_block_vec_kernel (BiCGStab with 8-row block Jacobi)",
+    "sddmm16": "sddmm_lanes_kernel (16 columns)",
+    "spgemm": "gemm_*_rows_kernel (A^2)",
+    "mixed": "csr_mixed_kernel (FP32 matrix, FP64 vectors)",
+    "jacobi_apply": "jacobi_block_apply_kernel (8-row blocks)",
+}
+
+
+def profile_op(op):
+    """Three launches of one operation on the 7-point 128^3 matrix (217 MB of
+    Csr, larger than L2), for a single-kernel ncu capture with -k and -c."""
+    import torch
+    from ginkgo_b200 import stencils
+    from ginkgo_b200._lib import call
+    from ginkgo_b200.matrix import Csr, CudaExecutor, _p, _stream, spgemm
+    from ginkgo_b200.solver import Bicgstab, BlockJacobi, Cg, Iteration, Jacobi, ResidualNorm
+    exe = CudaExecutor.create(0)
+    rp, ci, v = stencils.poisson_3d_7pt(128)
+    n = len(rp) - 1
+    A = Csr.read(exe, rp, ci, v)
+    rng = np.random.default_rng(0)
+    k = 16 if op in ("lb16", "sddmm16") else 1
+    x = torch.from_numpy(rng.standard_normal((n, k))).cuda()
+    y = torch.empty_like(x)
+    crit = (Iteration.build().with_max_iters(3), ResidualNorm.build().with_reduction_factor(1e-14))
+    jb = Jacobi.build().with_max_block_size(8).with_block_pointers(np.arange(0, n + 1, 8))
+    for _ in range(3):
+        if op in ("lb1", "lb16"):
+            A.set_strategy("load_balance").apply(x, y)
+        elif op in ("cg_block", "bicg_block"):
+            fac = Cg if op == "cg_block" else Bicgstab
+            s = fac.build().with_criteria(*crit).with_preconditioner(jb).on(exe).generate(A)
+            s.apply(x[:, 0].contiguous(), torch.zeros(n, dtype=torch.float64, device="cuda"))
+        elif op == "sddmm16":
+            g = torch.empty_like(A.values)
+            call("b2s_csr_sddmm_f64", n, _p(A.row_ptrs), _p(A.col_idxs), A.max_row_nnz, _p(x),
+                 x.stride(0), _p(y), y.stride(0), 16, -1.0, _p(g), _stream(g))
+        elif op == "spgemm":
+            spgemm(A, A)
+        elif op == "mixed":
+            A.convert_to_precision(torch.float32).apply(x, y)
+        elif op == "jacobi_apply":
+            BlockJacobi(A, 8, np.arange(0, n + 1, 8)).apply(x, y)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_op": op, "kernel": PROFILE_OPS[op], "n": n}))
 
 
 def ir_gmres_section(exe, stream, grid=96, reps=3):

@@ -149,14 +149,22 @@ template <typename T>
 __global__ void __launch_bounds__(kBlock)
     invert_diagonal_kernel(int64_t n, const int32_t* __restrict__ rp,
                            const int32_t* __restrict__ ci,
-                           const T* __restrict__ v, T* __restrict__ inv)
+                           const T* __restrict__ v, T* __restrict__ inv, int l1)
 {
     const int64_t row = blockIdx.x * int64_t(kBlock) + threadIdx.x;
     if (row >= n) return;
-    T d = T(0);
+    T d = T(0), off = T(0);
     for (int64_t e = rp[row]; e < rp[row + 1]; ++e) {
-        if (ci[e] == row) d = v[e];
+        if (ci[e] == row) {
+            d = v[e];
+        } else if (l1) {
+            off += v[e] < T(0) ? -v[e] : v[e];
+        }
     }
+    // scalar_l1 (reference/preconditioner/jacobi_kernels.cpp:726-745): the
+    // absolute sum of the off-diagonal entries, in storage order, added to
+    // the diagonal before the inversion
+    if (l1) d += off;
     inv[row] = d == T(0) ? T(1) : T(1) / d;
 }
 
@@ -331,12 +339,12 @@ int64_t b2s_csr_transpose_workspace_bytes(int64_t num_rows, int64_t num_cols,
                                        const int32_t* row_ptrs,                \
                                        const int32_t* col_idxs,                \
                                        const T* values, T* inv_diag,           \
-                                       void* stream)                           \
+                                       int aggregate_l1, void* stream)         \
     {                                                                          \
         if (num_rows == 0) return B2S_OK;                                      \
         invert_diagonal_kernel<T><<<ceildiv(num_rows, kBlock), kBlock, 0,      \
                                     as_stream(stream)>>>(                      \
-            num_rows, row_ptrs, col_idxs, values, inv_diag);                   \
+            num_rows, row_ptrs, col_idxs, values, inv_diag, aggregate_l1);     \
         B2S_LAUNCH_CHECK();                                                    \
         return B2S_OK;                                                         \
     }                                                                          \

@@ -31,7 +31,7 @@ __global__ void __launch_bounds__(kJacobiWarps * kWarp)
     jacobi_block_generate_kernel(int64_t n, const int32_t* __restrict__ rp,
                                  const int32_t* __restrict__ ci, const T* __restrict__ v,
                                  int64_t num_blocks, const int32_t* __restrict__ ptrs,
-                                 int max_bs, T* __restrict__ blocks)
+                                 int max_bs, T* __restrict__ blocks, int l1)
 {
     __shared__ T tile[kJacobiWarps][kMaxBs][kMaxBs + 1];
     __shared__ int perm_sh[kJacobiWarps][kMaxBs];
@@ -47,10 +47,19 @@ __global__ void __launch_bounds__(kJacobiWarps * kWarp)
     perm[lane] = lane;
     if (lane < bs) {
         const int row = s + lane;
+        T off = T(0);
         for (int k = rp[row]; k < rp[row + 1]; ++k) {
             const int c = ci[k] - s;
-            if (0 <= c && c < bs) A[lane][c] = v[k];
+            if (0 <= c && c < bs) {
+                A[lane][c] = v[k];
+            } else if (l1) {
+                off += magnitude(v[k]);
+            }
         }
+        // block_l1 (reference/preconditioner/jacobi_kernels.cpp:751-779): the
+        // absolute sum of the row's entries outside its block, in storage
+        // order, added to the row's diagonal (a missing diagonal counts as 0)
+        if (l1) A[lane][lane] += off;
     }
     __syncwarp();
     for (int k = 0; k < bs; ++k) {
@@ -179,14 +188,14 @@ __global__ void __launch_bounds__(kJacobiWarps * kWarp)
 template <typename T>
 int block_generate(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
                    int64_t num_blocks, const int32_t* ptrs, int max_bs, T* blocks,
-                   void* stream)
+                   int aggregate_l1, void* stream)
 {
     B2S_CHECK_ARG(n >= 0 && num_blocks >= 0, "negative size");
     B2S_CHECK_ARG(max_bs >= 1 && max_bs <= kMaxBs, "max_block_size must be 1..32");
     if (num_blocks == 0) return B2S_OK;
     jacobi_block_generate_kernel<T><<<ceildiv(num_blocks, kJacobiWarps),
                                       kJacobiWarps * kWarp, 0, as_stream(stream)>>>(
-        n, rp, ci, v, num_blocks, ptrs, max_bs, blocks);
+        n, rp, ci, v, num_blocks, ptrs, max_bs, blocks, aggregate_l1);
     B2S_LAUNCH_CHECK();
     return B2S_OK;
 }
@@ -252,19 +261,21 @@ int b2s_jacobi_storage_scheme(int max_block_size, int64_t num_blocks, int64_t* b
 int b2s_jacobi_block_generate_f64(int64_t num_rows, const int32_t* row_ptrs,
                                   const int32_t* col_idxs, const double* values,
                                   int64_t num_blocks, const int32_t* block_ptrs,
-                                  int max_block_size, double* blocks, void* stream)
+                                  int max_block_size, double* blocks, int aggregate_l1,
+                                  void* stream)
 {
     return block_generate(num_rows, row_ptrs, col_idxs, values, num_blocks, block_ptrs,
-                          max_block_size, blocks, stream);
+                          max_block_size, blocks, aggregate_l1, stream);
 }
 
 int b2s_jacobi_block_generate_f32(int64_t num_rows, const int32_t* row_ptrs,
                                   const int32_t* col_idxs, const float* values,
                                   int64_t num_blocks, const int32_t* block_ptrs,
-                                  int max_block_size, float* blocks, void* stream)
+                                  int max_block_size, float* blocks, int aggregate_l1,
+                                  void* stream)
 {
     return block_generate(num_rows, row_ptrs, col_idxs, values, num_blocks, block_ptrs,
-                          max_block_size, blocks, stream);
+                          max_block_size, blocks, aggregate_l1, stream);
 }
 
 int b2s_jacobi_block_apply_f64(int64_t num_rows, int64_t num_blocks,

@@ -142,12 +142,13 @@ class Jacobi:
     def build():
         return _Builder(JacobiFactory, max_block_size=32)
 
-    def __init__(self, A: Csr):
+    def __init__(self, A: Csr, aggregate_l1: bool = False):
         self.A = A
+        self.aggregate_l1 = bool(aggregate_l1)
         self.inv_diag = torch.empty(A.shape[0], dtype=A.dtype, device=A.values.device)
         call(f"b2s_jacobi_invert_diagonal_{_SFX[A.dtype]}", A.shape[0],
              _p(A.row_ptrs), _p(A.col_idxs), _p(A.values), _p(self.inv_diag),
-             _stream(self.inv_diag))
+             int(self.aggregate_l1), _stream(self.inv_diag))
 
     def apply(self, *args):
         """apply(b, x) or apply(alpha, b, beta, x)."""
@@ -192,8 +193,10 @@ class BlockJacobi:
     BiCGStab to p' and s (b2s_bicgstab_block_solve_*), GMRES and IR over
     GMRES to each Krylov vector (b2s_gmres_block_solve)."""
 
-    def __init__(self, A: Csr, max_block_size: int, block_pointers=None):
+    def __init__(self, A: Csr, max_block_size: int, block_pointers=None,
+                 aggregate_l1: bool = False):
         self.A = A
+        self.aggregate_l1 = bool(aggregate_l1)
         self.max_block_size = int(max_block_size)
         if not 1 <= self.max_block_size <= 32:
             raise ValueError("max_block_size must be 1..32")
@@ -219,7 +222,7 @@ class BlockJacobi:
         self.blocks = torch.zeros(max(int(space.value), 1), dtype=A.dtype, device=dev)
         call(f"b2s_jacobi_block_generate_{_SFX[A.dtype]}", A.shape[0], _p(A.row_ptrs),
              _p(A.col_idxs), _p(A.values), self.num_blocks, _p(self._ptrs), m,
-             _p(self.blocks), _stream(self.blocks))
+             _p(self.blocks), int(self.aggregate_l1), _stream(self.blocks))
 
     @property
     def inv_diag(self):
@@ -286,14 +289,19 @@ class BlockJacobi:
 
 
 class JacobiFactory:
-    def __init__(self, exec_, max_block_size=32, block_pointers=None):
+    """Jacobi::build() parameters: max_block_size (1 scalar, 2..32 blocks),
+    block_pointers, aggregate_l1 (include/ginkgo/core/preconditioner/
+    jacobi.hpp, parameters)."""
+
+    def __init__(self, exec_, max_block_size=32, block_pointers=None, aggregate_l1=False):
         self.max_block_size = int(max_block_size)
         self.block_pointers = block_pointers
+        self.aggregate_l1 = bool(aggregate_l1)
 
     def generate(self, A):
         if self.max_block_size == 1:
-            return Jacobi(A)
-        return BlockJacobi(A, self.max_block_size, self.block_pointers)
+            return Jacobi(A, self.aggregate_l1)
+        return BlockJacobi(A, self.max_block_size, self.block_pointers, self.aggregate_l1)
 
 
 # ---------------------------------------------------------------- logging --

@@ -246,17 +246,19 @@ int b2s_csr_transpose_f32(int64_t num_rows, int64_t num_cols, int64_t nnz,
 /* --------------------------------------------------------- Jacobi ------ */
 
 /* inv_diag = 1 / diag(A), 1 where the diagonal is zero or missing;
- * replaces the scalar Jacobi generate (jacobi::invert_diagonal,
- * core/preconditioner/jacobi_kernels.hpp:42-45, after extract_diagonal,
- * core/preconditioner/jacobi.cpp:337-369). */
+ * aggregate_l1 != 0 first adds the absolute sum of each row's off-diagonal
+ * entries to its diagonal (Jacobi's aggregate_l1, scalar_l1).  Replaces the
+ * scalar Jacobi generate (jacobi::invert_diagonal,
+ * core/preconditioner/jacobi_kernels.hpp:42-45, after extract_diagonal and
+ * scalar_l1, core/preconditioner/jacobi.cpp:337-369). */
 int b2s_jacobi_invert_diagonal_f64(int64_t num_rows, const int32_t* row_ptrs,
                                    const int32_t* col_idxs,
                                    const double* values, double* inv_diag,
-                                   void* stream);
+                                   int aggregate_l1, void* stream);
 int b2s_jacobi_invert_diagonal_f32(int64_t num_rows, const int32_t* row_ptrs,
                                    const int32_t* col_idxs,
                                    const float* values, float* inv_diag,
-                                   void* stream);
+                                   int aggregate_l1, void* stream);
 /* x = inv_diag .* b, or alpha inv_diag .* b + beta x; replaces
  * jacobi::simple_scalar_apply / scalar_apply
  * (core/preconditioner/jacobi_kernels.hpp:61-65, 79-85). */
@@ -300,14 +302,20 @@ int64_t b2s_jacobi_find_blocks(int64_t num_rows, const int32_t* row_ptrs,
 int b2s_jacobi_storage_scheme(int max_block_size, int64_t num_blocks, int64_t* block_offset,
                               int64_t* group_offset, int32_t* group_power,
                               int64_t* storage_space);
+/* aggregate_l1 != 0: each row's diagonal entry first gains the absolute sum
+ * of the row's entries outside its block (block_l1, reference/
+ * preconditioner/jacobi_kernels.cpp:751-779, a missing diagonal counting as
+ * 0 as after add_diagonal_elements). */
 int b2s_jacobi_block_generate_f64(int64_t num_rows, const int32_t* row_ptrs,
                                   const int32_t* col_idxs, const double* values,
                                   int64_t num_blocks, const int32_t* block_ptrs,
-                                  int max_block_size, double* blocks, void* stream);
+                                  int max_block_size, double* blocks, int aggregate_l1,
+                                  void* stream);
 int b2s_jacobi_block_generate_f32(int64_t num_rows, const int32_t* row_ptrs,
                                   const int32_t* col_idxs, const float* values,
                                   int64_t num_blocks, const int32_t* block_ptrs,
-                                  int max_block_size, float* blocks, void* stream);
+                                  int max_block_size, float* blocks, int aggregate_l1,
+                                  void* stream);
 int b2s_jacobi_block_apply_f64(int64_t num_rows, int64_t num_blocks,
                                const int32_t* block_ptrs, int max_block_size,
                                const double* blocks, const double* b, int64_t ldb,

@@ -347,6 +347,29 @@ bool scalar_jacobi_of(const LinOp* p, const V** inv_diag)
     return false;
 }
 
+// A block Jacobi preconditioner in full precision (max_block_size > 1, no
+// storage optimisation): its blocks are already in the interleaved layout
+// the fused solvers read, delimited by the first num_blocks + 1 entries of
+// the block_pointers parameter that generate() filled in.
+template <typename V>
+bool block_jacobi_of(const LinOp* p, int64* num_blocks, const int32** ptrs,
+                     int* max_block_size, const V** blocks)
+{
+    auto j = dynamic_cast<const preconditioner::Jacobi<V, int32>*>(p);
+    if (j == nullptr) return false;
+    const auto& par = j->get_parameters();
+    const auto& opt = par.storage_optimization;
+    if (par.max_block_size <= 1 || opt.is_block_wise ||
+        precision_reduction::storage_type(opt.of_all_blocks) != 0) {
+        return false;
+    }
+    *num_blocks = static_cast<int64>(j->get_num_blocks());
+    *ptrs = par.block_pointers.get_const_data();
+    *max_block_size = static_cast<int>(par.max_block_size);
+    *blocks = j->get_blocks();
+    return true;
+}
+
 // The solver-level hook of Cg<double>::apply_dense_impl on a CudaExecutor:
 // the whole loop in one fused call.  Returns false (nothing done) when the
 // combination is not the fused path's, so the caller runs the stock loop.
@@ -358,7 +381,14 @@ inline bool try_cg(const solver::Cg<double>* solver, const matrix::Dense<double>
         solver->get_system_matrix());
     if (!exec || !csr || b->get_size()[1] > 16) return false;
     const double* inv_diag = nullptr;
-    if (!scalar_jacobi_of<double>(solver->get_preconditioner().get(), &inv_diag)) return false;
+    int64 num_blocks = 0;
+    const int32* block_ptrs = nullptr;
+    int max_block_size = 0;
+    const double* blocks = nullptr;
+    const LinOp* prec = solver->get_preconditioner().get();
+    const bool block = block_jacobi_of<double>(prec, &num_blocks, &block_ptrs, &max_block_size,
+                                               &blocks);
+    if (!block && !scalar_jacobi_of<double>(prec, &inv_diag)) return false;
     int64 max_iters = std::numeric_limits<int64>::max();
     double reduction = 0.0;
     int mode = B2S_BASELINE_RHS_NORM;
@@ -367,10 +397,20 @@ inline bool try_cg(const solver::Cg<double>* solver, const matrix::Dense<double>
         return false;
     }
     const int64 n = csr->get_size()[0], k = b->get_size()[1];
-    array<char> ws(exec, b2s_cg_workspace_bytes(n, k, sizeof(double)));
     int64 iters = 0;
     std::vector<double> res(k);
     std::vector<uint8_t> status(k);  // gko::stopping_status bit layout
+    if (block) {
+        array<char> ws(exec, b2s_cg_block_workspace_bytes(n, k, sizeof(double)));
+        B2S_GKO_CALL(b2s_cg_block_solve_f64(
+            n, csr->get_const_row_ptrs(), csr->get_const_col_idxs(), csr->get_const_values(),
+            max_row_nnz_of(exec, csr.get()), num_blocks, block_ptrs, max_block_size, blocks,
+            b->get_const_values(), b->get_stride(), x->get_values(), x->get_stride(), k,
+            max_iters, reduction, mode, /*check_every=*/8, ws.get_data(), ws.get_size(),
+            &iters, res.data(), status.data(), exec->get_stream()));
+        return true;
+    }
+    array<char> ws(exec, b2s_cg_workspace_bytes(n, k, sizeof(double)));
     B2S_GKO_CALL(b2s_cg_solve_f64(
         n, csr->get_const_row_ptrs(), csr->get_const_col_idxs(), csr->get_const_values(),
         max_row_nnz_of(exec, csr.get()), inv_diag, b->get_const_values(), b->get_stride(),

@@ -32,11 +32,11 @@ def _csr(exe, m, dt):
 
 
 @pytest.mark.parametrize("dt,npdt", DT)
-@pytest.mark.parametrize("case", [c for c in G["dense"] if not c.get("aggregate_l1")],
-                         ids=lambda c: c["name"])
+@pytest.mark.parametrize("case", G["dense"], ids=lambda c: c["name"])
 def test_inverted_blocks_known_answers(exe, case, dt, npdt):
     A = _csr(exe, case["matrix"], dt)
-    bj = BlockJacobi(A, case["max_block_size"], case.get("block_ptrs"))
+    bj = BlockJacobi(A, case["max_block_size"], case.get("block_ptrs"),
+                     aggregate_l1=case.get("aggregate_l1", False))
     if case.get("transpose"):
         bj = bj.transpose()
     got = bj.to_dense()
@@ -159,3 +159,47 @@ def test_blocks_use_the_reference_interleaved_layout(exe, mbs, scheme):
             for j in range(e - s):
                 assert abs(raw[off + i + j * stride] - ref[s + i, s + j]) <= \
                     1e-11 * max(1.0, abs(ref[s + i, s + j])), (b, i, j)
+
+
+@pytest.mark.parametrize("dt,npdt", DT)
+@pytest.mark.parametrize("case", G["l1"], ids=lambda c: c["name"])
+def test_l1_known_answers(exe, case, dt, npdt):
+    # aggregate_l1 on the device: the scalar case's modified diagonal (as
+    # its inverse) and the block case's modified blocks (as their inverses)
+    m = case["matrix"]
+    A = _csr(exe, m, dt)
+    if case["kind"] == "scalar":
+        got = Jacobi(A, aggregate_l1=True).inv_diag.cpu().numpy()
+        exp = 1.0 / np.array(case["expected"], npdt)
+        np.testing.assert_array_equal(got, exp)
+    else:
+        ptrs = case["block_ptrs"]
+        bj = BlockJacobi(A, max(np.diff(ptrs)), ptrs, aggregate_l1=True)
+        d = np.array(case["expected"], np.float64)
+        exp = np.zeros_like(d)
+        for s0, e0 in zip(ptrs[:-1], ptrs[1:]):
+            exp[s0:e0, s0:e0] = J.invert_block(d[s0:e0, s0:e0].astype(npdt))
+        assert np.abs(bj.to_dense() - exp).max() <= 10 * np.finfo(npdt).eps
+
+
+@pytest.mark.parametrize("dt,npdt", DT)
+@pytest.mark.parametrize("mbs", [1, 4, 13])
+def test_l1_random_blocks_match_oracle(exe, dt, npdt, mbs):
+    # aggregate_l1 with rows reaching outside their blocks: the 27-point
+    # 8^3 operator in uniform blocks of mbs rows, against the oracle
+    from ginkgo_b200 import stencils
+    rp, ci, v = stencils.anisotropic_27pt(8)
+    n = len(rp) - 1
+    A = Csr.read(exe, rp, ci, v, dtype=dt)
+    ptrs = np.concatenate([np.arange(0, n, mbs), [n]]).astype(np.int32)
+    if mbs == 1:
+        got = Jacobi(A, aggregate_l1=True).inv_diag.cpu().numpy()
+        _, exp = J.generate(rp, ci, v.astype(npdt), 1, aggregate_l1=True, dtype=npdt)
+        np.testing.assert_array_equal(got, exp)
+        return
+    bj = BlockJacobi(A, mbs, ptrs, aggregate_l1=True)
+    ref = J.generate(rp, ci, v.astype(npdt), mbs, block_ptrs=ptrs, aggregate_l1=True,
+                     dtype=npdt)
+    exp = J.to_dense(ref, n)
+    tol = 1e-12 if npdt == np.float64 else 2e-5
+    assert np.abs(bj.to_dense() - exp).max() <= tol * max(1.0, np.abs(exp).max())
