@@ -23,7 +23,9 @@
 // One right-hand side on a large system runs the two SpMV passes split, so
 // the matrix streams through the pipelined Csr kernel with one gather per
 // stored entry (forming p' and s at every gathered column triples the
-// gathers once the vectors no longer sit in L2):
+// gathers once the vectors no longer sit in L2); four or more right-hand
+// sides always run split, with the column-slice SpMV (bicg_vec_k_kernel,
+// rhs_lanes_kernel, bicg_dot1k/2k_kernel), as does block Jacobi:
 //   bicg_pupdate  p' and y = D^-1 p'      csr_async  v = A y
 //   bicg_dot1     dot(rr, v) -> alpha      bicg_supdate  s, z = D^-1 s
 //   csr_async     t = A z                  bicg_dot2  dot(s, t), dot(t, t),
@@ -32,6 +34,7 @@
 // fused passes.
 #include "csr_async.cuh"
 #include "jacobi_scheme.cuh"
+#include "rhs_lanes.cuh"
 #include "solver_common.cuh"
 
 namespace b2s {
@@ -449,6 +452,47 @@ __global__ void __launch_bounds__(kSolverBlock)
     }
 }
 
+// The split passes' vector updates for K columns (several right-hand
+// sides): STEP 1 p' = r + tmp (p - omega v) and y = D^-1 p'; STEP 2
+// s = r - alpha v and z = D^-1 s.  Stopped columns are left as they are.
+template <typename T, int K, int STEP>
+__global__ void __launch_bounds__(kSolverBlock)
+    bicg_vec_k_kernel(int64_t n, const T* __restrict__ dinv, const T* __restrict__ r,
+                      const T* __restrict__ a_old, const T* __restrict__ v_old,
+                      T* __restrict__ out, T* __restrict__ prec, SolveCtl* ctl,
+                      BicgScalars<T>* sc)
+{
+    if (ctl->all_stopped) return;
+    bool active[K], from_r[K];
+    T c1[K], c2[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        active[j] = !has_stopped(ctl->status[j]);
+        if (STEP == 1) {
+            c2[j] = sc->omega[j];
+            from_r[j] = sc->prev_rho[j] * c2[j] == T(0);
+            c1[j] = from_r[j] ? T(0) : sc->rho[j] / sc->prev_rho[j] * sc->alpha[j] / c2[j];
+        } else {
+            from_r[j] = false;
+            c1[j] = sc->alpha[j];
+            c2[j] = T(0);
+        }
+    }
+    for (int64_t i = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * kSolverBlock) {
+        const T d = dinv ? dinv[i] : T(1);
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            if (!active[j]) continue;
+            const int64_t e = i * K + j;
+            const T val = STEP == 1 ? bicg_p(r[e], a_old[e], v_old[e], c1[j], c2[j], from_r[j])
+                                    : bicg_s(r[e], a_old[e], c1[j]);
+            out[e] = val;
+            prec[e] = dinv ? mul_rn(d, val) : val;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Block Jacobi (right preconditioning by the block-diagonal inverse M): the
 // preconditioned vectors M p' and M s are no longer row-wise scales, so the
@@ -663,8 +707,8 @@ BicgLayout bicg_layout(int64_t n, int K, bool with_yz = false)
     l.off_t = c.take<T>(n * K);
     l.off_partials = c.take<T>(int64_t(kSolverGrid) * 3 * K);
     // the SpMV inputs of the split passes (single column, or block Jacobi)
-    l.off_y = K == 1 || with_yz ? c.take<T>(n * K) : 0;
-    l.off_z = K == 1 || with_yz ? c.take<T>(n * K) : 0;
+    l.off_y = K == 1 || K >= 4 || with_yz ? c.take<T>(n * K) : 0;
+    l.off_z = K == 1 || K >= 4 || with_yz ? c.take<T>(n * K) : 0;
     l.bytes = c.used;
     return l;
 }
@@ -711,8 +755,8 @@ int bicgstab_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
     T* s = reinterpret_cast<T*>(w + lay.off_s);
     T* t = reinterpret_cast<T*>(w + lay.off_t);
     T* partials = reinterpret_cast<T*>(w + lay.off_partials);
-    T* yv = K == 1 || bp ? reinterpret_cast<T*>(w + lay.off_y) : nullptr;
-    T* zv = K == 1 || bp ? reinterpret_cast<T*>(w + lay.off_z) : nullptr;
+    T* yv = K == 1 || K >= 4 || bp ? reinterpret_cast<T*>(w + lay.off_y) : nullptr;
+    T* zv = K == 1 || K >= 4 || bp ? reinterpret_cast<T*>(w + lay.off_z) : nullptr;
 
     SolveCtl h{};
     h.max_iters = int(max_iters);
@@ -747,22 +791,41 @@ int bicgstab_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
         });
     };
     const bool split = K == 1 && n >= kBicgSplitRows;
-    // block Jacobi: the split passes with K columns
-    auto block_iteration = [&](cudaStream_t cs, int o, int nw) {
+    // the split passes with K columns: block Jacobi (any K), and four or
+    // more right-hand sides (forming p' and s at every gathered column
+    // would read 3 K values per stored entry); the SpMVs with lanes owning
+    // 16-byte column slices where K allows, else the pipelined kernel
+    auto split_k_iteration = [&](cudaStream_t cs, int o, int nw) {
         B2S_DISPATCH_RHS(K, {
             auto spmv_k = [&](const T* in, T* out) {
-                with_async_kernel<T, K, (K >= 2)>(lpr, [&](auto kernel) {
-                    const int64_t grid = std::min<int64_t>(async_need,
-                                                           async_resident_blocks(kernel));
-                    kernel<<<grid, kAsyncBlock, 0, cs>>>(n, rp, ci, v, in, K, out, K, nullptr,
-                                                         nullptr, &ctl->all_stopped);
-                });
+                if constexpr (K >= 4 && K % Vec16<T>::width == 0) {
+                    launch_csr_lanes<T, K>(n, rp, ci, v, in, K, out, K, nullptr, nullptr, cs,
+                                           &ctl->all_stopped);
+                } else {
+                    with_async_kernel<T, K, (K >= 2)>(lpr, [&](auto kernel) {
+                        const int64_t grid = std::min<int64_t>(async_need,
+                                                               async_resident_blocks(kernel));
+                        kernel<<<grid, kAsyncBlock, 0, cs>>>(n, rp, ci, v, in, K, out, K,
+                                                             nullptr, nullptr,
+                                                             &ctl->all_stopped);
+                    });
+                }
             };
-            launch_bicg_block_vec<T, K, 1>(n, *bp, r, p[o], vv[o], p[nw], yv, ctl, sc, cs);
+            if (bp) {
+                launch_bicg_block_vec<T, K, 1>(n, *bp, r, p[o], vv[o], p[nw], yv, ctl, sc, cs);
+            } else {
+                bicg_vec_k_kernel<T, K, 1><<<grid_vec, kSolverBlock, 0, cs>>>(
+                    n, dinv, r, p[o], vv[o], p[nw], yv, ctl, sc);
+            }
             spmv_k(yv, vv[nw]);
             bicg_dot1k_kernel<T, K><<<grid_vec, kSolverBlock, 0, cs>>>(n, rr, vv[nw], ctl, sc,
                                                                       partials);
-            launch_bicg_block_vec<T, K, 2>(n, *bp, r, vv[nw], nullptr, s, zv, ctl, sc, cs);
+            if (bp) {
+                launch_bicg_block_vec<T, K, 2>(n, *bp, r, vv[nw], nullptr, s, zv, ctl, sc, cs);
+            } else {
+                bicg_vec_k_kernel<T, K, 2><<<grid_vec, kSolverBlock, 0, cs>>>(
+                    n, dinv, r, vv[nw], nullptr, s, zv, ctl, sc);
+            }
             spmv_k(zv, t);
             bicg_dot2k_kernel<T, K><<<grid_vec, kSolverBlock, 0, cs>>>(n, s, t, ctl, sc,
                                                                       partials);
@@ -770,11 +833,12 @@ int bicgstab_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
                 n, nullptr, x, ldx, r, rr, yv, s, t, ctl, sc, partials, zv);
         });
     };
+    const bool split_k = bp != nullptr || K >= 4;
     auto capture = [&](cudaStream_t cs) -> int {
         for (int it = 0; it < chunk; ++it) {
             const int o = it % 2, nw = (it + 1) % 2;
-            if (bp) {
-                block_iteration(cs, o, nw);
+            if (split_k) {
+                split_k_iteration(cs, o, nw);
                 B2S_LAUNCH_CHECK();
                 continue;
             }

@@ -1112,6 +1112,11 @@ int gmres_engine(const GmresLayout& lay, int64_t n, int64_t nnz, const int32_t* 
 
     const int grid_vec = int(std::min<int64_t>(
         std::max<int64_t>(1, ceildiv(n, kSolverBlock)), solver_grid()));
+    // the update pass: one wave of resident blocks (it walks the row groups
+    // with a grid stride), instead of a second, partial wave
+    const int grid_upd = int(std::min<int64_t>(
+        std::max<int64_t>(1, ceildiv(ceildiv(n, rows_per_group<TB>()), kSolverBlock)),
+        std::min<int64_t>(solver_grid(), int64_t(update_min_blocks<TA, TB>()) * num_sms())));
     const int grid_dots = int(std::min<int64_t>(
         std::max<int64_t>(1, ceildiv(ceildiv(n, rows_per_group<TB>()), kSolverBlock)),
         std::min(kDotsMaxGrid, num_sms() * 4)));
@@ -1186,7 +1191,7 @@ int gmres_engine(const GmresLayout& lay, int64_t n, int64_t nnz, const int32_t* 
             }
             gmres_dots_kernel<TA, TB><<<grid_dots, kSolverBlock, 0, cs>>>(
                 n, ldv, V, dst, gs, partials, gpart, Gm);
-            gmres_update_kernel<TA, TB><<<grid_vec, kSolverBlock, 0, cs>>>(
+            gmres_update_kernel<TA, TB><<<grid_upd, kSolverBlock, 0, cs>>>(
                 n, ldv, V, dst, da, y, gs, partials, Hm, wq);
             if constexpr (kScaled) {
                 gmres_quantize_kernel<TA, TB, TA><<<grid_vec, kSolverBlock, 0, cs>>>(

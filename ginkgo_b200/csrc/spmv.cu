@@ -10,6 +10,7 @@
 
 #include "common.cuh"
 #include "csr_async.cuh"
+#include "rhs_lanes.cuh"
 #include "ell_rows.cuh"
 
 namespace b2s {
@@ -345,118 +346,6 @@ __global__ void __launch_bounds__(kBlock)
     T* dst = c + int64_t(row) * ldc;
 #pragma unroll
     for (int j = 0; j < K; ++j) dst[j] = combine(acc[j], alpha, beta, dst + j);
-}
-
-// ---------------------------------------------------------------------------
-// Four or more right-hand sides: KL = K / VW lanes share one row and each
-// owns VW consecutive columns (one 16-byte vector), so the lanes of a row
-// read one contiguous stretch of b(col, :) and write one of c(row, :); the
-// row's values and column indices are broadcast loads.  Used for Csr, Ell
-// and Sellp; needs 16-byte aligned b/c rows.
-// ---------------------------------------------------------------------------
-template <typename T>
-struct Vec16;
-template <>
-struct Vec16<double> {
-    using type = double2;
-    static constexpr int width = 2;
-};
-template <>
-struct Vec16<float> {
-    using type = float4;
-    static constexpr int width = 4;
-};
-
-template <typename T>
-__device__ __forceinline__ void fma_vec(typename Vec16<T>::type& acc, T a,
-                                        const T* p)
-{
-    const auto x = __ldg(reinterpret_cast<const typename Vec16<T>::type*>(p));
-    if constexpr (Vec16<T>::width == 2) {
-        acc.x += a * x.x;
-        acc.y += a * x.y;
-    } else {
-        acc.x += a * x.x;
-        acc.y += a * x.y;
-        acc.z += a * x.z;
-        acc.w += a * x.w;
-    }
-}
-
-template <typename T>
-__device__ __forceinline__ void store_vec(T* dst, const typename Vec16<T>::type& acc,
-                                          const T* alpha, const T* beta)
-{
-    constexpr int W = Vec16<T>::width;
-    const T* a = reinterpret_cast<const T*>(&acc);
-    T out[W];
-#pragma unroll
-    for (int u = 0; u < W; ++u) out[u] = combine(a[u], alpha, beta, dst + u);
-    *reinterpret_cast<typename Vec16<T>::type*>(dst) =
-        *reinterpret_cast<const typename Vec16<T>::type*>(out);
-}
-
-// FMT 0: Csr, 1: Ell, 2: Sellp
-template <typename T, int K, int FMT>
-__global__ void __launch_bounds__(kBlock)
-    rhs_lanes_kernel(int64_t n, const int32_t* __restrict__ rp,
-                     int64_t width_or_slice, int64_t stride,
-                     const uint64_t* __restrict__ slice_sets,
-                     const uint64_t* __restrict__ slice_lengths,
-                     const int32_t* __restrict__ ci, const T* __restrict__ v,
-                     const T* __restrict__ b, int64_t ldb, T* __restrict__ c,
-                     int64_t ldc, const T* __restrict__ alpha,
-                     const T* __restrict__ beta)
-{
-    using V = typename Vec16<T>::type;
-    constexpr int VW = Vec16<T>::width;
-    constexpr int KL = K / VW;
-    const int64_t g = blockIdx.x * int64_t(kBlock) + threadIdx.x;
-    const int64_t row = g / KL;
-    if (row >= n) return;
-    const int sub = int(g % KL);
-    const T* bc = b + sub * VW;
-    V acc;
-    {
-        T* a = reinterpret_cast<T*>(&acc);
-#pragma unroll
-        for (int u = 0; u < VW; ++u) a[u] = T(0);
-    }
-    int64_t first, step, len;
-    if constexpr (FMT == 0) {
-        first = rp[row];
-        len = rp[row + 1] - first;
-        step = 1;
-    } else if constexpr (FMT == 1) {
-        first = row;
-        len = width_or_slice;
-        step = stride;
-    } else {
-        const int64_t s = row / width_or_slice;
-        first = int64_t(slice_sets[s]) * width_or_slice + (row - s * width_or_slice);
-        len = int64_t(slice_lengths[s]);
-        step = width_or_slice;
-    }
-    int64_t i = 0;
-    for (; i + 4 <= len; i += 4) {
-        int32_t col[4];
-        T val[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            col[u] = __ldg(ci + first + (i + u) * step);
-            val[u] = __ldg(v + first + (i + u) * step);
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            if (FMT == 0 || col[u] != -1) fma_vec<T>(acc, val[u], bc + int64_t(col[u]) * ldb);
-        }
-    }
-    for (; i < len; ++i) {
-        const int32_t col = __ldg(ci + first + i * step);
-        const T val = __ldg(v + first + i * step);
-        if (FMT == 0 || col != -1) fma_vec<T>(acc, val, bc + int64_t(col) * ldb);
-    }
-    store_vec<T>(c + row * ldc + sub * VW, acc, alpha, beta);
 }
 
 // ---------------------------------------------------------------------------

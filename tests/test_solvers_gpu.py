@@ -329,6 +329,41 @@ def test_bicgstab_multi_rhs(exe):
     assert np.all(explicit_rel_res(rp, ci, v, x.cpu().numpy(), b) <= 3e-9)
 
 
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+@pytest.mark.parametrize("k", [3, 8, 16])
+def test_bicgstab_many_rhs_split_passes_match_oracle(exe, dt, k):
+    # four or more right-hand sides run the split passes (p' and s formed in
+    # their own pass, the column-slice SpMV, per-column dots); every column
+    # against the oracle's single-column BiCGStab, columns stopping at
+    # different iterations (the last one a multiple of the first)
+    from ginkgo_b200.solver import Bicgstab
+    npdt = np.float64 if dt == torch.float64 else np.float32
+    rp, ci, v = stencils.convection_diffusion_2d(40, 36, 1.0, 0.7, -0.4)
+    n = len(rp) - 1
+    b = np.random.default_rng(40 + k).standard_normal((n, k)).astype(npdt)
+    b[:, -1] = 3.0 * b[:, 0]
+    red = 1e-10 if dt == torch.float64 else 1e-5
+    A = Csr.read(exe, rp, ci, v, dtype=dt)
+    s = (Bicgstab.build().with_criteria(*crit(2000, red))
+         .with_preconditioner(Jacobi.build().with_max_block_size(1)).on(exe).generate(A))
+    x = torch.zeros((n, k), dtype=dt, device="cuda")
+    s.apply(torch.from_numpy(b).cuda(), x)
+    assert s.logger.has_converged
+    xg = x.cpu().numpy()
+    its = []
+    for j in range(k):
+        xo, it_o, _, conv_o = orc.bicgstab(rp, ci, v.astype(npdt), b[:, j].copy(),
+                                           max_iters=2000, reduction=red)
+        assert conv_o
+        its.append(it_o)
+        tol = 1e-7 if dt == torch.float64 else 5e-3
+        np.testing.assert_allclose(xg[:, j], xo, rtol=0, atol=tol * np.abs(xo).max())
+    slack = max(3, 0.05 * max(its)) if dt == torch.float64 else max(6, 0.2 * max(its))
+    assert abs(s.logger.num_iterations - max(its)) <= slack, (s.logger.num_iterations, its)
+    assert np.all(explicit_rel_res(rp, ci, v, xg, b.astype(np.float64))
+                  <= (2e-10 if dt == torch.float64 else 5e-5))
+
+
 def test_gmres_rejects_row_bound_below_longest_row(exe):
     # the column-major copy of A is sized by max_row_nnz: a bound below the
     # longest row is an argument error, not a silently truncated matrix
