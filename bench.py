@@ -269,11 +269,27 @@ def main():
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / 1e3 / steps
 
+    def time_graph(op, steps, warmup):
+        """Device time of op (one library call): the call is captured once in
+        a CUDA graph (the library launches on the current stream) and the
+        graph replayed, so the host cost of the Python binding (tensor
+        checks, ctypes marshalling: comparable to the 40 us kernel) does not
+        leave the GPU idle between steps.  The same kernel with the same
+        arguments runs every step."""
+        op()  # first-use set-up (occupancy queries) outside the capture
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            op()
+        out = time_op(g.replay, steps, warmup)
+        del g
+        return out
+
     # pick the faster Csr strategy for the headline (both are reported)
     per_strategy = {}
     for strat in ("classical", "load_balance"):
         A.set_strategy(strat)
-        per_strategy[strat] = time_op(lambda: A.apply(x, y), 20, 3)
+        per_strategy[strat] = time_graph(lambda: A.apply(x, y), 20, 3)
     strategy = (min(per_strategy, key=per_strategy.get)
                 if args.strategy == "auto" else args.strategy)
     A.set_strategy(strategy)
@@ -282,7 +298,7 @@ def main():
         torch.distributed.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
-        t_step = time_op(lambda: A.apply(x, y), args.steps, args.warmup)
+        t_step = time_graph(lambda: A.apply(x, y), args.steps, args.warmup)
         # end-to-end through the public API with host buffers
         xh = torch.from_numpy(np.random.default_rng(SEED).standard_normal(n)).pin_memory()
         yh = torch.empty(n, dtype=torch.float64).pin_memory()
@@ -317,6 +333,8 @@ def main():
                    "num_rhs": 1, "format": "csr", "strategy": strategy,
                    "value_type": "f64", "index_type": "int32",
                    "l2": "inputs (217 MB) larger than L2 (126 MB), no flush",
+                   "timing": "device: CUDA-graph replays of one A.apply call; "
+                             "e2e: direct A.apply calls with host copies",
                    "parallelism": f"replicas{world}"},
         "roofline": {"bound": "hbm", "achieved": round(gbs, 1),
                      "peak": peak, "unit": "GB/s",
@@ -333,7 +351,7 @@ def main():
         "clocks": clk.summary(),
     }
     if args.sweep:
-        result["sweep"] = sweep(exe, rp, ci, v, time_op)
+        result["sweep"] = sweep(exe, rp, ci, v, time_graph)
     if not args.no_solve:
         solve = ir_gmres_section(exe, stream)
         result["ir_gmres"] = solve
@@ -551,6 +569,8 @@ PROFILE_OPS = {
     "spgemm": "gemm_*_rows_kernel (A^2)",
     "mixed": "csr_mixed_kernel (FP32 matrix, FP64 vectors)",
     "jacobi_apply": "jacobi_block_apply_kernel (8-row blocks)",
+    "ell4": "rhs_lanes_kernel (Ell, 4 right-hand sides)",
+    "bicg16": "bicg_vec_lanes_kernel / bicg_update_lanes_kernel (BiCGStab, 16 RHS)",
 }
 
 
@@ -567,7 +587,7 @@ def profile_op(op):
     n = len(rp) - 1
     A = Csr.read(exe, rp, ci, v)
     rng = np.random.default_rng(0)
-    k = 16 if op in ("lb16", "sddmm16") else 1
+    k = 16 if op in ("lb16", "sddmm16", "bicg16") else 4 if op == "ell4" else 1
     x = torch.from_numpy(rng.standard_normal((n, k))).cuda()
     y = torch.empty_like(x)
     crit = (Iteration.build().with_max_iters(3), ResidualNorm.build().with_reduction_factor(1e-14))
@@ -589,6 +609,12 @@ def profile_op(op):
             A.convert_to_precision(torch.float32).apply(x, y)
         elif op == "jacobi_apply":
             BlockJacobi(A, 8, np.arange(0, n + 1, 8)).apply(x, y)
+        elif op == "ell4":
+            A.convert_to_ell().apply(x, y)
+        elif op == "bicg16":
+            s = (Bicgstab.build().with_criteria(*crit)
+                 .with_preconditioner(Jacobi.build().with_max_block_size(1)).on(exe).generate(A))
+            s.apply(x, torch.zeros_like(x))
     torch.cuda.synchronize()
     print(json.dumps({"profile_op": op, "kernel": PROFILE_OPS[op], "n": n}))
 

@@ -58,6 +58,71 @@ __device__ __forceinline__ T bicg_s(T r, T v, T alpha)
     return add_rn(r, -mul_rn(alpha, v));
 }
 
+// The last block's part of the update pass (thread 0): tot holds dot(rr, r)
+// and ||r||^2 per column; finalises the columns that stopped at s, advances
+// the iteration, swaps rho and applies the checks.
+template <typename T, int K>
+__device__ void bicg_update_finish(const T* tot, SolveCtl* ctl, BicgScalars<T>* sc)
+{
+    ctl->ticket = 0;
+    int all_after_s = 1;
+    for (int j = 0; j < K; ++j) all_after_s &= has_stopped(ctl->status[j]);
+    const int iter = all_after_s ? ctl->iter : ctl->iter + 1;
+    ctl->iter = iter;
+    int all = 1;
+    for (int j = 0; j < K; ++j) {
+        uint8_t st = ctl->status[j];
+        if (has_stopped(st)) {
+            st |= kFinalizedMask;
+        } else {
+            sc->prev_rho[j] = sc->rho[j];
+            sc->rho[j] = tot[j];
+            sc->tau[j] = sqrt(tot[K + j]);
+            if (residual_met(ctl, sc->tau[j], sc->rho[j], sc->start[j])) {
+                converge_status(st, kResidualId, true);
+            }
+            if (iter >= ctl->max_iters) stop_status(st, kIterationId, true);
+        }
+        ctl->status[j] = st;
+        all &= has_stopped(st);
+    }
+    ctl->all_stopped = all;
+}
+
+// The last block's part of the pass after the first SpMV (thread j < K):
+// alpha = rho / dot(rr, v).
+template <typename T, int K>
+__device__ void bicg_alpha_finish(const T* tot, SolveCtl* ctl, BicgScalars<T>* sc)
+{
+    const int j = threadIdx.x;
+    if (j < K && !has_stopped(ctl->status[j])) {
+        const T bv = tot[j];
+        sc->alpha[j] = bv != T(0) ? sc->rho[j] / bv : T(0);
+    }
+    if (threadIdx.x == 0) ctl->ticket = 0;
+}
+
+// The last block's part of the pass after the second SpMV (thread 0): tot
+// holds dot(s, t), dot(t, t) and ||s||^2 per column; the check on s
+// (without finalising: the update pass adds alpha y) and omega.
+template <typename T, int K>
+__device__ void bicg_omega_finish(const T* tot, SolveCtl* ctl, BicgScalars<T>* sc)
+{
+    ctl->ticket = 0;
+    for (int j = 0; j < K; ++j) {
+        uint8_t st = ctl->status[j];
+        if (has_stopped(st)) continue;
+        const T tau_s = sqrt(tot[2 * K + j]);
+        if (residual_met(ctl, tau_s, sc->rho[j], sc->start[j])) {
+            converge_status(st, kResidualId, false);
+            sc->tau[j] = tau_s;
+        }
+        ctl->status[j] = st;
+        const T tt = tot[K + j];
+        sc->omega[j] = tt != T(0) ? tot[j] / tt : T(0);
+    }
+}
+
 template <typename T, int K>
 __global__ void __launch_bounds__(kSolverBlock)
     bicg_init_kernel(int64_t n, const T* __restrict__ b, int64_t ldb, int k,
@@ -325,31 +390,7 @@ __global__ void __launch_bounds__(kSolverBlock)
     block_partials<T, 2 * K>(acc, partials, red);
     if (last_block_done(&ctl->ticket, &last)) {
         sum_partials<T, 2 * K>(partials, gridDim.x, tot, red);
-        if (threadIdx.x == 0) {
-            ctl->ticket = 0;
-            int all_after_s = 1;
-            for (int j = 0; j < K; ++j) all_after_s &= has_stopped(ctl->status[j]);
-            const int iter = all_after_s ? ctl->iter : ctl->iter + 1;
-            ctl->iter = iter;
-            int all = 1;
-            for (int j = 0; j < K; ++j) {
-                uint8_t st = ctl->status[j];
-                if (has_stopped(st)) {
-                    st |= kFinalizedMask;
-                } else {
-                    sc->prev_rho[j] = sc->rho[j];
-                    sc->rho[j] = tot[j];
-                    sc->tau[j] = sqrt(tot[K + j]);
-                    if (residual_met(ctl, sc->tau[j], sc->rho[j], sc->start[j])) {
-                        converge_status(st, kResidualId, true);
-                    }
-                    if (iter >= ctl->max_iters) stop_status(st, kIterationId, true);
-                }
-                ctl->status[j] = st;
-                all &= has_stopped(st);
-            }
-            ctl->all_stopped = all;
-        }
+        if (threadIdx.x == 0) bicg_update_finish<T, K>(tot, ctl, sc);
     }
 }
 
@@ -494,6 +535,222 @@ __global__ void __launch_bounds__(kSolverBlock)
 }
 
 // ---------------------------------------------------------------------------
+// The split passes for K >= 4 right-hand sides with 16-byte column slices
+// (K a multiple of VW = 16 / sizeof(T)): the n x K blocks are walked as one
+// flat array of 16-byte vectors, thread t owning the VW columns
+// (t mod KL) * VW.. of row t / KL (KL = K / VW); the grid stride is a
+// multiple of KL, so a thread keeps its columns and the per-column sums
+// reduce over the lanes that share them (shuffles over lane offsets KL,
+// 2 KL, ...), then over the block's warps and the blocks (partials
+// [sum][block][K], deterministic).  Same arithmetic as the row-wise
+// kernels above; stopped columns keep their values.
+// ---------------------------------------------------------------------------
+template <typename T, int K, int STEP>
+__global__ void __launch_bounds__(kSolverBlock)
+    bicg_vec_lanes_kernel(int64_t n, const T* __restrict__ dinv, const T* __restrict__ r,
+                          const T* __restrict__ a_old, const T* __restrict__ v_old,
+                          T* __restrict__ out, T* __restrict__ prec, SolveCtl* ctl,
+                          BicgScalars<T>* sc)
+{
+    constexpr int VW = int(16 / sizeof(T));
+    constexpr int KL = K / VW;
+    if (ctl->all_stopped) return;
+    const int64_t t0 = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x;
+    const int col0 = int(t0 % KL) * VW;
+    bool active[VW], from_r[VW];
+    T c1[VW], c2[VW];
+#pragma unroll
+    for (int u = 0; u < VW; ++u) {
+        const int j = col0 + u;
+        active[u] = !has_stopped(ctl->status[j]);
+        if (STEP == 1) {
+            c2[u] = sc->omega[j];
+            from_r[u] = sc->prev_rho[j] * c2[u] == T(0);
+            c1[u] = from_r[u] ? T(0) : sc->rho[j] / sc->prev_rho[j] * sc->alpha[j] / c2[u];
+        } else {
+            from_r[u] = false;
+            c1[u] = sc->alpha[j];
+            c2[u] = T(0);
+        }
+    }
+    const int64_t nvec = n * KL;
+    for (int64_t t = t0; t < nvec; t += int64_t(gridDim.x) * kSolverBlock) {
+        const int64_t i = t / KL, e = t * VW;
+        const T d = dinv ? dinv[i] : T(1);
+        T rv[VW], av[VW], vv[VW], val[VW], pv[VW];
+        ld_vec<T, VW>(r + e, rv);
+        ld_vec<T, VW>(a_old + e, av);
+        if (STEP == 1) ld_vec<T, VW>(v_old + e, vv);
+#pragma unroll
+        for (int u = 0; u < VW; ++u) {
+            if (active[u]) {
+                val[u] = STEP == 1 ? bicg_p(rv[u], av[u], vv[u], c1[u], c2[u], from_r[u])
+                                   : bicg_s(rv[u], av[u], c1[u]);
+            } else {
+                val[u] = STEP == 1 ? av[u] : rv[u];
+            }
+            pv[u] = dinv ? mul_rn(d, val[u]) : val[u];
+        }
+        st_vec<T, VW>(out + e, val);
+        st_vec<T, VW>(prec + e, pv);
+    }
+}
+
+// Sums NS products per column over the lanes that share the column slice,
+// the block's warps (red[W][NS * K]) and the blocks: partials[m][block][K].
+template <typename T, int K, int NS>
+__device__ __forceinline__ void lanes_partials(T (&acc)[NS][int(16 / sizeof(T))], int col0,
+                                               T* __restrict__ partials, T* red)
+{
+    constexpr int VW = int(16 / sizeof(T));
+    constexpr int KL = K / VW;
+    constexpr int W = kSolverBlock / kWarp;
+    const int lane = threadIdx.x % kWarp, wid = threadIdx.x / kWarp;
+#pragma unroll
+    for (int off = KL; off < kWarp; off *= 2) {
+#pragma unroll
+        for (int m = 0; m < NS; ++m) {
+#pragma unroll
+            for (int u = 0; u < VW; ++u) {
+                acc[m][u] += __shfl_xor_sync(0xffffffffu, acc[m][u], off);
+            }
+        }
+    }
+    if (lane < KL) {
+#pragma unroll
+        for (int m = 0; m < NS; ++m) {
+#pragma unroll
+            for (int u = 0; u < VW; ++u) red[wid * NS * K + m * K + col0 + u] = acc[m][u];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < NS * K) {
+        T s = T(0);
+        for (int w = 0; w < W; ++w) s += red[w * NS * K + threadIdx.x];
+        const int m = threadIdx.x / K, j = threadIdx.x % K;
+        partials[int64_t(m) * gridDim.x * K + int64_t(blockIdx.x) * K + j] = s;
+    }
+}
+
+// The last block: tot[m * K + j] = sum over blocks of partials[m][.][j].
+template <typename T, int K, int NS>
+__device__ __forceinline__ void lanes_totals(const T* __restrict__ partials, T* tot, T* red)
+{
+#pragma unroll
+    for (int m = 0; m < NS; ++m) {
+        sum_partials<T, K>(partials + int64_t(m) * gridDim.x * K, gridDim.x, tot + m * K, red);
+    }
+}
+
+// NS = 1: dot(rr, v) -> alpha; NS = 3: dot(s, t), dot(t, t), ||s||^2 ->
+// the check on s and omega
+template <typename T, int K, int NS>
+__global__ void __launch_bounds__(kSolverBlock)
+    bicg_dots_lanes_kernel(int64_t n, const T* __restrict__ a, const T* __restrict__ b,
+                           SolveCtl* ctl, BicgScalars<T>* sc, T* __restrict__ partials)
+{
+    constexpr int VW = int(16 / sizeof(T));
+    constexpr int KL = K / VW;
+    __shared__ T red[kSolverBlock / kWarp * NS * K];
+    __shared__ T tot[NS * K];
+    __shared__ int last;
+    if (ctl->all_stopped) return;
+    const int64_t t0 = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x;
+    const int col0 = int(t0 % KL) * VW;
+    T acc[NS][VW];
+#pragma unroll
+    for (int m = 0; m < NS; ++m) {
+#pragma unroll
+        for (int u = 0; u < VW; ++u) acc[m][u] = T(0);
+    }
+    const int64_t nvec = n * KL;
+    for (int64_t t = t0; t < nvec; t += int64_t(gridDim.x) * kSolverBlock) {
+        T av[VW], bv[VW];
+        ld_vec<T, VW>(a + t * VW, av);
+        ld_vec<T, VW>(b + t * VW, bv);
+#pragma unroll
+        for (int u = 0; u < VW; ++u) {
+            acc[0][u] += av[u] * bv[u];
+            if constexpr (NS == 3) {
+                acc[1][u] += bv[u] * bv[u];
+                acc[2][u] += av[u] * av[u];
+            }
+        }
+    }
+    lanes_partials<T, K, NS>(acc, col0, partials, red);
+    if (last_block_done(&ctl->ticket, &last)) {
+        lanes_totals<T, K, NS>(partials, tot, red);
+        if constexpr (NS == 1) {
+            bicg_alpha_finish<T, K>(tot, ctl, sc);
+        } else {
+            if (threadIdx.x == 0) bicg_omega_finish<T, K>(tot, ctl, sc);
+        }
+    }
+}
+
+// x += alpha y + omega z (alpha y alone for a column finalised at s),
+// r = s - omega t, then dot(rr, r) and ||r||^2 per column
+template <typename T, int K>
+__global__ void __launch_bounds__(kSolverBlock)
+    bicg_update_lanes_kernel(int64_t n, T* __restrict__ x, int64_t ldx, T* __restrict__ r,
+                             const T* __restrict__ rr, const T* __restrict__ y,
+                             const T* __restrict__ s, const T* __restrict__ t,
+                             const T* __restrict__ z, SolveCtl* ctl, BicgScalars<T>* sc,
+                             T* __restrict__ partials)
+{
+    constexpr int VW = int(16 / sizeof(T));
+    constexpr int KL = K / VW;
+    __shared__ T red[kSolverBlock / kWarp * 2 * K];
+    __shared__ T tot[2 * K];
+    __shared__ int last;
+    if (ctl->all_stopped) return;
+    const int64_t t0 = blockIdx.x * int64_t(kSolverBlock) + threadIdx.x;
+    const int col0 = int(t0 % KL) * VW;
+    int mode[VW];  // 0 frozen, 1 finalise at s, 2 full update
+    T alpha[VW], omega[VW];
+#pragma unroll
+    for (int u = 0; u < VW; ++u) {
+        const uint8_t st = ctl->status[col0 + u];
+        mode[u] = !has_stopped(st) ? 2 : (is_finalized(st) ? 0 : 1);
+        alpha[u] = sc->alpha[col0 + u];
+        omega[u] = sc->omega[col0 + u];
+    }
+    T acc[2][VW];
+#pragma unroll
+    for (int u = 0; u < VW; ++u) acc[0][u] = acc[1][u] = T(0);
+    const int64_t nvec = n * KL;
+    for (int64_t q = t0; q < nvec; q += int64_t(gridDim.x) * kSolverBlock) {
+        const int64_t i = q / KL, e = q * VW;
+        T yv[VW], sv[VW], tv[VW], zv[VW], rv[VW], hv[VW];
+        ld_vec<T, VW>(y + e, yv);
+        ld_vec<T, VW>(s + e, sv);
+        ld_vec<T, VW>(t + e, tv);
+        ld_vec<T, VW>(z + e, zv);
+        ld_vec<T, VW>(r + e, rv);
+        ld_vec<T, VW>(rr + e, hv);
+        T* xr = x + i * ldx + col0;
+#pragma unroll
+        for (int u = 0; u < VW; ++u) {
+            if (mode[u] == 1) {
+                xr[u] += alpha[u] * yv[u];
+            } else if (mode[u] == 2) {
+                xr[u] += alpha[u] * yv[u] + omega[u] * zv[u];
+                const T ri = sv[u] - omega[u] * tv[u];
+                rv[u] = ri;
+                acc[0][u] += hv[u] * ri;
+                acc[1][u] += ri * ri;
+            }
+        }
+        st_vec<T, VW>(r + e, rv);
+    }
+    lanes_partials<T, K, 2>(acc, col0, partials, red);
+    if (last_block_done(&ctl->ticket, &last)) {
+        lanes_totals<T, K, 2>(partials, tot, red);
+        if (threadIdx.x == 0) bicg_update_finish<T, K>(tot, ctl, sc);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Block Jacobi (right preconditioning by the block-diagonal inverse M): the
 // preconditioned vectors M p' and M s are no longer row-wise scales, so the
 // iteration runs split for any number of right-hand sides:
@@ -600,11 +857,7 @@ __global__ void __launch_bounds__(kSolverBlock)
     block_partials<T, K>(acc, partials, red);
     if (last_block_done(&ctl->ticket, &last)) {
         sum_partials<T, K>(partials, gridDim.x, tot, red);
-        if (threadIdx.x < K && !has_stopped(ctl->status[threadIdx.x])) {
-            const T bv = tot[threadIdx.x];
-            sc->alpha[threadIdx.x] = bv != T(0) ? sc->rho[threadIdx.x] / bv : T(0);
-        }
-        if (threadIdx.x == 0) ctl->ticket = 0;
+        bicg_alpha_finish<T, K>(tot, ctl, sc);
     }
 }
 
@@ -635,21 +888,7 @@ __global__ void __launch_bounds__(kSolverBlock)
     block_partials<T, 3 * K>(acc, partials, red);
     if (last_block_done(&ctl->ticket, &last)) {
         sum_partials<T, 3 * K>(partials, gridDim.x, tot, red);
-        if (threadIdx.x == 0) {
-            ctl->ticket = 0;
-            for (int j = 0; j < K; ++j) {
-                uint8_t st = ctl->status[j];
-                if (has_stopped(st)) continue;
-                const T tau_s = sqrt(tot[2 * K + j]);
-                if (residual_met(ctl, tau_s, sc->rho[j], sc->start[j])) {
-                    converge_status(st, kResidualId, false);
-                    sc->tau[j] = tau_s;
-                }
-                ctl->status[j] = st;
-                const T tt = tot[K + j];
-                sc->omega[j] = tt != T(0) ? tot[j] / tt : T(0);
-            }
-        }
+        if (threadIdx.x == 0) bicg_omega_finish<T, K>(tot, ctl, sc);
     }
 }
 
@@ -811,26 +1050,49 @@ int bicgstab_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
                     });
                 }
             };
+            constexpr bool kLanes = K >= 4 && K % Vec16<T>::width == 0;
+            // the flat vector passes: one wave of 16-byte vectors per thread
+            const int grid_lanes = int(std::min<int64_t>(
+                std::max<int64_t>(1, ceildiv(n * K / Vec16<T>::width, kSolverBlock)),
+                solver_grid()));
             if (bp) {
                 launch_bicg_block_vec<T, K, 1>(n, *bp, r, p[o], vv[o], p[nw], yv, ctl, sc, cs);
+            } else if constexpr (kLanes) {
+                bicg_vec_lanes_kernel<T, K, 1><<<grid_lanes, kSolverBlock, 0, cs>>>(
+                    n, dinv, r, p[o], vv[o], p[nw], yv, ctl, sc);
             } else {
                 bicg_vec_k_kernel<T, K, 1><<<grid_vec, kSolverBlock, 0, cs>>>(
                     n, dinv, r, p[o], vv[o], p[nw], yv, ctl, sc);
             }
             spmv_k(yv, vv[nw]);
-            bicg_dot1k_kernel<T, K><<<grid_vec, kSolverBlock, 0, cs>>>(n, rr, vv[nw], ctl, sc,
-                                                                      partials);
+            if constexpr (kLanes) {
+                bicg_dots_lanes_kernel<T, K, 1><<<grid_lanes, kSolverBlock, 0, cs>>>(
+                    n, rr, vv[nw], ctl, sc, partials);
+            } else {
+                bicg_dot1k_kernel<T, K><<<grid_vec, kSolverBlock, 0, cs>>>(n, rr, vv[nw], ctl,
+                                                                          sc, partials);
+            }
             if (bp) {
                 launch_bicg_block_vec<T, K, 2>(n, *bp, r, vv[nw], nullptr, s, zv, ctl, sc, cs);
+            } else if constexpr (kLanes) {
+                bicg_vec_lanes_kernel<T, K, 2><<<grid_lanes, kSolverBlock, 0, cs>>>(
+                    n, dinv, r, vv[nw], nullptr, s, zv, ctl, sc);
             } else {
                 bicg_vec_k_kernel<T, K, 2><<<grid_vec, kSolverBlock, 0, cs>>>(
                     n, dinv, r, vv[nw], nullptr, s, zv, ctl, sc);
             }
             spmv_k(zv, t);
-            bicg_dot2k_kernel<T, K><<<grid_vec, kSolverBlock, 0, cs>>>(n, s, t, ctl, sc,
-                                                                      partials);
-            bicg_update_kernel<T, K><<<grid_vec, kSolverBlock, 0, cs>>>(
-                n, nullptr, x, ldx, r, rr, yv, s, t, ctl, sc, partials, zv);
+            if constexpr (kLanes) {
+                bicg_dots_lanes_kernel<T, K, 3><<<grid_lanes, kSolverBlock, 0, cs>>>(
+                    n, s, t, ctl, sc, partials);
+                bicg_update_lanes_kernel<T, K><<<grid_lanes, kSolverBlock, 0, cs>>>(
+                    n, x, ldx, r, rr, yv, s, t, zv, ctl, sc, partials);
+            } else {
+                bicg_dot2k_kernel<T, K><<<grid_vec, kSolverBlock, 0, cs>>>(n, s, t, ctl, sc,
+                                                                          partials);
+                bicg_update_kernel<T, K><<<grid_vec, kSolverBlock, 0, cs>>>(
+                    n, nullptr, x, ldx, r, rr, yv, s, t, ctl, sc, partials, zv);
+            }
         });
     };
     const bool split_k = bp != nullptr || K >= 4;

@@ -265,20 +265,6 @@ __global__ void __launch_bounds__(kSolverBlock)
 // shuffle reduction runs per row.  Stopped columns are computed along
 // (their results are never used: the update pass freezes them).
 // ---------------------------------------------------------------------------
-template <typename T, int R>
-__device__ __forceinline__ void ld_vec(const T* p, T (&o)[R])
-{
-    static_assert(R * sizeof(T) == 16, "one 16-byte vector");
-    const uint4 u = *reinterpret_cast<const uint4*>(p);
-    memcpy(o, &u, 16);
-}
-template <typename T, int R>
-__device__ __forceinline__ void st_vec(T* p, const T (&v)[R])
-{
-    uint4 u;
-    memcpy(&u, v, 16);
-    *reinterpret_cast<uint4*>(p) = u;
-}
 
 template <typename T, int K>
 __global__ void __launch_bounds__(kSolverBlock)

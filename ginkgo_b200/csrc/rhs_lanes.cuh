@@ -2,6 +2,8 @@
 // the column-slice kernel shared by the SpMV entry points and the solvers.
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace b2s {
@@ -122,6 +124,93 @@ __global__ void __launch_bounds__(kLanesBlock)
     store_vec<T>(c + row * ldc + sub * VW, acc, alpha, beta);
 }
 
+
+// Ell (FMT 1) and Sellp (FMT 2) with two neighbouring rows per lane slot:
+// the rows' column indices and values at each entry are one 8- or 16-byte
+// vector load (the layouts are column-major, so rows r and r + 1 sit next
+// to each other), and each slot gathers two 16-byte pieces of b per entry.
+// Needs an even stride (Ell) or slice size (Sellp) and 16-byte aligned b
+// and c rows; a row pair whose second row lies past the storage (odd n with
+// stride n) falls back to single loads.
+template <typename T, int K, int FMT>
+__global__ void __launch_bounds__(kLanesBlock)
+    rhs_lanes2_kernel(int64_t n, int64_t width_or_slice, int64_t stride,
+                      const uint64_t* __restrict__ slice_sets,
+                      const uint64_t* __restrict__ slice_lengths,
+                      const int32_t* __restrict__ ci, const T* __restrict__ v,
+                      const T* __restrict__ b, int64_t ldb, T* __restrict__ c, int64_t ldc,
+                      const T* __restrict__ alpha, const T* __restrict__ beta)
+{
+    static_assert(FMT == 1 || FMT == 2, "Ell or Sellp");
+    using V = typename Vec16<T>::type;
+    using V2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+    constexpr int VW = Vec16<T>::width;
+    constexpr int KL = K / VW;
+    const int64_t g = blockIdx.x * int64_t(kLanesBlock) + threadIdx.x;
+    const int64_t r0 = 2 * (g / KL);
+    if (r0 >= n) return;
+    const int sub = int(g % KL);
+    const T* bc = b + sub * VW;
+    V acc0, acc1;
+    {
+        T* a0 = reinterpret_cast<T*>(&acc0);
+        T* a1 = reinterpret_cast<T*>(&acc1);
+#pragma unroll
+        for (int u = 0; u < VW; ++u) a0[u] = a1[u] = T(0);
+    }
+    int64_t first, step, len;
+    bool pair;
+    if constexpr (FMT == 1) {
+        first = r0;
+        len = width_or_slice;
+        step = stride;
+        pair = r0 + 1 < stride;
+    } else {
+        const int64_t sl = r0 / width_or_slice;
+        first = int64_t(slice_sets[sl]) * width_or_slice + (r0 - sl * width_or_slice);
+        len = int64_t(slice_lengths[sl]);
+        step = width_or_slice;
+        pair = true;
+    }
+    const bool second = r0 + 1 < n;
+    if (pair) {
+        // four entries' index and value pairs in flight before their gathers
+        // (padding-heavy slices are bound by these loads, not the gathers)
+        int64_t i = 0;
+        for (; i + 4 <= len; i += 4) {
+            int2 cc[4];
+            V2 vv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int64_t e = first + (i + u) * step;
+                cc[u] = __ldg(reinterpret_cast<const int2*>(ci + e));
+                vv[u] = __ldg(reinterpret_cast<const V2*>(v + e));
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (cc[u].x != -1) fma_vec<T>(acc0, vv[u].x, bc + int64_t(cc[u].x) * ldb);
+                if (second && cc[u].y != -1) {
+                    fma_vec<T>(acc1, vv[u].y, bc + int64_t(cc[u].y) * ldb);
+                }
+            }
+        }
+        for (; i < len; ++i) {
+            const int64_t e = first + i * step;
+            const int2 cc = __ldg(reinterpret_cast<const int2*>(ci + e));
+            const V2 vv = __ldg(reinterpret_cast<const V2*>(v + e));
+            if (cc.x != -1) fma_vec<T>(acc0, vv.x, bc + int64_t(cc.x) * ldb);
+            if (second && cc.y != -1) fma_vec<T>(acc1, vv.y, bc + int64_t(cc.y) * ldb);
+        }
+    } else {
+        for (int64_t i = 0; i < len; ++i) {
+            const int64_t e = first + i * step;
+            const int32_t col = __ldg(ci + e);
+            if (col != -1) fma_vec<T>(acc0, __ldg(v + e), bc + int64_t(col) * ldb);
+        }
+    }
+    store_vec<T>(c + r0 * ldc + sub * VW, acc0, alpha, beta);
+    if (second) store_vec<T>(c + (r0 + 1) * ldc + sub * VW, acc1, alpha, beta);
+}
 
 // Launches rhs_lanes_kernel on Csr for K right-hand sides (K >= 4 and a
 // multiple of the 16-byte vector width; b and c rows 16-byte aligned).

@@ -6,6 +6,7 @@
 #pragma once
 
 #include <algorithm>
+#include <cstring>
 #include <type_traits>
 #include <vector>
 
@@ -343,6 +344,22 @@ int run_graph_loop(cudaStream_t st, SolveCtl* ctl, int max_iters, int chunk,
     if (graph) cudaGraphDestroy(graph);
     cudaStreamDestroy(cap);
     return rc;
+}
+
+// One 16-byte vector of R values (R * sizeof(T) == 16, p 16-byte aligned).
+template <typename T, int R>
+__device__ __forceinline__ void ld_vec(const T* p, T (&o)[R])
+{
+    static_assert(R * sizeof(T) == 16, "one 16-byte vector");
+    const uint4 u = *reinterpret_cast<const uint4*>(p);
+    memcpy(o, &u, 16);
+}
+template <typename T, int R>
+__device__ __forceinline__ void st_vec(T* p, const T (&v)[R])
+{
+    uint4 u;
+    memcpy(&u, v, 16);
+    *reinterpret_cast<uint4*>(p) = u;
 }
 
 }  // namespace b2s

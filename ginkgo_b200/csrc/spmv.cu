@@ -166,8 +166,10 @@ __device__ __noinline__ void lb_long_row(const T* sv, const int32_t* sc, int s, 
     if (lane < K) dst[lane] = combine(a, alpha, beta, dst + lane);
 }
 
+// one right-hand side held to six blocks per SM (40 registers; at 48
+// registers the five resident blocks left half the warps idle)
 template <typename T, int K, bool VEC>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, (K == 1 ? 6 : 2))
     csr_lb_kernel(int64_t n, int64_t nc, const int32_t* __restrict__ own_first,
                   int32_t* __restrict__ tail_row, T* __restrict__ partials,
                   const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
@@ -504,6 +506,20 @@ void launch_lanes(int64_t n, const int32_t* rp, int64_t w_or_s, int64_t stride,
 {
     if constexpr (K >= 4 && K % Vec16<T>::width == 0) {
         constexpr int KL = K / Vec16<T>::width;
+        // Ell / Sellp: row pairs per lane slot when the column-major layout
+        // keeps rows r, r + 1 adjacent at 8-byte alignment
+        const bool aligned = reinterpret_cast<uintptr_t>(ci) % 8 == 0 &&
+                             reinterpret_cast<uintptr_t>(v) % (2 * sizeof(T)) == 0;
+        const bool pairs = aligned && ((FMT == 1 && stride % 2 == 0) ||
+                                       (FMT == 2 && w_or_s % 2 == 0));
+        if (FMT != 0 && pairs) {
+            if constexpr (FMT != 0) {
+                rhs_lanes2_kernel<T, K, FMT><<<ceildiv(ceildiv(n, 2) * KL, kBlock), kBlock, 0,
+                                               st>>>(n, w_or_s, stride, sets, lens, ci, v, b,
+                                                     ldb, c, ldc, alpha, beta);
+            }
+            return;
+        }
         rhs_lanes_kernel<T, K, FMT><<<ceildiv(n * KL, kBlock), kBlock, 0, st>>>(
             n, rp, w_or_s, stride, sets, lens, ci, v, b, ldb, c, ldc, alpha,
             beta);

@@ -173,6 +173,37 @@ def test_load_balance_chunk_boundaries(exe, dt, k):
     assert torch.equal(y, y3)
 
 
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+@pytest.mark.parametrize("k", [4, 8, 16])
+def test_ell_sellp_row_pairs_many_rhs(exe, dt, k):
+    # four or more right-hand sides on Ell / Sellp: row pairs per lane slot
+    # when the stride (Ell) or slice size (Sellp) is even, single rows when
+    # it is odd; an odd row count leaves the last pair half inside the
+    # matrix (with Ell stride n + 1 its second row is padding storage)
+    rng = np.random.default_rng(60 + k)
+    n = 4097
+    lens = rng.integers(0, 12, n)
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    ci = np.concatenate([np.sort(rng.choice(n, l, replace=False)) for l in lens]).astype(np.int32)
+    v = rng.standard_normal(int(rp[-1])).astype(NP[dt])
+    x = rng.standard_normal((n, k)).astype(NP[dt])
+    y0 = rng.standard_normal((n, k)).astype(NP[dt])
+    ref = orc.csr_spmv(rp, ci, v, x)
+    ref2 = orc.csr_spmv(rp, ci, v, x, y0, 0.5, -2.0)
+    A = Csr.read(exe, rp, ci, v, dtype=dt)
+    ops = [A.convert_to_ell(stride=n), A.convert_to_ell(stride=n + 1)]
+    ops += [A.convert_to_sellp(ss, 1) for ss in (2, 7, 32)]
+    xd = torch.from_numpy(x).cuda()
+    for op in ops:
+        y = torch.full((n, k), float("nan"), dtype=dt, device="cuda")
+        op.apply(xd, y)
+        assert_spmv_close(rp, ci, v, x, y.cpu().numpy(), ref, TOL[dt])
+        y2 = torch.from_numpy(y0).cuda()
+        op.apply(0.5, xd, -2.0, y2)
+        assert_spmv_close(rp, ci, v, x, y2.cpu().numpy(), ref2, TOL[dt] * 4,
+                          alpha=0.5, beta_y=2.0 * y0.astype(np.float64))
+
+
 @pytest.mark.parametrize("fmt", FORMATS)
 def test_empty_matrix(exe, fmt):
     A = Csr(exe, (0, 0), torch.zeros(1, dtype=torch.int32), torch.zeros(0, dtype=torch.int32),
