@@ -7,6 +7,10 @@
 // Jacobi kernels and the solvers that apply the blocks inside their passes.
 #pragma once
 
+#include <cuda_fp16.h>
+
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace b2s {
@@ -54,5 +58,135 @@ struct BlockPrec {
     int max_bs = 0;
     const T* blocks = nullptr;
 };
+
+// Adaptive precision.  A block's storage precision is precision_reduction's
+// byte (preserving << 4) | non-preserving (include/ginkgo/core/base/types.hpp,
+// precision_reduction), 0xff asking for autodetection.  The blocks of one
+// group share a precision; a reduced group holds its values as an array of
+// the storage type with the same interleaved indexing, from the start of the
+// group's slot (the reference's reinterpret_cast<resolved_precision*>(blocks
+// + group_offset) + block_offset, reference/preconditioner/
+// jacobi_kernels.cpp:380-395).
+constexpr uint8_t kP00 = 0x00, kP01 = 0x01, kP02 = 0x02, kP10 = 0x10, kP11 = 0x11,
+                  kP20 = 0x20, kAutodetect = 0xff;
+// precision_reduction_descriptor bits (core/preconditioner/jacobi_utils.hpp)
+constexpr uint32_t kD02 = 0x01, kD11 = 0x02, kD20 = 0x04, kD01 = 0x08, kD10 = 0x10;
+
+// Storage types: the value type, FP32, FP16 (gko::half), and the top 32 or
+// 16 bits of an FP64 value or the top 16 bits of an FP32 value
+// (truncated<T, N>).
+enum StorageKind { kFull, kF32, kF16, kHi32, kHi16F32, kHi16F64 };
+
+// GKO_PRECONDITIONER_JACOBI_RESOLVE_PRECISION (core/preconditioner/
+// jacobi_utils.hpp): reduce_precision<double> = float, of float = half, of
+// half = half; truncate_type<double> = truncated<double, 2>, of float =
+// truncated<float, 2>.  Encodings outside the six store at full precision.
+template <typename T>
+__host__ __device__ inline int storage_kind(uint8_t p)
+{
+    if (sizeof(T) == 8) {
+        switch (p) {
+        case kP01: return kF32;
+        case kP02: return kF16;
+        case kP10: return kHi32;
+        case kP11: return kHi16F32;
+        case kP20: return kHi16F64;
+        default: return kFull;
+        }
+    }
+    switch (p) {
+    case kP01:
+    case kP02:
+    case kP11: return kF16;
+    case kP10:
+    case kP20: return kHi16F32;
+    default: return kFull;
+    }
+}
+
+// FP32 to gko::half: round to nearest even, magnitudes below the smallest
+// normal half (2^-14) flushed to a zero of the same sign.
+__device__ __forceinline__ uint16_t half_bits(float f)
+{
+    if (fabsf(f) < 6.103515625e-05f) return (__float_as_uint(f) >> 16) & 0x8000u;
+    return __half_as_ushort(__float2half_rn(f));
+}
+
+// Element idx of a storage array of kind K starting at base.
+template <int K, typename T>
+__device__ __forceinline__ void store_reduced(void* base, int64_t idx, T v)
+{
+    if constexpr (K == kFull) {
+        static_cast<T*>(base)[idx] = v;
+    } else if constexpr (K == kF32) {
+        static_cast<float*>(base)[idx] = float(v);
+    } else if constexpr (K == kF16) {
+        static_cast<uint16_t*>(base)[idx] = half_bits(float(v));
+    } else if constexpr (K == kHi32) {
+        static_cast<uint32_t*>(base)[idx] =
+            uint32_t(uint64_t(__double_as_longlong(double(v))) >> 32);
+    } else if constexpr (K == kHi16F32) {
+        static_cast<uint16_t*>(base)[idx] = uint16_t(__float_as_uint(float(v)) >> 16);
+    } else {
+        static_cast<uint16_t*>(base)[idx] =
+            uint16_t(uint64_t(__double_as_longlong(double(v))) >> 48);
+    }
+}
+
+template <int K, typename T>
+__device__ __forceinline__ T load_reduced(const void* base, int64_t idx)
+{
+    if constexpr (K == kFull) {
+        return __ldg(static_cast<const T*>(base) + idx);
+    } else if constexpr (K == kF32) {
+        return T(__ldg(static_cast<const float*>(base) + idx));
+    } else if constexpr (K == kF16) {
+        return T(__half2float(__ushort_as_half(__ldg(static_cast<const uint16_t*>(base) + idx))));
+    } else if constexpr (K == kHi32) {
+        const uint64_t hi = __ldg(static_cast<const uint32_t*>(base) + idx);
+        return T(__longlong_as_double((long long)(hi << 32)));
+    } else if constexpr (K == kHi16F32) {
+        const uint32_t hi = __ldg(static_cast<const uint16_t*>(base) + idx);
+        return T(__uint_as_float(hi << 16));
+    } else {
+        const uint64_t hi = __ldg(static_cast<const uint16_t*>(base) + idx);
+        return T(__longlong_as_double((long long)(hi << 48)));
+    }
+}
+
+// A value rounded to storage kind K and read back.
+template <int K, typename T>
+__device__ __forceinline__ T roundtrip(T v)
+{
+    if constexpr (K == kFull) {
+        return v;
+    } else if constexpr (K == kF32) {
+        return T(float(v));
+    } else if constexpr (K == kF16) {
+        return T(__half2float(__ushort_as_half(half_bits(float(v)))));
+    } else if constexpr (K == kHi32) {
+        return T(__longlong_as_double(__double_as_longlong(double(v)) &
+                                      (long long)0xffffffff00000000ull));
+    } else if constexpr (K == kHi16F32) {
+        return T(__uint_as_float(__float_as_uint(float(v)) & 0xffff0000u));
+    } else {
+        return T(__longlong_as_double(__double_as_longlong(double(v)) &
+                                      (long long)0xffff000000000000ull));
+    }
+}
+
+// Runs f(std::integral_constant<int, K>{}) for the storage kind k.
+template <typename F>
+__device__ __forceinline__ void with_storage_kind(int k, F&& f)
+{
+    switch (k) {
+    case kF32: f(std::integral_constant<int, kF32>{}); break;
+    case kF16: f(std::integral_constant<int, kF16>{}); break;
+    case kHi32: f(std::integral_constant<int, kHi32>{}); break;
+    case kHi16F32: f(std::integral_constant<int, kHi16F32>{}); break;
+    case kHi16F64: f(std::integral_constant<int, kHi16F64>{}); break;
+    default: f(std::integral_constant<int, kFull>{}); break;
+    }
+}
 
 }  // namespace b2s

@@ -184,17 +184,39 @@ def find_blocks(row_ptrs, col_idxs, max_block_size):
     return out[:nb + 1].copy()
 
 
+# precision_reduction bytes, (preserving << 4) | non-preserving
+# (include/ginkgo/core/base/types.hpp)
+AUTODETECT = 0xFF
+
+
+def precision_reduction(preserving: int, nonpreserving: int) -> int:
+    """precision_reduction(preserving, nonpreserving) as its byte."""
+    return (int(preserving) << 4) | int(nonpreserving)
+
+
 class BlockJacobi:
-    """preconditioner::Jacobi with max_block_size 2..32 and full-precision
-    blocks (core/preconditioner/jacobi.cpp:370-420): the diagonal blocks
-    inverted on the device (b2s_jacobi_block_generate_*), applied as
-    x = D^-1 b or alpha D^-1 b + beta x.  The solvers apply the blocks
-    inside their passes: CG in its update pass (b2s_cg_block_solve_*),
-    BiCGStab to p' and s (b2s_bicgstab_block_solve_*), GMRES and IR over
-    GMRES to each Krylov vector (b2s_gmres_block_solve)."""
+    """preconditioner::Jacobi with max_block_size 2..32 (core/preconditioner/
+    jacobi.cpp:370-420): the diagonal blocks inverted on the device
+    (b2s_jacobi_block_generate_*), applied as x = D^-1 b or
+    alpha D^-1 b + beta x.  The solvers apply the blocks inside their
+    passes: CG in its update pass (b2s_cg_block_solve_*), BiCGStab to p' and
+    s (b2s_bicgstab_block_solve_*), GMRES and IR over GMRES to each Krylov
+    vector (b2s_gmres_block_solve).
+
+    storage_optimization (Jacobi's parameter of that name): None or
+    precision_reduction(0, 0) keeps full precision; one precision_reduction
+    byte applies to every block, AUTODETECT choosing per block from its
+    conditioning and `accuracy`; a sequence gives the blocks' requests in
+    turn, repeated as needed (jacobi::initialize_precisions).  The blocks of
+    a storage group share the most reduced precision all of them support
+    (b2s_jacobi_block_generate_adaptive_*); `block_precisions` and
+    `conditioning` hold the outcome.  The fused solvers read a
+    full-precision copy of the rounded blocks, so they compute exactly what
+    applying the reduced storage computes."""
 
     def __init__(self, A: Csr, max_block_size: int, block_pointers=None,
-                 aggregate_l1: bool = False):
+                 aggregate_l1: bool = False, storage_optimization=None,
+                 accuracy: float = 1e-1):
         self.A = A
         self.aggregate_l1 = bool(aggregate_l1)
         self.max_block_size = int(max_block_size)
@@ -220,9 +242,65 @@ class BlockJacobi:
         # block_interleaved_storage_scheme: (block_offset, group_offset, group_power)
         self.storage_scheme = (int(bo.value), int(go.value), int(gp.value))
         self.blocks = torch.zeros(max(int(space.value), 1), dtype=A.dtype, device=dev)
-        call(f"b2s_jacobi_block_generate_{_SFX[A.dtype]}", A.shape[0], _p(A.row_ptrs),
-             _p(A.col_idxs), _p(A.values), self.num_blocks, _p(self._ptrs), m,
-             _p(self.blocks), int(self.aggregate_l1), _stream(self.blocks))
+        self.accuracy = float(accuracy)
+        req = self._requests(storage_optimization)
+        self._full = None
+        if req is None:
+            self._prec = None
+            self.conditioning = None
+            call(f"b2s_jacobi_block_generate_{_SFX[A.dtype]}", A.shape[0], _p(A.row_ptrs),
+                 _p(A.col_idxs), _p(A.values), self.num_blocks, _p(self._ptrs), m,
+                 _p(self.blocks), int(self.aggregate_l1), _stream(self.blocks))
+            return
+        self._prec = torch.from_numpy(req).to(dev)
+        self.conditioning = torch.zeros(max(self.num_blocks, 1), dtype=A.dtype, device=dev)
+        wb = C.c_int64(0)
+        call("b2s_jacobi_adaptive_workspace_bytes", self.num_blocks, C.byref(wb))
+        ws = torch.empty(max(int(wb.value), 4), dtype=torch.uint8, device=dev)
+        acc = C.c_double(self.accuracy) if A.dtype == torch.float64 else C.c_float(self.accuracy)
+        call(f"b2s_jacobi_block_generate_adaptive_{_SFX[A.dtype]}", A.shape[0],
+             _p(A.row_ptrs), _p(A.col_idxs), _p(A.values), self.num_blocks, _p(self._ptrs), m,
+             acc, _p(self.conditioning), _p(self._prec), _p(self.blocks),
+             int(self.aggregate_l1), _p(ws), _stream(self.blocks))
+        self.conditioning = self.conditioning[:self.num_blocks]
+
+    def _requests(self, opt):
+        """The per-block precision requests, or None for full precision."""
+        if opt is None:
+            return None
+        if np.isscalar(opt):
+            if int(opt) == 0:
+                return None
+            req = np.full(self.num_blocks, int(opt), dtype=np.uint8)
+        else:
+            src = np.asarray(opt, dtype=np.uint8).reshape(-1)
+            if src.size == 0:
+                raise ValueError("storage_optimization is an empty sequence")
+            req = src[np.arange(self.num_blocks) % src.size]
+        return np.ascontiguousarray(req) if req.size else np.zeros(1, np.uint8)
+
+    @property
+    def adaptive(self) -> bool:
+        return self._prec is not None
+
+    @property
+    def block_precisions(self):
+        """The storage precision of each block (precision_reduction bytes),
+        or None for full precision."""
+        return None if self._prec is None else self._prec[:self.num_blocks].cpu().numpy()
+
+    @property
+    def full_blocks(self):
+        """The blocks at full precision in the interleaved layout (the
+        storage itself, or its widened copy when adaptive)."""
+        if self._prec is None:
+            return self.blocks
+        if self._full is None:
+            self._full = torch.empty_like(self.blocks)
+            call(f"b2s_jacobi_block_expand_{_SFX[self.A.dtype]}", self.num_blocks,
+                 self.max_block_size, _p(self._prec), _p(self.blocks), _p(self._full),
+                 _stream(self.blocks))
+        return self._full
 
     @property
     def inv_diag(self):
@@ -241,9 +319,15 @@ class BlockJacobi:
             beta = torch.as_tensor(be, dtype=self.A.dtype, device=dev).reshape(1)
         b2 = _check_dense(b, n, self.A.dtype, "b")
         x2 = _check_dense(x, n, self.A.dtype, "x")
-        call(f"b2s_jacobi_block_apply_{_SFX[self.A.dtype]}", n, self.num_blocks,
-             _p(self._ptrs), self.max_block_size, _p(self.blocks), _p(b2), b2.stride(0),
-             _p(x2), x2.stride(0), b2.shape[1], _p(alpha), _p(beta), _stream(x2))
+        if self._prec is None:
+            call(f"b2s_jacobi_block_apply_{_SFX[self.A.dtype]}", n, self.num_blocks,
+                 _p(self._ptrs), self.max_block_size, _p(self.blocks), _p(b2), b2.stride(0),
+                 _p(x2), x2.stride(0), b2.shape[1], _p(alpha), _p(beta), _stream(x2))
+        else:
+            call(f"b2s_jacobi_block_apply_adaptive_{_SFX[self.A.dtype]}", n, self.num_blocks,
+                 _p(self._ptrs), self.max_block_size, _p(self._prec), _p(self.blocks),
+                 _p(b2), b2.stride(0), _p(x2), x2.stride(0), b2.shape[1], _p(alpha),
+                 _p(beta), _stream(x2))
         return x
 
     def _positions(self):
@@ -260,13 +344,14 @@ class BlockJacobi:
         return (b >> gp) * go + (b & (gs - 1)) * bo + i + j * stride
 
     def block(self, b):
-        """The max_block_size x max_block_size slot of block b (host)."""
-        return self.blocks.cpu().numpy()[self._positions()[b]]
+        """The max_block_size x max_block_size slot of block b (host, full
+        precision)."""
+        return self.full_blocks.cpu().numpy()[self._positions()[b]]
 
     def to_dense(self):
         """The block-diagonal inverse as a dense host array."""
         n = self.A.shape[0]
-        blk = self.blocks.cpu().numpy()
+        blk = self.full_blocks.cpu().numpy()
         pos = self._positions()
         out = np.zeros((n, n), dtype=blk.dtype)
         for i, (s, e) in enumerate(zip(self.block_pointers[:-1], self.block_pointers[1:])):
@@ -282,26 +367,40 @@ class BlockJacobi:
         pos = self._positions()
         src = torch.from_numpy(pos.transpose(0, 2, 1).reshape(-1)).to(self.blocks.device)
         dst = torch.from_numpy(pos.reshape(-1)).to(self.blocks.device)
-        t.blocks = self.blocks.clone()
+        full = self.full_blocks
+        t.blocks = full.clone()
         if len(dst):
-            t.blocks[dst] = self.blocks[src]
+            t.blocks[dst] = full[src]
+        t._full = None
+        if self._prec is not None:
+            # the transposed values are the stored ones: rounding them to the
+            # same precisions is exact
+            t._full = t.blocks.clone()
+            call(f"b2s_jacobi_block_reduce_{_SFX[self.A.dtype]}", self.num_blocks,
+                 self.max_block_size, _p(self._prec), _p(t._full), _p(t.blocks),
+                 _stream(t.blocks))
         return t
 
 
 class JacobiFactory:
     """Jacobi::build() parameters: max_block_size (1 scalar, 2..32 blocks),
-    block_pointers, aggregate_l1 (include/ginkgo/core/preconditioner/
-    jacobi.hpp, parameters)."""
+    block_pointers, aggregate_l1, storage_optimization and accuracy
+    (include/ginkgo/core/preconditioner/jacobi.hpp, parameters; accuracy
+    defaults to 1e-1 as there)."""
 
-    def __init__(self, exec_, max_block_size=32, block_pointers=None, aggregate_l1=False):
+    def __init__(self, exec_, max_block_size=32, block_pointers=None, aggregate_l1=False,
+                 storage_optimization=None, accuracy=1e-1):
         self.max_block_size = int(max_block_size)
         self.block_pointers = block_pointers
         self.aggregate_l1 = bool(aggregate_l1)
+        self.storage_optimization = storage_optimization
+        self.accuracy = float(accuracy)
 
     def generate(self, A):
         if self.max_block_size == 1:
             return Jacobi(A, self.aggregate_l1)
-        return BlockJacobi(A, self.max_block_size, self.block_pointers, self.aggregate_l1)
+        return BlockJacobi(A, self.max_block_size, self.block_pointers, self.aggregate_l1,
+                           self.storage_optimization, self.accuracy)
 
 
 # ---------------------------------------------------------------- logging --
@@ -391,7 +490,7 @@ class _Solver:
             ws = self._workspace(nbytes)
             call(f"b2s_{name}_block_solve_{_SFX[A.dtype]}", n, _p(A.row_ptrs),
                  _p(A.col_idxs), _p(A.values), A.max_row_nnz, M.num_blocks, _p(M._ptrs),
-                 M.max_block_size, _p(M.blocks), *tail, _p(ws), ws.numel(), *outs)
+                 M.max_block_size, _p(M.full_blocks), *tail, _p(ws), ws.numel(), *outs)
         else:
             nbytes = getattr(lib(), f"b2s_{name}_workspace_bytes")(
                 n, k, A.values.element_size())
@@ -442,7 +541,7 @@ class _Solver:
         if isinstance(M, BlockJacobi):
             call("b2s_gmres_block_solve", variant, _ORTHO[self.f.ortho_method], n,
                  _p(A.row_ptrs), _p(A.col_idxs), _p(A.values), A.max_row_nnz, M.num_blocks,
-                 _p(M._ptrs), M.max_block_size, _p(M.blocks), *tail)
+                 _p(M._ptrs), M.max_block_size, _p(M.full_blocks), *tail)
         else:
             call("b2s_gmres_solve", variant, _ORTHO[self.f.ortho_method], n,
                  _p(A.row_ptrs), _p(A.col_idxs), _p(A.values), A.max_row_nnz,

@@ -327,6 +327,67 @@ int b2s_jacobi_block_apply_f32(int64_t num_rows, int64_t num_blocks,
                                float* x, int64_t ldx, int64_t num_rhs,
                                const float* alpha, const float* beta, void* stream);
 
+/* Adaptive-precision block Jacobi (Jacobi's storage_optimization; replaces
+ * jacobi::generate / apply / simple_apply with block_precisions,
+ * reference/preconditioner/jacobi_kernels.cpp:309-450, and the CUDA
+ * executor's adaptive instantiations of the same kernels).  Precisions are
+ * precision_reduction bytes, (preserving << 4) | non-preserving: 0x00 full,
+ * 0x01 reduce, 0x02 reduce twice, 0x10 truncate, 0x11 truncate the reduced
+ * type, 0x20 truncate twice, 0xff autodetect.  The blocks of one group
+ * (32 / pow2ceil(max_block_size) blocks) share the most reduced precision all
+ * of them support; a reduced group stores its values as an array of the
+ * storage type (FP32, FP16, or the top 32 / 16 bits of the value) with the
+ * interleaved indexing, from the start of the group's slot.
+ *
+ * generate_adaptive: block_precisions (num_blocks bytes, device) holds the
+ * requested precision of each block on entry and the chosen one on return;
+ * conditioning (num_blocks values) receives ||B||_inf ||B^-1||_inf per
+ * block; accuracy bounds cond * eps of an accepted storage; workspace holds
+ * b2s_jacobi_adaptive_workspace_bytes bytes.  apply_adaptive is
+ * b2s_jacobi_block_apply_* reading each group at its precision.
+ * expand widens the reduced storage to full precision (same layout, values
+ * exact) into full_blocks, reduce rounds full-precision storage to the
+ * given precisions; both work in place as well. */
+int b2s_jacobi_adaptive_workspace_bytes(int64_t num_blocks, int64_t* bytes);
+int b2s_jacobi_block_generate_adaptive_f64(int64_t num_rows, const int32_t* row_ptrs,
+                                           const int32_t* col_idxs, const double* values,
+                                           int64_t num_blocks, const int32_t* block_ptrs,
+                                           int max_block_size, double accuracy,
+                                           double* conditioning, uint8_t* block_precisions,
+                                           double* blocks, int aggregate_l1, void* workspace,
+                                           void* stream);
+int b2s_jacobi_block_generate_adaptive_f32(int64_t num_rows, const int32_t* row_ptrs,
+                                           const int32_t* col_idxs, const float* values,
+                                           int64_t num_blocks, const int32_t* block_ptrs,
+                                           int max_block_size, float accuracy,
+                                           float* conditioning, uint8_t* block_precisions,
+                                           float* blocks, int aggregate_l1, void* workspace,
+                                           void* stream);
+int b2s_jacobi_block_apply_adaptive_f64(int64_t num_rows, int64_t num_blocks,
+                                        const int32_t* block_ptrs, int max_block_size,
+                                        const uint8_t* block_precisions, const double* blocks,
+                                        const double* b, int64_t ldb, double* x, int64_t ldx,
+                                        int64_t num_rhs, const double* alpha,
+                                        const double* beta, void* stream);
+int b2s_jacobi_block_apply_adaptive_f32(int64_t num_rows, int64_t num_blocks,
+                                        const int32_t* block_ptrs, int max_block_size,
+                                        const uint8_t* block_precisions, const float* blocks,
+                                        const float* b, int64_t ldb, float* x, int64_t ldx,
+                                        int64_t num_rhs, const float* alpha,
+                                        const float* beta, void* stream);
+int b2s_jacobi_block_expand_f64(int64_t num_blocks, int max_block_size,
+                                const uint8_t* block_precisions, const double* blocks,
+                                double* full_blocks, void* stream);
+int b2s_jacobi_block_expand_f32(int64_t num_blocks, int max_block_size,
+                                const uint8_t* block_precisions, const float* blocks,
+                                float* full_blocks, void* stream);
+int b2s_jacobi_block_reduce_f64(int64_t num_blocks, int max_block_size,
+                                const uint8_t* block_precisions, const double* full_blocks,
+                                double* blocks, void* stream);
+int b2s_jacobi_block_reduce_f32(int64_t num_blocks, int max_block_size,
+                                const uint8_t* block_precisions, const float* full_blocks,
+                                float* blocks, void* stream);
+
 /* ------------------------------------------------ Krylov step kernels -- */
 
 /* Kernel-level stand-ins for a caller that keeps the reference's solver

@@ -21,6 +21,9 @@ B1 = [[4.0], [-1.0], [-2.0], [4.0], [-1.0]]
 X2 = [[1.0, 0.5], [-1.0, -0.5], [2.0, 1.0], [-2.0, -1.0], [3.0, 1.5]]
 B2 = [[4.0, -2.0], [-1.0, 4.0], [-2.0, 0.0], [4.0, -2.0], [-1.0, 4.0]]
 SRC = "reference/test/preconditioner/jacobi_kernels.cpp"
+# r<double> (core/test/utils.hpp:388-400): 10 epsilon of double, and its root
+R = 10 * 2.0 ** -52
+HALF_TOL = R ** 0.5
 
 cases = {
     "_about": __doc__.strip().splitlines()[0],
@@ -98,6 +101,29 @@ cases = {
          "block_ptrs": [0, 1, 2, 4],
          "expected": [[2.0, 1.0, 0.0, 0.0], [2.0, 4.0, 0.0, 0.0], [-5.0, 0.0, 6.0, 0.0],
                       [1.0, 0.0, -1.0, 2.0]]},
+    ],
+    # adaptive precision (storage_optimization): the precisions each block
+    # ends with (precision_reduction's byte, (preserving << 4) | nonpreserving,
+    # 255 = autodetect) for value type double, the conditioning, and the
+    # stored inverses as the tests read them back.  R = r<double> = 10 eps
+    "adaptive": [
+        {"name": "Jacobi.CanBeGeneratedWithAdaptivePrecision",
+         "source": SRC + ":35-62,110-127", "matrix": MTX, "max_block_size": 17,
+         "block_ptrs": [0, 2, 5], "precisions": [0x01, 0x00], "expected": [0x01, 0x00]},
+        {"name": "Jacobi.ComputesConditioning", "source": SRC + ":535-548",
+         "matrix": MTX, "max_block_size": 17, "block_ptrs": [0, 2, 5],
+         "precisions": [0x01, 0x00], "conditioning": [6.0 * 6.0 / 14.0, 7.0 * 28.0 / 48.0]},
+        {"name": "Jacobi.InvertsDiagonalBlocksWithAdaptivePrecisionAndSmallBlocks",
+         "source": SRC + ":419-448", "matrix": MTX, "max_block_size": 3,
+         "block_ptrs": [0, 2, 5], "precisions": [0x01, 0x00], "expected": [0x00, 0x00]},
+        {"name": "Jacobi.SelectsCorrectBlockPrecisions", "source": SRC + ":551-578",
+         "matrix": MTX, "max_block_size": 17, "block_ptrs": [0, 2, 5], "precisions": None,
+         "accuracy": 1.5e-3, "expected": [0x02, 0x01]},
+        {"name": "Jacobi.AvoidsPrecisionsThatOverflow", "source": SRC + ":581-623",
+         "matrix": {"row_ptrs": [0, 2, 4, 6, 8], "col_idxs": [0, 1, 0, 1, 2, 3, 2, 3],
+                    "values": [2.0, 1.0, 1.0, 2.0, HALF_TOL, -R, R, HALF_TOL]},
+         "max_block_size": 13, "block_ptrs": [0, 2, 4], "precisions": None,
+         "accuracy": 1e-1, "expected": [0x11, 0x11]},
     ],
 }
 with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "jacobi_cases.json"), "w") as f:

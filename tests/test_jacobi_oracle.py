@@ -83,3 +83,39 @@ def test_empty_matrix_has_no_blocks():
     # Jacobi.ConvertsEmptyToDense (reference/test/preconditioner/jacobi_kernels.cpp:1112-1121)
     p = J.generate(np.array([0]), np.array([], int), np.array([]), 32)
     assert J.to_dense(p, 0).shape == (0, 0)
+
+
+@pytest.mark.parametrize("case", G["adaptive"], ids=lambda c: c["name"])
+def test_adaptive_precision_known_answers(case):
+    # the precisions each block ends with (value type double) and the
+    # conditioning, as the reference's adaptive-precision tests state them
+    m = case["matrix"]
+    prec, chosen, conds = J.generate_adaptive(
+        m["row_ptrs"], m["col_idxs"], m["values"], case["max_block_size"], case["block_ptrs"],
+        accuracy=case.get("accuracy", 1e-1), precisions=case["precisions"])
+    if "expected" in case:
+        assert chosen == case["expected"]
+    if "conditioning" in case:
+        np.testing.assert_allclose(conds, case["conditioning"], rtol=1e-14)
+    # every stored inverse is the full-precision inverse rounded to its
+    # storage type and read back
+    full = J.generate(m["row_ptrs"], m["col_idxs"], m["values"], case["max_block_size"],
+                      block_ptrs=case["block_ptrs"])
+    for blk, ref, p in zip(prec[2], full[2], chosen):
+        np.testing.assert_array_equal(blk, J.storage_roundtrip(ref, p, np.float64))
+
+
+def test_storage_types_round_values_as_the_reference():
+    # truncated<double, 2> / <double, 4> keep the top 32 / 16 bits, truncated
+    # <float, 2> the top 16 bits of the FP32 value, half goes through FP32
+    # with values below its smallest normal flushed to zero
+    x = np.array([1.0 / 3.0, -2.5e-5, 65519.0, 70000.0, -0.0])
+    assert J.storage_roundtrip(x, J.P10, np.float64)[0] == np.float64(
+        np.array([0x3FD5555500000000], np.uint64).view(np.float64)[0])
+    assert J.storage_roundtrip(x, J.P20, np.float64)[0] == 0.328125
+    assert J.storage_roundtrip(x, J.P11, np.float64)[0] == 0.33203125
+    with np.errstate(over="ignore"):
+        h = J.storage_roundtrip(x, J.P02, np.float64)
+    assert h[0] == np.float64(np.float16(1.0 / 3.0))
+    assert h[1] == 0.0 and np.signbit(h[1])
+    assert h[2] == 65504.0 and np.isinf(h[3])
