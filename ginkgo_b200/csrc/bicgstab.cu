@@ -768,8 +768,8 @@ __global__ void __launch_bounds__(kSolverBlock)
 // core/solver/bicgstab.cpp:190-250 with the preconditioner applies at
 // :194 and :229.
 // ---------------------------------------------------------------------------
-template <typename T, int MB2, int K, int STEP>
-__global__ void __launch_bounds__(kSolverBlock)
+template <typename T, int MB2, int K, int STEP, int SK>
+__global__ void __launch_bounds__(kSolverBlock, (SK >= 0 && MB2 <= 8 ? 5 : 0))
     bicg_block_vec_kernel(int64_t n, BlockPrec<T> bp, const T* __restrict__ r,
                           const T* __restrict__ a_old, const T* __restrict__ v_old,
                           T* __restrict__ out, T* __restrict__ prec, SolveCtl* ctl,
@@ -808,11 +808,7 @@ __global__ void __launch_bounds__(kSolverBlock)
         const bool act = in_block && i < bs;
         const int64_t row = s0 + i;
         T inv[MB2];
-        const T* g = bp.blocks + grp * bsc.group + lane;
-#pragma unroll
-        for (int c = 0; c < MB2; ++c) {
-            inv[c] = in_group && c < bp.max_bs ? __ldg(g + c * bsc.stride) : T(0);
-        }
+        load_block_columns<SK>(bp, bsc, grp, lane, in_group, inv);
 #pragma unroll
         for (int j = 0; j < K; ++j) {
             if (!active[j]) continue;  // uniform
@@ -910,8 +906,11 @@ void launch_bicg_block_vec(int64_t n, const BlockPrec<T>& bp, const T* r, const 
     const int grid = bicg_block_grid(bp);
 #define B2S_BICG_BLOCK(MB)                                                        \
     case MB:                                                                      \
-        bicg_block_vec_kernel<T, MB, K, STEP><<<grid, kSolverBlock, 0, st>>>(     \
-            n, bp, r, a_old, v_old, out, prec, ctl, sc);                          \
+        with_pass_kind<T, K == 1>(bp, [&](auto sk) {                              \
+            bicg_block_vec_kernel<T, MB, K, STEP, decltype(sk)::value>            \
+                <<<grid, kSolverBlock, 0, st>>>(n, bp, r, a_old, v_old, out, prec, \
+                                                ctl, sc);                         \
+        });                                                                       \
         break;
     switch (kMaxBs / block_scheme(bp.max_bs).gs) {
         B2S_BICG_BLOCK(2)
@@ -1194,7 +1193,8 @@ int64_t b2s_bicgstab_block_workspace_bytes(int64_t num_rows, int64_t num_rhs,
     int b2s_bicgstab_block_solve_##S(                                         \
         int64_t num_rows, const int32_t* row_ptrs, const int32_t* col_idxs,   \
         const T* values, int64_t max_row_nnz, int64_t num_blocks,             \
-        const int32_t* block_ptrs, int max_block_size, const T* blocks,       \
+        const int32_t* block_ptrs, int max_block_size,                        \
+        const uint8_t* block_precisions, const T* blocks,       \
         const T* b, int64_t ldb, T* x, int64_t ldx, int64_t num_rhs,          \
         int64_t max_iters, double reduction_factor, int residual_mode,        \
         int64_t check_every, void* workspace, int64_t workspace_bytes,        \
@@ -1206,6 +1206,12 @@ int64_t b2s_bicgstab_block_workspace_bytes(int64_t num_rows, int64_t num_rhs,
         bp.ptrs = block_ptrs;                                                 \
         bp.max_bs = max_block_size;                                           \
         bp.blocks = blocks;                                                   \
+        bp.prec = block_precisions;                                           \
+        if (bp.prec && workspace && workspace_bytes >= int64_t(sizeof(int))) { \
+            /* the workspace's first word as scratch, before the solve */       \
+            B2S_CUDA_TRY(resolve_storage_kind(bp, static_cast<int*>(workspace), \
+                                              as_stream(stream)));        \
+        }                                                                 \
         return bicgstab_solve<T>(num_rows, row_ptrs, col_idxs, values,        \
                                  max_row_nnz, nullptr, &bp, b, ldb, x, ldx,   \
                                  num_rhs, max_iters, reduction_factor,        \

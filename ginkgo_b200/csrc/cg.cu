@@ -499,8 +499,11 @@ __global__ void __launch_bounds__(kSolverBlock)
 // ||b||^2 (cg::initialize and the first z = M r, core/solver/cg.cpp:
 // 122-149).
 // ---------------------------------------------------------------------------
-template <typename T, int MB2, int K, bool INIT>
-__global__ void __launch_bounds__(kSolverBlock)
+// A fixed storage kind widens its loads in registers; holding those
+// instances to five blocks per SM keeps them at the full-precision pass's 48
+// registers (64 otherwise); a minimum of 0 leaves the others unconstrained.
+template <typename T, int MB2, int K, bool INIT, int SK>
+__global__ void __launch_bounds__(kSolverBlock, (SK >= 0 && MB2 <= 8 ? 5 : 0))
     cg_block_kernel(int64_t n, BlockPrec<T> bp, const T* __restrict__ b, int64_t ldb, int k,
                     T* __restrict__ x, int64_t ldx, T* __restrict__ r, T* __restrict__ z,
                     T* __restrict__ p, const T* __restrict__ q, SolveCtl* ctl,
@@ -538,11 +541,7 @@ __global__ void __launch_bounds__(kSolverBlock)
         const bool act = in_block && i < bs;
         const int64_t row = s + i;
         T inv[MB2];
-        const T* g = bp.blocks + grp * bsc.group + lane;
-#pragma unroll
-        for (int c = 0; c < MB2; ++c) {
-            inv[c] = in_group && c < bp.max_bs ? __ldg(g + c * bsc.stride) : T(0);
-        }
+        load_block_columns<SK>(bp, bsc, grp, lane, in_group, inv);
 #pragma unroll
         for (int j = 0; j < K; ++j) {
             T rn = T(0);
@@ -600,8 +599,11 @@ void launch_cg_block(int64_t n, const BlockPrec<T>& bp, const T* b, int64_t ldb,
     const int mb2 = kMaxBs / bsc.gs;
 #define B2S_CG_BLOCK(MB)                                                           \
     case MB:                                                                       \
-        cg_block_kernel<T, MB, K, INIT><<<grid, kSolverBlock, 0, st>>>(            \
-            n, bp, b, ldb, k, x, ldx, r, z, p, q, ctl, sc, partials);              \
+        with_pass_kind<T, K == 1>(bp, [&](auto sk) {                               \
+            cg_block_kernel<T, MB, K, INIT, decltype(sk)::value>                   \
+                <<<grid, kSolverBlock, 0, st>>>(n, bp, b, ldb, k, x, ldx, r, z, p, q, \
+                                                ctl, sc, partials);                \
+        });                                                                        \
         break;
     switch (mb2) {
         B2S_CG_BLOCK(2)
@@ -836,7 +838,8 @@ int64_t b2s_cg_block_workspace_bytes(int64_t num_rows, int64_t num_rhs,
     int b2s_cg_block_solve_##S(                                               \
         int64_t num_rows, const int32_t* row_ptrs, const int32_t* col_idxs,  \
         const T* values, int64_t max_row_nnz, int64_t num_blocks,            \
-        const int32_t* block_ptrs, int max_block_size, const T* blocks,       \
+        const int32_t* block_ptrs, int max_block_size,                        \
+        const uint8_t* block_precisions, const T* blocks,       \
         const T* b, int64_t ldb, T* x, int64_t ldx, int64_t num_rhs,          \
         int64_t max_iters, double reduction_factor, int residual_mode,        \
         int64_t check_every, void* workspace, int64_t workspace_bytes,        \
@@ -848,6 +851,12 @@ int64_t b2s_cg_block_workspace_bytes(int64_t num_rows, int64_t num_rhs,
         bp.ptrs = block_ptrs;                                                 \
         bp.max_bs = max_block_size;                                           \
         bp.blocks = blocks;                                                   \
+        bp.prec = block_precisions;                                           \
+        if (bp.prec && workspace && workspace_bytes >= int64_t(sizeof(int))) { \
+            /* the workspace's first word as scratch, before the solve */       \
+            B2S_CUDA_TRY(resolve_storage_kind(bp, static_cast<int*>(workspace), \
+                                              as_stream(stream)));        \
+        }                                                                 \
         return cg_solve<T>(num_rows, row_ptrs, col_idxs, values, max_row_nnz, \
                            nullptr, &bp, b, ldb, x, ldx, num_rhs, max_iters,  \
                            reduction_factor, residual_mode, check_every,      \

@@ -915,12 +915,44 @@ GmresLayout gmres_layout(int64_t n, int64_t nnz, int64_t max_row_nnz, int d, boo
 // shuffles.  The blocks are FP64 in every variant; an FP32 Arnoldi cycle
 // rounds M y to FP32.
 // ---------------------------------------------------------------------------
-template <typename TA, int MB2>
+// z = sum over c of M(i, c) v_c for the lane's row i of its block in group
+// grp, v distributed one value per lane (column c of the block at lane
+// base + c), the blocks read as load_block_columns reads them for SK.  Every
+// lane takes part in the shuffles.
+template <int SK, int MB2>
+__device__ double block_times(const BlockPrec<double>& bp, const BlockScheme& bsc,
+                              int64_t grp, int lane, bool in_group, int base, bool act, int bs,
+                              double v)
+{
+    double z = 0.0;
+    const double* gb = bp.blocks + grp * bsc.group;
+    auto run = [&](auto kc) {
+        constexpr int K = decltype(kc)::value;
+#pragma unroll
+        for (int c = 0; c < MB2; ++c) {
+            if (c < bp.max_bs) {
+                const double inv =
+                    in_group ? load_reduced<K, double>(gb, lane + c * bsc.stride) : 0.0;
+                const double vc = __shfl_sync(0xffffffffu, v, (base + c) % kWarp);
+                if (act && c < bs) z += inv * vc;
+            }
+        }
+    };
+    if constexpr (SK == kSkMixed) {
+        with_storage_kind(storage_kind<double>(bp.prec[grp * bsc.gs]), run);
+    } else if constexpr (SK == kSkFull) {
+        run(std::integral_constant<int, kFull>{});
+    } else {
+        run(std::integral_constant<int, SK>{});
+    }
+    return z;
+}
+
+template <typename TA, int MB2, int SK>
 __global__ void __launch_bounds__(kSolverBlock)
     gmres_block_apply_kernel(int64_t n, BlockPrec<double> bp, TA* __restrict__ y,
                              const int* __restrict__ skip)
 {
-    constexpr unsigned kFull = 0xffffffffu;
     if (*skip) return;
     const BlockScheme bsc = block_scheme(bp.max_bs);
     const int lane = threadIdx.x % kWarp;
@@ -937,28 +969,18 @@ __global__ void __launch_bounds__(kSolverBlock)
                               block_extent(bp.ptrs, blk, n, bp.max_bs, s, bs);
         const bool act = in_block && i < bs;
         const double yv = act ? double(y[s + i]) : 0.0;
-        const double* g = bp.blocks + grp * bsc.group + lane;
-        double z = 0.0;
-#pragma unroll
-        for (int c = 0; c < MB2; ++c) {
-            if (c < bp.max_bs) {
-                const double inv = in_group ? __ldg(g + c * bsc.stride) : 0.0;
-                const double yc = __shfl_sync(kFull, yv, (base + c) % kWarp);
-                if (act && c < bs) z += inv * yc;
-            }
-        }
+        const double z = block_times<SK, MB2>(bp, bsc, grp, lane, in_group, base, act, bs, yv);
         if (act) y[s + i] = TA(z);
     }
 }
 
-template <typename TA, typename TB, int MB2>
+template <typename TA, typename TB, int MB2, int SK>
 __global__ void __launch_bounds__(kSolverBlock)
     gmres_xupdate_block_kernel(int64_t n, int64_t ldv, const TB* __restrict__ V,
                                BlockPrec<double> bp, double* __restrict__ x,
                                const double* __restrict__ b, double* __restrict__ r,
                                GmresState* st)
 {
-    constexpr unsigned kFull = 0xffffffffu;
     __shared__ TA ys[kMaxKrylov];
     if (st->done) return;
     const int m = st->final_iter;
@@ -984,17 +1006,8 @@ __global__ void __launch_bounds__(kSolverBlock)
 #pragma unroll 4
             for (int q = 0; q < m; ++q) u += ys[q] * from_basis<TA>(V[int64_t(q) * ldv + row]);
         }
-        const double uv = double(u);
-        const double* g = bp.blocks + grp * bsc.group + lane;
-        double z = 0.0;
-#pragma unroll
-        for (int c = 0; c < MB2; ++c) {
-            if (c < bp.max_bs) {
-                const double inv = in_group ? __ldg(g + c * bsc.stride) : 0.0;
-                const double uc = __shfl_sync(kFull, uv, (base + c) % kWarp);
-                if (act && c < bs) z += inv * uc;
-            }
-        }
+        const double z =
+            block_times<SK, MB2>(bp, bsc, grp, lane, in_group, base, act, bs, double(u));
         if (act) {
             if (m > 0) x[row] += z;
             r[row] = b[row];
@@ -1011,18 +1024,21 @@ inline int block_grid(const BlockPrec<double>& bp)
                                  solver_grid()));
 }
 
-// Calls f(std::integral_constant<int, MB2>) for the block size class of bp.
+// Calls f(std::integral_constant<int, MB2>, std::integral_constant<int, SK>)
+// for the block size class of bp and the way its blocks are read.
 template <typename F>
 void with_block_class(const BlockPrec<double>& bp, F&& f)
 {
-    switch (kMaxBs / block_scheme(bp.max_bs).gs) {
-    case 1: f(std::integral_constant<int, 1>{}); break;
-    case 2: f(std::integral_constant<int, 2>{}); break;
-    case 4: f(std::integral_constant<int, 4>{}); break;
-    case 8: f(std::integral_constant<int, 8>{}); break;
-    case 16: f(std::integral_constant<int, 16>{}); break;
-    default: f(std::integral_constant<int, 32>{}); break;
-    }
+    with_pass_kind<double, true>(bp, [&](auto ap) {
+        switch (kMaxBs / block_scheme(bp.max_bs).gs) {
+        case 1: f(std::integral_constant<int, 1>{}, ap); break;
+        case 2: f(std::integral_constant<int, 2>{}, ap); break;
+        case 4: f(std::integral_constant<int, 4>{}, ap); break;
+        case 8: f(std::integral_constant<int, 8>{}, ap); break;
+        case 16: f(std::integral_constant<int, 16>{}, ap); break;
+        default: f(std::integral_constant<int, 32>{}, ap); break;
+        }
+    });
 }
 
 template <typename TA, typename TB>
@@ -1128,15 +1144,15 @@ int gmres_engine(const GmresLayout& lay, int64_t n, int64_t nnz, const int32_t* 
     // cycle is over)
     auto block_apply = [&](cudaStream_t cs) {
         if (!bp) return;
-        with_block_class(*bp, [&](auto mb) {
-            gmres_block_apply_kernel<TA, decltype(mb)::value>
+        with_block_class(*bp, [&](auto mb, auto ap) {
+            gmres_block_apply_kernel<TA, decltype(mb)::value, decltype(ap)::value>
                 <<<block_grid(*bp), kSolverBlock, 0, cs>>>(n, *bp, y, &gs->idle);
         });
     };
     auto restart = [&](cudaStream_t cs) {
         if (bp) {
-            with_block_class(*bp, [&](auto mb) {
-                gmres_xupdate_block_kernel<TA, TB, decltype(mb)::value>
+            with_block_class(*bp, [&](auto mb, auto ap) {
+                gmres_xupdate_block_kernel<TA, TB, decltype(mb)::value, decltype(ap)::value>
                     <<<block_grid(*bp), kSolverBlock, 0, cs>>>(n, ldv, V, *bp, x, b, r, gs);
             });
         } else {
@@ -1455,7 +1471,8 @@ int b2s_gmres_block_solve(int variant, int ortho_method, int64_t num_rows,
                           const int32_t* row_ptrs, const int32_t* col_idxs,
                           const double* values, int64_t max_row_nnz, int64_t num_blocks,
                           const int32_t* block_ptrs, int max_block_size,
-                          const double* blocks, const double* b, int64_t ldb, double* x,
+                          const uint8_t* block_precisions, const double* blocks,
+                          const double* b, int64_t ldb, double* x,
                           int64_t ldx, int64_t num_rhs, int64_t krylov_dim,
                           int64_t max_iters, double reduction_factor, int baseline,
                           double inner_reduction, void* workspace,
@@ -1468,6 +1485,11 @@ int b2s_gmres_block_solve(int variant, int ortho_method, int64_t num_rows,
     bp.ptrs = block_ptrs;
     bp.max_bs = max_block_size;
     bp.blocks = blocks;
+    bp.prec = block_precisions;
+    if (bp.prec && workspace && workspace_bytes >= int64_t(sizeof(int))) {
+        // the workspace's first word as scratch, before the solve
+        B2S_CUDA_TRY(resolve_storage_kind(bp, static_cast<int*>(workspace), as_stream(stream)));
+    }
     return gmres_dispatch(variant, ortho_method, num_rows, row_ptrs, col_idxs, values,
                           max_row_nnz, nullptr, &bp, b, ldb, x, ldx, num_rhs, krylov_dim,
                           max_iters, reduction_factor, baseline, inner_reduction, workspace,

@@ -57,6 +57,8 @@ struct BlockPrec {
     const int32_t* ptrs = nullptr;
     int max_bs = 0;
     const T* blocks = nullptr;
+    const uint8_t* prec = nullptr;  // per-block storage precisions, or null: full
+    int kind = -1;  // with prec: the storage kind all groups share, or -1 (mixed)
 };
 
 // Adaptive precision.  A block's storage precision is precision_reduction's
@@ -187,6 +189,97 @@ __device__ __forceinline__ void with_storage_kind(int k, F&& f)
     case kHi16F64: f(std::integral_constant<int, kHi16F64>{}); break;
     default: f(std::integral_constant<int, kFull>{}); break;
     }
+}
+
+// How a block pass reads the blocks (a template parameter of the passes, so
+// the full-precision instances keep their register counts): kSkFull without
+// precisions, kSkMixed with a switch on each group's storage, or one
+// StorageKind every group shares.
+constexpr int kSkFull = -2, kSkMixed = -1;
+
+// inv[c] = column c (< max_bs) of the row this lane holds in group grp of
+// bp's blocks, widened to T; zero for lanes outside the group and columns
+// past max_bs.
+template <int SK, int MB2, typename T>
+__device__ __forceinline__ void load_block_columns(const BlockPrec<T>& bp,
+                                                   const BlockScheme& bsc, int64_t grp,
+                                                   int lane, bool in_group, T (&inv)[MB2])
+{
+    const T* gb = bp.blocks + grp * bsc.group;
+    auto load = [&](auto kc) {
+        constexpr int K = decltype(kc)::value;
+#pragma unroll
+        for (int c = 0; c < MB2; ++c) {
+            inv[c] = in_group && c < bp.max_bs ? load_reduced<K, T>(gb, lane + c * bsc.stride)
+                                               : T(0);
+        }
+    };
+    if constexpr (SK == kSkMixed) {
+        with_storage_kind(storage_kind<T>(bp.prec[grp * bsc.gs]), load);
+    } else if constexpr (SK == kSkFull) {
+        load(std::integral_constant<int, kFull>{});
+    } else {
+        load(std::integral_constant<int, SK>{});
+    }
+}
+
+namespace {  // a copy per translation unit
+
+// *out = the storage kind every group of the precisions shares, or
+// kSkMixed.  One block.
+template <typename T>
+__global__ void storage_summary_kernel(int64_t num_groups, int gs,
+                                       const uint8_t* __restrict__ prec, int* out)
+{
+    const int first = storage_kind<T>(prec[0]);
+    int differ = 0;
+    for (int64_t g = threadIdx.x; g < num_groups; g += blockDim.x) {
+        differ |= storage_kind<T>(prec[g * gs]) != first;
+    }
+    differ = __syncthreads_or(differ);
+    if (threadIdx.x == 0) *out = differ ? kSkMixed : first;
+}
+
+}  // namespace
+
+// bp.kind from bp.prec; scratch is one int of device memory.  Waits for the
+// stream.
+template <typename T>
+inline cudaError_t resolve_storage_kind(BlockPrec<T>& bp, int* scratch, cudaStream_t st)
+{
+    bp.kind = kSkMixed;
+    if (bp.prec == nullptr || bp.num_blocks <= 0) return cudaSuccess;
+    const BlockScheme bsc = block_scheme(bp.max_bs);
+    storage_summary_kernel<T><<<1, 1024, 0, st>>>((bp.num_blocks + bsc.gs - 1) / bsc.gs, bsc.gs,
+                                                 bp.prec, scratch);
+    int kind = kSkMixed;
+    cudaError_t e = cudaMemcpyAsync(&kind, scratch, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    bp.kind = kind;
+    return e;
+}
+
+// The pass instance for bp: fixed storage kinds for the single right-hand
+// side (K1), where the pass is bandwidth-bound; the per-group switch
+// otherwise.  Calls f(std::integral_constant<int, SK>).
+template <typename T, bool K1, typename F>
+inline void with_pass_kind(const BlockPrec<T>& bp, F&& f)
+{
+    if (bp.prec == nullptr) {
+        f(std::integral_constant<int, kSkFull>{});
+        return;
+    }
+    if constexpr (K1) {
+        if (bp.kind == kF16) {
+            f(std::integral_constant<int, kF16>{});
+            return;
+        }
+        if (sizeof(T) == 8 && bp.kind == kF32) {
+            f(std::integral_constant<int, kF32>{});
+            return;
+        }
+    }
+    f(std::integral_constant<int, kSkMixed>{});
 }
 
 }  // namespace b2s

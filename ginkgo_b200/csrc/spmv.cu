@@ -166,10 +166,11 @@ __device__ __noinline__ void lb_long_row(const T* sv, const int32_t* sc, int s, 
     if (lane < K) dst[lane] = combine(a, alpha, beta, dst + lane);
 }
 
-// one right-hand side held to six blocks per SM (40 registers; at 48
-// registers the five resident blocks left half the warps idle)
+// (holding one right-hand side to six blocks per SM, 40 registers, measured
+// 4 % slower on the 7-point 128^3 matrix and 22 % slower on the power-law
+// matrix than the unconstrained 48 registers and five blocks)
 template <typename T, int K, bool VEC>
-__global__ void __launch_bounds__(kBlock, (K == 1 ? 6 : 2))
+__global__ void __launch_bounds__(kBlock)
     csr_lb_kernel(int64_t n, int64_t nc, const int32_t* __restrict__ own_first,
                   int32_t* __restrict__ tail_row, T* __restrict__ partials,
                   const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
@@ -234,6 +235,93 @@ __global__ void __launch_bounds__(kBlock, (K == 1 ? 6 : 2))
         }
         if (lane == 0) tail_row[ch] = tail ? rt : -1;
         __syncwarp();  // the stage is refilled for the next chunk
+    }
+}
+
+// load_balance with one right-hand side, products first: each lane loads
+// entries lane, lane + 32, ... of the chunk and gathers b at their columns,
+// so all of the chunk's gathers are in flight at once (a lane-per-row loop
+// over rows of ~20 entries waits for one gather round per four entries);
+// the products go to shared memory and the owned rows are summed from there
+// (a lane per row in entry order, which rounds as the reference executor's
+// row loop; the whole warp for a row of more than 32 entries in the chunk),
+// with the same ownership, tail partials and fix-up as csr_lb_kernel.
+constexpr int kLbPerLane = kLbChunk / kWarp;
+
+template <typename T>
+__global__ void __launch_bounds__(kBlock)
+    csr_lb1_kernel(int64_t n, int64_t nc, const int32_t* __restrict__ own_first,
+                   int32_t* __restrict__ tail_row, T* __restrict__ partials,
+                   const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                   const T* __restrict__ v, const T* __restrict__ b, int64_t ldb,
+                   T* __restrict__ c, int64_t ldc, const T* __restrict__ alpha,
+                   const T* __restrict__ beta)
+{
+    constexpr unsigned kFull = 0xffffffffu;
+    __shared__ T sp_all[kBlock / kWarp][kLbChunk];
+    const int lane = threadIdx.x % kWarp, wid = threadIdx.x / kWarp;
+    T* sp = sp_all[wid];
+    const int64_t nwarps = int64_t(gridDim.x) * (kBlock / kWarp);
+    const int64_t nnz = __ldg(rp + n);
+    for (int64_t ch = blockIdx.x * int64_t(kBlock / kWarp) + wid; ch < nc; ch += nwarps) {
+        const int64_t e0 = ch * kLbChunk;
+        const int len = int(min(int64_t(kLbChunk), nnz - e0));  // entries in the chunk
+        T pv[kLbPerLane];
+        int32_t pc[kLbPerLane];
+#pragma unroll
+        for (int j = 0; j < kLbPerLane; ++j) {
+            const int i = lane + j * kWarp;
+            pc[j] = i < len ? ld_stream(ci + e0 + i) : 0;
+            pv[j] = i < len ? ld_stream(v + e0 + i) : T(0);
+        }
+#pragma unroll
+        for (int j = 0; j < kLbPerLane; ++j) {
+            if (lane + j * kWarp < len) pv[j] = pv[j] * __ldg(b + int64_t(pc[j]) * ldb);
+        }
+#pragma unroll
+        for (int j = 0; j < kLbPerLane; ++j) sp[lane + j * kWarp] = pv[j];
+        __syncwarp();
+        const int r0 = own_first[ch], r1 = own_first[ch + 1];
+        for (int rb = r0; rb < r1; rb += kWarp) {
+            const int r = rb + lane;
+            const bool valid = r < r1;
+            const int s = valid ? int(max(int64_t(__ldg(rp + r)) - e0, int64_t(0))) : 0;
+            const int e = valid ? int(int64_t(__ldg(rp + r + 1)) - e0) : 0;
+            const bool longseg = e - s > kWarp;
+            if (valid && !longseg) {
+                T acc = T(0);
+                for (int i = s; i < e; ++i) acc += sp[i];
+                T* dst = c + int64_t(r) * ldc;
+                *dst = combine(acc, alpha, beta, dst);
+            }
+            unsigned mask = __ballot_sync(kFull, longseg);
+            while (mask) {
+                const int bit = __ffs(mask) - 1;
+                mask &= mask - 1;
+                const int rl = __shfl_sync(kFull, r, bit);
+                const int sl = __shfl_sync(kFull, s, bit);
+                const int el = __shfl_sync(kFull, e, bit);
+                T acc = T(0);
+                for (int i = sl + lane; i < el; i += kWarp) acc += sp[i];
+                acc = warp_sum(acc);
+                if (lane == 0) {
+                    T* dst = c + int64_t(rl) * ldc;
+                    *dst = combine(acc, alpha, beta, dst);
+                }
+            }
+        }
+        // the row that continues past the chunk: its part here, as a partial
+        const int rt = r1;
+        const int64_t st = rt < n ? int64_t(__ldg(rp + rt)) : nnz;
+        const bool tail = st < e0 + len;
+        if (tail) {
+            T acc = T(0);
+            for (int i = int(max(st - e0, int64_t(0))) + lane; i < len; i += kWarp) acc += sp[i];
+            acc = warp_sum(acc);
+            if (lane == 0) partials[ch * kLbSlot] = acc;
+        }
+        if (lane == 0) tail_row[ch] = tail ? rt : -1;
+        __syncwarp();  // the products are rewritten for the next chunk
     }
 }
 
@@ -506,12 +594,15 @@ void launch_lanes(int64_t n, const int32_t* rp, int64_t w_or_s, int64_t stride,
 {
     if constexpr (K >= 4 && K % Vec16<T>::width == 0) {
         constexpr int KL = K / Vec16<T>::width;
-        // Ell / Sellp: row pairs per lane slot when the column-major layout
-        // keeps rows r, r + 1 adjacent at 8-byte alignment
+        // Ell: row pairs per lane slot when the column-major layout keeps
+        // rows r, r + 1 adjacent at 8-byte alignment (0.84-0.90 of the
+        // single-row time at 4 and 16 columns on the 7-point 128^3 matrix).
+        // Sellp keeps one row per slot: on the power-law matrix its longest
+        // slices (1,805 entries) doubled the per-thread chain and took 1.3 to
+        // 2.4 times as long with pairs.
         const bool aligned = reinterpret_cast<uintptr_t>(ci) % 8 == 0 &&
                              reinterpret_cast<uintptr_t>(v) % (2 * sizeof(T)) == 0;
-        const bool pairs = aligned && ((FMT == 1 && stride % 2 == 0) ||
-                                       (FMT == 2 && w_or_s % 2 == 0));
+        const bool pairs = aligned && FMT == 1 && stride % 2 == 0;
         if (FMT != 0 && pairs) {
             if constexpr (FMT != 0) {
                 rhs_lanes2_kernel<T, K, FMT><<<ceildiv(ceildiv(n, 2) * KL, kBlock), kBlock, 0,
@@ -610,8 +701,14 @@ int csr_spmv(int strategy, int64_t n, int64_t num_cols, const int32_t* rp,
                         launched = true;
                     }
                 }
+                if constexpr (K == 1) {
+                    csr_lb1_kernel<T><<<grid, kBlock, 0, st>>>(
+                        n, nc, own_first, tail_row, partials, rp, ci, v, bb, ldb, cc, ldc,
+                        alpha, beta);
+                    launched = true;
+                }
                 if (launched) {
-                    // the column-slice form above
+                    // the column-slice or one-column form above
                 } else if (vec) {
                     csr_lb_kernel<T, K, true><<<grid, kBlock, 0, st>>>(
                         n, nc, own_first, tail_row, partials, rp, ci, v, bb, ldb, cc, ldc,

@@ -210,9 +210,8 @@ class BlockJacobi:
     turn, repeated as needed (jacobi::initialize_precisions).  The blocks of
     a storage group share the most reduced precision all of them support
     (b2s_jacobi_block_generate_adaptive_*); `block_precisions` and
-    `conditioning` hold the outcome.  The fused solvers read a
-    full-precision copy of the rounded blocks, so they compute exactly what
-    applying the reduced storage computes."""
+    `conditioning` hold the outcome.  The apply and the fused solvers read
+    each group at its storage precision, widened to the value type."""
 
     def __init__(self, A: Csr, max_block_size: int, block_pointers=None,
                  aggregate_l1: bool = False, storage_optimization=None,
@@ -490,7 +489,8 @@ class _Solver:
             ws = self._workspace(nbytes)
             call(f"b2s_{name}_block_solve_{_SFX[A.dtype]}", n, _p(A.row_ptrs),
                  _p(A.col_idxs), _p(A.values), A.max_row_nnz, M.num_blocks, _p(M._ptrs),
-                 M.max_block_size, _p(M.full_blocks), *tail, _p(ws), ws.numel(), *outs)
+                 M.max_block_size, _p(M._prec), _p(M.blocks), *tail, _p(ws), ws.numel(),
+                 *outs)
         else:
             nbytes = getattr(lib(), f"b2s_{name}_workspace_bytes")(
                 n, k, A.values.element_size())
@@ -541,7 +541,7 @@ class _Solver:
         if isinstance(M, BlockJacobi):
             call("b2s_gmres_block_solve", variant, _ORTHO[self.f.ortho_method], n,
                  _p(A.row_ptrs), _p(A.col_idxs), _p(A.values), A.max_row_nnz, M.num_blocks,
-                 _p(M._ptrs), M.max_block_size, _p(M.full_blocks), *tail)
+                 _p(M._ptrs), M.max_block_size, _p(M._prec), _p(M.blocks), *tail)
         else:
             call("b2s_gmres_solve", variant, _ORTHO[self.f.ortho_method], n,
                  _p(A.row_ptrs), _p(A.col_idxs), _p(A.values), A.max_row_nnz,

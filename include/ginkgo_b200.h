@@ -592,8 +592,11 @@ int b2s_cg_solve_f32(int64_t num_rows, const int32_t* row_ptrs,
 /* CG preconditioned by block Jacobi: num_blocks blocks delimited by
  * block_ptrs (num_blocks + 1 entries covering 0..num_rows, each block at
  * most max_block_size rows), inverses in the interleaved storage that
- * b2s_jacobi_block_generate_* writes.  z = M^-1 r is formed inside the
- * update pass, one warp per group of blocks, and stored; otherwise as
+ * b2s_jacobi_block_generate_* writes, or the adaptive storage of
+ * b2s_jacobi_block_generate_adaptive_* with its block_precisions (NULL for
+ * full-precision blocks; each group is read at its precision and widened).
+ * z = M^-1 r is formed inside the update pass, one warp per group of
+ * blocks, and stored; otherwise as
  * b2s_cg_solve_*.  The workspace query adds the stored z.  Replaces
  * Cg<V>::apply_dense_impl with a Jacobi<V> preconditioner of block size
  * > 1 (z = M r at core/solver/cg.cpp:146-149; Jacobi::apply_impl,
@@ -604,6 +607,7 @@ int b2s_cg_block_solve_f64(int64_t num_rows, const int32_t* row_ptrs,
                            const int32_t* col_idxs, const double* values,
                            int64_t max_row_nnz, int64_t num_blocks,
                            const int32_t* block_ptrs, int max_block_size,
+                           const uint8_t* block_precisions,
                            const double* blocks, const double* b, int64_t ldb,
                            double* x, int64_t ldx, int64_t num_rhs,
                            int64_t max_iters, double reduction_factor,
@@ -615,6 +619,7 @@ int b2s_cg_block_solve_f32(int64_t num_rows, const int32_t* row_ptrs,
                            const int32_t* col_idxs, const float* values,
                            int64_t max_row_nnz, int64_t num_blocks,
                            const int32_t* block_ptrs, int max_block_size,
+                           const uint8_t* block_precisions,
                            const float* blocks, const float* b, int64_t ldb,
                            float* x, int64_t ldx, int64_t num_rhs,
                            int64_t max_iters, double reduction_factor,
@@ -662,6 +667,7 @@ int b2s_bicgstab_block_solve_f64(int64_t num_rows, const int32_t* row_ptrs,
                                  const int32_t* col_idxs, const double* values,
                                  int64_t max_row_nnz, int64_t num_blocks,
                                  const int32_t* block_ptrs, int max_block_size,
+                                 const uint8_t* block_precisions,
                                  const double* blocks, const double* b, int64_t ldb,
                                  double* x, int64_t ldx, int64_t num_rhs,
                                  int64_t max_iters, double reduction_factor,
@@ -673,6 +679,7 @@ int b2s_bicgstab_block_solve_f32(int64_t num_rows, const int32_t* row_ptrs,
                                  const int32_t* col_idxs, const float* values,
                                  int64_t max_row_nnz, int64_t num_blocks,
                                  const int32_t* block_ptrs, int max_block_size,
+                                 const uint8_t* block_precisions,
                                  const float* blocks, const float* b, int64_t ldb,
                                  float* x, int64_t ldx, int64_t num_rhs,
                                  int64_t max_iters, double reduction_factor,
@@ -764,8 +771,9 @@ int b2s_gmres_block_solve(int variant, int ortho_method, int64_t num_rows,
                           const int32_t* row_ptrs, const int32_t* col_idxs,
                           const double* values, int64_t max_row_nnz,
                           int64_t num_blocks, const int32_t* block_ptrs,
-                          int max_block_size, const double* blocks,
-                          const double* b, int64_t ldb, double* x, int64_t ldx,
+                          int max_block_size, const uint8_t* block_precisions,
+                          const double* blocks, const double* b, int64_t ldb,
+                          double* x, int64_t ldx,
                           int64_t num_rhs, int64_t krylov_dim, int64_t max_iters,
                           double reduction_factor, int baseline,
                           double inner_reduction, void* workspace,

@@ -404,7 +404,8 @@ inline bool try_cg(const solver::Cg<double>* solver, const matrix::Dense<double>
         array<char> ws(exec, b2s_cg_block_workspace_bytes(n, k, sizeof(double)));
         B2S_GKO_CALL(b2s_cg_block_solve_f64(
             n, csr->get_const_row_ptrs(), csr->get_const_col_idxs(), csr->get_const_values(),
-            max_row_nnz_of(exec, csr.get()), num_blocks, block_ptrs, max_block_size, blocks,
+            max_row_nnz_of(exec, csr.get()), num_blocks, block_ptrs, max_block_size,
+            /*block_precisions=*/nullptr, blocks,
             b->get_const_values(), b->get_stride(), x->get_values(), x->get_stride(), k,
             max_iters, reduction, mode, /*check_every=*/8, ws.get_data(), ws.get_size(),
             &iters, res.data(), status.data(), exec->get_stream()));
