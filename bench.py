@@ -615,6 +615,7 @@ PROFILE_OPS = {
     "lb1": "csr_lb_kernel (load_balance, one right-hand side)",
     "lb16": "csr_lb_lanes_kernel (load_balance, 16 right-hand sides)",
     "cg_block": "cg_block_kernel (CG update pass with 8-row block Jacobi)",
+    "cg_block_f16": "cg_block_kernel (CG update pass, 8-row blocks stored in FP16)",
     "bicg_block": "bicg_block_vec_kernel (BiCGStab with 8-row block Jacobi)",
     "sddmm16": "sddmm_lanes_kernel (16 columns)",
     "spgemm": "gemm_*_rows_kernel (A^2)",
@@ -646,8 +647,10 @@ def profile_op(op):
     for _ in range(3):
         if op in ("lb1", "lb16"):
             A.set_strategy("load_balance").apply(x, y)
-        elif op in ("cg_block", "bicg_block"):
-            fac = Cg if op == "cg_block" else Bicgstab
+        elif op in ("cg_block", "bicg_block", "cg_block_f16"):
+            fac = Bicgstab if op == "bicg_block" else Cg
+            if op == "cg_block_f16":
+                jb = jb.with_storage_optimization(0x02)  # precision_reduction(0, 2)
             s = fac.build().with_criteria(*crit).with_preconditioner(jb).on(exe).generate(A)
             s.apply(x[:, 0].contiguous(), torch.zeros(n, dtype=torch.float64, device="cuda"))
         elif op == "sddmm16":

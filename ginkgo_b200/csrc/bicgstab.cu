@@ -807,8 +807,8 @@ __global__ void __launch_bounds__(kSolverBlock, (SK >= 0 && MB2 <= 8 ? 5 : 0))
                               block_extent(bp.ptrs, blk, n, bp.max_bs, s0, bs);
         const bool act = in_block && i < bs;
         const int64_t row = s0 + i;
-        T inv[MB2];
-        load_block_columns<SK>(bp, bsc, grp, lane, in_group, inv);
+        BlockRow<SK, MB2, T> inv;
+        inv.load(bp, bsc, grp, lane, in_group);
 #pragma unroll
         for (int j = 0; j < K; ++j) {
             if (!active[j]) continue;  // uniform
@@ -907,9 +907,9 @@ void launch_bicg_block_vec(int64_t n, const BlockPrec<T>& bp, const T* r, const 
 #define B2S_BICG_BLOCK(MB)                                                        \
     case MB:                                                                      \
         with_pass_kind<T, K == 1>(bp, [&](auto sk) {                              \
-            bicg_block_vec_kernel<T, MB, K, STEP, decltype(sk)::value>            \
-                <<<grid, kSolverBlock, 0, st>>>(n, bp, r, a_old, v_old, out, prec, \
-                                                ctl, sc);                         \
+            auto kernel = bicg_block_vec_kernel<T, MB, K, STEP, decltype(sk)::value>; \
+            kernel<<<pgrid(kernel, grid), kSolverBlock, 0, st>>>(                 \
+                n, bp, r, a_old, v_old, out, prec, ctl, sc);                      \
         });                                                                       \
         break;
     switch (kMaxBs / block_scheme(bp.max_bs).gs) {
@@ -1010,11 +1010,11 @@ int bicgstab_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
     const int chunk = int(std::max<int64_t>(2, (check_every + 1) / 2 * 2));
     B2S_DISPATCH_RHS(K, {
         B2S_DISPATCH_SW(sw, {
-            residual_kernel<T, SW, K><<<grid_spmv, kSolverBlock, 0, st>>>(
+            residual_kernel<T, SW, K><<<pgrid(residual_kernel<T, SW, K>, grid_spmv), kSolverBlock, 0, st>>>(
                 n, rp, ci, v, x, ldx, b, ldb, int(k), r);
         });
         B2S_LAUNCH_CHECK();
-        bicg_init_kernel<T, K><<<grid_vec, kSolverBlock, 0, st>>>(
+        bicg_init_kernel<T, K><<<pgrid(bicg_init_kernel<T, K>, grid_vec), kSolverBlock, 0, st>>>(
             n, b, ldb, int(k), r, rr, p[0], vv[0], ctl, sc, partials);
         B2S_LAUNCH_CHECK();
     });
@@ -1057,39 +1057,39 @@ int bicgstab_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
             if (bp) {
                 launch_bicg_block_vec<T, K, 1>(n, *bp, r, p[o], vv[o], p[nw], yv, ctl, sc, cs);
             } else if constexpr (kLanes) {
-                bicg_vec_lanes_kernel<T, K, 1><<<grid_lanes, kSolverBlock, 0, cs>>>(
+                bicg_vec_lanes_kernel<T, K, 1><<<pgrid(bicg_vec_lanes_kernel<T, K, 1>, grid_lanes), kSolverBlock, 0, cs>>>(
                     n, dinv, r, p[o], vv[o], p[nw], yv, ctl, sc);
             } else {
-                bicg_vec_k_kernel<T, K, 1><<<grid_vec, kSolverBlock, 0, cs>>>(
+                bicg_vec_k_kernel<T, K, 1><<<pgrid(bicg_vec_k_kernel<T, K, 1>, grid_vec), kSolverBlock, 0, cs>>>(
                     n, dinv, r, p[o], vv[o], p[nw], yv, ctl, sc);
             }
             spmv_k(yv, vv[nw]);
             if constexpr (kLanes) {
-                bicg_dots_lanes_kernel<T, K, 1><<<grid_lanes, kSolverBlock, 0, cs>>>(
+                bicg_dots_lanes_kernel<T, K, 1><<<pgrid(bicg_dots_lanes_kernel<T, K, 1>, grid_lanes), kSolverBlock, 0, cs>>>(
                     n, rr, vv[nw], ctl, sc, partials);
             } else {
-                bicg_dot1k_kernel<T, K><<<grid_vec, kSolverBlock, 0, cs>>>(n, rr, vv[nw], ctl,
+                bicg_dot1k_kernel<T, K><<<pgrid(bicg_dot1k_kernel<T, K>, grid_vec), kSolverBlock, 0, cs>>>(n, rr, vv[nw], ctl,
                                                                           sc, partials);
             }
             if (bp) {
                 launch_bicg_block_vec<T, K, 2>(n, *bp, r, vv[nw], nullptr, s, zv, ctl, sc, cs);
             } else if constexpr (kLanes) {
-                bicg_vec_lanes_kernel<T, K, 2><<<grid_lanes, kSolverBlock, 0, cs>>>(
+                bicg_vec_lanes_kernel<T, K, 2><<<pgrid(bicg_vec_lanes_kernel<T, K, 2>, grid_lanes), kSolverBlock, 0, cs>>>(
                     n, dinv, r, vv[nw], nullptr, s, zv, ctl, sc);
             } else {
-                bicg_vec_k_kernel<T, K, 2><<<grid_vec, kSolverBlock, 0, cs>>>(
+                bicg_vec_k_kernel<T, K, 2><<<pgrid(bicg_vec_k_kernel<T, K, 2>, grid_vec), kSolverBlock, 0, cs>>>(
                     n, dinv, r, vv[nw], nullptr, s, zv, ctl, sc);
             }
             spmv_k(zv, t);
             if constexpr (kLanes) {
-                bicg_dots_lanes_kernel<T, K, 3><<<grid_lanes, kSolverBlock, 0, cs>>>(
+                bicg_dots_lanes_kernel<T, K, 3><<<pgrid(bicg_dots_lanes_kernel<T, K, 3>, grid_lanes), kSolverBlock, 0, cs>>>(
                     n, s, t, ctl, sc, partials);
-                bicg_update_lanes_kernel<T, K><<<grid_lanes, kSolverBlock, 0, cs>>>(
+                bicg_update_lanes_kernel<T, K><<<pgrid(bicg_update_lanes_kernel<T, K>, grid_lanes), kSolverBlock, 0, cs>>>(
                     n, x, ldx, r, rr, yv, s, t, zv, ctl, sc, partials);
             } else {
-                bicg_dot2k_kernel<T, K><<<grid_vec, kSolverBlock, 0, cs>>>(n, s, t, ctl, sc,
+                bicg_dot2k_kernel<T, K><<<pgrid(bicg_dot2k_kernel<T, K>, grid_vec), kSolverBlock, 0, cs>>>(n, s, t, ctl, sc,
                                                                           partials);
-                bicg_update_kernel<T, K><<<grid_vec, kSolverBlock, 0, cs>>>(
+                bicg_update_kernel<T, K><<<pgrid(bicg_update_kernel<T, K>, grid_vec), kSolverBlock, 0, cs>>>(
                     n, nullptr, x, ldx, r, rr, yv, s, t, ctl, sc, partials, zv);
             }
         });
@@ -1104,30 +1104,30 @@ int bicgstab_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
                 continue;
             }
             if (split) {
-                bicg_pupdate_kernel<T><<<grid_vec, kSolverBlock, 0, cs>>>(
+                bicg_pupdate_kernel<T><<<pgrid(bicg_pupdate_kernel<T>, grid_vec), kSolverBlock, 0, cs>>>(
                     n, dinv, r, p[o], vv[o], p[nw], yv, ctl, sc);
                 async_spmv(cs, yv, vv[nw]);
-                bicg_dot1_kernel<T><<<grid_vec, kSolverBlock, 0, cs>>>(n, rr, vv[nw], ctl, sc,
+                bicg_dot1_kernel<T><<<pgrid(bicg_dot1_kernel<T>, grid_vec), kSolverBlock, 0, cs>>>(n, rr, vv[nw], ctl, sc,
                                                                       partials);
-                bicg_supdate_kernel<T><<<grid_vec, kSolverBlock, 0, cs>>>(
+                bicg_supdate_kernel<T><<<pgrid(bicg_supdate_kernel<T>, grid_vec), kSolverBlock, 0, cs>>>(
                     n, dinv, r, vv[nw], s, zv, ctl, sc);
                 async_spmv(cs, zv, t);
-                bicg_dot2_kernel<T><<<grid_vec, kSolverBlock, 0, cs>>>(n, s, t, ctl, sc,
+                bicg_dot2_kernel<T><<<pgrid(bicg_dot2_kernel<T>, grid_vec), kSolverBlock, 0, cs>>>(n, s, t, ctl, sc,
                                                                       partials);
-                bicg_update_kernel<T, 1><<<grid_vec, kSolverBlock, 0, cs>>>(
+                bicg_update_kernel<T, 1><<<pgrid(bicg_update_kernel<T, 1>, grid_vec), kSolverBlock, 0, cs>>>(
                     n, dinv, x, ldx, r, rr, p[nw], s, t, ctl, sc, partials);
                 B2S_LAUNCH_CHECK();
                 continue;
             }
             B2S_DISPATCH_RHS(K, {
                 B2S_DISPATCH_SW(sw, {
-                    bicg_spmv1_kernel<T, SW, K><<<grid_spmv, kSolverBlock, 0, cs>>>(
+                    bicg_spmv1_kernel<T, SW, K><<<pgrid(bicg_spmv1_kernel<T, SW, K>, grid_spmv), kSolverBlock, 0, cs>>>(
                         n, rp, ci, v, dinv, r, rr, p[o], vv[o], p[nw], vv[nw],
                         ctl, sc, partials);
-                    bicg_spmv2_kernel<T, SW, K><<<grid_spmv, kSolverBlock, 0, cs>>>(
+                    bicg_spmv2_kernel<T, SW, K><<<pgrid(bicg_spmv2_kernel<T, SW, K>, grid_spmv), kSolverBlock, 0, cs>>>(
                         n, rp, ci, v, dinv, r, vv[nw], s, t, ctl, sc, partials);
                 });
-                bicg_update_kernel<T, K><<<grid_vec, kSolverBlock, 0, cs>>>(
+                bicg_update_kernel<T, K><<<pgrid(bicg_update_kernel<T, K>, grid_vec), kSolverBlock, 0, cs>>>(
                     n, dinv, x, ldx, r, rr, p[nw], s, t, ctl, sc, partials);
             });
             B2S_LAUNCH_CHECK();

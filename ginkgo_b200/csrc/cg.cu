@@ -540,8 +540,8 @@ __global__ void __launch_bounds__(kSolverBlock, (SK >= 0 && MB2 <= 8 ? 5 : 0))
                               block_extent(bp.ptrs, blk, n, bp.max_bs, s, bs);
         const bool act = in_block && i < bs;
         const int64_t row = s + i;
-        T inv[MB2];
-        load_block_columns<SK>(bp, bsc, grp, lane, in_group, inv);
+        BlockRow<SK, MB2, T> inv;
+        inv.load(bp, bsc, grp, lane, in_group);
 #pragma unroll
         for (int j = 0; j < K; ++j) {
             T rn = T(0);
@@ -600,9 +600,9 @@ void launch_cg_block(int64_t n, const BlockPrec<T>& bp, const T* b, int64_t ldb,
 #define B2S_CG_BLOCK(MB)                                                           \
     case MB:                                                                       \
         with_pass_kind<T, K == 1>(bp, [&](auto sk) {                               \
-            cg_block_kernel<T, MB, K, INIT, decltype(sk)::value>                   \
-                <<<grid, kSolverBlock, 0, st>>>(n, bp, b, ldb, k, x, ldx, r, z, p, q, \
-                                                ctl, sc, partials);                \
+            auto kernel = cg_block_kernel<T, MB, K, INIT, decltype(sk)::value>;    \
+            kernel<<<pgrid(kernel, grid), kSolverBlock, 0, st>>>(                  \
+                n, bp, b, ldb, k, x, ldx, r, z, p, q, ctl, sc, partials);          \
         });                                                                        \
         break;
     switch (mb2) {
@@ -697,7 +697,7 @@ int cg_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
 
     B2S_DISPATCH_RHS(K, {
         B2S_DISPATCH_SW(sw, {
-            residual_kernel<T, SW, K><<<grid_spmv, kSolverBlock, 0, st>>>(
+            residual_kernel<T, SW, K><<<pgrid(residual_kernel<T, SW, K>, grid_spmv), kSolverBlock, 0, st>>>(
                 n, rp, ci, v, x, ldx, b, ldb, int(k), r);
         });
         B2S_LAUNCH_CHECK();
@@ -705,7 +705,7 @@ int cg_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
             launch_cg_block<T, K, true>(n, *bp, b, ldb, int(k), x, ldx, r, z, p[0], nullptr,
                                         ctl, sc, partials, st);
         } else {
-            cg_init_kernel<T, K><<<grid_vec, kSolverBlock, 0, st>>>(
+            cg_init_kernel<T, K><<<pgrid(cg_init_kernel<T, K>, grid_vec), kSolverBlock, 0, st>>>(
                 n, dinv, b, ldb, int(k), r, p[0], ctl, sc, partials);
         }
         B2S_LAUNCH_CHECK();
@@ -714,18 +714,18 @@ int cg_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
     const int lpr = async_lanes_per_row(max_row_nnz);
     const int64_t async_need = ceildiv(ceildiv(n, kWarp / lpr), kAsyncBlock / kWarp);
     auto launch_split = [&](cudaStream_t cs, T* po, T* pn) {
-        cg_pupdate_kernel<T><<<grid_vec, kSolverBlock, 0, cs>>>(n, dinv, zr, po, pn, ctl, sc);
+        cg_pupdate_kernel<T><<<pgrid(cg_pupdate_kernel<T>, grid_vec), kSolverBlock, 0, cs>>>(n, dinv, zr, po, pn, ctl, sc);
         with_async_kernel<T, 1, false>(lpr, [&](auto kernel) {
             const int64_t grid = std::min<int64_t>(async_need, async_resident_blocks(kernel));
             kernel<<<grid, kAsyncBlock, 0, cs>>>(n, rp, ci, v, pn, 1, q, 1, nullptr, nullptr,
                                                  &ctl->all_stopped);
         });
-        cg_pq_kernel<T><<<grid_vec, kSolverBlock, 0, cs>>>(n, pn, q, ctl, sc, partials);
+        cg_pq_kernel<T><<<pgrid(cg_pq_kernel<T>, grid_vec), kSolverBlock, 0, cs>>>(n, pn, q, ctl, sc, partials);
         if (bp) {
             launch_cg_block<T, 1, false>(n, *bp, nullptr, 0, 1, x, ldx, r, z, pn, q, ctl, sc,
                                          partials, cs);
         } else {
-            cg_update_kernel<T, 1><<<grid_vec, kSolverBlock, 0, cs>>>(n, dinv, x, ldx, r, pn,
+            cg_update_kernel<T, 1><<<pgrid(cg_update_kernel<T, 1>, grid_vec), kSolverBlock, 0, cs>>>(n, dinv, x, ldx, r, pn,
                                                                       q, ctl, sc, partials);
         }
     };
@@ -748,25 +748,25 @@ int cg_solve(int64_t n, const int32_t* rp, const int32_t* ci, const T* v,
                         solver_grid()));
                     const int gu = int(std::min<int64_t>(
                         std::max<int64_t>(1, ceildiv(n * K / VW, kSolverBlock)), solver_grid()));
-                    cg_spmv_lanes_kernel<T, K><<<gs, kSolverBlock, 0, cs>>>(
+                    cg_spmv_lanes_kernel<T, K><<<pgrid(cg_spmv_lanes_kernel<T, K>, gs), kSolverBlock, 0, cs>>>(
                         n, rp, ci, v, dinv, zr, po, pn, q, ctl, sc, partials);
                     if (bp) {
                         launch_cg_block<T, K, false>(n, *bp, nullptr, 0, int(k), x, ldx, r, z,
                                                      pn, q, ctl, sc, partials, cs);
                     } else {
-                        cg_update_lanes_kernel<T, K><<<gu, kSolverBlock, 0, cs>>>(
+                        cg_update_lanes_kernel<T, K><<<pgrid(cg_update_lanes_kernel<T, K>, gu), kSolverBlock, 0, cs>>>(
                             n, dinv, x, ldx, r, pn, q, ctl, sc, partials);
                     }
                 } else {
                     B2S_DISPATCH_SW(sw, {
-                        cg_spmv_kernel<T, SW, K><<<grid_spmv, kSolverBlock, 0, cs>>>(
+                        cg_spmv_kernel<T, SW, K><<<pgrid(cg_spmv_kernel<T, SW, K>, grid_spmv), kSolverBlock, 0, cs>>>(
                             n, rp, ci, v, dinv, zr, po, pn, q, ctl, sc, partials);
                     });
                     if (bp) {
                         launch_cg_block<T, K, false>(n, *bp, nullptr, 0, int(k), x, ldx, r, z,
                                                      pn, q, ctl, sc, partials, cs);
                     } else {
-                        cg_update_kernel<T, K><<<grid_vec, kSolverBlock, 0, cs>>>(
+                        cg_update_kernel<T, K><<<pgrid(cg_update_kernel<T, K>, grid_vec), kSolverBlock, 0, cs>>>(
                             n, dinv, x, ldx, r, pn, q, ctl, sc, partials);
                     }
                 }

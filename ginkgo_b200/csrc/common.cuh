@@ -5,6 +5,9 @@
 #include <stdint.h>
 
 #include <cstdio>
+#include <mutex>
+#include <utility>
+#include <vector>
 
 #include "../../include/ginkgo_b200.h"
 
@@ -19,6 +22,37 @@ constexpr int kMaxSMs = 148;
 // Multiprocessors of the current device (cudaDevAttrMultiProcessorCount),
 // looked up once per device; kMaxSMs when the query fails.
 int num_sms();
+
+// The grid of a persistent (grid-stride) kernel launched with `threads`
+// threads per block: `grid` cut to the blocks of `kernel` resident at once
+// on all SMs (the occupancy query cached per kernel), so its last blocks do
+// not run as a partial second wave: eight 256-thread blocks per SM are 1.6
+// waves of a 48-register kernel, which holds five.
+template <typename Kern>
+int resident_grid(Kern kernel, int threads, int64_t grid)
+{
+    static std::mutex m;
+    static std::vector<std::pair<const void*, int>> cache;
+    const void* key = reinterpret_cast<const void*>(kernel);
+    int per_sm = 0;
+    {
+        std::lock_guard<std::mutex> lock(m);
+        for (const auto& e : cache) {
+            if (e.first == key) per_sm = e.second;
+        }
+        if (per_sm == 0) {
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) !=
+                    cudaSuccess ||
+                per_sm < 1) {
+                (void)cudaGetLastError();
+                per_sm = 64;  // unknown: leave the grid as it is
+            }
+            cache.emplace_back(key, per_sm);
+        }
+    }
+    const int64_t resident = int64_t(per_sm) * num_sms();
+    return int(grid < 1 ? 1 : (grid < resident ? grid : resident));
+}
 
 // Thread-local last-error message, read through b2s_last_error().
 void set_error(const char* fmt, ...);

@@ -1145,18 +1145,20 @@ int gmres_engine(const GmresLayout& lay, int64_t n, int64_t nnz, const int32_t* 
     auto block_apply = [&](cudaStream_t cs) {
         if (!bp) return;
         with_block_class(*bp, [&](auto mb, auto ap) {
-            gmres_block_apply_kernel<TA, decltype(mb)::value, decltype(ap)::value>
-                <<<block_grid(*bp), kSolverBlock, 0, cs>>>(n, *bp, y, &gs->idle);
+            auto kernel = gmres_block_apply_kernel<TA, decltype(mb)::value, decltype(ap)::value>;
+            kernel<<<pgrid(kernel, block_grid(*bp)), kSolverBlock, 0, cs>>>(n, *bp, y, &gs->idle);
         });
     };
     auto restart = [&](cudaStream_t cs) {
         if (bp) {
             with_block_class(*bp, [&](auto mb, auto ap) {
-                gmres_xupdate_block_kernel<TA, TB, decltype(mb)::value, decltype(ap)::value>
-                    <<<block_grid(*bp), kSolverBlock, 0, cs>>>(n, ldv, V, *bp, x, b, r, gs);
+                auto kernel =
+                    gmres_xupdate_block_kernel<TA, TB, decltype(mb)::value, decltype(ap)::value>;
+                kernel<<<pgrid(kernel, block_grid(*bp)), kSolverBlock, 0, cs>>>(n, ldv, V, *bp,
+                                                                                 x, b, r, gs);
             });
         } else {
-            gmres_xupdate_kernel<TA, TB><<<grid_vec, kSolverBlock, 0, cs>>>(n, ldv, V, da, x,
+            gmres_xupdate_kernel<TA, TB><<<pgrid(gmres_xupdate_kernel<TA, TB>, grid_vec), kSolverBlock, 0, cs>>>(n, ldv, V, da, x,
                                                                             b, r, gs);
         }
         with_async_kernel<double, 1, false>(lpr, [&](auto kernel) {
@@ -1164,10 +1166,10 @@ int gmres_engine(const GmresLayout& lay, int64_t n, int64_t nnz, const int32_t* 
             kernel<<<grid, kAsyncBlock, 0, cs>>>(n, rp, ci, v64, x, 1, r, 1,
                                                  &gs->minus_one, &gs->one, &gs->done);
         });
-        gmres_restart_kernel<TA, TB><<<grid_vec, kSolverBlock, 0, cs>>>(n, r, b, V, da, y,
+        gmres_restart_kernel<TA, TB><<<pgrid(gmres_restart_kernel<TA, TB>, grid_vec), kSolverBlock, 0, cs>>>(n, r, b, V, da, y,
                                                                         gs, partials);
         if constexpr (kScaled) {
-            gmres_quantize_kernel<TA, TB, double><<<grid_vec, kSolverBlock, 0, cs>>>(
+            gmres_quantize_kernel<TA, TB, double><<<pgrid(gmres_quantize_kernel<TA, TB, double>, grid_vec), kSolverBlock, 0, cs>>>(
                 n, ldv, r, V, da, y, gs, 1);
         }
         block_apply(cs);
@@ -1205,12 +1207,12 @@ int gmres_engine(const GmresLayout& lay, int64_t n, int64_t nnz, const int32_t* 
                                                          nullptr, nullptr, &gs->idle);
                 });
             }
-            gmres_dots_kernel<TA, TB><<<grid_dots, kSolverBlock, 0, cs>>>(
+            gmres_dots_kernel<TA, TB><<<pgrid(gmres_dots_kernel<TA, TB>, grid_dots), kSolverBlock, 0, cs>>>(
                 n, ldv, V, dst, gs, partials, gpart, Gm);
-            gmres_update_kernel<TA, TB><<<grid_upd, kSolverBlock, 0, cs>>>(
+            gmres_update_kernel<TA, TB><<<pgrid(gmres_update_kernel<TA, TB>, grid_upd), kSolverBlock, 0, cs>>>(
                 n, ldv, V, dst, da, y, gs, partials, Hm, wq);
             if constexpr (kScaled) {
-                gmres_quantize_kernel<TA, TB, TA><<<grid_vec, kSolverBlock, 0, cs>>>(
+                gmres_quantize_kernel<TA, TB, TA><<<pgrid(gmres_quantize_kernel<TA, TB, TA>, grid_vec), kSolverBlock, 0, cs>>>(
                     n, ldv, wq, V, da, y, gs, 0);
             }
             block_apply(cs);

@@ -135,25 +135,55 @@ __device__ __forceinline__ void store_reduced(void* base, int64_t idx, T v)
     }
 }
 
+// The word one stored value of kind K occupies, and its value widened to T.
+template <int K, typename T>
+struct StorageWord {
+    using type = T;
+};
+template <typename T>
+struct StorageWord<kF32, T> {
+    using type = float;
+};
+template <typename T>
+struct StorageWord<kF16, T> {
+    using type = uint16_t;
+};
+template <typename T>
+struct StorageWord<kHi32, T> {
+    using type = uint32_t;
+};
+template <typename T>
+struct StorageWord<kHi16F32, T> {
+    using type = uint16_t;
+};
+template <typename T>
+struct StorageWord<kHi16F64, T> {
+    using type = uint16_t;
+};
+
+template <int K, typename T>
+__device__ __forceinline__ T widen(typename StorageWord<K, T>::type w)
+{
+    if constexpr (K == kFull) {
+        return w;
+    } else if constexpr (K == kF32) {
+        return T(w);
+    } else if constexpr (K == kF16) {
+        return T(__half2float(__ushort_as_half(w)));
+    } else if constexpr (K == kHi32) {
+        return T(__longlong_as_double((long long)(uint64_t(w) << 32)));
+    } else if constexpr (K == kHi16F32) {
+        return T(__uint_as_float(uint32_t(w) << 16));
+    } else {
+        return T(__longlong_as_double((long long)(uint64_t(w) << 48)));
+    }
+}
+
 template <int K, typename T>
 __device__ __forceinline__ T load_reduced(const void* base, int64_t idx)
 {
-    if constexpr (K == kFull) {
-        return __ldg(static_cast<const T*>(base) + idx);
-    } else if constexpr (K == kF32) {
-        return T(__ldg(static_cast<const float*>(base) + idx));
-    } else if constexpr (K == kF16) {
-        return T(__half2float(__ushort_as_half(__ldg(static_cast<const uint16_t*>(base) + idx))));
-    } else if constexpr (K == kHi32) {
-        const uint64_t hi = __ldg(static_cast<const uint32_t*>(base) + idx);
-        return T(__longlong_as_double((long long)(hi << 32)));
-    } else if constexpr (K == kHi16F32) {
-        const uint32_t hi = __ldg(static_cast<const uint16_t*>(base) + idx);
-        return T(__uint_as_float(hi << 16));
-    } else {
-        const uint64_t hi = __ldg(static_cast<const uint16_t*>(base) + idx);
-        return T(__longlong_as_double((long long)(hi << 48)));
-    }
+    using W = typename StorageWord<K, T>::type;
+    return widen<K, T>(__ldg(static_cast<const W*>(base) + idx));
 }
 
 // A value rounded to storage kind K and read back.
@@ -222,6 +252,39 @@ __device__ __forceinline__ void load_block_columns(const BlockPrec<T>& bp,
         load(std::integral_constant<int, SK>{});
     }
 }
+
+// The row of a block group that one lane holds (as load_block_columns), kept
+// as stored words for a fixed storage kind and widened where each column is
+// used, so that all of the row's loads are in flight before the first
+// conversion waits for one.
+template <int SK, int MB2, typename T>
+struct BlockRow {
+    using Word = typename StorageWord<(SK >= 0 ? SK : int(kFull)), T>::type;
+    Word w[MB2];
+
+    __device__ __forceinline__ void load(const BlockPrec<T>& bp, const BlockScheme& bsc,
+                                         int64_t grp, int lane, bool in_group)
+    {
+        if constexpr (SK >= 0) {
+            const Word* g = reinterpret_cast<const Word*>(bp.blocks + grp * bsc.group) + lane;
+#pragma unroll
+            for (int c = 0; c < MB2; ++c) {
+                w[c] = in_group && c < bp.max_bs ? __ldg(g + c * bsc.stride) : Word(0);
+            }
+        } else {
+            load_block_columns<SK>(bp, bsc, grp, lane, in_group, w);
+        }
+    }
+
+    __device__ __forceinline__ T operator[](int c) const
+    {
+        if constexpr (SK >= 0) {
+            return widen<SK, T>(w[c]);
+        } else {
+            return w[c];
+        }
+    }
+};
 
 namespace {  // a copy per translation unit
 

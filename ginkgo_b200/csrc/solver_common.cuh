@@ -22,6 +22,14 @@ constexpr int kMaxRhs = 16;
 constexpr int kSolverGrid = kMaxSMs * 8;
 inline int64_t solver_grid() { return std::min(kSolverGrid, num_sms() * 8); }
 
+// The grid of a persistent (grid-stride) solver kernel: resident_grid with
+// kSolverBlock threads.
+template <typename Kern>
+int pgrid(Kern kernel, int64_t grid)
+{
+    return resident_grid(kernel, kSolverBlock, grid);
+}
+
 // stopping_status bit layout of the reference
 // (include/ginkgo/core/stop/stopping_status.hpp:21-121): bit 7 converged,
 // bit 6 finalized, bits 0-5 the id of the criterion that stopped it.

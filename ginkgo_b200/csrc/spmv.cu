@@ -695,14 +695,16 @@ int csr_spmv(int strategy, int64_t n, int64_t num_cols, const int32_t* rp,
                 bool launched = false;
                 if constexpr (K >= 4 && K % Vec16<T>::width == 0) {
                     if (lanes) {
-                        csr_lb_lanes_kernel<T, K><<<grid, kBlock, 0, st>>>(
+                        auto kernel = csr_lb_lanes_kernel<T, K>;
+                        kernel<<<resident_grid(kernel, kBlock, grid), kBlock, 0, st>>>(
                             n, nc, own_first, tail_row, partials, rp, ci, v, bb, ldb, cc, ldc,
                             alpha, beta);
                         launched = true;
                     }
                 }
                 if constexpr (K == 1) {
-                    csr_lb1_kernel<T><<<grid, kBlock, 0, st>>>(
+                    auto kernel = csr_lb1_kernel<T>;
+                    kernel<<<resident_grid(kernel, kBlock, grid), kBlock, 0, st>>>(
                         n, nc, own_first, tail_row, partials, rp, ci, v, bb, ldb, cc, ldc,
                         alpha, beta);
                     launched = true;
@@ -710,11 +712,13 @@ int csr_spmv(int strategy, int64_t n, int64_t num_cols, const int32_t* rp,
                 if (launched) {
                     // the column-slice or one-column form above
                 } else if (vec) {
-                    csr_lb_kernel<T, K, true><<<grid, kBlock, 0, st>>>(
+                    auto kernel = csr_lb_kernel<T, K, true>;
+                    kernel<<<resident_grid(kernel, kBlock, grid), kBlock, 0, st>>>(
                         n, nc, own_first, tail_row, partials, rp, ci, v, bb, ldb, cc, ldc,
                         alpha, beta);
                 } else {
-                    csr_lb_kernel<T, K, false><<<grid, kBlock, 0, st>>>(
+                    auto kernel = csr_lb_kernel<T, K, false>;
+                    kernel<<<resident_grid(kernel, kBlock, grid), kBlock, 0, st>>>(
                         n, nc, own_first, tail_row, partials, rp, ci, v, bb, ldb, cc, ldc,
                         alpha, beta);
                 }
