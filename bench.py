@@ -616,6 +616,8 @@ PROFILE_OPS = {
     "lb16": "csr_lb_lanes_kernel (load_balance, 16 right-hand sides)",
     "cg_block": "cg_block_kernel (CG update pass with 8-row block Jacobi)",
     "cg_block_f16": "cg_block_kernel (CG update pass, 8-row blocks stored in FP16)",
+    "lb1_b": "csr_lb1_kernel (load_balance, one column, power-law matrix B)",
+    "classical_b": "csr classical (one column, power-law matrix B)",
     "bicg_block": "bicg_block_vec_kernel (BiCGStab with 8-row block Jacobi)",
     "sddmm16": "sddmm_lanes_kernel (16 columns)",
     "spgemm": "gemm_*_rows_kernel (A^2)",
@@ -628,14 +630,19 @@ PROFILE_OPS = {
 
 def profile_op(op):
     """Three launches of one operation on the 7-point 128^3 matrix (217 MB of
-    Csr, larger than L2), for a single-kernel ncu capture with -k and -c."""
+    Csr, larger than L2; matrix B for the *_b operations), for a
+    single-kernel ncu capture with -k and -c."""
     import torch
     from ginkgo_b200 import stencils
     from ginkgo_b200._lib import call
     from ginkgo_b200.matrix import Csr, CudaExecutor, _p, _stream, spgemm
     from ginkgo_b200.solver import Bicgstab, BlockJacobi, Cg, Iteration, Jacobi, ResidualNorm
     exe = CudaExecutor.create(0)
-    rp, ci, v = stencils.poisson_3d_7pt(128)
+    if op.endswith("_b"):
+        # matrix B: power-law, n = 4M, 80M entries (1 GB of Csr)
+        rp, ci, v = stencils.power_law(4_000_000, seed=0, mu=2.5, sigma=1.0, max_len=4096)
+    else:
+        rp, ci, v = stencils.poisson_3d_7pt(128)
     n = len(rp) - 1
     A = Csr.read(exe, rp, ci, v)
     rng = np.random.default_rng(0)
@@ -645,8 +652,10 @@ def profile_op(op):
     crit = (Iteration.build().with_max_iters(3), ResidualNorm.build().with_reduction_factor(1e-14))
     jb = Jacobi.build().with_max_block_size(8).with_block_pointers(np.arange(0, n + 1, 8))
     for _ in range(3):
-        if op in ("lb1", "lb16"):
+        if op in ("lb1", "lb16", "lb1_b"):
             A.set_strategy("load_balance").apply(x, y)
+        elif op == "classical_b":
+            A.apply(x, y)
         elif op in ("cg_block", "bicg_block", "cg_block_f16"):
             fac = Bicgstab if op == "bicg_block" else Cg
             if op == "cg_block_f16":
