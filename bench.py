@@ -535,7 +535,8 @@ def profile_tour():
     SDDMM of the differentiable solve, mixed-type Csr/Ell SpMV, block Jacobi
     (blocks of 8), 10 Arnoldi steps of GMRES and of every CB-GMRES basis
     format, CG / BiCGStab / GMRES with block Jacobi inside (blocks of 8),
-    SpGEMM (A^2), SpGEAM and the Hybrid conversions and SpMV."""
+    CG with adaptive-precision blocks and their apply, SpGEMM (A^2), SpGEAM
+    and the Hybrid conversions and SpMV."""
     import torch
     from ginkgo_b200 import stencils
     from ginkgo_b200._lib import call
@@ -599,6 +600,13 @@ def profile_tour():
                 Gmres.build().with_krylov_dim(30).with_criteria(*crit10)):
         s = fac.with_preconditioner(jb).on(exe).generate(A)
         s.apply(b1, torch.zeros(n, dtype=torch.float64, device="cuda"))
+    # adaptive-precision blocks (autodetection: FP16 storage on this matrix)
+    # inside CG, and their stand-alone apply
+    jba = (Jacobi.build().with_max_block_size(8).with_block_pointers(np.arange(0, n + 1, 8))
+           .with_storage_optimization(0xFF))
+    s = Cg.build().with_criteria(*crit).with_preconditioner(jba).on(exe).generate(A)
+    s.apply(b1, torch.zeros(n, dtype=torch.float64, device="cuda"))
+    s.precond.apply(x1, y1)
     # sparse products: A^2 (SpGEMM), A + A (SpGEAM), Csr -> Hybrid -> SpMV, Csr
     from ginkgo_b200.matrix import spgeam, spgemm
     spgemm(A, A)
