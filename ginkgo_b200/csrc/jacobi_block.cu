@@ -408,13 +408,7 @@ __global__ void __launch_bounds__(kJacobiWarps * kWarp)
     T inv[MB2];
     auto load = [&](auto kc) {
         constexpr int K = decltype(kc)::value;
-        const void* g = blocks + grp * sc.group;
-#pragma unroll
-        for (int inner = 0; inner < MB2; ++inner) {
-            inv[inner] = in_group && inner < max_bs
-                             ? load_reduced<K, T>(g, lane + inner * sc.stride)
-                             : T(0);
-        }
+        load_widened<K, MB2>(blocks + grp * sc.group, lane, sc.stride, in_group, max_bs, inv);
     };
     if constexpr (AP) {
         with_storage_kind(storage_kind<T>(precisions[grp * sc.gs]), load);

@@ -221,6 +221,22 @@ __device__ __forceinline__ void with_storage_kind(int k, F&& f)
     }
 }
 
+// inv[c] = element lane + c * stride of the storage array of kind K at base,
+// widened to T (zero past max_bs or outside the group): every word is loaded
+// before the first is widened, so the loads are in flight together.
+template <int K, int MB2, typename T>
+__device__ __forceinline__ void load_widened(const void* base, int lane, int64_t stride,
+                                             bool in_group, int max_bs, T (&inv)[MB2])
+{
+    using W = typename StorageWord<K, T>::type;
+    const W* g = static_cast<const W*>(base) + lane;
+    W w[MB2];
+#pragma unroll
+    for (int c = 0; c < MB2; ++c) w[c] = in_group && c < max_bs ? __ldg(g + c * stride) : W(0);
+#pragma unroll
+    for (int c = 0; c < MB2; ++c) inv[c] = widen<K, T>(w[c]);
+}
+
 // How a block pass reads the blocks (a template parameter of the passes, so
 // the full-precision instances keep their register counts): kSkFull without
 // precisions, kSkMixed with a switch on each group's storage, or one

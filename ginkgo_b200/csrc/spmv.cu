@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(kBlock)
 constexpr int kLbPerLane = kLbChunk / kWarp;
 
 template <typename T>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, 5)
     csr_lb1_kernel(int64_t n, int64_t nc, const int32_t* __restrict__ own_first,
                    int32_t* __restrict__ tail_row, T* __restrict__ partials,
                    const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
@@ -266,6 +266,9 @@ __global__ void __launch_bounds__(kBlock)
     for (int64_t ch = blockIdx.x * int64_t(kBlock / kWarp) + wid; ch < nc; ch += nwarps) {
         const int64_t e0 = ch * kLbChunk;
         const int len = int(min(int64_t(kLbChunk), nnz - e0));  // entries in the chunk
+        // the owned rows and the first 32 rows' extents are loaded alongside
+        // the entries and the gathers, not after them
+        const int r0 = __ldg(own_first + ch), r1 = __ldg(own_first + ch + 1);
         T pv[kLbPerLane];
         int32_t pc[kLbPerLane];
 #pragma unroll
@@ -274,6 +277,10 @@ __global__ void __launch_bounds__(kBlock)
             pc[j] = i < len ? ld_stream(ci + e0 + i) : 0;
             pv[j] = i < len ? ld_stream(v + e0 + i) : T(0);
         }
+        const int rf = r0 + lane;
+        const int64_t rs0 = rf < r1 ? int64_t(__ldg(rp + rf)) : 0;
+        const int64_t re0 = rf < r1 ? int64_t(__ldg(rp + rf + 1)) : 0;
+        const int64_t st = r1 < n ? int64_t(__ldg(rp + r1)) : nnz;
 #pragma unroll
         for (int j = 0; j < kLbPerLane; ++j) {
             if (lane + j * kWarp < len) pv[j] = pv[j] * __ldg(b + int64_t(pc[j]) * ldb);
@@ -281,12 +288,16 @@ __global__ void __launch_bounds__(kBlock)
 #pragma unroll
         for (int j = 0; j < kLbPerLane; ++j) sp[lane + j * kWarp] = pv[j];
         __syncwarp();
-        const int r0 = own_first[ch], r1 = own_first[ch + 1];
         for (int rb = r0; rb < r1; rb += kWarp) {
             const int r = rb + lane;
             const bool valid = r < r1;
-            const int s = valid ? int(max(int64_t(__ldg(rp + r)) - e0, int64_t(0))) : 0;
-            const int e = valid ? int(int64_t(__ldg(rp + r + 1)) - e0) : 0;
+            int64_t rs = rs0, re = re0;
+            if (rb != r0) {
+                rs = valid ? int64_t(__ldg(rp + r)) : 0;
+                re = valid ? int64_t(__ldg(rp + r + 1)) : 0;
+            }
+            const int s = valid ? int(max(rs - e0, int64_t(0))) : 0;
+            const int e = valid ? int(re - e0) : 0;
             const bool longseg = e - s > kWarp;
             if (valid && !longseg) {
                 T acc = T(0);
@@ -312,7 +323,6 @@ __global__ void __launch_bounds__(kBlock)
         }
         // the row that continues past the chunk: its part here, as a partial
         const int rt = r1;
-        const int64_t st = rt < n ? int64_t(__ldg(rp + rt)) : nnz;
         const bool tail = st < e0 + len;
         if (tail) {
             T acc = T(0);
