@@ -222,3 +222,28 @@ def test_uniform_batch_ell_layout():
     with pytest.raises(ValueError):
         BatchEll.uniform(FakeExec(), 3, n, 5, torch.from_numpy(eci[:-1]),
                          torch.from_numpy(vals))
+
+
+def test_adaptive_jacobi_entries_reject_bad_arguments_before_device_work():
+    import ctypes as C
+    from ginkgo_b200 import _lib
+    lib = _lib.lib()
+    fake = C.c_void_p(256)  # never dereferenced: validation fails first
+    nbytes = C.c_int64(0)
+    assert lib.b2s_jacobi_adaptive_workspace_bytes(1000, C.byref(nbytes)) == 0
+    assert nbytes.value == 4000  # one descriptor word per block
+    assert lib.b2s_jacobi_adaptive_workspace_bytes(-1, C.byref(nbytes)) == -1
+    # generation: conditioning, precisions, blocks and workspace are required
+    args = [10, fake, fake, fake, 5, fake, 2, 0.1]
+    assert lib.b2s_jacobi_block_generate_adaptive_f64(*args, None, fake, fake, 0, fake,
+                                                      None) == -1
+    assert lib.b2s_jacobi_block_generate_adaptive_f64(*args, fake, fake, fake, 0, None,
+                                                      None) == -1
+    assert lib.b2s_jacobi_block_generate_adaptive_f32(10, fake, fake, fake, 5, fake, 33, 0.1,
+                                                      fake, fake, fake, 0, fake, None) == -1
+    # apply without precisions, expand / reduce with a bad block size
+    assert lib.b2s_jacobi_block_apply_adaptive_f64(10, 5, fake, 2, None, fake, fake, 1, fake,
+                                                   1, 1, None, None, None) == -1
+    assert lib.b2s_jacobi_block_expand_f64(5, 0, fake, fake, fake, None) == -1
+    assert lib.b2s_jacobi_block_reduce_f32(5, 33, fake, fake, fake, None) == -1
+    assert lib.b2s_jacobi_block_expand_f32(5, 4, None, fake, fake, None) == -1
