@@ -396,8 +396,10 @@ __global__ void __launch_bounds__(kJacobiWarps * kWarp)
     const BlockScheme sc = block_scheme(max_bs);
     const int lane = threadIdx.x % kWarp, w = threadIdx.x / kWarp;
     const int sub = lane / max_bs, r = lane % max_bs;
-    const int64_t grp = int64_t(blockIdx.x) * kJacobiWarps + w;
-    if (grp * sc.gs >= num_blocks) return;  // the whole warp: uniform
+    const int64_t nwarps = int64_t(gridDim.x) * kJacobiWarps;
+    // persistent: a warp walks the groups with a grid stride (uniform per warp)
+    for (int64_t grp = int64_t(blockIdx.x) * kJacobiWarps + w; grp * sc.gs < num_blocks;
+         grp += nwarps) {
     const int64_t blk = grp * sc.gs + sub;
     int s = 0, bs = 0;
     const bool in_block = sub < sc.gs && blk < num_blocks &&
@@ -445,6 +447,7 @@ __global__ void __launch_bounds__(kJacobiWarps * kWarp)
             }
         }
     }
+    }
 }
 
 template <typename T>
@@ -477,8 +480,9 @@ int block_apply(int64_t n, int64_t num_blocks, const int32_t* ptrs, int max_bs,
     const int64_t grid = ceildiv(ceildiv(num_blocks, sc.gs), kJacobiWarps);
     cudaStream_t st = as_stream(stream);
     auto launch = [&](auto kernel) {
-        kernel<<<grid, kJacobiWarps * kWarp, 0, st>>>(n, num_blocks, ptrs, max_bs, precisions,
-                                                      blocks, b, ldb, x, ldx, k, alpha, beta);
+        kernel<<<resident_grid(kernel, kJacobiWarps * kWarp, grid), kJacobiWarps * kWarp, 0,
+                 st>>>(n, num_blocks, ptrs, max_bs, precisions, blocks, b, ldb, x, ldx, k,
+                       alpha, beta);
     };
     const int mb2 = kMaxBs / sc.gs;
 #define B2S_JAC_APPLY_AP(MB, AP)                                             \
