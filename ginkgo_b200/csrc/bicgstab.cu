@@ -769,7 +769,7 @@ __global__ void __launch_bounds__(kSolverBlock)
 // :194 and :229.
 // ---------------------------------------------------------------------------
 template <typename T, int MB2, int K, int STEP, int SK>
-__global__ void __launch_bounds__(kSolverBlock, (SK >= 0 && MB2 <= 8 ? 5 : 0))
+__global__ void __launch_bounds__(kSolverBlock, (MB2 > 8 ? 0 : SK == kF16 ? 6 : SK >= 0 ? 5 : 0))
     bicg_block_vec_kernel(int64_t n, BlockPrec<T> bp, const T* __restrict__ r,
                           const T* __restrict__ a_old, const T* __restrict__ v_old,
                           T* __restrict__ out, T* __restrict__ prec, SolveCtl* ctl,

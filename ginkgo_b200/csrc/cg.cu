@@ -503,7 +503,7 @@ __global__ void __launch_bounds__(kSolverBlock)
 // instances to five blocks per SM keeps them at the full-precision pass's 48
 // registers (64 otherwise); a minimum of 0 leaves the others unconstrained.
 template <typename T, int MB2, int K, bool INIT, int SK>
-__global__ void __launch_bounds__(kSolverBlock, (SK >= 0 && MB2 <= 8 ? 5 : 0))
+__global__ void __launch_bounds__(kSolverBlock, (MB2 > 8 ? 0 : SK == kF16 ? 6 : SK >= 0 ? 5 : 0))
     cg_block_kernel(int64_t n, BlockPrec<T> bp, const T* __restrict__ b, int64_t ldb, int k,
                     T* __restrict__ x, int64_t ldx, T* __restrict__ r, T* __restrict__ z,
                     T* __restrict__ p, const T* __restrict__ q, SolveCtl* ctl,
