@@ -15,7 +15,8 @@
 // ignores the old c.  Values and products are formed in the arithmetic type
 // and the result rounded once to the output type.
 //
-// Kernels: Csr, one subwarp of SW lanes per row (SW from the longest row),
+// Kernels: Csr with one column, the pipelined kernel (csr_async_mixed_kernel);
+// with several, one subwarp of SW lanes per row (SW from the longest row),
 // KC columns per pass; Ell, one thread per row over the column-major slots.
 // Uniform types are accepted too, but the tuned kernels of spmv.cu
 // (b2s_csr_spmv_f64/_f32, b2s_ell_spmv_*) are the fast path for them.
@@ -23,6 +24,7 @@
 #include <type_traits>
 
 #include "common.cuh"
+#include "csr_async.cuh"
 
 namespace b2s {
 namespace {
@@ -130,6 +132,104 @@ __global__ void dense_convert_kernel(int64_t n, int64_t k, const TS* __restrict_
     dst[r * ldd + j] = TD(src[r * lds + j]);
 }
 
+// One column: the pipelined Csr kernel of csr_async.cuh with the matrix,
+// input and output types apart (a warp stages the next group's values and
+// column indices with cp.async while it sums the current group, LPR lanes
+// per row; groups beyond the stage are summed by the whole warp from
+// global memory).  Values and gathered inputs are widened to the
+// arithmetic type, the sum rounded once to the output type.
+template <typename TM, typename TI, typename TO, int LPR>
+__global__ void __launch_bounds__(kAsyncBlock)
+    csr_async_mixed_kernel(int64_t n, const int32_t* __restrict__ rp,
+                           const int32_t* __restrict__ ci, const TM* __restrict__ v,
+                           const TI* __restrict__ b, int64_t ldb, TO* __restrict__ c,
+                           int64_t ldc, const TM* __restrict__ alpha,
+                           const TO* __restrict__ beta)
+{
+    using TA = arith_t<TM, TI, TO>;
+    constexpr unsigned kFull = 0xffffffffu;
+    constexpr int R = kWarp / LPR;  // rows per group
+    constexpr int kCap = kAsyncCap;
+    __shared__ AsyncStage<TM> stages[kAsyncBlock / kWarp][2];
+    const int lane = threadIdx.x % kWarp, wid = threadIdx.x / kWarp;
+    const int myrow = lane / LPR, sub = lane % LPR;
+    const int64_t ngroups = (n + R - 1) / R;
+    const int64_t nwarps = int64_t(gridDim.x) * (kAsyncBlock / kWarp);
+    AsyncStage<TM>* st = stages[wid];
+    auto load_ptrs = [&](int64_t g, int& p, int& pe) {
+        const int64_t row0 = g * R;
+        const int64_t pl = row0 + lane;
+        p = __ldg(rp + (pl < n ? pl : n));
+        pe = __ldg(rp + (row0 + R < n ? row0 + R : n));
+    };
+    auto desc = [&](int p, int pe, int& rs, int& re, int& start, int& cnt) {
+        rs = __shfl_sync(kFull, p, myrow);
+        const int nx = __shfl_sync(kFull, p, myrow + 1 < kWarp ? myrow + 1 : kWarp - 1);
+        re = myrow + 1 < R ? nx : pe;
+        start = __shfl_sync(kFull, p, 0);
+        cnt = pe - start;
+    };
+    auto issue = [&](int s, int start, int cnt) {
+        for (int i = lane; i < cnt; i += kWarp) {
+            cp_async_elem(&st[s].vals[i], v + start + i);
+            cp_async_elem(&st[s].cols[i], ci + start + i);
+        }
+    };
+    int64_t g = blockIdx.x * int64_t(kAsyncBlock / kWarp) + wid;
+    if (g >= ngroups) return;  // whole warp
+    int rs, re, start, cnt, p, pe;
+    load_ptrs(g, p, pe);
+    desc(p, pe, rs, re, start, cnt);
+    if (cnt <= kCap) issue(0, start, cnt);
+    cp_async_commit();
+    int pn = 0, pen = 0;
+    if (g + nwarps < ngroups) load_ptrs(g + nwarps, pn, pen);
+    int s = 0;
+    for (; g < ngroups; g += nwarps) {
+        const int64_t gn = g + nwarps;
+        int nrs = 0, nre = 0, nstart = 0, ncnt = 0;
+        if (gn < ngroups) {
+            desc(pn, pen, nrs, nre, nstart, ncnt);
+            if (ncnt <= kCap) issue(s ^ 1, nstart, ncnt);
+            if (gn + nwarps < ngroups) load_ptrs(gn + nwarps, pn, pen);
+        }
+        cp_async_commit();
+        cp_async_wait_one();
+        __syncwarp();
+        TA acc = TA(0);
+        const int64_t row = g * R + myrow;
+        if (cnt <= kCap) {
+            const TM* cv = st[s].vals;
+            const int32_t* cc = st[s].cols;
+#pragma unroll 4
+            for (int i = rs - start + sub; i < re - start; i += LPR) {
+                acc += TA(cv[i]) * TA(__ldg(b + int64_t(cc[i]) * ldb));
+            }
+            if constexpr (LPR > 1) acc = subwarp_sum<LPR>(acc);
+        } else {
+            for (int l = 0; l < R; ++l) {
+                const int s0 = __shfl_sync(kFull, rs, l * LPR);
+                const int e0 = __shfl_sync(kFull, re, l * LPR);
+                TA a = TA(0);
+                for (int ee = s0 + lane; ee < e0; ee += kWarp) {
+                    a += TA(ld_stream(v + ee)) * TA(__ldg(b + int64_t(ld_stream(ci + ee)) * ldb));
+                }
+                a = warp_sum(a);
+                if (myrow == l) acc = a;
+            }
+        }
+        if (row < n && sub == 0) {
+            c[row * ldc] = finish<TA, TO, TM>(acc, alpha, beta, c + row * ldc);
+        }
+        __syncwarp();  // stage s is refilled two groups later
+        s ^= 1;
+        rs = nrs;
+        re = nre;
+        start = nstart;
+        cnt = ncnt;
+    }
+}
+
 // subwarp width for rows of up to max_row_nnz entries
 inline int mixed_subwarp(int64_t max_row_nnz)
 {
@@ -141,6 +241,25 @@ int csr_mixed(int64_t n, const int32_t* rp, const int32_t* ci, const void* v,
               int64_t max_row_nnz, const void* b, int64_t ldb, void* c, int64_t ldc,
               int64_t k, const void* alpha, const void* beta, cudaStream_t st)
 {
+    if (k == 1) {
+        // one column: the pipelined kernel (persistent, one wave)
+        const int lpr = async_lanes_per_row(max_row_nnz);
+        auto launch = [&](auto kernel) {
+            const int64_t need = ceildiv(ceildiv(n, kWarp / lpr), kAsyncBlock / kWarp);
+            const int64_t grid = std::min<int64_t>(need, async_resident_blocks(kernel));
+            kernel<<<grid, kAsyncBlock, 0, st>>>(
+                n, rp, ci, static_cast<const TM*>(v), static_cast<const TI*>(b), ldb,
+                static_cast<TO*>(c), ldc, static_cast<const TM*>(alpha),
+                static_cast<const TO*>(beta));
+        };
+        switch (lpr) {
+        case 1: launch(csr_async_mixed_kernel<TM, TI, TO, 1>); break;
+        case 2: launch(csr_async_mixed_kernel<TM, TI, TO, 2>); break;
+        default: launch(csr_async_mixed_kernel<TM, TI, TO, 4>); break;
+        }
+        B2S_LAUNCH_CHECK();
+        return B2S_OK;
+    }
     const int sw = mixed_subwarp(max_row_nnz);
     for (int64_t c0 = 0; c0 < k; c0 += 16) {
         const int kc = int(std::min<int64_t>(16, k - c0));
