@@ -596,23 +596,34 @@ bool lanes_ok(const T* b, int64_t ldb, const T* c, int64_t ldc, int64_t col0,
            vec_ok(static_cast<const T*>(c), ldc, col0, kk);
 }
 
+// Longest Sellp slice (entries per row) for which rows are paired per lane
+// slot with four or more right-hand sides.
+constexpr int64_t kPairMaxSlice = 64;
+
 template <typename T, int K, int FMT>
 void launch_lanes(int64_t n, const int32_t* rp, int64_t w_or_s, int64_t stride,
                   const uint64_t* sets, const uint64_t* lens, const int32_t* ci,
                   const T* v, const T* b, int64_t ldb, T* c, int64_t ldc,
-                  const T* alpha, const T* beta, cudaStream_t st)
+                  const T* alpha, const T* beta, cudaStream_t st,
+                  int64_t max_slice_len = 0)
 {
     if constexpr (K >= 4 && K % Vec16<T>::width == 0) {
         constexpr int KL = K / Vec16<T>::width;
         // Ell: row pairs per lane slot when the column-major layout keeps
         // rows r, r + 1 adjacent at 8-byte alignment (0.84-0.90 of the
         // single-row time at 4 and 16 columns on the 7-point 128^3 matrix).
-        // Sellp keeps one row per slot: on the power-law matrix its longest
-        // slices (1,805 entries) doubled the per-thread chain and took 1.3 to
-        // 2.4 times as long with pairs.
+        // Sellp pairs its rows only when the caller gives the longest slice
+        // and it is short: on the power-law matrix its longest slices (1,805
+        // entries) doubled the per-thread chain and took 1.3 to 2.4 times as
+        // long with pairs.
         const bool aligned = reinterpret_cast<uintptr_t>(ci) % 8 == 0 &&
                              reinterpret_cast<uintptr_t>(v) % (2 * sizeof(T)) == 0;
-        const bool pairs = aligned && FMT == 1 && stride % 2 == 0;
+        // (Sellp FP32 with four columns measured 9 % slower with pairs, so
+        // FP32 pairs need eight or more)
+        const bool pairs = aligned && ((FMT == 1 && stride % 2 == 0) ||
+                                       (FMT == 2 && w_or_s % 2 == 0 && max_slice_len > 0 &&
+                                        max_slice_len <= kPairMaxSlice &&
+                                        (sizeof(T) == 8 || K >= 8)));
         if (FMT != 0 && pairs) {
             if constexpr (FMT != 0) {
                 rhs_lanes2_kernel<T, K, FMT><<<ceildiv(ceildiv(n, 2) * KL, kBlock), kBlock, 0,
@@ -839,7 +850,7 @@ int sellp_spmv(int64_t n, int64_t num_cols, int64_t slice_size,
                const uint64_t* slice_sets, const uint64_t* slice_lengths,
                const int32_t* ci, const T* v, const T* b, int64_t ldb, T* c,
                int64_t ldc, int64_t k, const T* alpha, const T* beta,
-               void* stream)
+               void* stream, int64_t max_slice_len = 0)
 {
     B2S_CHECK_ARG(n >= 0 && k >= 0, "negative size");
     B2S_CHECK_ARG(slice_size >= 1 && slice_size <= (1 << 20),
@@ -890,7 +901,7 @@ int sellp_spmv(int64_t n, int64_t num_cols, int64_t slice_size,
             B2S_DISPATCH_K(kk, VEC, {
                 launch_lanes<T, K, 2>(n, nullptr, slice_size, 0, slice_sets,
                                       slice_lengths, ci, v, b + col0, ldb,
-                                      c + col0, ldc, alpha, beta, st);
+                                      c + col0, ldc, alpha, beta, st, max_slice_len);
             });
             B2S_LAUNCH_CHECK();
             col0 += kk;
@@ -976,6 +987,20 @@ int b2s_csr_load_balance_setup(int64_t num_rows, int64_t nnz,
         return sellp_spmv<T>(num_rows, num_cols, slice_size, slice_sets,       \
                              slice_lengths, col_idxs, values, b, ldb, c, ldc,  \
                              num_rhs, alpha, beta, stream);                    \
+    }                                                                          \
+    int b2s_sellp_spmv_hinted_##S(int64_t num_rows, int64_t num_cols,          \
+                                  int64_t slice_size, const uint64_t* slice_sets, \
+                                  const uint64_t* slice_lengths,               \
+                                  const int32_t* col_idxs, const T* values,    \
+                                  const T* b, int64_t ldb, T* c, int64_t ldc,  \
+                                  int64_t num_rhs, const T* alpha,             \
+                                  const T* beta, int64_t max_slice_length,     \
+                                  void* stream)                                \
+    {                                                                          \
+        B2S_CHECK_ARG(max_slice_length >= 0, "negative max_slice_length");     \
+        return sellp_spmv<T>(num_rows, num_cols, slice_size, slice_sets,       \
+                             slice_lengths, col_idxs, values, b, ldb, c, ldc,  \
+                             num_rhs, alpha, beta, stream, max_slice_length);  \
     }
 
 B2S_SPMV_ENTRIES(double, f64)

@@ -326,6 +326,9 @@ class Sellp(_SparseBase):
         self.slice_sets, self.slice_lengths = slice_sets, slice_lengths
         self.col_idxs, self.values = col_idxs, values
         self.dtype = values.dtype
+        # the longest slice, for the SpMV's choice of one or two rows per
+        # lane slot (read back once here)
+        self.max_slice_length = int(slice_lengths.max().item()) if slice_lengths.numel() else 0
 
     @property
     def num_stored_elements(self):
@@ -342,10 +345,11 @@ class Sellp(_SparseBase):
             xt = _convert(x2, self.dtype) if beta is not None else \
                 torch.empty(x2.shape, dtype=self.dtype, device=x2.device)
             beta = None if beta is None else beta.to(self.dtype)
-        call(f"b2s_sellp_spmv_{_SFX[self.dtype]}", self.shape[0], self.shape[1],
+        call(f"b2s_sellp_spmv_hinted_{_SFX[self.dtype]}", self.shape[0], self.shape[1],
              self.slice_size, _p(self.slice_sets), _p(self.slice_lengths),
              _p(self.col_idxs), _p(self.values), _p(bt), bt.stride(0), _p(xt),
-             xt.stride(0), xt.shape[1], _p(alpha), _p(beta), _stream(xt))
+             xt.stride(0), xt.shape[1], _p(alpha), _p(beta), self.max_slice_length,
+             _stream(xt))
         if xt is not x2:
             call("b2s_dense_convert", _VT[xt.dtype], _VT[x2.dtype], x2.shape[0], x2.shape[1],
                  _p(xt), xt.stride(0), _p(x2), x2.stride(0), _stream(x2))

@@ -116,6 +116,22 @@ int b2s_sellp_spmv_f32(int64_t num_rows, int64_t num_cols, int64_t slice_size,
                        const float* values, const float* b, int64_t ldb,
                        float* c, int64_t ldc, int64_t num_rhs,
                        const float* alpha, const float* beta, void* stream);
+/* The same with the caller's knowledge of the longest slice
+ * (max_slice_length = the largest slice_lengths entry; 0 when not known):
+ * with four or more right-hand sides, slices of at most 64 entries per row
+ * let each lane slot take two neighbouring rows. */
+int b2s_sellp_spmv_hinted_f64(int64_t num_rows, int64_t num_cols, int64_t slice_size,
+                              const uint64_t* slice_sets, const uint64_t* slice_lengths,
+                              const int32_t* col_idxs, const double* values, const double* b,
+                              int64_t ldb, double* c, int64_t ldc, int64_t num_rhs,
+                              const double* alpha, const double* beta,
+                              int64_t max_slice_length, void* stream);
+int b2s_sellp_spmv_hinted_f32(int64_t num_rows, int64_t num_cols, int64_t slice_size,
+                              const uint64_t* slice_sets, const uint64_t* slice_lengths,
+                              const int32_t* col_idxs, const float* values, const float* b,
+                              int64_t ldb, float* c, int64_t ldc, int64_t num_rhs,
+                              const float* alpha, const float* beta,
+                              int64_t max_slice_length, void* stream);
 
 /* Value type codes of the mixed-type entry points. */
 #define B2S_VALUE_F64 0
