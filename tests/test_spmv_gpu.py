@@ -202,6 +202,22 @@ def test_ell_sellp_row_pairs_many_rhs(exe, dt, k):
         op.apply(0.5, xd, -2.0, y2)
         assert_spmv_close(rp, ci, v, x, y2.cpu().numpy(), ref2, TOL[dt] * 4,
                           alpha=0.5, beta_y=2.0 * y0.astype(np.float64))
+    # Sellp through the plain entry point (no longest-slice hint: one row
+    # per lane slot) and through the hinted one with a hint that rules pairs
+    # out (a slice longer than the pairing bound): the same products
+    from ginkgo_b200._lib import call
+    from ginkgo_b200.matrix import _p, _stream
+    sfx = "f64" if dt == torch.float64 else "f32"
+    S = A.convert_to_sellp(32, 1)
+    assert 0 < S.max_slice_length <= 12
+    for entry, hint in ((f"b2s_sellp_spmv_{sfx}", None), (f"b2s_sellp_spmv_hinted_{sfx}", 100)):
+        y = torch.full((n, k), float("nan"), dtype=dt, device="cuda")
+        args = [n, n, 32, _p(S.slice_sets), _p(S.slice_lengths), _p(S.col_idxs), _p(S.values),
+                _p(xd), xd.stride(0), _p(y), y.stride(0), k, None, None]
+        if hint is not None:
+            args.append(hint)
+        call(entry, *args, _stream(y))
+        assert_spmv_close(rp, ci, v, x, y.cpu().numpy(), ref, TOL[dt])
 
 
 @pytest.mark.parametrize("fmt", FORMATS)
