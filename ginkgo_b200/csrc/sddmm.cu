@@ -4,11 +4,15 @@
 // gradient dL/dA = -lambda x^T restricted to A's pattern, the backward of the
 // differentiable solve.  u, w row-major n x k / m x k with leading
 // dimensions.  Narrow blocks (k * sizeof(T) < 32 bytes): one subwarp per
-// row, the row's u(row, :) in registers.  Wider blocks: one warp per row and
-// L = k * sizeof(T) / 16 lanes per stored entry, each lane owning one
-// 16-byte slice of the columns, so w(col, :) of an entry is one coalesced
-// load of k * sizeof(T) bytes and the warp serves 32 / L entries at a time;
-// the slices' partial dots are summed across the L lanes.
+// row, the row's u(row, :) in registers.  Wider blocks: one warp per 32
+// consecutive rows, walking their stored entries as one flat range in chunks
+// of 32 (each lane loads one column index and finds its entry's row by a
+// shuffle search over the rows' starts), L = k * sizeof(T) / 16 lanes per
+// entry, each owning one 16-byte slice of the columns, so w(col, :) and
+// u(row, :) of an entry are coalesced loads of k * sizeof(T) bytes; the loads
+// of up to four steps of 32 / L entries are issued before any of their sums,
+// the slices' partial dots are summed across the L lanes, and the chunk's 32
+// results are stored as one coalesced write.
 #include <algorithm>
 
 #include "common.cuh"
@@ -53,26 +57,63 @@ __global__ void __launch_bounds__(kBlock)
     constexpr int VW = int(16 / sizeof(T));  // values per lane slice
     constexpr int L = K / VW;                // lanes per entry
     constexpr int EPW = kWarp / L;           // entries per warp step
+    constexpr int U = L < 4 ? L : 4;         // steps whose loads are issued together
+    static_assert(L % U == 0, "a 32-entry chunk is L steps");
+    constexpr unsigned kFull = 0xffffffffu;
     const int lane = threadIdx.x % kWarp;
     const int slot = lane / L, part = lane % L;
     const int64_t nwarps = int64_t(gridDim.x) * (kBlock / kWarp);
-    for (int64_t row = (blockIdx.x * int64_t(kBlock) + threadIdx.x) / kWarp; row < n;
-         row += nwarps) {
-        T ur[VW];
-        RowLoad<T, VW, true>::load(u + row * ldu + part * VW, ur);
-        const int b = rp[row], e_end = rp[row + 1];
-        // warp-uniform trip count: every lane reaches the shuffles
-        for (int e0 = b; e0 < e_end; e0 += EPW) {
-            const int e = e0 + slot;
-            T acc = T(0);
-            if (e < e_end) {
-                T wr[VW];
-                RowLoad<T, VW, true>::load(w + int64_t(ci[e]) * ldw + part * VW, wr);
+    const int64_t nblk = (n + kWarp - 1) / kWarp;
+    for (int64_t rb = (blockIdx.x * int64_t(kBlock) + threadIdx.x) / kWarp; rb < nblk;
+         rb += nwarps) {
+        // the warp owns rows [r0, r0 + nr); lane j holds the start of row r0 + j
+        const int64_t r0 = rb * kWarp;
+        const int nr = int(n - r0 < kWarp ? n - r0 : kWarp);
+        const int rs = rp[r0 + (lane < nr ? lane : nr)];
+        const int e_end = rp[r0 + nr];
+        const int e_beg = __shfl_sync(kFull, rs, 0);
+        for (int c0 = e_beg; c0 < e_end; c0 += kWarp) {
+            // lane l loads entry c0 + l's column and finds its row: the last
+            // j < nr with rs_j <= c0 + l (rs is non-decreasing, rs_0 = e_beg)
+            const int e = c0 + lane;
+            const int cnt = e_end - c0 < kWarp ? e_end - c0 : kWarp;
+            const int col = lane < cnt ? ci[e] : 0;
+            int ro = 0;
 #pragma unroll
-                for (int q = 0; q < VW; ++q) acc += ur[q] * wr[q];
+            for (int step = 16; step > 0; step >>= 1) {
+                const int v = __shfl_sync(kFull, rs, ro + step);
+                if (ro + step < nr && v <= e) ro += step;
             }
-            acc = subwarp_sum<L>(acc);
-            if (part == 0 && e < e_end) out[e] = alpha * acc;
+            // steps of EPW entries, U of them with all their loads in flight;
+            // entry c0 + l's dot ends in lane l, stored once per chunk
+            const int nst = (cnt + EPW - 1) / EPW;
+            T mine = T(0);
+            for (int s0 = 0; s0 < nst; s0 += U) {
+                T wr[U][VW], ur[U][VW];
+#pragma unroll
+                for (int q = 0; q < U; ++q) {
+                    const int idx = (s0 + q) * EPW + slot;
+                    const int c = __shfl_sync(kFull, col, idx);
+                    const int r = __shfl_sync(kFull, ro, idx);
+                    if (idx < cnt) {
+                        RowLoad<T, VW, true>::load(w + int64_t(c) * ldw + part * VW, wr[q]);
+                        RowLoad<T, VW, true>::load(u + (r0 + r) * ldu + part * VW, ur[q]);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < U; ++q) {
+                    const int idx = (s0 + q) * EPW + slot;
+                    T acc = T(0);
+                    if (idx < cnt) {
+#pragma unroll
+                        for (int p = 0; p < VW; ++p) acc += ur[q][p] * wr[q][p];
+                    }
+                    acc = subwarp_sum<L>(acc);
+                    const T got = __shfl_sync(kFull, acc, (lane % EPW) * L);
+                    if (lane / EPW == s0 + q) mine = got;
+                }
+            }
+            if (lane < cnt) out[e] = alpha * mine;
         }
     }
 }
@@ -93,12 +134,14 @@ int sddmm(int64_t n, const int32_t* rp, const int32_t* ci, int64_t max_row_nnz,
                          reinterpret_cast<uintptr_t>(w) % 16 == 0 && ldu % VW == 0 &&
                          ldw % VW == 0;
     if (aligned && (k == 16 || (k == 8 && sizeof(T) == 4) || (k == 4 && sizeof(T) == 8))) {
-        const int64_t grid = std::min<int64_t>(ceildiv(n, kBlock / kWarp),
-                                               int64_t(num_sms()) * 16);
+        // one warp per 32 rows, one wave of resident blocks
+        const int64_t want = ceildiv(ceildiv(n, int64_t(kWarp)), int64_t(kBlock / kWarp));
         if (k == 16) {
+            const int grid = resident_grid(sddmm_lanes_kernel<T, 16>, kBlock, want);
             sddmm_lanes_kernel<T, 16><<<grid, kBlock, 0, st>>>(n, rp, ci, u, ldu, w, ldw,
                                                                T(alpha), out);
         } else {
+            const int grid = resident_grid(sddmm_lanes_kernel<T, 2 * VW>, kBlock, want);
             sddmm_lanes_kernel<T, 2 * VW><<<grid, kBlock, 0, st>>>(n, rp, ci, u, ldu, w,
                                                                    ldw, T(alpha), out);
         }
