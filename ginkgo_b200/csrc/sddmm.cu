@@ -10,7 +10,8 @@
 // shuffle search over the rows' starts), L = k * sizeof(T) / 16 lanes per
 // entry, each owning one 16-byte slice of the columns, so w(col, :) and
 // u(row, :) of an entry are coalesced loads of k * sizeof(T) bytes; the loads
-// of up to four steps of 32 / L entries are issued before any of their sums,
+// of two (FP64) or four (FP32) steps of 32 / L entries are issued before any
+// of their sums,
 // the slices' partial dots are summed across the L lanes, and the chunk's 32
 // results are stored as one coalesced write.
 #include <algorithm>
@@ -48,7 +49,7 @@ __global__ void __launch_bounds__(kBlock)
 }
 
 template <typename T, int K>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, sizeof(T) == 8 ? 5 : 1)
     sddmm_lanes_kernel(int64_t n, const int32_t* __restrict__ rp,
                        const int32_t* __restrict__ ci, const T* __restrict__ u,
                        int64_t ldu, const T* __restrict__ w, int64_t ldw, T alpha,
@@ -57,7 +58,12 @@ __global__ void __launch_bounds__(kBlock)
     constexpr int VW = int(16 / sizeof(T));  // values per lane slice
     constexpr int L = K / VW;                // lanes per entry
     constexpr int EPW = kWarp / L;           // entries per warp step
-    constexpr int U = L < 4 ? L : 4;         // steps whose loads are issued together
+    // steps whose loads are issued together: two in FP64, held to 48
+    // registers for five blocks per SM (16 FP64 columns on the 7-point 128^3
+    // pattern: 350 us, against 408 us for four steps at three blocks per
+    // SM); four in FP32 (172 us, against 179 us for two)
+    constexpr int UMAX = sizeof(T) == 8 ? 2 : 4;
+    constexpr int U = L < UMAX ? L : UMAX;
     static_assert(L % U == 0, "a 32-entry chunk is L steps");
     constexpr unsigned kFull = 0xffffffffu;
     const int lane = threadIdx.x % kWarp;
